@@ -1,0 +1,339 @@
+#!/usr/bin/env python3
+"""Benchmark of the TD hot path on B200.
+
+Workload (one step): the plain-FP64 pressurised penny crack in full space --
+traction influence assembly of a ~2000-triangle crack (every triangle on every
+collocation point, the 3N x 3N system A = -[Atn;Atss;Atds]) followed by the
+dense LU solve A D = b with uniform normal traction -1e-3 (mu = 1, nu = 0.25).
+The mesh is seeded synthetic data (Delaunay of a jittered hexagonal lattice).
+
+Metric: TD pair-evaluations per second over the whole step (pairs per step /
+step time), FP64.  Also reported: the split between assembly and solve, the
+roofline of the TD pair kernel and of the solve, an end-to-end number through
+the host C ABI (pinned host buffers in and out), the CPU baseline, clocks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank solves its own replica (the dense LU does not
+shard without an exchange step); value = all ranks' pairs / max step time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+# Algorithmic FP64 operations per pair-evaluation of the assembly kernel:
+# full-space strain of all three unit slip modes (2960, counted with the
+# oracle's counting scalar on this mesh's collocation pairs) plus the strain ->
+# traction epilogue (288 = 3 modes x 96).  Frozen values, see DESIGN.md.
+FALG_ASSEMBLY_FS = 2960.0 + 288.0
+SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
+NU, G = 0.25, 1.0
+TRACTION = -1e-3
+
+METRIC = "TD pair-evals/s (FS penny crack: influence assembly + FP64 LU solve)"
+UNIT = "pair-evals/s"
+
+
+def workload():
+    from cutanddisplacejulia_b200 import geometry, workloads
+    P1, P2, P3 = workloads.penny(seed=0, spacing=SPACING)
+    nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
+    return P1, P2, P3, nrm, mid, lam
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads):
+    """One step on the CPU: the oracle (restatement of the reference, all
+    threads) assembles A, LAPACK (numpy, all threads) solves it."""
+    import numpy as np
+    from oracle import oracle as O
+    n = len(P1)
+    t0 = time.perf_counter()
+    A = O.influence_traction(nrm, mid, P1, P2, P3, NU, G, lam, 0, nthreads=nthreads, want_A=True)
+    t1 = time.perf_counter()
+    b = np.concatenate([np.full(n, TRACTION), np.zeros(2 * n)])
+    np.linalg.solve(A, b)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+    from oracle import oracle as O
+    O.build()
+    P1, P2, P3, nrm, mid, lam = workload()
+    n = len(P1)
+    nthreads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads)
+    ta, ts = 0.0, 0.0
+    for _ in range(args.steps):
+        a, s = cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads)
+        ta += a
+        ts += s
+    step_s = (ta + ts) / args.steps
+    value = n * n / step_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "penny crack, full space, %d triangles, 3N=%d unknowns, spacing %.2f" % (n, 3 * n,
+                                                                                                     SPACING),
+                   "inputs": "host memory"},
+        "breakdown_ms": {"assembly": ta / args.steps * 1e3, "solve": ts / args.steps * 1e3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": "full workload per step: oracle assembly (%d threads) + numpy LAPACK gesv" % nthreads},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import cutanddisplacejulia_b200 as cad
+    from cutanddisplacejulia_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    P1, P2, P3, nrm, mid, lam = workload()
+    n = len(P1)
+    n3 = 3 * n
+
+    def col(a):   # N x 3 -> column-major flat device array (Julia layout)
+        return torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device=dev)
+
+    dP1, dP2, dP3, dN, dM = col(P1), col(P2), col(P3), col(nrm), col(mid)
+    b0 = torch.zeros(n3, dtype=torch.float64, device=dev)
+    b0[:n] = TRACTION
+    A = torch.empty(n3 * n3, dtype=torch.float64, device=dev)
+    x = torch.empty(n3, dtype=torch.float64, device=dev)
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    _lib.check(L.cad_set_stream(ctx, ctypes.c_void_p(stream.cuda_stream)), ctx)
+
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.cad_fp64_fma_probe(ctx, 20000, ctypes.byref(peak)), ctx)
+    fp64_peak_tflops = peak.value
+
+    def step(evs=None):
+        if evs:
+            evs[0].record(stream)
+        _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
+                                      dP3.data_ptr(), n, NU, G, lam, 0, A.data_ptr(), n3), ctx)
+        if evs:
+            evs[1].record(stream)
+        x.copy_(b0)
+        _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, x.data_ptr(), n3, 1), ctx)
+        if evs:
+            evs[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    asm_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    sol_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    pair_kernel_ms = L.cad_last_time_ms(ctx, 0)   # last pair-kernel launch alone (library events)
+    ms_step = ms_total / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+
+    # solution quality: relative residual of the last solve against a fresh A
+    _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(),
+                                  n, NU, G, lam, 0, A.data_ptr(), n3), ctx)
+    Am = A.view(n3, n3).t()      # column-major storage
+    resid = float(torch.linalg.vector_norm(Am @ x - b0) / torch.linalg.vector_norm(b0))
+
+    # end to end through the host C ABI: pinned host inputs, slips back to host
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t
+    hP1, hP2, hP3 = (pinned(np.asfortranarray(p).ravel(order="F")) for p in (P1, P2, P3))
+    hN, hM = pinned(np.asfortranarray(nrm).ravel(order="F")), pinned(np.asfortranarray(mid).ravel(order="F"))
+    hTn = pinned(np.full(n, TRACTION))
+    hZ = pinned(np.zeros(n))
+    hDn, hDss, hDds = (torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(3))
+
+    def e2e_call():
+        _lib.check(L.cad_slip_calculator(ctx, hP1.data_ptr(), hP2.data_ptr(), hP3.data_ptr(), n, NU, G, lam,
+                                         hM.data_ptr(), hN.data_ptr(), 0, hTn.data_ptr(), hZ.data_ptr(),
+                                         hZ.data_ptr(), hDn.data_ptr(), hDss.data_ptr(), hDds.data_ptr(), None,
+                                         None), ctx)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_call()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_call()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = (5 * 3 * n + 3 * n) * 8
+    d2h = 3 * n * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        nth = os.cpu_count() or 1
+        a_s, s_s = cpu_reference_step(P1, P2, P3, nrm, mid, lam, nth)
+        cpu = {"value": n * n / (a_s + s_s), "unit": UNIT, "cores": nth, "kind": "port",
+               "sample": "one full step (oracle assembly + numpy LAPACK gesv) on %d host threads: "
+                         "assembly %.3f s, solve %.3f s" % (nth, a_s, s_s)}
+
+    pairs = float(n) * n
+    # assembly time per step over the timed region (pair kernel + the two small
+    # per-element prep kernels, all on this stream): the launch duration used
+    achieved = FALG_ASSEMBLY_FS * pairs / (asm_ms * 1e-3) / 1e12
+    lu_flops = (2.0 / 3.0) * n3 ** 3 + 2.0 * n3 * n3
+    solve_tflops = lu_flops / (sol_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": world * pairs / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "penny crack, full space, %d triangles, 3N=%d unknowns, FP64 assembly + LU" % (n, n3),
+                   "pairs_per_step": pairs, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (A is %.0f MB per step)" % (n3 * n3 * 8 / 1e6)},
+        "breakdown_ms": {"assembly": asm_ms, "td_pair_kernel_last": pair_kernel_ms, "solve": sol_ms},
+        "residual": resid,
+        "clocks": clk,
+        "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "api": "cad_slip_calculator (host C ABI, pinned host buffers)"},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"kernel": "td_pair_kernel<FS, strain, A-matrix>", "bound": "fp64",
+                     "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak_tflops,
+                     "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
+                     "falg_per_pair": FALG_ASSEMBLY_FS, "traffic": None,
+                     "step_share": asm_ms / ms_step},
+        "roofline_solve": {"kernel": "dense LU (cusolverDnDgetrf + getrs)", "bound": "fp64",
+                           "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
+                           "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

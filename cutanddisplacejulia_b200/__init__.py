@@ -1,0 +1,19 @@
+"""B200-native triangular-dislocation (TD) path of CutAndDisplaceJulia.
+
+The hot path -- TD strain / displacement influence of every triangle on every
+observation point (full and half space), the traction influence assembly and
+the dense slip solve -- runs in libcad_td.so (CUDA, sm_100a) behind a C ABI
+(include/cad_td.h).  This package is the Python host mirror of the
+reference's Julia interface (same function names, argument order, field
+orders and error messages); julia/CutAndDisplaceB200.jl is the Julia one.
+"""
+from ._lib import CadError, context, load  # noqa: F401
+from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTractions3D,  # noqa: F401
+                       KnockOutFixedRows, SetupTractionVector, SlipCalculator3D, solve)
+from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint,  # noqa: F401
+                       CreateP1P2P3, ElasticConstantsCheck)
+from .structs import (DispInf, Disps, MixedBoundaryConditions, StrainInf, Strains, Stresses,  # noqa: F401
+                      TractionInf, Tractions)
+from .td import TD, TD_sum  # noqa: F401
+
+__version__ = "1.0.0"

@@ -1,0 +1,112 @@
+"""ctypes binding of libcad_td.so (the C ABI declared in include/cad_td.h).
+
+The library must be built (cutanddisplacejulia_b200.build.build()); there is
+no CPU fallback: every call goes to the CUDA library or raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcad_td.so")
+
+CAD_OK = 0
+CAD_ERR_DIMS = 1
+CAD_ERR_HS_ABOVE_SURFACE = 2
+CAD_ERR_UNSUPPORTED = 3
+CAD_ERR_CUDA = 4
+CAD_ERR_OOM = 5
+CAD_ERR_TIMEOUT = 6
+CAD_ERR_NOT_CONVERGED = 7
+CAD_ERR_SINGULAR = 8
+CAD_ERR_ARG = 9
+
+# Every symbol include/cad_td.h declares (checked by the tests).
+EXPORTS = [
+    "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
+    "cad_version", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
+    "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
+    "cad_solve_dev",
+]
+
+
+class CadError(RuntimeError):
+    """Error raised by the library (message text follows the reference's `error(...)`)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+_ctx = {}
+
+P = ctypes.c_void_p
+I64 = ctypes.c_int64
+D = ctypes.c_double
+INT = ctypes.c_int
+
+
+def load():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CadError(CAD_ERR_CUDA, f"libcad_td.so is not built ({LIB_PATH}); run cutanddisplacejulia_b200.build.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    L.cad_init.argtypes = [INT, ctypes.POINTER(P)]
+    L.cad_destroy.argtypes = [P]
+    L.cad_last_error.argtypes = [P]
+    L.cad_last_error.restype = ctypes.c_char_p
+    L.cad_set_stream.argtypes = [P, P]
+    L.cad_get_stream.argtypes = [P]
+    L.cad_get_stream.restype = P
+    L.cad_last_time_ms.argtypes = [P, INT]
+    L.cad_last_time_ms.restype = D
+    L.cad_version.restype = ctypes.c_char_p
+    L.cad_fp64_fma_probe.argtypes = [P, I64, ctypes.POINTER(D)]
+    td = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, D, INT, INT, INT, P, P]
+    L.cad_td_inf.argtypes = td
+    L.cad_td_sum_eval.argtypes = td
+    L.cad_td_sum.argtypes = [P, I64, I64, P, P, P, P]
+    L.cad_influence_traction.argtypes = [P, P, P, P, P, P, I64, D, D, D, P, INT, P]
+    L.cad_slip_calculator.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, P, P, P]
+    L.cad_solve.argtypes = [P, I64, P, P, I64, P]
+    tdd = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
+    L.cad_td_inf_dev.argtypes = tdd
+    L.cad_td_sum_eval_dev.argtypes = tdd
+    L.cad_assemble_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, P, I64]
+    L.cad_solve_dev.argtypes = [P, I64, P, I64, P, I64, I64]
+    _lib = L
+    return L
+
+
+def context(device: int = 0):
+    """Process-wide context for `device` (created on first use)."""
+    with _lock:
+        if device not in _ctx:
+            L = load()
+            h = P()
+            rc = L.cad_init(device, ctypes.byref(h))
+            if rc != CAD_OK:
+                raise CadError(rc, f"cad_init failed on device {device} (status {rc}); a CUDA device is required")
+            _ctx[device] = h
+        return _ctx[device]
+
+
+def check(rc, ctx):
+    if rc != CAD_OK:
+        msg = load().cad_last_error(ctx)
+        raise CadError(rc, msg.decode() if msg else f"status {rc}")
+
+
+def ptr_array(arrays):
+    """double* const* from a list of numpy arrays (None -> NULL)."""
+    arr = (P * len(arrays))()
+    for k, a in enumerate(arrays):
+        arr[k] = None if a is None else a.ctypes.data
+    return arr

@@ -1,0 +1,129 @@
+"""Host mirror of the reference's influence assembly and plain slip solve:
+CalculateInfluenceMatrices3D (src/CalculateInfluenceMatrices3D.jl:2-48),
+SlipCalculator3D (src/SlipCalculator3D.jl:1-33), SetupTractionVector
+(src/SetupTractionVector.jl), CalculateNormalAndShearTractions3D
+(src/CalculateNormalAndShearTractions3D.jl), KnockOutFixedRows
+(src/KnockOutFixedRows.jl).  Influence evaluation, traction conversion,
+assembly and LU run in libcad_td.so; the per-element boundary-condition
+algebra (O(N)) runs on the host as in the reference.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .geometry import ss_ds_dirs
+from .structs import MixedBoundaryConditions, Stresses, TractionInf, Tractions
+
+
+def _tri(P):
+    return np.asfortranarray(np.asarray(P, dtype=np.float64).reshape(-1, 3))
+
+
+def _col(a, n):
+    a = np.asarray(a, dtype=np.float64).reshape(-1)
+    if a.size == 1 and n != 1:
+        a = np.full(n, float(a[0]))
+    return np.ascontiguousarray(a)
+
+
+def CalculateNormalAndShearTractions3D(sxx, syy, szz, sxy, sxz, syz, FaceNormalVector):
+    """Normal and shear tractions of a stress state on each element: (Tn, Tds, Tss)."""
+    n = np.asarray(FaceNormalVector, dtype=np.float64).reshape(-1, 3)
+    cx, cy, cz = n[:, 0], n[:, 1], n[:, 2]
+    N = n.shape[0]
+    sxx, syy, szz, sxy, sxz, syz = (_col(s, N) for s in (sxx, syy, szz, sxy, sxz, syz))
+    ss, ds = ss_ds_dirs(cx, cy, cz)
+    Tn = sxx * cx * cx + syy * cy * cy + szz * cz * cz + 2 * sxy * cx * cy + 2 * syz * cy * cz + 2 * sxz * cz * cx
+    Tx = sxx * cx + sxy * cy + sxz * cz
+    Ty = sxy * cx + syy * cy + syz * cz
+    Tz = sxz * cx + syz * cy + szz * cz
+
+    def chosen(D):
+        a = (Tx * (1 - cx * cx) - Ty * cx * cy - Tz * cz * cx) * D[:, 0]
+        b = (Tx * -(cx * cy) + Ty * (1 - cy * cy) - Tz * cy * cz) * D[:, 1]
+        c = (Tx * -(cz * cx) - Ty * cy * cz + Tz * (1 - cz * cz)) * D[:, 2]
+        return a + b + c
+
+    return Tn, chosen(ds), chosen(ss)
+
+
+def SetupTractionVector(BoundaryConditions, FaceNormalVector, n, G, lam):
+    """(Tn, Tds, Tss) for Stresses, Tractions or MixedBoundaryConditions."""
+    bc = BoundaryConditions
+    if isinstance(bc, Stresses):
+        return CalculateNormalAndShearTractions3D(*bc, FaceNormalVector)
+    if isinstance(bc, Tractions):
+        return _col(bc.Tn, n), _col(bc.Tds, n), _col(bc.Tss, n)
+    if isinstance(bc, MixedBoundaryConditions):
+        sTn, sTds, sTss = SetupTractionVector(bc.Stresses, FaceNormalVector, n, G, lam)
+        Tn, Tds, Tss = SetupTractionVector(bc.Tractions, FaceNormalVector, n, G, lam)
+        return Tn + sTn, Tds + sTds, Tss + sTss
+    raise TypeError("unsupported boundary condition type %r" % type(bc).__name__)
+
+
+def KnockOutFixedRows(FixedEls, Tn, Tds, Tss):
+    fixed = np.asarray(FixedEls).reshape(-1) == 1
+    if np.any(fixed):
+        Tn, Tds, Tss = Tn.copy(), Tds.copy(), Tss.copy()
+        Tn[fixed] = 0.0
+        Tds[fixed] = 0.0
+        Tss[fixed] = 0.0
+    return Tn, Tds, Tss
+
+
+def CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, nu, G, lam, FixedEls, HSFlag, n,
+                                 device=0):
+    """Traction influence matrices (TractionInf of nine n x n arrays)."""
+    P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+    N = P1.shape[0]
+    nrm = _tri(FaceNormalVector)
+    mid = _tri(MidPoint)
+    fixed = None if FixedEls is None else np.ascontiguousarray(np.asarray(FixedEls, dtype=np.float64).reshape(-1))
+    out = [np.zeros((N, N), order="F") for _ in range(9)]
+    ctx = _lib.context(device)
+    rc = _lib.load().cad_influence_traction(ctx, nrm.ctypes.data, mid.ctypes.data, P1.ctypes.data, P2.ctypes.data,
+                                            P3.ctypes.data, N, float(nu), float(G), float(lam),
+                                            fixed.ctypes.data if fixed is not None else None, int(HSFlag),
+                                            _lib.ptr_array(out))
+    _lib.check(rc, ctx)
+    return TractionInf(*out)
+
+
+def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag, BoundaryConditions, FixedEls,
+                     device=0):
+    """Plain (frictionless) slip solve: returns (Dn, Dss, Dds, A, b)."""
+    P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+    N = P1.shape[0]
+    nrm = _tri(FaceNormalVector)
+    mid = _tri(MidPoint)
+    Tn, Tds, Tss = SetupTractionVector(BoundaryConditions, nrm, N, G, lam)
+    if FixedEls is not None:
+        Tn, Tds, Tss = KnockOutFixedRows(FixedEls, Tn, Tds, Tss)
+        if np.any(np.asarray(FixedEls).reshape(-1) == 1):
+            raise _lib.CadError(_lib.CAD_ERR_UNSUPPORTED, "fixed elements are not supported by this entry point")
+    Tn, Tss, Tds = _col(Tn, N), _col(Tss, N), _col(Tds, N)
+    Dn, Dss, Dds = np.zeros(N), np.zeros(N), np.zeros(N)
+    A = np.zeros((3 * N, 3 * N), order="F")
+    b = np.zeros(3 * N)
+    ctx = _lib.context(device)
+    rc = _lib.load().cad_slip_calculator(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu), float(G),
+                                         float(lam), mid.ctypes.data, nrm.ctypes.data, int(HSFlag), Tn.ctypes.data,
+                                         Tss.ctypes.data, Tds.ctypes.data, Dn.ctypes.data, Dss.ctypes.data,
+                                         Dds.ctypes.data, A.ctypes.data, b.ctypes.data)
+    _lib.check(rc, ctx)
+    return Dn, Dss, Dds, A, b
+
+
+def solve(A, B, device=0):
+    """Dense A \\ B by LU with partial pivoting on the GPU."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asarray(B, dtype=np.float64)
+    vec = B.ndim == 1
+    Bf = np.asfortranarray(B.reshape(B.shape[0], -1))
+    n, nrhs = A.shape[0], Bf.shape[1]
+    X = np.zeros((n, nrhs), order="F")
+    ctx = _lib.context(device)
+    rc = _lib.load().cad_solve(ctx, n, A.ctypes.data, Bf.ctypes.data, nrhs, X.ctypes.data)
+    _lib.check(rc, ctx)
+    return X[:, 0] if vec else X

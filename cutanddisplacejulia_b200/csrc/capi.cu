@@ -1,0 +1,534 @@
+// C ABI of libcad_td.so (declared in include/cad_td.h).
+//
+// Each context owns a CUDA stream, a cuSOLVER handle for the dense LU, and a
+// set of device workspaces that grow on demand and are reused across calls
+// (no allocation in steady state).  Host-pointer entry points copy inputs in,
+// run the device path and copy results out; *_dev entry points run the device
+// path directly on caller-provided device memory.
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/cad_td.h"
+#include "td_device.cuh"
+#include "td_kernels.h"
+
+using namespace cad;
+
+namespace cad {
+size_t tri_record_bytes() { return sizeof(TriDev); }
+}
+
+namespace {
+
+enum Slot { S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_COUNT };
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct cad_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    DevBuf buf[S_COUNT];
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool timed[2] = {false, false};
+    std::string err;
+};
+
+namespace {
+
+int fail(cad_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(cad_ctx* c, cudaError_t e, const char* what)
+{
+    const int code = (e == cudaErrorMemoryAllocation) ? CAD_ERR_OOM : CAD_ERR_CUDA;
+    return fail(c, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (expr);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #expr);        \
+    } while (0)
+
+int ensure(cad_ctx* ctx, Slot s, size_t bytes, void** out)
+{
+    DevBuf& b = ctx->buf[s];
+    if (bytes == 0) bytes = 16;
+    if (b.bytes < bytes) {
+        if (b.p) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            CK(cudaFree(b.p));
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        const size_t grown = bytes + bytes / 8;
+        CK(cudaMalloc(&b.p, grown));
+        b.bytes = grown;
+    }
+    *out = b.p;
+    return CAD_OK;
+}
+
+int set_device(cad_ctx* ctx)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    return CAD_OK;
+}
+
+// Triangles per block along grid.y: enough blocks to fill every SM several
+// times while keeping each block's triangle loop long enough to amortise the
+// shared-memory staging.
+int64_t pick_chunk(int64_t M, int64_t N, bool sum_mode)
+{
+    if (N <= 0) return 1;
+    const int64_t tiles = (M + kPairThreads - 1) / kPairThreads;
+    const int64_t target_blocks = 148 * 16;
+    int64_t nchunk = (target_blocks + tiles - 1) / tiles;
+    if (!sum_mode) nchunk = nchunk < (N + 7) / 8 ? (N + 7) / 8 : nchunk;   // at most 8 triangles per block
+    if (nchunk > N) nchunk = N;
+    if (nchunk < 1) nchunk = 1;
+    return (N + nchunk - 1) / nchunk;
+}
+
+int hs_check(cad_ctx* ctx, const double* Z, int64_t M, const double* P1, const double* P2, const double* P3,
+             int64_t N)
+{
+    void* flag;
+    if (int r = ensure(ctx, S_FLAG, sizeof(int), &flag)) return r;
+    CK(launch_hs_check(Z, M, P1, P2, P3, N, (int*)flag, ctx->stream));
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) return fail(ctx, CAD_ERR_HS_ABOVE_SURFACE, "Half-space solution: Z coordinates must be negative!");
+    return CAD_OK;
+}
+
+// Device path shared by the TD entry points (inputs already on the device).
+int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+              const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds, const double* Dn,
+              double nu, int disp, int strain, int hs, int out_kind, double* strain_out, double* disp_out,
+              double* sum_out /* 9 x M for OUT_SUM */)
+{
+    if (hs == 1 && N > 0)
+        if (int r = hs_check(ctx, Z, M, P1, P2, P3, N)) return r;
+    if (M == 0 || N == 0) {
+        if (out_kind == OUT_SUM && sum_out) CK(cudaMemsetAsync(sum_out, 0, 9 * M * sizeof(double), ctx->stream));
+        return CAD_OK;
+    }
+    void* tri;
+    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    CK(launch_td_setup(P1, P2, P3, N, Dss, Dds, Dn, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
+    PairArgs a{};
+    a.X = X; a.Y = Y; a.Z = Z; a.M = M; a.tri = (const TriDev*)tri; a.N = N;
+    a.tri_chunk = pick_chunk(M, N, out_kind == OUT_SUM);
+    a.strain = strain_out; a.disp = disp_out;
+    const int64_t nchunk = (N + a.tri_chunk - 1) / a.tri_chunk;
+    if (out_kind == OUT_SUM) {
+        void* part;
+        if (int r = ensure(ctx, S_PART, (size_t)nchunk * 9 * M * sizeof(double), &part)) return r;
+        a.partial = (double*)part;
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(launch_td_pairs(a, out_kind, hs == 1, strain == 1, disp == 1, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->timed[0] = true;
+    if (out_kind == OUT_SUM) {
+        const int mask = (strain == 1 ? 0x3f : 0) | (disp == 1 ? 0x1c0 : 0);
+        CK(launch_sum_chunks(a.partial, nchunk, M, mask, sum_out, ctx->stream));
+    }
+    return CAD_OK;
+}
+
+int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, const double* P1, const double* P2,
+                    const double* P3, int64_t N, double nu, double G, double lambda, int hs, int out_kind,
+                    double* trac_out, double* A, int64_t lda)
+{
+    void* obs;
+    void* dirs;
+    if (int r = ensure(ctx, S_OBS, (size_t)3 * N * sizeof(double), &obs)) return r;
+    if (int r = ensure(ctx, S_DIRS, (size_t)9 * N * sizeof(double), &dirs)) return r;
+    double* X = (double*)obs;
+    CK(launch_colloc(normals, mid, N, X, X + N, X + 2 * N, (double*)dirs, ctx->stream));
+    if (hs == 1 && N > 0)
+        if (int r = hs_check(ctx, X + 2 * N, N, P1, P2, P3, N)) return r;
+    if (N == 0) return CAD_OK;
+    void* tri;
+    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    CK(launch_td_setup(P1, P2, P3, N, nullptr, nullptr, nullptr, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
+    PairArgs a{};
+    a.X = X; a.Y = X + N; a.Z = X + 2 * N; a.M = N; a.tri = (const TriDev*)tri; a.N = N;
+    a.tri_chunk = pick_chunk(N, N, false);
+    a.lambda = lambda; a.G = G; a.dirs = (const double*)dirs;
+    a.trac = trac_out; a.A = A; a.lda = lda;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(launch_td_pairs(a, out_kind, hs == 1, true, false, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->timed[0] = true;
+    return CAD_OK;
+}
+
+int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
+{
+    if (n == 0 || nrhs == 0) return CAD_OK;
+    if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
+        return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
+    int lwork = 0;
+    if (cusolverDnDgetrf_bufferSize(ctx->solver, (int)n, (int)n, A, (int)lda, &lwork) != CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
+    void *work, *piv, *info;
+    if (int r = ensure(ctx, S_WORK, (size_t)lwork * sizeof(double), &work)) return r;
+    if (int r = ensure(ctx, S_PIV, (size_t)n * sizeof(int), &piv)) return r;
+    if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    if (cusolverDnDgetrf(ctx->solver, (int)n, (int)n, A, (int)lda, (double*)work, (int*)piv, (int*)info) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrf failed");
+    if (cusolverDnDgetrs(ctx->solver, CUBLAS_OP_N, (int)n, (int)nrhs, A, (int)lda, (int*)piv, B, (int)ldb,
+                         (int*)info) != CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrs failed");
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    ctx->timed[1] = true;
+    return CAD_OK;
+}
+
+int copy_fields_out(cad_ctx* ctx, const double* dev, int nfield, int64_t count, double* const* host)
+{
+    for (int f = 0; f < nfield; ++f)
+        if (host[f])
+            CK(cudaMemcpyAsync(host[f], dev + f * count, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return CAD_OK;
+}
+
+int upload(cad_ctx* ctx, double* dst, const double* src, int64_t count)
+{
+    if (count > 0) CK(cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return CAD_OK;
+}
+
+bool bad_flag(int f) { return f != 0 && f != 1; }
+
+}  // namespace
+
+extern "C" {
+
+const char* cad_version(void) { return "cad_td 1.0 (sm_100a, FP64)"; }
+
+int cad_init(int device, cad_ctx** out)
+{
+    if (!out) return CAD_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return CAD_ERR_CUDA;
+    cad_ctx* ctx = new cad_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) !=
+                                                   cudaSuccess) {
+        delete ctx;
+        return CAD_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    for (auto& e : ctx->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cad_destroy(ctx);
+            return CAD_ERR_CUDA;
+        }
+    if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS) {
+        cad_destroy(ctx);
+        return CAD_ERR_CUDA;
+    }
+    *out = ctx;
+    return CAD_OK;
+}
+
+int cad_destroy(cad_ctx* ctx)
+{
+    if (!ctx) return CAD_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->buf)
+        if (b.p) cudaFree(b.p);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->solver) cusolverDnDestroy(ctx->solver);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return CAD_OK;
+}
+
+const char* cad_last_error(const cad_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cad_set_stream(cad_ctx* ctx, void* stream)
+{
+    if (int r = set_device(ctx)) return r;
+    ctx->stream = (cudaStream_t)stream;   // NULL is CUDA's default stream, as everywhere in CUDA
+    if (cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "cusolverDnSetStream failed");
+    return CAD_OK;
+}
+
+void* cad_get_stream(const cad_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+double cad_last_time_ms(const cad_ctx* ctx, int which)
+{
+    if (!ctx || which < 0 || which > 1 || !ctx->timed[which]) return -1.0;
+    float ms = 0.f;
+    if (cudaEventSynchronize(ctx->ev[2 * which + 1]) != cudaSuccess) return -1.0;
+    if (cudaEventElapsedTime(&ms, ctx->ev[2 * which], ctx->ev[2 * which + 1]) != cudaSuccess) return -1.0;
+    return (double)ms;
+}
+
+// ------------------------------------------------------------------- TD
+static int td_host(cad_ctx* ctx, bool sum_mode, const double* X, const double* Y, const double* Z, int64_t M,
+                   const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                   const double* Dds, const double* Dn, double nu, int disp, int strain, int hs,
+                   double* const* strain_out, double* const* disp_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (M < 0 || N < 0 || bad_flag(disp) || bad_flag(strain) || bad_flag(hs))
+        return fail(ctx, CAD_ERR_ARG, "invalid size or flag");
+    if ((M > 0 && (!X || !Y || !Z)) || (N > 0 && (!P1 || !P2 || !P3 || !Dss || !Dds || !Dn)))
+        return fail(ctx, CAD_ERR_ARG, "null input pointer");
+    const int ns = sum_mode ? 6 : 18, nd = sum_mode ? 3 : 9;
+    if ((strain == 1 && !strain_out) || (disp == 1 && !disp_out)) return fail(ctx, CAD_ERR_ARG, "null output list");
+    void *obs, *geom, *slip, *out;
+    if (int r = ensure(ctx, S_OBS, (size_t)3 * M * sizeof(double), &obs)) return r;
+    if (int r = ensure(ctx, S_GEOM, (size_t)9 * N * sizeof(double), &geom)) return r;
+    if (int r = ensure(ctx, S_SLIP, (size_t)3 * N * sizeof(double), &slip)) return r;
+    double* o = (double*)obs;
+    double* g = (double*)geom;
+    double* s = (double*)slip;
+    if (int r = upload(ctx, o, X, M)) return r;
+    if (int r = upload(ctx, o + M, Y, M)) return r;
+    if (int r = upload(ctx, o + 2 * M, Z, M)) return r;
+    if (int r = upload(ctx, g, P1, 3 * N)) return r;
+    if (int r = upload(ctx, g + 3 * N, P2, 3 * N)) return r;
+    if (int r = upload(ctx, g + 6 * N, P3, 3 * N)) return r;
+    if (int r = upload(ctx, s, Dss, N)) return r;
+    if (int r = upload(ctx, s + N, Dds, N)) return r;
+    if (int r = upload(ctx, s + 2 * N, Dn, N)) return r;
+    const int64_t per = sum_mode ? M : M * N;
+    const size_t out_words = sum_mode ? (size_t)9 * M : (size_t)((strain == 1 ? ns : 0) + (disp == 1 ? nd : 0)) * per;
+    if (int r = ensure(ctx, S_OUT, out_words * sizeof(double), &out)) return r;
+    double* ob = (double*)out;
+    double* so = ob;
+    double* dout = sum_mode ? ob + 6 * M : ob + (strain == 1 ? ns * per : 0);
+    int r = td_device(ctx, o, o + M, o + 2 * M, M, g, g + 3 * N, g + 6 * N, N, s, s + N, s + 2 * N, nu, disp, strain,
+                      hs, sum_mode ? OUT_SUM : OUT_INF, so, dout, sum_mode ? ob : nullptr);
+    if (r) return r;
+    if (strain == 1)
+        if (int rr = copy_fields_out(ctx, so, ns, per, strain_out)) return rr;
+    if (disp == 1)
+        if (int rr = copy_fields_out(ctx, dout, nd, per, disp_out)) return rr;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_td_inf(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+               const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds,
+               const double* Dn, double nu, double G, int disp_flag, int strain_flag, int hs_flag,
+               double* const* strain_out, double* const* disp_out)
+{
+    (void)G;
+    return td_host(ctx, false, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag,
+                   strain_out, disp_out);
+}
+
+int cad_td_sum_eval(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M,
+                    const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                    const double* Dds, const double* Dn, double nu, double G, int disp_flag, int strain_flag,
+                    int hs_flag, double* const* strain_out, double* const* disp_out)
+{
+    (void)G;
+    return td_host(ctx, true, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag,
+                   strain_out, disp_out);
+}
+
+int cad_td_sum(cad_ctx* ctx, int64_t M, int64_t N, const double* const* strain_in, const double* const* disp_in,
+               double* const* strain_out, double* const* disp_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (M < 0 || N < 0) return fail(ctx, CAD_ERR_ARG, "invalid size");
+    const int64_t MN = M * N;
+    for (int kind = 0; kind < 2; ++kind) {
+        const double* const* in = kind == 0 ? strain_in : disp_in;
+        double* const* out = kind == 0 ? strain_out : disp_out;
+        if (!in) continue;
+        if (!out) return fail(ctx, CAD_ERR_ARG, "null output list");
+        const int nf = kind == 0 ? 6 : 3;
+        void *dev_in, *dev_out;
+        if (int r = ensure(ctx, S_A, (size_t)3 * nf * MN * sizeof(double), &dev_in)) return r;
+        if (int r = ensure(ctx, S_OUT, (size_t)nf * M * sizeof(double), &dev_out)) return r;
+        for (int f = 0; f < 3 * nf; ++f)
+            if (int r = upload(ctx, (double*)dev_in + f * MN, in[f], MN)) return r;
+        CK(launch_td_sum((const double*)dev_in, M, N, nf, (double*)dev_out, ctx->stream));
+        if (int r = copy_fields_out(ctx, (const double*)dev_out, nf, M, out)) return r;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return CAD_OK;
+}
+
+// ------------------------------------------------------------- assembly
+static int upload_geometry(cad_ctx* ctx, const double* normals, const double* mid, const double* P1,
+                           const double* P2, const double* P3, int64_t N, double** g)
+{
+    void* geom;
+    if (int r = ensure(ctx, S_GEOM, (size_t)15 * N * sizeof(double), &geom)) return r;
+    *g = (double*)geom;
+    if (int r = upload(ctx, *g, P1, 3 * N)) return r;
+    if (int r = upload(ctx, *g + 3 * N, P2, 3 * N)) return r;
+    if (int r = upload(ctx, *g + 6 * N, P3, 3 * N)) return r;
+    if (int r = upload(ctx, *g + 9 * N, normals, 3 * N)) return r;
+    if (int r = upload(ctx, *g + 12 * N, mid, 3 * N)) return r;
+    return CAD_OK;
+}
+
+int cad_influence_traction(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                           const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                           const double* fixed_els, int hs_flag, double* const* trac_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || !trac_out) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (fixed_els)
+        for (int64_t i = 0; i < N; ++i)
+            if (fixed_els[i] == 1.0)
+                return fail(ctx, CAD_ERR_UNSUPPORTED, "fixed elements are not supported by this entry point");
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    void* out;
+    if (int r = ensure(ctx, S_OUT, (size_t)9 * N * N * sizeof(double), &out)) return r;
+    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_TRAC,
+                            (double*)out, nullptr, 0);
+    if (r) return r;
+    if (int rr = copy_fields_out(ctx, (const double*)out, 9, N * N, trac_out)) return rr;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                        double G, double lambda, const double* midpoints, const double* normals, int hs_flag,
+                        const double* Tn, const double* Tss, const double* Tds, double* Dn, double* Dss,
+                        double* Dds, double* A_out, double* b_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || !Tn || !Tss || !Tds || !Dn || !Dss || !Dds)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    const int64_t n3 = 3 * N;
+    void *A, *b;
+    if (int r = ensure(ctx, S_A, (size_t)n3 * n3 * sizeof(double), &A)) return r;
+    if (int r = ensure(ctx, S_B, (size_t)n3 * sizeof(double), &b)) return r;
+    double* bd = (double*)b;
+    if (int r = upload(ctx, bd, Tn, N)) return r;
+    if (int r = upload(ctx, bd + N, Tss, N)) return r;
+    if (int r = upload(ctx, bd + 2 * N, Tds, N)) return r;
+    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
+                            nullptr, (double*)A, n3);
+    if (r) return r;
+    if (A_out) CK(cudaMemcpyAsync(A_out, A, (size_t)n3 * n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (b_out) CK(cudaMemcpyAsync(b_out, bd, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if ((r = solve_device(ctx, n3, (double*)A, n3, bd, n3, 1))) return r;
+    int info = 0;
+    CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dn, bd, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dss, bd + N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dds, bd + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    return CAD_OK;
+}
+
+int cad_solve(cad_ctx* ctx, int64_t n, const double* A, const double* B, int64_t nrhs, double* X)
+{
+    if (int r = set_device(ctx)) return r;
+    if (n < 0 || nrhs < 0 || (n > 0 && (!A || !B || !X))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    void *Ad, *Bd;
+    if (int r = ensure(ctx, S_A, (size_t)n * n * sizeof(double), &Ad)) return r;
+    if (int r = ensure(ctx, S_B, (size_t)n * nrhs * sizeof(double), &Bd)) return r;
+    if (int r = upload(ctx, (double*)Ad, A, n * n)) return r;
+    if (int r = upload(ctx, (double*)Bd, B, n * nrhs)) return r;
+    if (int r = solve_device(ctx, n, (double*)Ad, n, (double*)Bd, n, nrhs)) return r;
+    int info = 0;
+    if (n > 0) {
+        CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(X, Bd, (size_t)n * nrhs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    return CAD_OK;
+}
+
+// ------------------------------------------------------------ device API
+int cad_td_inf_dev(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+                   const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds,
+                   const double* Dn, double nu, int disp_flag, int strain_flag, int hs_flag, double* strain_out,
+                   double* disp_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (M < 0 || N < 0 || bad_flag(disp_flag) || bad_flag(strain_flag) || bad_flag(hs_flag))
+        return fail(ctx, CAD_ERR_ARG, "invalid size or flag");
+    return td_device(ctx, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag, OUT_INF,
+                     strain_out, disp_out, nullptr);
+}
+
+int cad_td_sum_eval_dev(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M,
+                        const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                        const double* Dds, const double* Dn, double nu, int disp_flag, int strain_flag,
+                        int hs_flag, double* strain_out, double* disp_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (M < 0 || N < 0 || bad_flag(disp_flag) || bad_flag(strain_flag) || bad_flag(hs_flag))
+        return fail(ctx, CAD_ERR_ARG, "invalid size or flag");
+    void* out;
+    if (int r = ensure(ctx, S_OUT, (size_t)9 * M * sizeof(double), &out)) return r;
+    int r = td_device(ctx, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag, OUT_SUM,
+                      nullptr, nullptr, (double*)out);
+    if (r) return r;
+    if (strain_flag == 1 && strain_out)
+        CK(cudaMemcpyAsync(strain_out, out, 6 * M * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (disp_flag == 1 && disp_out)
+        CK(cudaMemcpyAsync(disp_out, (double*)out + 6 * M, 3 * M * sizeof(double), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    return CAD_OK;
+}
+
+int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                     const double* P2, const double* P3, int64_t N, double nu, double G, double lambda, int hs_flag,
+                     double* A, int64_t lda)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || lda < 3 * N) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    return assemble_device(ctx, normals, midpoints, P1, P2, P3, N, nu, G, lambda, hs_flag, OUT_AMAT, nullptr, A, lda);
+}
+
+int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
+{
+    if (int r = set_device(ctx)) return r;
+    if (n < 0 || nrhs < 0 || lda < n || ldb < n) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (int r = solve_device(ctx, n, A, lda, B, ldb, nrhs)) return r;
+    int info = 0;
+    if (n > 0) {
+        CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    return CAD_OK;
+}
+
+}  // extern "C"

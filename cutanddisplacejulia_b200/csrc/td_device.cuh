@@ -1,0 +1,652 @@
+// Device-side triangular dislocation (TD) evaluation for one (observation,
+// triangle) pair: full-space strain / displacement, the half-space free-surface
+// correction and the image dislocation.
+//
+// Semantics follow the reference's per-point arithmetic in src/TD.jl:
+//   frame + TDCS coordinates       CalculateLocalTriCoords! :712-732, GlobalToTDECoords :870-908
+//   interior angles, side vectors  CalcTDVectsAndAngles :962-1008
+//   configuration selection        trimodefinder :1010-1079
+//   full-space strain / disp       TDstrainFS :1499-1620 + TDSetupS :1623-1750,
+//                                  TDdispFS :735-867 + TDSetupD :1081-1173
+//   free-surface correction        AngSetupStrainFSC :1867-2081, AngSetupDispFSC :1258-1409
+//   image dislocation              ComputeStrainInfluences :670-708, ComputeDispInfluences :631-668
+// The closed-form angular-dislocation terms come from tde_closed_form.cuh.
+//
+// Data layout: everything that depends only on the triangle (frames, angles,
+// per-dislocation constants of every closed-form term, slip rotations) is
+// computed once per triangle by td_setup_kernel into a TriDev record; the pair
+// kernels stage one TriDev at a time in shared memory and every thread of the
+// block (one observation point each) reads it as a broadcast.
+#pragma once
+#include <cfloat>
+#include <cstddef>
+#include <cstdint>
+
+#include "tde_closed_form.cuh"
+
+namespace cad {
+
+// ------------------------------------------------------------------ records
+struct AngDis {          // one angular dislocation of a TD frame (configuration I)
+    double cosT, sinT;   // side-vector z and y components; configuration II negates both
+    double tv1, tv2;     // vertex y, z in TDCS
+    double sinADE1;      // sin(alpha - pi) / (8 pi (1 - nu))
+    ang_dis_strain_k ks;
+    ang_dis_disp_k kd;
+};
+
+struct Frame {           // a TD (real or image) in its own coordinate system
+    double P2[3];
+    double Vn[3], Vs[3], Vd[3];
+    double p1y, p1z, p3y, p3z;          // TDCS (y, z) of P1 and P3; P2 is the origin
+    double t23y, t32x, t31y, t13x, base; // configuration-test constants
+    AngDis v[3];                         // at P1 (side -e13), P2 (e12), P3 (e23)
+    int flat;                            // all vertex z exactly 0
+    int pad_;
+};
+
+struct FscSide {         // one TD side PA -> PB of the free-surface correction
+    int skip;
+    int pad_;
+    double ey1[3], ey2[3], ey3[3];
+    double PA[3];
+    double y1B, y2B, y3B;
+    double beta;
+    double cs[3][3];     // ADCS slip of each unit mode m (Dn, Dss, Dds), component g
+    double cd[3][3];     // the same scaled by 1 / (4 pi (1 - nu)) for displacements
+    ang_dis_strain_fsc_k ks[2][2];   // [0: beta, 1: pi - beta][0: at PA, 1: at PB]
+    ang_dis_disp_fsc_k kd[2][2];     // [0: beta, 1: beta - pi][0: at PA, 1: at PB]
+};
+
+struct TriDev {
+    double Dss, Dds, Dn;
+    double K8;           // 1 / (8 pi (1 - nu))
+    Frame real;
+    Frame image;
+    FscSide side[3];
+};
+
+// Number of doubles of a TriDev needed by a full-space-only kernel.
+constexpr int kTriWordsFS = (int)(offsetof(TriDev, image) / sizeof(double));
+constexpr int kTriWordsHS = (int)(sizeof(TriDev) / sizeof(double));
+
+// ------------------------------------------------------------------ helpers
+CAD_HD double qnan()
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double(0x7ff8000000000000LL);
+#else
+    return __builtin_nan("");
+#endif
+}
+
+// Unfused arithmetic for the quantities that feed exact comparisons (TDCS
+// coordinates, barycentric configuration test, side test), so that those
+// decisions match an unfused FP64 evaluation bit for bit.
+CAD_HD double mul_rn(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    double r = a * b;
+#if !defined(__CUDACC__) && defined(__GNUC__) && defined(__x86_64__)
+    asm("" : "+x"(r));   // plain C++ test build: keep the product out of any fused multiply-add
+#endif
+    return r;
+#endif
+}
+CAD_HD double add_rn(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+CAD_HD double sub_rn(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+CAD_HD double dot3_rn(double a0, double a1, double a2, double b0, double b1, double b2)
+{
+    return add_rn(add_rn(mul_rn(a0, b0), mul_rn(a1, b1)), mul_rn(a2, b2));
+}
+
+// Symmetric tensor t (xx,yy,zz,xy,xz,yz) -> A-rotated, A column-major 3x3
+// (TensorTransformation3D! form).
+CAD_HD void tensor_rot(double t[6], const double* A)
+{
+    const double Txx = t[0], Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
+    t[0] = A[0] * A[0] * Txx + 2.0 * A[0] * A[3] * Txy + 2.0 * A[0] * A[6] * Txz + 2.0 * A[3] * A[6] * Tyz +
+           A[3] * A[3] * Tyy + A[6] * A[6] * Tzz;
+    t[1] = A[1] * A[1] * Txx + 2.0 * A[1] * A[4] * Txy + 2.0 * A[1] * A[7] * Txz + 2.0 * A[4] * A[7] * Tyz +
+           A[4] * A[4] * Tyy + A[7] * A[7] * Tzz;
+    t[2] = A[2] * A[2] * Txx + 2.0 * A[2] * A[5] * Txy + 2.0 * A[2] * A[8] * Txz + 2.0 * A[5] * A[8] * Tyz +
+           A[5] * A[5] * Tyy + A[8] * A[8] * Tzz;
+    t[3] = A[0] * A[1] * Txx + (A[0] * A[4] + A[1] * A[3]) * Txy + (A[0] * A[7] + A[1] * A[6]) * Txz +
+           (A[3] * A[7] + A[4] * A[6]) * Tyz + A[3] * A[4] * Tyy + A[6] * A[7] * Tzz;
+    t[4] = A[0] * A[2] * Txx + (A[0] * A[5] + A[2] * A[3]) * Txy + (A[0] * A[8] + A[2] * A[6]) * Txz +
+           (A[3] * A[8] + A[5] * A[6]) * Tyz + A[3] * A[5] * Tyy + A[6] * A[8] * Tzz;
+    t[5] = A[1] * A[2] * Txx + (A[2] * A[4] + A[1] * A[5]) * Txy + (A[2] * A[7] + A[1] * A[8]) * Txz +
+           (A[5] * A[7] + A[4] * A[8]) * Tyz + A[4] * A[5] * Tyy + A[7] * A[8] * Tzz;
+}
+
+// Rotation of a tensor about the TDCS x axis by the side angle (the B matrix
+// [1 0 0; 0 c -s; 0 s c] of TDSetupS, stored column-major), written out.
+CAD_HD void tensor_rot_x(double t[6], double c, double s)
+{
+    const double Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
+    const double cc = c * c, ss = s * s, cs = c * s;
+    t[1] = 2.0 * cs * Tyz + cc * Tyy + ss * Tzz;
+    t[2] = -2.0 * cs * Tyz + ss * Tyy + cc * Tzz;
+    t[3] = c * Txy + s * Txz;
+    t[4] = -s * Txy + c * Txz;
+    t[5] = (cc - ss) * Tyz + cs * (Tzz - Tyy);
+}
+
+// Observation point -> TDCS of frame f.
+CAD_HD void to_tdcs(const Frame& f, double X, double Y, double Z, double& x, double& y,
+                                        double& z)
+{
+    const double dX = sub_rn(X, f.P2[0]), dY = sub_rn(Y, f.P2[1]), dZ = sub_rn(Z, f.P2[2]);
+    x = dot3_rn(f.Vn[0], f.Vn[1], f.Vn[2], dX, dY, dZ);
+    y = dot3_rn(f.Vs[0], f.Vs[1], f.Vs[2], dX, dY, dZ);
+    z = dot3_rn(f.Vd[0], f.Vd[1], f.Vd[2], dX, dY, dZ);
+}
+
+// Artefact-free configuration: +1 (I), -1 (II), 0 (on a side, in the TD plane).
+CAD_HD int trimode(const Frame& f, double x, double y, double z)
+{
+    const double dy = sub_rn(y, f.p3y), dz = sub_rn(z, f.p3z);
+    const double a = add_rn(mul_rn(f.t23y, dy), mul_rn(f.t32x, dz)) / f.base;
+    const double b = add_rn(mul_rn(f.t31y, dy), mul_rn(f.t13x, dz)) / f.base;
+    const double c = sub_rn(sub_rn(1.0, a), b);
+    bool casen = false, casez = false;
+    if (a <= 0.0 && b > c && c > a) casen = true;
+    else if (b <= 0.0 && c > a && a > b) casen = true;
+    else if (c <= 0.0 && a > b && b > c) casen = true;
+    else if (a == 0.0 && b >= 0.0 && c >= 0.0) casez = true;
+    else if (a >= 0.0 && b == 0.0 && c >= 0.0) casez = true;
+    else if (a >= 0.0 && b >= 0.0 && c == 0.0) casez = true;
+    if (casez && x != 0.0) casez = false;
+    return casez ? 0 : (casen ? -1 : 1);
+}
+
+// ------------------------------------------------------ full-space strain
+// One angular dislocation's contribution for all three unit modes, added to
+// E[m][k] (TDCS).  sgn = +1 for configuration I, -1 for II.
+CAD_HD void ad_strain(const AngDis& v, double sgn, double x, double y, double z, double Dss,
+                                          double Dds, double Dn, double K8, double E[3][6])
+{
+    const double CosT = sgn * v.cosT, SinT = sgn * v.sinT;
+    const double dy = y - v.tv1, dz = z - v.tv2;
+    const double Yr = CosT * dy - SinT * dz;
+    const double Zr = SinT * dy + CosT * dz;
+    double o[21];
+    ang_dis_strain(v.ks, x, Yr, Zr, o);
+    const double exxBx = o[0], exxBy = o[1], exxBz = o[2];
+    const double eyyBx = o[3], eyyBy = o[4], eyyBz = o[5];
+    const double ezzBx = o[6], ezzBy = o[7], ezzBz = o[8];
+    const double exyBx = o[9], exyBy = o[10], exyBz = o[11];
+    const double exzBx = o[12], exzBy = o[13], exzBz = o[14];
+    const double eyzBx = o[15], eyzBy = o[16], eyzBz = o[17];
+    const double rFx = o[18], rFy = o[19], rFz = o[20];
+    const double sinADE1 = v.sinADE1;
+    if (Dn != 0.0) {
+        const double E3 = Dn * K8;
+        double t[6];
+        t[0] = Dn * rFx + E3 * exxBx;
+        t[1] = E3 * eyyBx;
+        t[2] = E3 * ezzBx;
+        t[3] = 0.5 * Dn * rFy - E3 * exyBx;
+        t[4] = 0.5 * Dn * rFz - E3 * exzBx;
+        t[5] = E3 * eyzBx;
+        tensor_rot_x(t, CosT, SinT);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[0][k] += t[k];
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const double slip = q == 0 ? Dss : Dds;
+        if (!(slip != 0.0)) continue;
+        // in-plane slip (strike, dip) of this mode in ADCS
+        const double Ds = q == 0 ? CosT * Dss : -SinT * Dds;
+        const double Dd = q == 0 ? SinT * Dss : CosT * Dds;
+        const double E5 = Ds * K8;
+        const double E4 = E5 * x;
+        const double dsa = Dd * sinADE1;
+        const double dsax = dsa * x;
+        double t[6];
+        t[0] = -E4 * exxBy + dsax * exxBz;
+        t[1] = Ds * rFy - E4 * eyyBy + dsax * eyyBz;
+        t[2] = -E4 * ezzBy + Dd * rFz + dsax * ezzBz;
+        t[3] = 0.5 * Ds * rFx + E5 * exyBy - dsa * exyBz;
+        t[4] = E5 * exzBy + 0.5 * Dd * rFx - dsa * exzBz;
+        t[5] = 0.5 * Ds * rFz - E4 * eyzBy + 0.5 * Dd * rFy - dsax * eyzBz;
+        tensor_rot_x(t, CosT, SinT);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[1 + q][k] += t[k];
+    }
+}
+
+// Full-space strain of frame f at one point, added into E (EFCS).  For the
+// image frame the accumulated value is first carried into the image TDCS and
+// the result carried back, as the reference does; a flat (z = 0) image
+// triangle keeps the reference's detached xz / yz components.
+template <bool IMAGE>
+CAD_HD void strain_fs(const Frame& f, double X, double Y, double Z, double Dss, double Dds,
+                                          double Dn, double K8, double E[3][6])
+{
+    double x, y, z;
+    to_tdcs(f, X, Y, Z, x, y, z);
+    const int mode = trimode(f, x, y, z);
+    double keep_xz[3], keep_yz[3];
+    const bool detach = IMAGE && f.flat;
+    if (IMAGE) {
+        const double RotInv[9] = {f.Vn[0], f.Vs[0], f.Vd[0], f.Vn[1], f.Vs[1], f.Vd[1], f.Vn[2], f.Vs[2], f.Vd[2]};
+#pragma unroll
+        for (int m = 0; m < 3; ++m) tensor_rot(E[m], RotInv);
+        if (detach) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                keep_xz[m] = E[m][4];
+                keep_yz[m] = E[m][5];
+                E[m][4] = -E[m][4];
+                E[m][5] = -E[m][5];
+            }
+        }
+    }
+    const double sgn = mode == -1 ? -1.0 : 1.0;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) ad_strain(f.v[a], sgn, x, y, z, Dss, Dds, Dn, K8, E);
+    if (mode == 0) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) E[m][k] = qnan();
+    }
+    const double Rot[9] = {f.Vn[0], f.Vn[1], f.Vn[2], f.Vs[0], f.Vs[1], f.Vs[2], f.Vd[0], f.Vd[1], f.Vd[2]};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) tensor_rot(E[m], Rot);
+    if (detach) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            E[m][4] = keep_xz[m];
+            E[m][5] = keep_yz[m];
+        }
+    }
+}
+
+// -------------------------------------------------- full-space displacement
+CAD_HD void ad_disp(const AngDis& v, double sgn, double x, double y, double z, double Dss,
+                                        double Dds, double Dn, double K8, double U[3][3])
+{
+    const double CosT = sgn * v.cosT, SinT = sgn * v.sinT;
+    const double dy = y - v.tv1, dz = z - v.tv2;
+    const double Yr = CosT * dy - SinT * dz;
+    const double Zr = SinT * dy + CosT * dz;
+    double o[9];
+    ang_dis_disp(v.kd, x, Yr, Zr, o);
+    const double ux = o[0], uy = o[1], uz = o[2], vx = o[3], vy = o[4], vz = o[5], wx = o[6], wy = o[7], wz = o[8];
+    const double sinADE1 = v.sinADE1;
+    // back-rotation of (y, z) components: (c u + s w, -s u + c w)
+    if (Dn != 0.0) {
+        const double c = Dn * K8;
+        const double a = c * vx, b = c * wx;
+        U[0][0] += c * ux;
+        U[0][1] += CosT * a + SinT * b;
+        U[0][2] += -SinT * a + CosT * b;
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const double slip = q == 0 ? Dss : Dds;
+        if (!(slip != 0.0)) continue;
+        const double Ds = q == 0 ? CosT * Dss : -SinT * Dds;
+        const double Dd = q == 0 ? SinT * Dss : CosT * Dds;
+        const double cs = Ds * K8, cd = Dd * sinADE1;
+        const double a = x * (cs * vy + cd * vz);
+        const double b = x * (cs * wy + cd * wz);
+        U[1 + q][0] += cs * uy + cd * uz;
+        U[1 + q][1] += CosT * a + SinT * b;
+        U[1 + q][2] += -SinT * a + CosT * b;
+    }
+}
+
+template <bool IMAGE>
+CAD_HD void disp_fs(const Frame& f, double X, double Y, double Z, double Dss, double Dds,
+                                        double Dn, double K8, double U[3][3])
+{
+    double x, y, z;
+    to_tdcs(f, X, Y, Z, x, y, z);
+    const int mode = trimode(f, x, y, z);
+    const bool detach = IMAGE && f.flat;
+    double keep_z[3];
+    if (IMAGE) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double a = U[m][0], b = U[m][1], c = U[m][2];
+            U[m][0] = f.Vn[0] * a + f.Vn[1] * b + f.Vn[2] * c;
+            U[m][1] = f.Vs[0] * a + f.Vs[1] * b + f.Vs[2] * c;
+            U[m][2] = f.Vd[0] * a + f.Vd[1] * b + f.Vd[2] * c;
+        }
+        if (detach) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                keep_z[m] = U[m][2];
+                U[m][2] = -U[m][2];
+            }
+        }
+    }
+    const double sgn = mode == -1 ? -1.0 : 1.0;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) ad_disp(f.v[a], sgn, x, y, z, Dss, Dds, Dn, K8, U);
+    if (mode == 0) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) U[m][c] = qnan();
+    }
+    {   // Burgers' function (solid angle of the TD seen from the point)
+        const double a1 = -x, a2 = f.p1y - y, a3 = f.p1z - z;
+        const double b2 = -y, b3 = -z;
+        const double c2 = f.p3y - y, c3 = f.p3z - z;
+        const double a12 = a1 * a1;
+        const double na = sqrt(a12 + a2 * a2 + a3 * a3);
+        const double nb = sqrt(a12 + b2 * b2 + b3 * b3);
+        const double nc = sqrt(a12 + c2 * c2 + c3 * c3);
+        const double one = a1 * (b2 * c3 - b3 * c2) - a2 * (a1 * c3 - b3 * a1) + a3 * (a1 * c2 - b2 * a1);
+        const double ab = a1 * a1 + a2 * b2 + a3 * b3;
+        const double ac = a1 * a1 + a2 * c2 + a3 * c3;
+        const double bc = a1 * a1 + b2 * c2 + b3 * c3;
+        const double two = na * nb * nc + ab * nc + ac * nb + bc * na;
+        const double Fi = -0.5 * M_1_PI * atan2(one, two);
+        U[0][0] += Dn * Fi;
+        U[1][1] += Dss * Fi;
+        U[2][2] += Dds * Fi;
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const double a = U[m][0], b = U[m][1], c = U[m][2];
+        U[m][0] = f.Vn[0] * a + f.Vs[0] * b + f.Vd[0] * c;
+        U[m][1] = f.Vn[1] * a + f.Vs[1] * b + f.Vd[1] * c;
+        U[m][2] = f.Vn[2] * a + f.Vs[2] * b + f.Vd[2] * c;
+    }
+    if (detach) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) U[m][2] = keep_z[m];
+    }
+}
+
+// --------------------------------------------------- free-surface correction
+// Observation point -> ADCS of a side, relative to PA.
+CAD_HD void to_adcs(const FscSide& s, double X, double Y, double Z, double& x, double& y,
+                                        double& z)
+{
+    const double dX = sub_rn(X, s.PA[0]), dY = sub_rn(Y, s.PA[1]), dZ = sub_rn(Z, s.PA[2]);
+    x = add_rn(add_rn(mul_rn(s.ey1[0], dX), mul_rn(s.ey2[0], dY)), mul_rn(s.ey3[0], dZ));
+    y = add_rn(add_rn(mul_rn(s.ey1[1], dX), mul_rn(s.ey2[1], dY)), mul_rn(s.ey3[1], dZ));
+    z = add_rn(add_rn(mul_rn(s.ey1[2], dX), mul_rn(s.ey2[2], dY)), mul_rn(s.ey3[2], dZ));
+}
+
+CAD_HD void fsc_strain_eval(const ang_dis_strain_fsc_k& k, double y1, double y2, double y3,
+                                                double v[18])
+{
+    ang_dis_strain_fsc_g0(k, y1, y2, y3, v);
+    ang_dis_strain_fsc_g1(k, y1, y2, y3, v + 6);
+    ang_dis_strain_fsc_g2(k, y1, y2, y3, v + 12);
+}
+
+// One side's harmonic correction to the strain, added into E (EFCS).
+CAD_HD void fsc_strain(const FscSide& s, double X, double Y, double Z, double Dss, double Dds,
+                                           double Dn, double E[3][6])
+{
+    double x, y, z;
+    to_adcs(s, X, Y, Z, x, y, z);
+    const bool flip = mul_rn(s.beta, x) >= 0.0;
+    const int c = flip ? 1 : 0;
+    const double f = flip ? -1.0 : 1.0;
+    // d = (term at PB) - (term at PA), formed before any slip product: far
+    // from the side the two terms nearly cancel, and differencing them first
+    // keeps the products from rounding the two halves differently.
+    double d[18];
+    fsc_strain_eval(s.ks[c][0], f * x, f * y, z, d);
+#pragma unroll
+    for (int q = 0; q < 18; ++q) d[q] = -d[q];
+    {
+        double v[18];
+        fsc_strain_eval(s.ks[c][1], f * (x - s.y1B), f * (y - s.y2B), z - s.y3B, v);
+#pragma unroll
+        for (int q = 0; q < 18; ++q) d[q] += v[q];
+    }
+    double T[3][6];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        // configuration flip negates the first two ADCS slip components and
+        // the 13 / 23 strain components
+        const double c0 = f * s.cs[m][0], c1 = f * s.cs[m][1], c2 = s.cs[m][2];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double fk = (k >= 4) ? f : 1.0;
+            const double h = (k >= 3) ? 0.5 : 1.0;
+            T[m][k] = h * fk * (c0 * d[k] + c1 * d[6 + k] + c2 * d[12 + k]);
+        }
+    }
+    const double AFlip[9] = {s.ey1[0], s.ey1[1], s.ey1[2], s.ey2[0], s.ey2[1], s.ey2[2], s.ey3[0], s.ey3[1], s.ey3[2]};
+    const double slip[3] = {Dn, Dss, Dds};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!(slip[m] != 0.0)) continue;
+        tensor_rot(T[m], AFlip);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[m][k] += T[m][k];
+    }
+}
+
+// One side's harmonic correction to the displacement, added into U (EFCS).
+CAD_HD void fsc_disp(const FscSide& s, double X, double Y, double Z, double Dss, double Dds,
+                                         double Dn, double U[3][3])
+{
+    double x, y, z;
+    to_adcs(s, X, Y, Z, x, y, z);
+    const int c = mul_rn(s.beta, x) >= 0.0 ? 1 : 0;
+    double uA[9], uB[9];
+    ang_dis_disp_fsc(s.kd[c][0], x, y, z, uA);
+    ang_dis_disp_fsc(s.kd[c][1], x - s.y1B, y - s.y2B, z - s.y3B, uB);
+    const double slip[3] = {Dn, Dss, Dds};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!(slip[m] != 0.0)) continue;
+        double u[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            u[d] = s.cd[m][0] * (uB[3 * d] - uA[3 * d]) + s.cd[m][1] * (uB[3 * d + 1] - uA[3 * d + 1]) +
+                   s.cd[m][2] * (uB[3 * d + 2] - uA[3 * d + 2]);
+        // ADCS -> EFCS: rows (ey1, ey2, ey3) as in the reference's VxR, VyR, VzR
+        U[m][0] += s.ey1[0] * u[0] + s.ey1[1] * u[1] + s.ey1[2] * u[2];
+        U[m][1] += s.ey2[0] * u[0] + s.ey2[1] * u[1] + s.ey2[2] * u[2];
+        U[m][2] += s.ey3[0] * u[0] + s.ey3[1] * u[1] + s.ey3[2] * u[2];
+    }
+}
+
+// -------------------------------------------------------- triangle setup
+// The per-triangle setup uses unfused arithmetic throughout: it is negligible
+// work, and the half-space terms of the two ends of a side cancel far from the
+// side, which amplifies any inconsistency between the side angle beta and the
+// side vector (fused rounding of |S| alone is enough to show).
+CAD_HD double sq_rn(double a) { return mul_rn(a, a); }
+CAD_HD double norm3_rn(double a, double b, double c) { return sqrt(add_rn(add_rn(sq_rn(a), sq_rn(b)), sq_rn(c))); }
+CAD_HD void cross3_rn(const double a[3], const double b[3], double c[3])
+{
+    c[0] = sub_rn(mul_rn(a[1], b[2]), mul_rn(a[2], b[1]));
+    c[1] = sub_rn(mul_rn(a[2], b[0]), mul_rn(a[0], b[2]));
+    c[2] = sub_rn(mul_rn(a[0], b[1]), mul_rn(a[1], b[0]));
+}
+
+CAD_HD void build_frame(const double P1[3], const double P2[3], const double P3[3], double nu, Frame& f)
+{
+    double a[3], b[3], Vn[3], Vs[3], Vd[3];
+    for (int i = 0; i < 3; ++i) { a[i] = sub_rn(P2[i], P1[i]); b[i] = sub_rn(P3[i], P1[i]); }
+    cross3_rn(a, b, Vn);
+    const double nn = norm3_rn(Vn[0], Vn[1], Vn[2]);
+    for (int i = 0; i < 3; ++i) Vn[i] = Vn[i] / nn;
+    const double eZ[3] = {0.0, 0.0, 1.0};
+    cross3_rn(eZ, Vn, Vs);
+    if (Vs[0] == 0.0 && Vs[1] == 0.0 && Vs[2] == 0.0) {   // horizontal TD
+        Vs[0] = mul_rn(0.0, Vn[2]);
+        Vs[1] = mul_rn(1.0, Vn[2]);
+        Vs[2] = mul_rn(0.0, Vn[2]);
+    }
+    const double ns = norm3_rn(Vs[0], Vs[1], Vs[2]);
+    for (int i = 0; i < 3; ++i) Vs[i] = Vs[i] / ns;
+    cross3_rn(Vn, Vs, Vd);
+    for (int i = 0; i < 3; ++i) { f.P2[i] = P2[i]; f.Vn[i] = Vn[i]; f.Vs[i] = Vs[i]; f.Vd[i] = Vd[i]; }
+
+    double p1[3], p3[3];
+    {
+        const double d1[3] = {sub_rn(P1[0], P2[0]), sub_rn(P1[1], P2[1]), sub_rn(P1[2], P2[2])};
+        const double d3[3] = {sub_rn(P3[0], P2[0]), sub_rn(P3[1], P2[1]), sub_rn(P3[2], P2[2])};
+        p1[0] = dot3_rn(Vn[0], Vn[1], Vn[2], d1[0], d1[1], d1[2]);
+        p1[1] = dot3_rn(Vs[0], Vs[1], Vs[2], d1[0], d1[1], d1[2]);
+        p1[2] = dot3_rn(Vd[0], Vd[1], Vd[2], d1[0], d1[1], d1[2]);
+        p3[0] = dot3_rn(Vn[0], Vn[1], Vn[2], d3[0], d3[1], d3[2]);
+        p3[1] = dot3_rn(Vs[0], Vs[1], Vs[2], d3[0], d3[1], d3[2]);
+        p3[2] = dot3_rn(Vd[0], Vd[1], Vd[2], d3[0], d3[1], d3[2]);
+    }
+    f.p1y = p1[1]; f.p1z = p1[2]; f.p3y = p3[1]; f.p3z = p3[2];
+    double e12[3], e13[3], e23[3];
+    for (int i = 0; i < 3; ++i) { e12[i] = sub_rn(0.0, p1[i]); e13[i] = sub_rn(p3[i], p1[i]); e23[i] = sub_rn(p3[i], 0.0); }
+    const double n12 = norm3_rn(e12[0], e12[1], e12[2]);
+    const double n13 = norm3_rn(e13[0], e13[1], e13[2]);
+    const double n23 = norm3_rn(e23[0], e23[1], e23[2]);
+    for (int i = 0; i < 3; ++i) { e12[i] /= n12; e13[i] /= n13; e23[i] /= n23; }
+    const double A = acos(dot3_rn(e12[0], e12[1], e12[2], e13[0], e13[1], e13[2]));
+    const double B = acos(dot3_rn(-e12[0], -e12[1], -e12[2], e23[0], e23[1], e23[2]));
+    const double C = acos(dot3_rn(e23[0], e23[1], e23[2], e13[0], e13[1], e13[2]));
+
+    // configuration test constants (trimodefinder on the TDCS (y, z) plane)
+    f.t23y = sub_rn(0.0, p3[2]);
+    f.t32x = sub_rn(p3[1], 0.0);
+    f.t13x = sub_rn(p1[1], p3[1]);
+    const double t13y = sub_rn(p1[2], p3[2]);
+    f.t31y = sub_rn(p3[2], p1[2]);
+    f.base = add_rn(mul_rn(f.t23y, f.t13x), mul_rn(f.t32x, t13y));
+
+    const double alpha[3] = {A, B, C};
+    const double side_y[3] = {-e13[1], e12[1], e23[1]};
+    const double side_z[3] = {-e13[2], e12[2], e23[2]};
+    const double tv1[3] = {p1[1], 0.0, p3[1]};
+    const double tv2[3] = {p1[2], 0.0, p3[2]};
+    for (int v = 0; v < 3; ++v) {
+        AngDis& d = f.v[v];
+        d.cosT = side_z[v];
+        d.sinT = side_y[v];
+        d.tv1 = tv1[v];
+        d.tv2 = tv2[v];
+        const double Ang = -M_PI + alpha[v];
+        const double cosA = cos(Ang), sinA = sin(Ang);
+        d.sinADE1 = sinA / 8.0 / M_PI / sub_rn(1.0, nu);
+        ang_dis_strain_setup(cosA, sinA, nu, add_rn(mul_rn(2.0, nu), 1.0), d.sinADE1, d.ks);
+        ang_dis_disp_setup(cosA, sinA, sub_rn(1.0, nu), sub_rn(1.0, mul_rn(2.0, nu)), mul_rn(cosA, cosA), d.sinADE1,
+                           d.kd);
+    }
+    f.flat = (P1[2] == 0.0 && P2[2] == 0.0 && P3[2] == 0.0) ? 1 : 0;
+    f.pad_ = 0;
+}
+
+CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real, double Dss, double Dds,
+                       double Dn, double nu, FscSide& s)
+{
+    const double S[3] = {sub_rn(PB[0], PA[0]), sub_rn(PB[1], PA[1]), sub_rn(PB[2], PA[2])};
+    const double Sv = norm3_rn(S[0], S[1], S[2]);
+    const double beta = acos(-S[2] / Sv);
+    s.beta = beta;
+    s.skip = (fabs(beta) < DBL_EPSILON) || (fabs(M_PI - beta) < DBL_EPSILON) || (fabs(1.0 / tan(beta)) > 5e3);
+    s.pad_ = 0;
+    for (int i = 0; i < 3; ++i) s.PA[i] = PA[i];
+    if (s.skip) return;
+    const double n1 = norm3_rn(S[0], S[1], 0.0);
+    const double e1[3] = {S[0] / n1, S[1] / n1, 0.0 / n1};
+    const double e3[3] = {-0.0, -0.0, -1.0};
+    double e2[3];
+    cross3_rn(e3, e1, e2);
+    for (int i = 0; i < 3; ++i) { s.ey1[i] = e1[i]; s.ey2[i] = e2[i]; s.ey3[i] = e3[i]; }
+    s.y1B = add_rn(add_rn(mul_rn(e1[0], S[0]), mul_rn(e2[0], S[1])), mul_rn(e3[0], S[2]));
+    s.y2B = add_rn(add_rn(mul_rn(e1[1], S[0]), mul_rn(e2[1], S[1])), mul_rn(e3[1], S[2]));
+    s.y3B = add_rn(add_rn(mul_rn(e1[2], S[0]), mul_rn(e2[2], S[1])), mul_rn(e3[2], S[2]));
+    // unit-mode slip vectors: TDCS (n, s, d) -> EFCS -> ADCS
+    const double slip[3] = {Dn, Dss, Dds};
+    const double* axes[3] = {real.Vn, real.Vs, real.Vd};
+    for (int m = 0; m < 3; ++m) {
+        double w[3];
+        for (int i = 0; i < 3; ++i) w[i] = mul_rn(axes[m][i], slip[m]);
+        for (int g = 0; g < 3; ++g) {
+            s.cs[m][g] = add_rn(add_rn(mul_rn(e1[g], w[0]), mul_rn(e2[g], w[1])), mul_rn(e3[g], w[2]));
+            s.cd[m][g] = s.cs[m][g] / 4.0 / M_PI / sub_rn(1.0, nu);
+        }
+    }
+    const double a_end[2] = {-PA[2], -PB[2]};
+    const double pibs = M_PI - beta, pibd = -M_PI + beta;
+    for (int e = 0; e < 2; ++e) {
+        ang_dis_strain_fsc_setup(cos(beta), sin(beta), 1.0 / tan(beta), nu, a_end[e], s.ks[0][e]);
+        ang_dis_strain_fsc_setup(cos(pibs), sin(pibs), 1.0 / tan(pibs), nu, a_end[e], s.ks[1][e]);
+        ang_dis_disp_fsc_setup(cos(beta), sin(beta), 1.0 / tan(beta), 1.0 / tan(beta / 2.0), nu, a_end[e],
+                               s.kd[0][e]);
+        ang_dis_disp_fsc_setup(cos(pibd), sin(pibd), 1.0 / tan(pibd), 1.0 / tan(pibd / 2.0), nu, a_end[e],
+                               s.kd[1][e]);
+    }
+}
+
+// ------------------------------------------------------------ pair drivers
+template <bool HS>
+CAD_HD void pair_strain(const TriDev& t, double X, double Y, double Z, double E[3][6])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[m][k] = 0.0;
+    strain_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+    if (HS) {
+#pragma unroll 1
+        for (int sd = 0; sd < 3; ++sd)
+            if (!t.side[sd].skip) fsc_strain(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, E);
+        strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+    }
+}
+
+template <bool HS>
+CAD_HD void pair_disp(const TriDev& t, double X, double Y, double Z, double U[3][3])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) U[m][c] = 0.0;
+    disp_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+    if (HS) {
+#pragma unroll 1
+        for (int sd = 0; sd < 3; ++sd)
+            if (!t.side[sd].skip) fsc_disp(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, U);
+        disp_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+    }
+}
+
+CAD_HD void build_triangle(const double a[3], const double b[3], const double c[3], double Dss, double Dds,
+                           double Dn, double nu, bool hs, TriDev& t)
+{
+    t.Dss = Dss;
+    t.Dds = Dds;
+    t.Dn = Dn;
+    t.K8 = 1.0 / (8.0 * M_PI * (1.0 - nu));
+    build_frame(a, b, c, nu, t.real);
+    if (!hs) return;
+    const double ai[3] = {a[0], a[1], -a[2]}, bi[3] = {b[0], b[1], -b[2]}, ci[3] = {c[0], c[1], -c[2]};
+    build_frame(ai, bi, ci, nu, t.image);
+    build_side(a, b, t.real, t.Dss, t.Dds, t.Dn, nu, t.side[0]);
+    build_side(b, c, t.real, t.Dss, t.Dds, t.Dn, nu, t.side[1]);
+    build_side(c, a, t.real, t.Dss, t.Dds, t.Dn, nu, t.side[2]);
+}
+
+}  // namespace cad

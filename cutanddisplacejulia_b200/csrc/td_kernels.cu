@@ -1,0 +1,314 @@
+// TD pair kernels for sm_100a (FP64 CUDA-core work; no tensor-core shape).
+//
+// Work decomposition: one thread per observation point, one block per
+// (128-point tile, chunk of triangles).  The block stages one triangle's
+// precomputed record (TriDev) at a time in shared memory; every thread reads
+// it as a broadcast, evaluates its pair and writes the pair's outputs
+// (consecutive threads = consecutive rows of a column-major M x N influence
+// matrix, so every store is coalesced).
+//
+// Output modes:
+//   OUT_INF   18 strain and / or 9 displacement influence matrices (TD overload
+//             src/TD.jl:135-216)
+//   OUT_SUM   per-chunk partial sums over triangles of strain (6) and
+//             displacement (3) (TD summing overload src/TD.jl:219-410); a
+//             second kernel adds the chunks in index order (deterministic)
+//   OUT_TRAC  9 traction influence matrices, strain converted in registers
+//             (ConvertStrainInfMatsToTraction, src/CalculateInfluenceMatrices3D.jl:73-114)
+//   OUT_AMAT  the 3N x 3N system matrix -[Atn;Atss;Atds] (src/SlipCalculator3D.jl:13-16)
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "td_device.cuh"
+#include "td_kernels.h"
+
+namespace cad {
+
+// ------------------------------------------------------------ setup kernel
+__global__ void td_setup_kernel(const double* __restrict__ P1, const double* __restrict__ P2,
+                                const double* __restrict__ P3, int64_t N, const double* __restrict__ Dss,
+                                const double* __restrict__ Dds, const double* __restrict__ Dn, int64_t slip_stride,
+                                double nu, int hs, TriDev* __restrict__ out)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    TriDev& t = out[j];
+    const double a[3] = {P1[j], P1[j + N], P1[j + 2 * N]};
+    const double b[3] = {P2[j], P2[j + N], P2[j + 2 * N]};
+    const double c[3] = {P3[j], P3[j + N], P3[j + 2 * N]};
+    build_triangle(a, b, c, Dss ? Dss[j * slip_stride] : 1.0, Dds ? Dds[j * slip_stride] : 1.0,
+                   Dn ? Dn[j * slip_stride] : 1.0, nu, hs != 0, t);
+}
+
+// ------------------------------------------------ half-space argument check
+// flag |= 1 when any vertex or observation z > 0 (src/TD.jl:606-619).
+__global__ void hs_check_kernel(const double* __restrict__ Z, int64_t M, const double* __restrict__ P1,
+                                const double* __restrict__ P2, const double* __restrict__ P3, int64_t N,
+                                int* __restrict__ flag)
+{
+    int bad = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M + N; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < M) bad |= Z[i] > 0.0;
+        else {
+            const int64_t j = i - M;
+            bad |= (P1[j + 2 * N] > 0.0) | (P2[j + 2 * N] > 0.0) | (P3[j + 2 * N] > 0.0);
+        }
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// ---------------------------------------------------- collocation points
+// obs = incentre - 1e-12 * normal (SetupCollationPoints,
+// src/CalculateInfluenceMatrices3D.jl:52-71) and the strike / dip directions
+// of every element (CalculateSSandDSDirs, src/CalculateSSandDSDirs.jl:417-481).
+__global__ void colloc_kernel(const double* __restrict__ normals, const double* __restrict__ mid, int64_t N,
+                              double* __restrict__ X, double* __restrict__ Y, double* __restrict__ Z,
+                              double* __restrict__ dirs /* 9 x N: n, ss, ds */)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double cx = normals[i], cy = normals[i + N], cz = normals[i + 2 * N];
+    X[i] = mid[i] - cx * 1e-12;
+    Y[i] = mid[i + N] - cy * 1e-12;
+    Z[i] = mid[i + 2 * N] - cz * 1e-12;
+    const double inv = 1.0 / sqrt(cx * cx + cy * cy);
+    double ss[3] = {-(cy * inv), cx * inv, 0.0};
+    const double dsz = cos(acos(cz) - M_PI / 2.0);
+    double L = sin(acos(dsz));
+    if (cz < 0.0) L = -L;
+    const double a = atan2(cy, cx);
+    double ds[3] = {-(cos(a) * L), -(sin(a) * L), dsz};
+    if (cx == 0.0 && cy == 0.0) {
+        ds[0] = -1.0; ds[1] = 0.0; ds[2] = 0.0;
+        ss[0] = 0.0; ss[1] = cz < 1.0 ? -1.0 : 1.0; ss[2] = 0.0;
+    }
+    dirs[i] = cx; dirs[i + N] = cy; dirs[i + 2 * N] = cz;
+    for (int k = 0; k < 3; ++k) { dirs[i + (3 + k) * N] = ss[k]; dirs[i + (6 + k) * N] = ds[k]; }
+}
+
+// Unit-mode strain -> (Tn, Tss, Tds) on the element with normal n, strike ss,
+// dip ds (Hooke, CalculateNormalTraction3D!, TractionVectorCartesianComponents3D!,
+// CalculateTractionInChosenDirection3D!).
+__device__ __forceinline__ void strain_to_traction(const double e[6], double lam, double G2, const double n[3],
+                                                   const double ss[3], const double ds[3], double out[3])
+{
+    const double cons = lam * (e[0] + e[1] + e[2]);
+    const double Sxx = G2 * e[0] + cons, Syy = G2 * e[1] + cons, Szz = G2 * e[2] + cons;
+    const double Sxy = G2 * e[3], Sxz = G2 * e[4], Syz = G2 * e[5];
+    const double cx = n[0], cy = n[1], cz = n[2];
+    out[0] = Sxx * (cx * cx) + Syy * (cy * cy) + Szz * (cz * cz) + 2.0 * Sxy * (cx * cy) + 2.0 * Syz * (cy * cz) +
+             2.0 * Sxz * (cz * cx);
+    const double Tx = Sxx * cx + Sxy * cy + Sxz * cz;
+    const double Ty = Sxy * cx + Syy * cy + Syz * cz;
+    const double Tz = Sxz * cx + Syz * cy + Szz * cz;
+    // traction projected onto the plane: t - (t.n) n
+    const double tn = Tx * cx + Ty * cy + Tz * cz;
+    const double px = Tx - tn * cx, py = Ty - tn * cy, pz = Tz - tn * cz;
+    out[1] = px * ss[0] + py * ss[1] + pz * ss[2];
+    out[2] = px * ds[0] + py * ds[1] + pz * ds[2];
+}
+
+// ------------------------------------------------------------- pair kernel
+template <bool HS, bool STRAIN, bool DISP, int OUT>
+__global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
+{
+    extern __shared__ double smem[];
+    constexpr int words = HS ? kTriWordsHS : kTriWordsFS;
+    const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
+    const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
+    const bool active = i < a.M;
+    double X = 0.0, Y = 0.0, Z = 0.0;
+    if (active) { X = a.X[i]; Y = a.Y[i]; Z = a.Z[i]; }
+    const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
+    const int64_t j1 = min(a.N, j0 + a.tri_chunk);
+    const int64_t MN = a.M * a.N;
+    double sumE[6] = {0, 0, 0, 0, 0, 0}, sumU[3] = {0, 0, 0};
+    double n[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, ds[3] = {0, 0, 0};
+    if ((OUT == OUT_TRAC || OUT == OUT_AMAT) && active) {
+        for (int k = 0; k < 3; ++k) {
+            n[k] = a.dirs[i + k * a.M];
+            ss[k] = a.dirs[i + (3 + k) * a.M];
+            ds[k] = a.dirs[i + (6 + k) * a.M];
+        }
+    }
+    for (int64_t j = j0; j < j1; ++j) {
+        __syncthreads();
+        const double* src = reinterpret_cast<const double*>(a.tri + j);
+        for (int w = threadIdx.x; w < words; w += kPairThreads) smem[w] = src[w];
+        __syncthreads();
+        if (!active) continue;
+        if (STRAIN) {
+            double E[3][6];
+            pair_strain<HS>(t, X, Y, Z, E);
+            if (OUT == OUT_INF) {
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) a.strain[(6 * m + k) * MN + i + a.M * j] = E[m][k];
+            } else if (OUT == OUT_SUM) {
+#pragma unroll
+                for (int k = 0; k < 6; ++k) sumE[k] += (E[0][k] + E[1][k]) + E[2][k];
+            } else {
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    double tr[3];
+                    strain_to_traction(E[m], a.lambda, 2.0 * a.G, n, ss, ds, tr);
+                    if (OUT == OUT_TRAC) {
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) a.trac[(3 * m + r) * MN + i + a.M * j] = tr[r];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 3; ++r)
+                            a.A[(int64_t)(r * a.N + i) + a.lda * (int64_t)(m * a.N + j)] = -tr[r];
+                    }
+                }
+            }
+        }
+        if (DISP) {
+            double U[3][3];
+            pair_disp<HS>(t, X, Y, Z, U);
+            if (OUT == OUT_INF) {
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) a.disp[(3 * m + c) * MN + i + a.M * j] = U[m][c];
+            } else if (OUT == OUT_SUM) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sumU[c] += (U[0][c] + U[1][c]) + U[2][c];
+            }
+        }
+    }
+    if (OUT == OUT_SUM && active) {
+        double* p = a.partial + (int64_t)blockIdx.y * 9 * a.M;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p[k * a.M + i] = sumE[k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) p[(6 + c) * a.M + i] = sumU[c];
+    }
+}
+
+// Adds the per-chunk partial sums in chunk order: out[f][i] = sum_c partial[c][f][i].
+__global__ void sum_chunks_kernel(const double* __restrict__ partial, int64_t nchunk, int64_t M, int fields_mask,
+                                  double* __restrict__ out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (i >= M || !((fields_mask >> f) & 1)) return;
+    double s = 0.0;
+    for (int64_t c = 0; c < nchunk; ++c) s += partial[(c * 9 + f) * M + i];
+    out[f * M + i] = s;
+}
+
+// TD_sum (src/TD_sum.jl:1-41): sum the three modes, then across the N columns.
+// in: nf*3 matrices M x N (field f of mode m at in + (m*nf + f)*M*N), out: nf x M.
+__global__ void td_sum_kernel(const double* __restrict__ in, int64_t M, int64_t N, int nf, double* __restrict__ out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (i >= M) return;
+    const int64_t MN = M * N;
+    double s = 0.0;
+    for (int64_t j = 0; j < N; ++j) {
+        const int64_t o = i + M * j;
+        s += (in[(0 * nf + f) * MN + o] + in[(1 * nf + f) * MN + o]) + in[(2 * nf + f) * MN + o];
+    }
+    out[f * M + i] = s;
+}
+
+// ------------------------------------------------------------ launchers
+template <bool HS, bool STRAIN, bool DISP, int OUT>
+static cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
+{
+    const size_t smem = (HS ? kTriWordsHS : kTriWordsFS) * sizeof(double);
+    auto kern = td_pair_kernel<HS, STRAIN, DISP, OUT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t ntile = (a.M + kPairThreads - 1) / kPairThreads;
+    const int64_t nchunk = (a.N + a.tri_chunk - 1) / a.tri_chunk;
+    if (ntile == 0 || nchunk == 0) return cudaSuccess;
+    dim3 grid((unsigned)ntile, (unsigned)nchunk);
+    kern<<<grid, kPairThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+#define CAD_DISPATCH_FLAGS(OUTK)                                                              \
+    if (hs) {                                                                                 \
+        if (strain && disp) return launch_pair<true, true, true, OUTK>(a, st);                \
+        if (strain) return launch_pair<true, true, false, OUTK>(a, st);                       \
+        if (disp) return launch_pair<true, false, true, OUTK>(a, st);                         \
+    } else {                                                                                  \
+        if (strain && disp) return launch_pair<false, true, true, OUTK>(a, st);               \
+        if (strain) return launch_pair<false, true, false, OUTK>(a, st);                      \
+        if (disp) return launch_pair<false, false, true, OUTK>(a, st);                        \
+    }                                                                                         \
+    return cudaSuccess;
+
+cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bool disp, cudaStream_t st)
+{
+    switch (out) {
+        case OUT_INF: { CAD_DISPATCH_FLAGS(OUT_INF) }
+        case OUT_SUM: { CAD_DISPATCH_FLAGS(OUT_SUM) }
+        case OUT_TRAC:
+            if (hs) return launch_pair<true, true, false, OUT_TRAC>(a, st);
+            return launch_pair<false, true, false, OUT_TRAC>(a, st);
+        case OUT_AMAT:
+            if (hs) return launch_pair<true, true, false, OUT_AMAT>(a, st);
+            return launch_pair<false, true, false, OUT_AMAT>(a, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                            const double* Dds, const double* Dn, int64_t slip_stride, double nu, bool hs,
+                            TriDev* out, cudaStream_t st)
+{
+    if (N == 0) return cudaSuccess;
+    const int bs = 64;
+    td_setup_kernel<<<(unsigned)((N + bs - 1) / bs), bs, 0, st>>>(P1, P2, P3, N, Dss, Dds, Dn, slip_stride, nu,
+                                                                  hs ? 1 : 0, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hs_check(const double* Z, int64_t M, const double* P1, const double* P2, const double* P3,
+                            int64_t N, int* flag, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+    if (e != cudaSuccess || M + N == 0) return e;
+    const int bs = 256;
+    int64_t nb = (M + N + bs - 1) / bs;
+    if (nb > 1184) nb = 1184;
+    hs_check_kernel<<<(unsigned)nb, bs, 0, st>>>(Z, M, P1, P2, P3, N, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_colloc(const double* normals, const double* mid, int64_t N, double* X, double* Y, double* Z,
+                          double* dirs, cudaStream_t st)
+{
+    if (N == 0) return cudaSuccess;
+    const int bs = 128;
+    colloc_kernel<<<(unsigned)((N + bs - 1) / bs), bs, 0, st>>>(normals, mid, N, X, Y, Z, dirs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_chunks(const double* partial, int64_t nchunk, int64_t M, int fields_mask, double* out,
+                              cudaStream_t st)
+{
+    if (M == 0) return cudaSuccess;
+    const int bs = 256;
+    dim3 grid((unsigned)((M + bs - 1) / bs), 9);
+    sum_chunks_kernel<<<grid, bs, 0, st>>>(partial, nchunk, M, fields_mask, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_td_sum(const double* in, int64_t M, int64_t N, int nf, double* out, cudaStream_t st)
+{
+    if (M == 0) return cudaSuccess;
+    const int bs = 256;
+    dim3 grid((unsigned)((M + bs - 1) / bs), (unsigned)nf);
+    td_sum_kernel<<<grid, bs, 0, st>>>(in, M, N, nf, out);
+    return cudaGetLastError();
+}
+
+}  // namespace cad

@@ -1,0 +1,47 @@
+// Internal launch interface of the TD pair kernels (host side of td_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace cad {
+
+struct TriDev;
+
+constexpr int kPairThreads = 128;
+
+enum OutKind { OUT_INF = 0, OUT_SUM = 1, OUT_TRAC = 2, OUT_AMAT = 3 };
+
+struct PairArgs {
+    const double* X;
+    const double* Y;
+    const double* Z;
+    int64_t M;
+    const TriDev* tri;
+    int64_t N;
+    int64_t tri_chunk;   // triangles per block (grid.y = ceil(N / tri_chunk))
+    double lambda, G;
+    double* strain;      // OUT_INF: 18 x M x N
+    double* disp;        // OUT_INF: 9 x M x N
+    double* partial;     // OUT_SUM: nchunk x 9 x M
+    double* trac;        // OUT_TRAC: 9 x M x N
+    double* A;           // OUT_AMAT: 3N x 3N column-major, leading dimension lda
+    int64_t lda;
+    const double* dirs;  // OUT_TRAC / OUT_AMAT: 9 x M (normal, strike, dip of each observed element)
+};
+
+size_t tri_record_bytes();
+
+cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                            const double* Dds, const double* Dn, int64_t slip_stride, double nu, bool hs,
+                            TriDev* out, cudaStream_t st);
+cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bool disp, cudaStream_t st);
+cudaError_t launch_hs_check(const double* Z, int64_t M, const double* P1, const double* P2, const double* P3,
+                            int64_t N, int* flag, cudaStream_t st);
+cudaError_t launch_colloc(const double* normals, const double* mid, int64_t N, double* X, double* Y, double* Z,
+                          double* dirs, cudaStream_t st);
+cudaError_t launch_sum_chunks(const double* partial, int64_t nchunk, int64_t M, int fields_mask, double* out,
+                              cudaStream_t st);
+cudaError_t launch_td_sum(const double* in, int64_t M, int64_t N, int nf, double* out, cudaStream_t st);
+
+}  // namespace cad

@@ -1,0 +1,132 @@
+"""Host-side mesh geometry and elastic-constant helpers that feed the TD path:
+CreateFaceNormalAndMidPoint (src/CreateFaceNormalAndMidPoint.jl:137-185 with
+CreateTriangleNormal! and CreateMidPoint!), CreateP1P2P3
+(src/CreateP1P2P3.jl, by direct indexing instead of a search),
+CalculateSSandDSDirs (src/CalculateSSandDSDirs.jl), AreaOfTriangle3D and
+ElasticConstantsCheck(G, nu) (src/ElasticConstantsCheck.jl:83-95), plus
+readers for the reference's mesh formats (ASCII STL, GoCad TSurf, OFF).
+O(N) host work; not on the GPU hot path."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def CreateFaceNormalAndMidPoint(P1, P2, P3):
+    """Unit normal of (P2-P1)x(P3-P1) and the incentre of every triangle."""
+    P1, P2, P3 = (np.asarray(p, dtype=np.float64).reshape(-1, 3) for p in (P1, P2, P3))
+    U, V = P2 - P1, P3 - P1
+    Nv = np.cross(U, V)
+    normal = Nv / np.sqrt((Nv * Nv).sum(1))[:, None]
+    c = np.sqrt(((P1 - P2) ** 2).sum(1))
+    a = np.sqrt(((P2 - P3) ** 2).sum(1))
+    b = np.sqrt(((P1 - P3) ** 2).sum(1))
+    if np.any((a == 0) | (b == 0) | (c == 0)):
+        raise ValueError("Slither triangles or triangles with no area exist on your surface")
+    mid = (P1 * a[:, None] + P2 * b[:, None] + P3 * c[:, None]) / (a + b + c)[:, None]
+    return normal, mid
+
+
+def CreateP1P2P3(Triangles, Points):
+    """Vertex lists from a triangle index table (1-based ids in Points[:, 0])."""
+    Points = np.asarray(Points, dtype=np.float64)
+    ids = Points[:, 0].astype(np.int64)
+    lookup = {v: k for k, v in enumerate(ids)}
+    T = np.asarray(Triangles, dtype=np.int64)
+    rows = np.vectorize(lookup.__getitem__)(T)
+    xyz = Points[:, 1:4]
+    return xyz[rows[:, 0]], xyz[rows[:, 1]], xyz[rows[:, 2]]
+
+
+def ss_ds_dirs(cx, cy, cz):
+    """Strike-slip and dip-slip direction cosines of element normals."""
+    cx, cy, cz = (np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in (cx, cy, cz))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        nrm = np.sqrt(cx * cx + cy * cy)
+        r1, r2 = cx / nrm, cy / nrm
+    ss = np.stack([-r2, r1, np.zeros_like(cx)], axis=1)
+    dsz = np.cos(np.arccos(cz) - np.pi / 2)
+    L = np.sin(np.arccos(dsz))
+    L = np.where(cz < 0, -L, L)
+    a = np.arctan2(cy, cx)
+    ds = np.stack([-np.cos(a) * L, -np.sin(a) * L, dsz], axis=1)
+    vert = (cx == 0) & (cy == 0)
+    ds[vert] = [-1.0, 0.0, 0.0]
+    ss[vert & (cz < 1.0)] = [0.0, -1.0, 0.0]
+    ss[vert & ~(cz < 1.0)] = [0.0, 1.0, 0.0]
+    return ss, ds
+
+
+CalculateSSandDSDirs = ss_ds_dirs
+
+
+def AreaOfTriangle3D(P1, P2, P3):
+    """Heron area and half perimeter of every triangle."""
+    a = np.sqrt(((P2 - P3) ** 2).sum(1))
+    b = np.sqrt(((P1 - P3) ** 2).sum(1))
+    c = np.sqrt(((P1 - P2) ** 2).sum(1))
+    s = (a + b + c) / 2
+    return np.sqrt(s * (s - a) * (s - b) * (s - c)), s
+
+
+def ElasticConstantsCheck(G, nu):
+    """(K, E, lambda, nu, G) from the shear modulus and Poisson's ratio."""
+    K = (2 * G * (1 + nu)) / (3 * (1 - 2 * nu))
+    E = 2 * G * (1 + nu)
+    lam = (2 * G * nu) / (1 - 2 * nu)
+    return K, E, lam, nu, G
+
+
+def read_stl(path):
+    """ASCII STL (src/STLReader.jl): Points (id, x, y, z), Triangles (1-based)."""
+    pts = []
+    with open(path) as f:
+        for line in f:
+            tok = line.split()
+            if tok and tok[0] == "vertex":
+                pts.append([float(t) for t in tok[1:4]])
+    pts = np.asarray(pts, dtype=np.float64)
+    n = len(pts)
+    Points = np.column_stack([np.arange(1, n + 1, dtype=np.float64), pts])
+    Triangles = np.arange(1, n + 1, dtype=np.int64).reshape(-1, 3)
+    return Points, Triangles
+
+
+def read_gocad(path):
+    """GoCad ASCII TSurf (src/GoCadAsciiReader.jl): VRTX / ATOM / TRGL records, renumbered 1..n."""
+    coords, tris = {}, []
+    with open(path) as f:
+        for line in f:
+            tok = line.split()
+            if not tok:
+                continue
+            if tok[0] == "PROJECTION":
+                raise ValueError("More than one Gocad ascii surface in the file, this function can only deal with 1")
+            if tok[0] in ("VRTX", "PVRTX"):
+                coords[int(tok[1])] = [float(t) for t in tok[2:5]]
+            elif tok[0] in ("ATOM", "PATOM"):
+                coords[int(tok[1])] = coords[int(tok[2])]
+            elif tok[0] == "TRGL":
+                tris.append([int(t) for t in tok[1:4]])
+    ids = sorted(coords)
+    new = {v: k + 1 for k, v in enumerate(ids)}
+    Points = np.array([[new[v]] + coords[v] for v in ids], dtype=np.float64)
+    Triangles = np.array([[new[v] for v in t] for t in tris], dtype=np.int64)
+    return Points, Triangles
+
+
+def read_off(path):
+    """OFF mesh (src/OFFReader.jl): 0-based face indices become 1-based."""
+    with open(path) as f:
+        tok = [t for line in f for t in line.split("#")[0].split()]
+    assert tok[0].upper().endswith("OFF")
+    nv, nf = int(tok[1]), int(tok[2])
+    k = 4
+    pts = np.array(tok[k:k + 3 * nv], dtype=np.float64).reshape(nv, 3)
+    k += 3 * nv
+    tris = []
+    for _ in range(nf):
+        c = int(tok[k])
+        tris.append([int(t) + 1 for t in tok[k + 1:k + 1 + c]])
+        k += 1 + c
+    Points = np.column_stack([np.arange(1, nv + 1, dtype=np.float64), pts])
+    return Points, np.asarray(tris, dtype=np.int64)

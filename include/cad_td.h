@@ -1,0 +1,148 @@
+/*
+ * cad_td.h -- C ABI of the B200 triangular-dislocation library (libcad_td.so).
+ *
+ * Drop-in boundary for the hot path of CutAndDisplaceJulia: the bodies of the
+ * Threads.@threads loops of TD (src/TD.jl:146-214 and :273-384), TD_sum
+ * (src/TD_sum.jl:1-41), the traction assembly of CalculateInfluenceMatrices3D
+ * (src/CalculateInfluenceMatrices3D.jl:2-48, :73-114) and the dense solve
+ * D = A\b of SlipCalculator3D (src/SlipCalculator3D.jl:1-33).  Julia binds
+ * these with ccall; every argument is a plain pointer or
+ * number, nothing here depends on any framework type.
+ *
+ * Conventions (all follow the reference's Julia layout):
+ *   - FP64 everywhere.
+ *   - Vertex lists P1, P2, P3 are N x 3 column-major (x of all triangles, then
+ *     y, then z), exactly like Julia's P1List.
+ *   - An influence matrix is M x N column-major: row = observation point,
+ *     column = triangle.
+ *   - Slip arguments are in the reference's order: Dss, Dds, Dn.
+ *   - Host-pointer entry points take caller-owned host arrays (the library
+ *     copies in and out); *_dev entry points take device pointers on the
+ *     context's device and run asynchronously on the context's stream.
+ *   - Every function returns a status code; cad_last_error() gives the message.
+ *
+ * Status codes mirror the reference's errors:
+ *   CAD_ERR_DIMS             "Element size inputs must be the same dimensions"   (src/TD.jl:424)
+ *   CAD_ERR_HS_ABOVE_SURFACE "Half-space solution: Z coordinates must be negative!" (src/TD.jl:617)
+ * NaN outputs for observation points that lie on a triangle edge in the
+ * triangle's plane are data, not errors (src/TD.jl:808-818, :1572-1595).
+ */
+#ifndef CAD_TD_H
+#define CAD_TD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CAD_OK 0
+#define CAD_ERR_DIMS 1
+#define CAD_ERR_HS_ABOVE_SURFACE 2
+#define CAD_ERR_UNSUPPORTED 3
+#define CAD_ERR_CUDA 4
+#define CAD_ERR_OOM 5
+#define CAD_ERR_TIMEOUT 6
+#define CAD_ERR_NOT_CONVERGED 7
+#define CAD_ERR_SINGULAR 8
+#define CAD_ERR_ARG 9
+
+typedef struct cad_ctx cad_ctx;
+
+/* Context: one device, one stream, its own workspace.  A context is used by
+ * one host thread at a time; separate contexts may run concurrently. */
+int cad_init(int device, cad_ctx** ctx);
+int cad_destroy(cad_ctx* ctx);
+const char* cad_last_error(const cad_ctx* ctx);
+/* Run on an existing cudaStream_t (passed as void*; NULL is CUDA's default
+ * stream).  The context starts on its own stream: cad_get_stream() before the
+ * first cad_set_stream() returns it, for switching back. */
+int cad_set_stream(cad_ctx* ctx, void* stream);
+void* cad_get_stream(const cad_ctx* ctx);
+/* Device time (ms, CUDA events on the context stream) of the most recent
+ * launch of: 0 = TD pair kernel, 1 = dense factorisation + solve. */
+double cad_last_time_ms(const cad_ctx* ctx, int which);
+/* Library version string. */
+const char* cad_version(void);
+/* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 flops
+ * per FMA), the denominator of the TD kernels' roofline.  No counterpart in
+ * the reference (a measurement utility). */
+int cad_fp64_fma_probe(cad_ctx* ctx, int64_t iters, double* tflops);
+
+/* ---------------------------------------------------------------- TD ----
+ * TD influence-matrix overloads (replaces src/TD.jl:77-133 allocation and the
+ * loop body of src/TD.jl:135-216).  strain_out: 18 pointers to M x N arrays in
+ * StrainInf field order (exxDn, eyyDn, ezzDn, exyDn, exzDn, eyzDn, then the
+ * same for Dss and Dds); disp_out: 9 pointers in DispInf order (DnUx, DnUy,
+ * DnUz, DssUx, ..., DdsUz).  A flag of 0 leaves the matching pointer array
+ * unused (it may be NULL).  G is accepted for signature parity; the reference
+ * does not use it for strain or displacement. */
+int cad_td_inf(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+               const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds,
+               const double* Dn, double nu, double G, int disp_flag, int strain_flag, int hs_flag,
+               double* const* strain_out, double* const* disp_out);
+
+/* TD summing overload (replaces the loop of src/TD.jl:219-410): strain_out 6
+ * pointers (exx, eyy, ezz, exy, exz, eyz), disp_out 3 pointers (Ux, Uy, Uz),
+ * each of length M: the sum over triangles and slip modes.  Deterministic
+ * (fixed summation order), unlike the reference's shared accumulation. */
+int cad_td_sum_eval(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M,
+                    const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                    const double* Dds, const double* Dn, double nu, double G, int disp_flag, int strain_flag,
+                    int hs_flag, double* const* strain_out, double* const* disp_out);
+
+/* TD_sum (src/TD_sum.jl:1-41): sum 18 strain / 9 displacement influence
+ * matrices (M x N, field orders as above) over modes and columns.  Either
+ * input array may be NULL (then its outputs are untouched). */
+int cad_td_sum(cad_ctx* ctx, int64_t M, int64_t N, const double* const* strain_in, const double* const* disp_in,
+               double* const* strain_out, double* const* disp_out);
+
+/* ------------------------------------------------------------ assembly ---
+ * CalculateInfluenceMatrices3D (src/CalculateInfluenceMatrices3D.jl:2-48):
+ * normals and midpoints N x 3 (FaceNormalVector, MidPoint), vertex lists
+ * N x 3; trac_out: 9 pointers to N x N arrays in TractionInf order (DnTn,
+ * DnTss, DnTds, DssTn, DssTss, DssTds, DdsTn, DdsTss, DdsTds).  fixed_els may
+ * be NULL; a fixed element (value 1) is not supported in this version and
+ * returns CAD_ERR_UNSUPPORTED. */
+int cad_influence_traction(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                           const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                           const double* fixed_els, int hs_flag, double* const* trac_out);
+
+/* SlipCalculator3D for traction-vector boundary conditions
+ * (src/SlipCalculator3D.jl:1-33): assembles A = -[Atn;Atss;Atds] (3N x 3N) and
+ * solves A D = [Tn; Tss; Tds] by LU with partial pivoting.  Outputs Dn, Dss,
+ * Dds (N each); A_out (3N x 3N) and b_out (3N) may be NULL. */
+int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                        double G, double lambda, const double* midpoints, const double* normals, int hs_flag,
+                        const double* Tn, const double* Tss, const double* Tds, double* Dn, double* Dss,
+                        double* Dds, double* A_out, double* b_out);
+
+/* Dense solve A X = B (the `\` of src/SlipCalculator3D.jl:22): A n x n, B n x
+ * nrhs, both column-major host arrays; X n x nrhs. */
+int cad_solve(cad_ctx* ctx, int64_t n, const double* A, const double* B, int64_t nrhs, double* X);
+
+/* ------------------------------------------------ device-pointer variants ---
+ * Same semantics, device pointers, asynchronous on the context stream (the
+ * half-space argument check synchronises once).  Multi-field outputs are one
+ * contiguous buffer: field f of an M x N result starts at out + f*M*N. */
+int cad_td_inf_dev(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+                   const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds,
+                   const double* Dn, double nu, int disp_flag, int strain_flag, int hs_flag, double* strain_out,
+                   double* disp_out);
+int cad_td_sum_eval_dev(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M,
+                        const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                        const double* Dds, const double* Dn, double nu, int disp_flag, int strain_flag,
+                        int hs_flag, double* strain_out, double* disp_out);
+/* Assemble A = -[Atn;Atss;Atds] (3N x 3N, leading dimension lda >= 3N). */
+int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                     const double* P2, const double* P3, int64_t N, double nu, double G, double lambda, int hs_flag,
+                     double* A, int64_t lda);
+/* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
+ * (n x nrhs, ldb) by the solution. */
+int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAD_TD_H */

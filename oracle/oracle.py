@@ -40,6 +40,7 @@ def lib():
         i64, c_int, dbl = ctypes.c_int64, ctypes.c_int, ctypes.c_double
         L.cado_td_inf.argtypes = [d, d, d, i64, d, d, d, i64, d, d, d, dbl, dbl, c_int, c_int, c_int, c_int, d, d]
         L.cado_td_sum_eval.argtypes = L.cado_td_inf.argtypes
+        L.cado_td_inf_ld.argtypes = [d, d, d, i64, d, d, d, i64, d, d, d, dbl, c_int, c_int, c_int, c_int, d, d]
         L.cado_strain_to_traction.argtypes = [d, i64, i64, d, dbl, dbl, c_int, d]
         L.cado_influence_traction.argtypes = [d, d, d, d, d, i64, dbl, dbl, dbl, c_int, c_int, d, d]
         L.cado_normal_shear_tractions.argtypes = [d, d, d, d, d, d, d, i64, d, d, d]
@@ -96,6 +97,20 @@ def td_inf(X, Y, Z, P1, P2, P3, Dss, Dds, Dn, nu, G, disp, strain, hs, nthreads=
     rc = lib().cado_td_inf(_p(X), _p(Y), _p(Z), M, _p(P1), _p(P2), _p(P3), N, _p(_vec(Dss)), _p(_vec(Dds)),
                            _p(_vec(Dn)), float(nu), float(G), int(disp), int(strain), int(hs),
                            nthreads or nthreads_default(), _p(S), _p(D))
+    _check(rc)
+    return (S.transpose(0, 2, 1) if S is not None else None, D.transpose(0, 2, 1) if D is not None else None)
+
+
+def td_inf_ld(X, Y, Z, P1, P2, P3, Dss, Dds, Dn, nu, disp, strain, hs, nthreads=None):
+    """td_inf evaluated in long double (accuracy referee), rounded to double."""
+    X, Y, Z = _vec(X), _vec(Y), _vec(Z)
+    P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+    M, N = X.size, P1.shape[0]
+    S = np.empty((18, N, M)) if strain == 1 else None
+    D = np.empty((9, N, M)) if disp == 1 else None
+    rc = lib().cado_td_inf_ld(_p(X), _p(Y), _p(Z), M, _p(P1), _p(P2), _p(P3), N, _p(_vec(Dss)), _p(_vec(Dds)),
+                              _p(_vec(Dn)), float(nu), int(disp), int(strain), int(hs),
+                              nthreads or nthreads_default(), _p(S), _p(D))
     _check(rc)
     return (S.transpose(0, 2, 1) if S is not None else None, D.transpose(0, 2, 1) if D is not None else None)
 

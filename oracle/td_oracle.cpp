@@ -136,6 +136,12 @@ void strain_to_traction(const double e[6], double lambda, double G, const double
 
 }  // namespace
 
+namespace cad_oracle {
+inline long double sq(long double x) { return x * x; }
+inline long double cube(long double x) { return x * x * x; }
+inline long double ipow(long double x, int n) { return std::pow(x, (long double)n); }
+}  // namespace cad_oracle
+
 extern "C" {
 
 // TD influence-matrix overload.  strain_out: 18 fields x (M x N), StrainInf
@@ -166,6 +172,44 @@ int cado_td_inf(const double* X, const double* Y, const double* Z, int64_t M, co
                 pair_disp(t, X[i], Y[i], Z[i], Dss[j], Dds[j], Dn[j], nu, hs == 1, U);
                 for (int m = 0; m < 3; ++m)
                     for (int cc = 0; cc < 3; ++cc) disp_out[(3 * m + cc) * MN + i + M * j] = U[m][cc];
+            }
+        }
+    });
+    return OK;
+}
+
+// The same influence-matrix computation carried out in long double (x87
+// extended precision): an accuracy referee that tells how far any FP64
+// evaluation of the closed form (this oracle's or the GPU's) is from the
+// mathematically exact value on a given geometry.  Results rounded to double.
+int cado_td_inf_ld(const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+                   const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds,
+                   const double* Dn, double nu, int disp, int strain, int hs, int nthreads, double* strain_out,
+                   double* disp_out)
+{
+    if (hs == 1 && hs_violation(Z, M, P1, P2, P3, N)) return ERR_HS_ABOVE;
+    const int64_t MN = M * N;
+    parallel_for(N, nthreads, 1, [&](int64_t j) {
+        long double a[3], b[3], c[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = P1[j + N * k];
+            b[k] = P2[j + N * k];
+            c[k] = P3[j + N * k];
+        }
+        TriangleState<long double> t;
+        build_triangle(a, b, c, t);
+        for (int64_t i = 0; i < M; ++i) {
+            if (strain == 1) {
+                long double E[3][6];
+                pair_strain<long double>(t, X[i], Y[i], Z[i], Dss[j], Dds[j], Dn[j], nu, hs == 1, E);
+                for (int m = 0; m < 3; ++m)
+                    for (int k = 0; k < 6; ++k) strain_out[(6 * m + k) * MN + i + M * j] = (double)E[m][k];
+            }
+            if (disp == 1) {
+                long double U[3][3];
+                pair_disp<long double>(t, X[i], Y[i], Z[i], Dss[j], Dds[j], Dn[j], nu, hs == 1, U);
+                for (int m = 0; m < 3; ++m)
+                    for (int cc = 0; cc < 3; ++cc) disp_out[(3 * m + cc) * MN + i + M * j] = (double)U[m][cc];
             }
         }
     });
