@@ -22,13 +22,14 @@ CAD_ERR_TIMEOUT = 6
 CAD_ERR_NOT_CONVERGED = 7
 CAD_ERR_SINGULAR = 8
 CAD_ERR_ARG = 9
+CAD_ERR_TOO_LARGE = 10
 
 # Every symbol include/cad_td.h declares (checked by the tests).
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
     "cad_version", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
     "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
-    "cad_solve_dev",
+    "cad_solve_dev", "cad_td_sum_eval_noalloc",
 ]
 
 
@@ -81,6 +82,7 @@ def load():
     L.cad_td_sum_eval_dev.argtypes = tdd
     L.cad_assemble_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, P, I64]
     L.cad_solve_dev.argtypes = [P, I64, P, I64, P, I64, I64]
+    L.cad_td_sum_eval_noalloc.argtypes = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
     _lib = L
     return L
 

@@ -8,7 +8,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcad_td.so")
-SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu"]
+SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu", "noalloc.cu"]
 HEADERS = ["td_device.cuh", "tde_closed_form.cuh", "td_kernels.h", os.path.join("..", "..", "include", "cad_td.h")]
 
 NVCC_FLAGS = [

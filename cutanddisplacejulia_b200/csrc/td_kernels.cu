@@ -201,6 +201,21 @@ __global__ void sum_chunks_kernel(const double* __restrict__ partial, int64_t nc
     out[f * M + i] = s;
 }
 
+// As sum_chunks_kernel, with strain fields (0-5) and displacement fields
+// (6-8) written to two separate outputs (6 x M and 3 x M).
+__global__ void sum_chunks_split_kernel(const double* __restrict__ partial, int64_t nchunk, int64_t M,
+                                        int fields_mask, double* __restrict__ strain_out,
+                                        double* __restrict__ disp_out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (i >= M || !((fields_mask >> f) & 1)) return;
+    double s = 0.0;
+    for (int64_t c = 0; c < nchunk; ++c) s += partial[(c * 9 + f) * M + i];
+    if (f < 6) strain_out[f * M + i] = s;
+    else disp_out[(f - 6) * M + i] = s;
+}
+
 // TD_sum (src/TD_sum.jl:1-41): sum the three modes, then across the N columns.
 // in: nf*3 matrices M x N (field f of mode m at in + (m*nf + f)*M*N), out: nf x M.
 __global__ void td_sum_kernel(const double* __restrict__ in, int64_t M, int64_t N, int nf, double* __restrict__ out)
@@ -299,6 +314,16 @@ cudaError_t launch_sum_chunks(const double* partial, int64_t nchunk, int64_t M, 
     const int bs = 256;
     dim3 grid((unsigned)((M + bs - 1) / bs), 9);
     sum_chunks_kernel<<<grid, bs, 0, st>>>(partial, nchunk, M, fields_mask, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_chunks_split(const double* partial, int64_t nchunk, int64_t M, int fields_mask,
+                                    double* strain_out, double* disp_out, cudaStream_t st)
+{
+    if (M == 0) return cudaSuccess;
+    const int bs = 256;
+    dim3 grid((unsigned)((M + bs - 1) / bs), 9);
+    sum_chunks_split_kernel<<<grid, bs, 0, st>>>(partial, nchunk, M, fields_mask, strain_out, disp_out);
     return cudaGetLastError();
 }
 

@@ -42,6 +42,8 @@ cudaError_t launch_colloc(const double* normals, const double* mid, int64_t N, d
                           double* dirs, cudaStream_t st);
 cudaError_t launch_sum_chunks(const double* partial, int64_t nchunk, int64_t M, int fields_mask, double* out,
                               cudaStream_t st);
+cudaError_t launch_sum_chunks_split(const double* partial, int64_t nchunk, int64_t M, int fields_mask,
+                                    double* strain_out, double* disp_out, cudaStream_t st);
 cudaError_t launch_td_sum(const double* in, int64_t M, int64_t N, int nf, double* out, cudaStream_t st);
 
 }  // namespace cad

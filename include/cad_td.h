@@ -46,6 +46,7 @@ extern "C" {
 #define CAD_ERR_NOT_CONVERGED 7
 #define CAD_ERR_SINGULAR 8
 #define CAD_ERR_ARG 9
+#define CAD_ERR_TOO_LARGE 10
 
 typedef struct cad_ctx cad_ctx;
 
@@ -140,6 +141,29 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
 /* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
  * (n x nrhs, ldb) by the solution. */
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
+
+/* -------------------------------------------------- no-allocation variant ---
+ * Summing-overload evaluation that allocates no device memory, for callers
+ * that cannot allow a library to call cudaMalloc: hosts whose device memory is
+ * owned by their own pool and budget (a hidden allocation can fail under
+ * memory pressure or break the pool's accounting), and services that fix each
+ * tenant's device memory at start-up.  No counterpart in the reference.
+ *
+ * Same arguments and results as cad_td_sum_eval_dev (device pointers: X, Y, Z
+ * of length M; P1, P2, P3 N x 3; slips of length N; strain_out 6 x M;
+ * disp_out 3 x M), but no context: it runs on `stream` (NULL is CUDA's
+ * default stream) and returns only a status code.  Its intermediates live in
+ * one fixed device array of about 25 MiB that every GPU loading the library
+ * reserves until the process exits; limits are N <= 1024 triangles and
+ * M <= 16384 points (CAD_ERR_TOO_LARGE beyond).  Calls share that array, so
+ * calls that overlap on the GPU race; order them on one stream.  The first
+ * call on a device looks up the array's address with that device current:
+ * make it before any stream capture.  The half-space check synchronises the
+ * stream once, as in the other entry points. */
+int cad_td_sum_eval_noalloc(void* stream, const double* X, const double* Y, const double* Z, int64_t M,
+                            const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
+                            const double* Dds, const double* Dn, double nu, int disp_flag, int strain_flag,
+                            int hs_flag, double* strain_out, double* disp_out);
 
 #ifdef __cplusplus
 }
