@@ -37,20 +37,40 @@ if ROOT not in sys.path:
 # oracle's counting scalar on this mesh's collocation pairs) plus the strain ->
 # traction epilogue (288 = 3 modes x 96).  Frozen values, see DESIGN.md.
 FALG_ASSEMBLY_FS = 2960.0 + 288.0
+# Half-space strain of all three unit modes (43867 on the dipping-crack
+# collocation pairs) plus the same traction epilogue.
+FALG_ASSEMBLY_HS = 43867.0 + 288.0
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
 
-METRIC = "TD pair-evals/s (FS penny crack: influence assembly + FP64 LU solve)"
 UNIT = "pair-evals/s"
+WORKLOADS = {
+    "penny": ("TD pair-evals/s (FS penny crack: influence assembly + FP64 LU solve)",
+              "penny crack, full space, %d triangles, 3N=%d unknowns, FP64 assembly + LU"),
+    "dipping": ("TD pair-evals/s (HS dipping crack: influence assembly + FP64 LU solve)",
+                "2x1 crack dipping 60 deg, top at depth 2, half space, %d triangles, 3N=%d unknowns, "
+                "FP64 assembly + LU"),
+}
+METRIC = WORKLOADS["penny"][0]
 
 
-def workload():
-    from cutanddisplacejulia_b200 import geometry, workloads
-    P1, P2, P3 = workloads.penny(seed=0, spacing=SPACING)
-    nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+def workload(kind="penny", ntri=10000):
+    """Geometry, Lame lambda, half-space flag and the traction vector (Tn, Tss, Tds)."""
+    import numpy as np
+
+    from cutanddisplacejulia_b200 import assembly, geometry, workloads
     _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
-    return P1, P2, P3, nrm, mid, lam
+    if kind == "penny":
+        P1, P2, P3 = workloads.penny(seed=0, spacing=SPACING)
+        nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+        n = len(P1)
+        return P1, P2, P3, nrm, mid, lam, 0, (np.full(n, TRACTION), np.zeros(n), np.zeros(n))
+    P1, P2, P3 = workloads.dipping_rect(seed=0, ntri=ntri)
+    nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    s = workloads.remote_stress(seed=0)
+    Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*s, nrm)
+    return P1, P2, P3, nrm, mid, lam, 1, (Tn, Tss, Tds)
 
 
 class ClockSampler:
@@ -99,17 +119,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads):
+def cpu_reference_step(wl, nthreads):
     """One step on the CPU: the oracle (restatement of the reference, all
     threads) assembles A, LAPACK (numpy, all threads) solves it."""
     import numpy as np
     from oracle import oracle as O
-    n = len(P1)
+    P1, P2, P3, nrm, mid, lam, hs, T = wl
     t0 = time.perf_counter()
-    A = O.influence_traction(nrm, mid, P1, P2, P3, NU, G, lam, 0, nthreads=nthreads, want_A=True)
+    A = O.influence_traction(nrm, mid, P1, P2, P3, NU, G, lam, hs, nthreads=nthreads, want_A=True)
     t1 = time.perf_counter()
-    b = np.concatenate([np.full(n, TRACTION), np.zeros(2 * n)])
-    np.linalg.solve(A, b)
+    np.linalg.solve(A, np.concatenate(T))
     t2 = time.perf_counter()
     return t1 - t0, t2 - t1
 
@@ -120,25 +139,23 @@ def run_reference(args, rank):
     import numpy as np  # noqa: F401
     from oracle import oracle as O
     O.build()
-    P1, P2, P3, nrm, mid, lam = workload()
-    n = len(P1)
+    wl = workload(args.workload, args.ntri)
+    n = len(wl[0])
     nthreads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads)
+        cpu_reference_step(wl, nthreads)
     ta, ts = 0.0, 0.0
     for _ in range(args.steps):
-        a, s = cpu_reference_step(P1, P2, P3, nrm, mid, lam, nthreads)
+        a, s = cpu_reference_step(wl, nthreads)
         ta += a
         ts += s
     step_s = (ta + ts) / args.steps
     value = n * n / step_s
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": WORKLOADS[args.workload][0], "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "penny crack, full space, %d triangles, 3N=%d unknowns, spacing %.2f" % (n, 3 * n,
-                                                                                                     SPACING),
-                   "inputs": "host memory"},
+        "config": {"workload": WORKLOADS[args.workload][1] % (n, 3 * n), "inputs": "host memory"},
         "breakdown_ms": {"assembly": ta / args.steps * 1e3, "solve": ts / args.steps * 1e3},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                          "sample": "full workload per step: oracle assembly (%d threads) + numpy LAPACK gesv" % nthreads},
@@ -157,7 +174,8 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    P1, P2, P3, nrm, mid, lam = workload()
+    wl = workload(args.workload, args.ntri)
+    P1, P2, P3, nrm, mid, lam, hs, T = wl
     n = len(P1)
     n3 = 3 * n
 
@@ -165,8 +183,7 @@ def run_ours(args, rank, world, local_rank):
         return torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device=dev)
 
     dP1, dP2, dP3, dN, dM = col(P1), col(P2), col(P3), col(nrm), col(mid)
-    b0 = torch.zeros(n3, dtype=torch.float64, device=dev)
-    b0[:n] = TRACTION
+    b0 = torch.tensor(np.concatenate(T), dtype=torch.float64, device=dev)
     A = torch.empty(n3 * n3, dtype=torch.float64, device=dev)
     x = torch.empty(n3, dtype=torch.float64, device=dev)
     L = _lib.load()
@@ -183,7 +200,7 @@ def run_ours(args, rank, world, local_rank):
         if evs:
             evs[0].record(stream)
         _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
-                                      dP3.data_ptr(), n, NU, G, lam, 0, A.data_ptr(), n3), ctx)
+                                      dP3.data_ptr(), n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
         if evs:
             evs[1].record(stream)
         x.copy_(b0)
@@ -224,7 +241,7 @@ def run_ours(args, rank, world, local_rank):
 
     # solution quality: relative residual of the last solve against a fresh A
     _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(),
-                                  n, NU, G, lam, 0, A.data_ptr(), n3), ctx)
+                                  n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
     Am = A.view(n3, n3).t()      # column-major storage
     resid = float(torch.linalg.vector_norm(Am @ x - b0) / torch.linalg.vector_norm(b0))
 
@@ -234,14 +251,13 @@ def run_ours(args, rank, world, local_rank):
         return t
     hP1, hP2, hP3 = (pinned(np.asfortranarray(p).ravel(order="F")) for p in (P1, P2, P3))
     hN, hM = pinned(np.asfortranarray(nrm).ravel(order="F")), pinned(np.asfortranarray(mid).ravel(order="F"))
-    hTn = pinned(np.full(n, TRACTION))
-    hZ = pinned(np.zeros(n))
+    hTn, hTss, hTds = (pinned(t) for t in T)
     hDn, hDss, hDds = (torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(3))
 
     def e2e_call():
         _lib.check(L.cad_slip_calculator(ctx, hP1.data_ptr(), hP2.data_ptr(), hP3.data_ptr(), n, NU, G, lam,
-                                         hM.data_ptr(), hN.data_ptr(), 0, hTn.data_ptr(), hZ.data_ptr(),
-                                         hZ.data_ptr(), hDn.data_ptr(), hDss.data_ptr(), hDds.data_ptr(), None,
+                                         hM.data_ptr(), hN.data_ptr(), hs, hTn.data_ptr(), hTss.data_ptr(),
+                                         hTds.data_ptr(), hDn.data_ptr(), hDss.data_ptr(), hDds.data_ptr(), None,
                                          None), ctx)
 
     for _ in range(max(1, args.warmup)):
@@ -265,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
         from oracle import oracle as O
         O.build()
         nth = os.cpu_count() or 1
-        a_s, s_s = cpu_reference_step(P1, P2, P3, nrm, mid, lam, nth)
+        a_s, s_s = cpu_reference_step(wl, nth)
         cpu = {"value": n * n / (a_s + s_s), "unit": UNIT, "cores": nth, "kind": "port",
                "sample": "one full step (oracle assembly + numpy LAPACK gesv) on %d host threads: "
                          "assembly %.3f s, solve %.3f s" % (nth, a_s, s_s)}
@@ -273,14 +289,15 @@ def run_ours(args, rank, world, local_rank):
     pairs = float(n) * n
     # assembly time per step over the timed region (pair kernel + the two small
     # per-element prep kernels, all on this stream): the launch duration used
-    achieved = FALG_ASSEMBLY_FS * pairs / (asm_ms * 1e-3) / 1e12
+    falg = FALG_ASSEMBLY_HS if hs else FALG_ASSEMBLY_FS
+    achieved = falg * pairs / (asm_ms * 1e-3) / 1e12
     lu_flops = (2.0 / 3.0) * n3 ** 3 + 2.0 * n3 * n3
     solve_tflops = lu_flops / (sol_ms * 1e-3) / 1e12
     line = {
-        "metric": METRIC, "value": world * pairs / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world,
+        "metric": WORKLOADS[args.workload][0], "value": world * pairs / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "penny crack, full space, %d triangles, 3N=%d unknowns, FP64 assembly + LU" % (n, n3),
+        "config": {"workload": WORKLOADS[args.workload][1] % (n, n3),
                    "pairs_per_step": pairs, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (A is %.0f MB per step)" % (n3 * n3 * 8 / 1e6)},
         "breakdown_ms": {"assembly": asm_ms, "td_pair_kernel_last": pair_kernel_ms, "solve": sol_ms},
@@ -290,11 +307,11 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "api": "cad_slip_calculator (host C ABI, pinned host buffers)"},
         "gpu_launches": 3 * args.steps,
-        "roofline": {"kernel": "td_pair_kernel<FS, strain, A-matrix>", "bound": "fp64",
+        "roofline": {"kernel": "td_pair_kernel<%s, strain, A-matrix>" % ("HS" if hs else "FS"), "bound": "fp64",
                      "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak_tflops,
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
-                     "falg_per_pair": FALG_ASSEMBLY_FS, "traffic": None,
+                     "falg_per_pair": falg, "traffic": None,
                      "step_share": asm_ms / ms_step},
         "roofline_solve": {"kernel": "dense LU (cusolverDnDgetrf + getrs)", "bound": "fp64",
                            "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
@@ -312,6 +329,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="penny",
+                    help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
+    ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

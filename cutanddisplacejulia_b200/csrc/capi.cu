@@ -1,18 +1,19 @@
 // C ABI of libcad_td.so (declared in include/cad_td.h).
 //
-// Each context owns a CUDA stream, a cuSOLVER handle for the dense LU, and a
-// set of device workspaces that grow on demand and are reused across calls
+// Each context owns a CUDA stream, a cuBLAS handle (GEMMs of the dense LU in
+// csrc/lu.cu), and a set of device workspaces that grow on demand and are reused across calls
 // (no allocation in steady state).  Host-pointer entry points copy inputs in,
 // run the device path and copy results out; *_dev entry points run the device
 // path directly on caller-provided device memory.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 
 #include <cstdio>
 #include <cstring>
 #include <string>
 
 #include "../../include/cad_td.h"
+#include "lu.h"
 #include "td_device.cuh"
 #include "td_kernels.h"
 
@@ -24,7 +25,9 @@ size_t tri_record_bytes() { return sizeof(TriDev); }
 
 namespace {
 
-enum Slot { S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_COUNT };
+enum Slot { S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM, S_COUNT };
+
+constexpr int kLuBlock = 256;   // outer block width of the LU
 
 struct DevBuf {
     void* p = nullptr;
@@ -37,7 +40,9 @@ struct cad_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    cusolverDnHandle_t solver = nullptr;
+    cublasHandle_t blas = nullptr;
+    cudaStream_t side_stream = nullptr;   // the LU's look-ahead trailing updates
+    cublasHandle_t side_blas = nullptr;
     DevBuf buf[S_COUNT];
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed[2] = {false, false};
@@ -187,22 +192,33 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (n == 0 || nrhs == 0) return CAD_OK;
     if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
         return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
-    int lwork = 0;
-    if (cusolverDnDgetrf_bufferSize(ctx->solver, (int)n, (int)n, A, (int)lda, &lwork) != CUSOLVER_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrf_bufferSize failed");
-    void *work, *piv, *info;
-    if (int r = ensure(ctx, S_WORK, (size_t)lwork * sizeof(double), &work)) return r;
+    void *work, *piv, *info, *perm;
+    if (int r = ensure(ctx, S_WORK, (size_t)n * nrhs * sizeof(double), &work)) return r;
     if (int r = ensure(ctx, S_PIV, (size_t)n * sizeof(int), &piv)) return r;
+    if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    if (cusolverDnDgetrf(ctx->solver, (int)n, (int)n, A, (int)lda, (double*)work, (int*)piv, (int*)info) !=
-        CUSOLVER_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrf failed");
-    if (cusolverDnDgetrs(ctx->solver, CUBLAS_OP_N, (int)n, (int)nrhs, A, (int)lda, (int*)piv, B, (int)ldb,
-                         (int*)info) != CUSOLVER_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "cusolverDnDgetrs failed");
+    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas};
+    const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
+                                           (int*)info, kLuBlock, true, true);
+    if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
+    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
+    CK(cudaMemcpy2DAsync(B, ldb * sizeof(double), work, n * sizeof(double), n * sizeof(double), nrhs,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     ctx->timed[1] = true;
+    return CAD_OK;
+}
+
+// info of the last factorisation: 0 when every pivot was non-zero
+int read_info(cad_ctx* ctx, int* info)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // negative: a leaf of the factorisation gave up waiting on a pivot exchange
+    if (h < 0) return fail(ctx, CAD_ERR_TIMEOUT, "LU factorisation: a pivot exchange wait ran out");
+    *info = (h == INT32_MAX) ? 0 : h;
     return CAD_OK;
 }
 
@@ -247,8 +263,11 @@ int cad_init(int device, cad_ctx** out)
             cad_destroy(ctx);
             return CAD_ERR_CUDA;
         }
-    if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS) {
+    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
+        cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cublasCreate(&ctx->side_blas) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetStream(ctx->side_blas, ctx->side_stream) != CUBLAS_STATUS_SUCCESS) {
         cad_destroy(ctx);
         return CAD_ERR_CUDA;
     }
@@ -265,7 +284,10 @@ int cad_destroy(cad_ctx* ctx)
         if (b.p) cudaFree(b.p);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
-    if (ctx->solver) cusolverDnDestroy(ctx->solver);
+    if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
+    if (ctx->blas) cublasDestroy(ctx->blas);
+    if (ctx->side_blas) cublasDestroy(ctx->side_blas);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return CAD_OK;
@@ -277,8 +299,8 @@ int cad_set_stream(cad_ctx* ctx, void* stream)
 {
     if (int r = set_device(ctx)) return r;
     ctx->stream = (cudaStream_t)stream;   // NULL is CUDA's default stream, as everywhere in CUDA
-    if (cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "cusolverDnSetStream failed");
+    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "cublasSetStream failed");
     return CAD_OK;
 }
 
@@ -445,7 +467,8 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
     if (b_out) CK(cudaMemcpyAsync(b_out, bd, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if ((r = solve_device(ctx, n3, (double*)A, n3, bd, n3, 1))) return r;
     int info = 0;
-    CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (n3 > 0)
+        if ((r = read_info(ctx, &info))) return r;
     CK(cudaMemcpyAsync(Dn, bd, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(Dss, bd + N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(Dds, bd + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -465,8 +488,8 @@ int cad_solve(cad_ctx* ctx, int64_t n, const double* A, const double* B, int64_t
     if (int r = upload(ctx, (double*)Bd, B, n * nrhs)) return r;
     if (int r = solve_device(ctx, n, (double*)Ad, n, (double*)Bd, n, nrhs)) return r;
     int info = 0;
-    if (n > 0) {
-        CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (n > 0 && nrhs > 0) {
+        if (int r = read_info(ctx, &info)) return r;
         CK(cudaMemcpyAsync(X, Bd, (size_t)n * nrhs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(cudaStreamSynchronize(ctx->stream));
@@ -523,10 +546,8 @@ int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, in
     if (n < 0 || nrhs < 0 || lda < n || ldb < n) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     if (int r = solve_device(ctx, n, A, lda, B, ldb, nrhs)) return r;
     int info = 0;
-    if (n > 0) {
-        CK(cudaMemcpyAsync(&info, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-    }
+    if (n > 0 && nrhs > 0)
+        if (int r = read_info(ctx, &info)) return r;
     if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
     return CAD_OK;
 }

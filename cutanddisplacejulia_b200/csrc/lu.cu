@@ -1,0 +1,749 @@
+// Dense LU with partial pivoting and triangular solves (the `A\b` of
+// SlipCalculator3D, src/SlipCalculator3D.jl:22) for sm_100a.
+//
+// Right-looking blocked LU (outer block nb).  Each nb-wide panel is factorised
+// recursively: the left half, then a row swap, a triangular solve and a GEMM
+// update of the right half, then the right half.  The recursion stops at
+// narrow leaves that one thread-block cluster factorises with its rows held in
+// distributed shared memory: per column, every CTA proposes its largest
+// |entry|, the cluster agrees on the pivot through DSMEM, the pivot row and the
+// displaced row are exchanged through DSMEM, and every CTA updates its own rows
+// -- two hardware cluster barriers per column, no global-memory spin.  Rank-nb
+// trailing updates and the intra-panel updates are plain cuBLAS GEMMs (DGEMM,
+// or SGEMM on TF32 tensor cores for the single-precision factorisation).
+//
+// Pivot choice is LAPACK's: the first row of largest magnitude; scaling by the
+// reciprocal pivot; ipiv[k] = absolute row swapped with row k.
+#include <cooperative_groups.h>
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <vector>
+
+#include "lu.h"
+
+namespace cg = cooperative_groups;
+
+namespace cad {
+
+namespace {
+
+constexpr int kLeafThreads = 512;
+constexpr int kLeafWarps = kLeafThreads / 32;
+constexpr int kMaxCluster = 16;
+constexpr int kLeafRegs = 32;   // row values one leaf thread keeps in registers (RPT * W)
+constexpr int kMaxSwaps = 256;  // pivots one row-swap launch applies (outer block width bound)
+
+// A pivot candidate as integers: |value| orders like the bit pattern of the
+// non-negative double, so hi = 1 + its high word (0: no candidate), lo = its
+// low word; ties go to the smaller position (LAPACK's first largest entry).
+struct __align__(16) Key {
+    unsigned hi, lo, pos, who;
+};
+__device__ __forceinline__ bool key_better(const Key& a, const Key& b)
+{
+    return a.hi > b.hi || (a.hi == b.hi && (a.lo > b.lo || (a.lo == b.lo && a.pos < b.pos)));
+}
+__device__ __forceinline__ Key key_of(double v, int pos, unsigned who)
+{
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(fabs(v));
+    return Key{(unsigned)(bits >> 32) + 1u, (unsigned)bits, (unsigned)pos, who};
+}
+// the warp's best key in every lane: three integer warp reductions instead of
+// a shuffle tree of double compares
+__device__ __forceinline__ Key warp_key_max(const Key& k)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned mhi = __reduce_max_sync(full, k.hi);
+    const unsigned mlo = __reduce_max_sync(full, k.hi == mhi ? k.lo : 0u);
+    const bool tie = k.hi == mhi && k.lo == mlo;
+    const unsigned mpos = __reduce_min_sync(full, tie ? k.pos : 0xffffffffu);
+    const unsigned win = __ballot_sync(full, tie && k.pos == mpos);
+    return Key{mhi, mlo, mpos, __shfl_sync(full, k.who, __ffs(win) - 1)};
+}
+
+// ------------------------------------------------------------ leaf (cluster)
+// DSMEM pushes: st.async stores into another CTA's shared memory that count
+// their bytes on that CTA's mbarrier, so a receiver waits on its own barrier
+// for exactly the bytes it expects -- no cluster-wide barrier (whose
+// release/acquire fence costs about a microsecond) per column.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned cluster_map(unsigned addr, unsigned rank)
+{
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_async_b64(unsigned addr, unsigned long long v, unsigned mbar)
+{
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(addr), "l"(v), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void st_async_b32(unsigned addr, unsigned v, unsigned mbar)
+{
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(addr), "r"(v), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void st_async_word(unsigned addr, double v, unsigned mbar)
+{
+    st_async_b64(addr, (unsigned long long)__double_as_longlong(v), mbar);
+}
+__device__ __forceinline__ void st_async_word(unsigned addr, float v, unsigned mbar)
+{
+    st_async_b32(addr, __float_as_uint(v), mbar);
+}
+__device__ __forceinline__ void st_async_v4(unsigned addr, unsigned a, unsigned b, unsigned c, unsigned d, unsigned mbar)
+{
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(addr),
+                 "r"(a), "r"(b), "r"(c), "r"(d), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned mbar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(unsigned mbar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned mbar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+
+// try_wait rounds before a leaf gives up on a push and reports failure
+constexpr long kWaitLimit = 1L << 20;
+
+// Factorises the m x w panel at A (leading dimension lda, w <= W) in place.
+// CTA q of the cluster owns panel rows [q*R, (q+1)*R), R = 512 * RPT; thread t
+// keeps rows t + 512*k (k < RPT) in registers for the whole leaf and never
+// moves them -- each row carries its current logical position.  Per column j:
+// every warp reduces its candidates, every warp then reduces the 16 warp
+// results, and one warp pushes the CTA's best row, the reciprocal of its pivot
+// entry and its key into slot [j & 1][q] of every CTA of the cluster; each CTA
+// waits on its own barrier for the C payloads, picks the pivot and updates its
+// rows from the pivot row in shared memory.  Two slots suffice: a CTA pushes
+// column j + 2 only after every CTA's column j + 1 payload reached it, and a
+// CTA sends that payload only once all its threads are done with column j.
+// Rows are stored to their final positions at the end.  piv[c] = piv_base +
+// position swapped with c (LAPACK order); info: smallest zero-pivot column
+// (1-based, + col_base), or -1 if a wait ran out.
+template <typename T, int W, int RPT>
+__global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict__ A, int64_t lda, int m, int w,
+                                                                int* __restrict__ piv, int piv_base,
+                                                                int* __restrict__ info, int col_base)
+{
+    static_assert(W * RPT <= kLeafRegs && W <= 32, "leaf tile exceeds its register budget");
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int C = (int)cluster.num_blocks();
+    __shared__ __align__(16) T s_row[2][kMaxCluster][W];
+    __shared__ __align__(16) T s_rinv[2][kMaxCluster];
+    __shared__ __align__(16) Key s_ckey[2][kMaxCluster];
+    __shared__ __align__(8) unsigned long long s_bar[2];
+    __shared__ Key s_wkey[2][kLeafWarps];   // by column parity: a fast warp may write column j + 1's
+                                            // while a slow one still reads column j's
+    __shared__ int s_hist[W];
+    __shared__ int s_fail;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // bytes one column delivers to each CTA: C rows, reciprocals and keys
+    const unsigned col_bytes = (unsigned)C * (unsigned)(W * sizeof(T) + sizeof(T) + sizeof(Key));
+    if (tid == 0) {
+        s_fail = 0;
+        mbar_init(smem_u32(&s_bar[0]), 1);
+        mbar_init(smem_u32(&s_bar[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_arrive_expect(smem_u32(&s_bar[0]), col_bytes);
+        if (w > 1) mbar_arrive_expect(smem_u32(&s_bar[1]), col_bytes);
+    }
+    T x[RPT][W];
+    int pos[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int row = crank * (kLeafThreads * RPT) + k * kLeafThreads + tid;
+        pos[k] = row < m ? row : INT_MAX;
+#pragma unroll
+        for (int c = 0; c < W; ++c)
+            x[k][c] = (row < m && c < w) ? A[(int64_t)row + (int64_t)c * lda] : (T)0;
+    }
+    cluster.sync();   // barriers initialised and every CTA running before the first push
+
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+        if (j >= w) break;
+        const int par = j & 1;
+        Key key{0u, 0u, 0xffffffffu, 0u};
+        T piv_val = (T)0;
+#pragma unroll
+        for (int k = 0; k < RPT; ++k)
+            if (pos[k] != INT_MAX && pos[k] >= j) {
+                const Key kk = key_of((double)x[k][j], pos[k], (unsigned)((k << 10) | tid));
+                if (key_better(kk, key)) {
+                    key = kk;
+                    piv_val = x[k][j];
+                }
+            }
+        const T inv_c = piv_val != (T)0 ? (T)1 / piv_val : (T)0;
+        const Key wk = warp_key_max(key);
+        if (lane == 0) s_wkey[par][warp] = wk;
+        __syncthreads();
+        const Key b = warp_key_max(lane < kLeafWarps ? s_wkey[par][lane] : Key{0u, 0u, 0xffffffffu, 0u});
+        // one warp pushes this CTA's payload for column j to every CTA: the
+        // best row (zeros if none), its reciprocal and its key
+        const int pusher = b.hi != 0u ? (int)((b.who & 1023u) >> 5) : 0;
+        if (warp == pusher) {
+            const int src = (int)(b.who & 31u), kk = (int)(b.who >> 10);
+            T mine = (T)0;
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                T v = x[0][cc];
+#pragma unroll
+                for (int k = 1; k < RPT; ++k)
+                    if (k == kk) v = x[k][cc];
+                v = __shfl_sync(0xffffffffu, v, src);
+                if (lane == cc) mine = v;
+            }
+            T rinv = __shfl_sync(0xffffffffu, inv_c, src);
+            if (b.hi == 0u) mine = rinv = (T)0;
+            const unsigned bar = smem_u32(&s_bar[par]);
+            const unsigned row_addr = smem_u32(&s_row[par][crank][lane]);
+            const unsigned rinv_addr = smem_u32(&s_rinv[par][crank]);
+            const unsigned key_addr = smem_u32(&s_ckey[par][crank]);
+            for (int q = 0; q < C; ++q) {
+                const unsigned rbar = cluster_map(bar, (unsigned)q);
+                if (lane < W)
+                    st_async_word(cluster_map(row_addr, (unsigned)q), mine, rbar);
+            }
+            if (lane < C) {
+                const unsigned rbar = cluster_map(bar, (unsigned)lane);
+                st_async_word(cluster_map(rinv_addr, (unsigned)lane), rinv, rbar);
+                st_async_v4(cluster_map(key_addr, (unsigned)lane), b.hi, b.lo, b.pos, b.who, rbar);
+            }
+        }
+        // wait for the C payloads of column j
+        {
+            const unsigned bar = smem_u32(&s_bar[par]);
+            const unsigned parity = (unsigned)((j >> 1) & 1);
+            long spins = 0;
+            while (!mbar_try_wait(bar, parity))
+                if (++spins > kWaitLimit) {
+                    s_fail = 1;
+                    break;
+                }
+        }
+        __syncwarp();
+        if (tid == 0 && j + 2 < w) mbar_arrive_expect(smem_u32(&s_bar[par]), col_bytes);
+        Key g = lane < C ? s_ckey[par][lane] : Key{0u, 0u, 0xffffffffu, 0u};
+        g.who = (unsigned)lane;
+        g = warp_key_max(g);
+        const bool ok = g.hi > 1u || (g.hi == 1u && g.lo != 0u);
+        const int p = ok ? (int)g.pos : j;
+        if (tid == 0) {
+            s_hist[j] = p;
+            if (!ok && crank == 0) atomicMin(info, col_base + j + 1);
+        }
+        if (ok) {
+            const T* u = s_row[par][g.who];
+            const T inv = s_rinv[par][g.who];
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                int ps = pos[k];
+                if (ps == p) ps = j;
+                else if (ps == j) ps = p;
+                pos[k] = ps;
+                if (ps != INT_MAX && ps > j) {
+                    const T l = x[k][j] * inv;
+                    x[k][j] = l;
+#pragma unroll
+                    for (int cc = j + 1; cc < W; ++cc) x[k][cc] -= l * u[cc];
+                }
+            }
+        }
+    }
+    cluster.sync();   // every push has landed and been read before any CTA exits
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+        if (pos[k] != INT_MAX)
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+                if (c < w) A[(int64_t)pos[k] + (int64_t)c * lda] = x[k][c];
+    __syncthreads();
+    if (crank == 0 && tid < w) piv[tid] = piv_base + s_hist[tid];
+    if (tid == 0 && s_fail) atomicMin(info, -1);
+}
+
+// ------------------------------------------------------------ row swaps
+// Applies the swaps row k <-> row piv[k] - row_base (k = 0..npiv-1, in order,
+// rows relative to the block top) to columns [0, ncol1) of A1 and [0, ncol2)
+// of A2.  Every CTA first derives the net movement: each touched row follows
+// its content through the swap sequence, giving at most 2 * npiv (dst, src)
+// pairs; then one warp per column gathers the sources and stores them.
+template <typename T>
+__global__ void __launch_bounds__(256) laswp_kernel(T* __restrict__ A1, int ncol1, T* __restrict__ A2, int ncol2,
+                                                    int64_t lda, const int* __restrict__ piv, int npiv, int row_base)
+{
+    constexpr int kPer = 2 * kMaxSwaps / 32;
+    __shared__ int s_piv[kMaxSwaps];
+    __shared__ int s_dst[2 * kMaxSwaps], s_src[2 * kMaxSwaps];
+    __shared__ int s_count;
+    for (int k = threadIdx.x; k < npiv; k += blockDim.x) s_piv[k] = piv[k] - row_base;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * npiv; t += blockDim.x) {
+        int row = t;
+        bool track = true;
+        if (t >= npiv) {   // a pivot row below the block's first npiv rows, tracked once
+            const int kk = t - npiv;
+            row = s_piv[kk];
+            track = row >= npiv;
+            for (int k = 0; k < kk && track; ++k) track = s_piv[k] != row;
+        }
+        if (!track) continue;
+        int at = row;
+        for (int k = 0; k < npiv; ++k) {
+            const int q = s_piv[k];
+            at = at == k ? q : (at == q ? k : at);
+        }
+        if (at != row) {
+            const int slot = atomicAdd(&s_count, 1);
+            s_dst[slot] = at;
+            s_src[slot] = row;
+        }
+    }
+    __syncthreads();
+    const int count = s_count;
+    if (count == 0) return;
+    const int lane = threadIdx.x & 31;
+    int dst[kPer], src[kPer];
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+        const int e = lane + 32 * t;
+        dst[t] = e < count ? s_dst[e] : -1;
+        src[t] = e < count ? s_src[e] : 0;
+    }
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int col = wid; col < ncol1 + ncol2; col += nw) {
+        T* a = col < ncol1 ? A1 + (int64_t)col * lda : A2 + (int64_t)(col - ncol1) * lda;
+        T v[kPer];
+#pragma unroll
+        for (int t = 0; t < kPer; ++t) v[t] = dst[t] >= 0 ? a[src[t]] : (T)0;
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kPer; ++t)
+            if (dst[t] >= 0) a[dst[t]] = v[t];
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------- triangular diagonal blocks
+// B (b x ncol, ldb) := L^-1 B with L the b x b unit lower triangle at L (ldl),
+// or U^-1 B with U upper, non-unit; b <= 64.  A CTA of 4 warps takes 32
+// columns (8 per warp); lane l holds rows l and l + 32; the solved row c is
+// broadcast from its lane by shuffles.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(128) trsm_diag_kernel(const T* __restrict__ L, int64_t ldl, int b, T* __restrict__ B,
+                                                        int64_t ldb, int ncol)
+{
+    __shared__ T s_L[64 * 64];
+    __shared__ T s_inv[64];   // UPPER: reciprocal diagonal
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int col0 = blockIdx.x * 32 + warp * 8;
+    {
+        // every load of the block and of the right-hand sides in flight at once
+        T t[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const int e = threadIdx.x + 128 * i, r = e & 63, c = e >> 6;
+            t[i] = (r < b && c < b) ? L[r + (int64_t)c * ldl] : (T)0;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) s_L[threadIdx.x + 128 * i] = t[i];
+    }
+    T x[2][8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h, col = col0 + k;
+            x[h][k] = (r < b && col < ncol) ? B[r + (int64_t)col * ldb] : (T)0;
+        }
+    __syncthreads();
+    if (UPPER && threadIdx.x < 64) s_inv[threadIdx.x] = threadIdx.x < b ? (T)1 / s_L[threadIdx.x * 65] : (T)1;
+    if (UPPER) __syncthreads();
+    // row c = 32 * hc + cc is solved, then broadcast from lane cc; the loop
+    // over cc stays rolled (a fully unrolled 64-step solve overflows the
+    // instruction cache), the register half hc is static
+    if (!UPPER) {
+#pragma unroll
+        for (int hc = 0; hc < 2; ++hc)
+#pragma unroll 2
+            for (int cc = 0; cc < 32; ++cc) {
+                const int c = 32 * hc + cc;
+                if (c >= b) break;
+                const T l0 = s_L[c * 64 + lane], l1 = s_L[c * 64 + 32 + lane];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const T xc = __shfl_sync(0xffffffffu, x[hc][k], cc);
+                    if (hc == 0 && lane > c) x[0][k] -= l0 * xc;
+                    if (32 + lane > c) x[1][k] -= l1 * xc;
+                }
+            }
+    } else {
+#pragma unroll
+        for (int hc = 1; hc >= 0; --hc)
+#pragma unroll 2
+            for (int cc = 31; cc >= 0; --cc) {
+                const int c = 32 * hc + cc;
+                if (c >= b) continue;
+                const T d = s_inv[c], u0 = s_L[c * 64 + lane], u1 = s_L[c * 64 + 32 + lane];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const T xc = __shfl_sync(0xffffffffu, x[hc][k], cc) * d;
+                    if (lane == cc) x[hc][k] = xc;
+                    if (lane < c) x[0][k] -= u0 * xc;
+                    if (hc == 1 && 32 + lane < c) x[1][k] -= u1 * xc;
+                }
+            }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h, col = col0 + k;
+            if (r < b && col < ncol) B[r + (int64_t)col * ldb] = x[h][k];
+        }
+}
+
+// perm[i] = source row of row i after all n pivots (ipiv applied in order),
+// built by one thread in shared memory.
+__global__ void pivots_to_perm_kernel(const int* __restrict__ ipiv, int n, int* __restrict__ perm)
+{
+    extern __shared__ int s_perm[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_perm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < n; ++k) {
+            const int q = ipiv[k];
+            const int t = s_perm[k];
+            s_perm[k] = s_perm[q];
+            s_perm[q] = t;
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = s_perm[i];
+}
+
+// Y[i, c] = X[perm[i], c]
+template <typename T>
+__global__ void permute_rows_kernel(const T* __restrict__ X, int64_t ldx, const int* __restrict__ perm, int n,
+                                    int ncol, T* __restrict__ Y, int64_t ldy)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (i < n && c < ncol) Y[i + (int64_t)c * ldy] = X[perm[i] + (int64_t)c * ldx];
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+// ------------------------------------------------------------ GEMM wrapper
+// C (m x n, ldc) -= A (m x k, lda) * B (k x n, ldb)
+cublasStatus_t gemm_sub(cublasHandle_t h, int m, int n, int k, const double* A, int64_t lda, const double* B,
+                        int64_t ldb, double* C, int64_t ldc)
+{
+    const double one = 1.0, mone = -1.0;
+    return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, (int)lda, B, (int)ldb, &one, C, (int)ldc);
+}
+cublasStatus_t gemm_sub(cublasHandle_t h, int m, int n, int k, const float* A, int64_t lda, const float* B,
+                        int64_t ldb, float* C, int64_t ldc)
+{
+    const float one = 1.0f, mone = -1.0f;
+    return cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, CUDA_R_32F, (int)lda, B, CUDA_R_32F, (int)ldb,
+                        &one, C, CUDA_R_32F, (int)ldc, CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
+}
+
+template <typename T>
+struct Lu {
+    cublasHandle_t h;   // the handle and stream the next launches go to
+    cudaStream_t st;
+    cublasHandle_t main_h, side_h;
+    cudaStream_t main_st, side_st;
+    int* ipiv;    // absolute pivots, device
+    int* info;
+    int cluster;  // largest leaf cluster (16 where the device co-schedules it, else 8)
+    cudaError_t err = cudaSuccess;
+    cublasStatus_t berr = CUBLAS_STATUS_SUCCESS;
+
+    bool ok() const { return err == cudaSuccess && berr == CUBLAS_STATUS_SUCCESS; }
+
+    // rows per leaf thread for an m-row panel: the fewest that fit one cluster
+    int leaf_rpt(int m) const
+    {
+        int rpt = 1;
+        while (rpt < 8 && (int64_t)cluster * kLeafThreads * rpt < m) rpt *= 2;
+        return rpt;
+    }
+    int leaf_width(int m) const { return kLeafRegs / leaf_rpt(m); }
+
+    // swaps rows k <-> piv[k] - row_base (k < npiv, in order) of the column
+    // blocks (A1, ncol1) and (A2, ncol2), both relative to the same block top
+    void laswp(const int* piv, int npiv, int row_base, T* A1, int ncol1, T* A2, int ncol2, int64_t lda)
+    {
+        if (npiv <= 0 || ncol1 + ncol2 <= 0 || !ok()) return;
+        const int ncol = ncol1 + ncol2;
+        const int blocks = (ncol + 7) / 8 < 148 * 2 ? (ncol + 7) / 8 : 148 * 2;
+        laswp_kernel<T><<<blocks, 256, 0, st>>>(A1, ncol1, A2, ncol2, lda, piv, npiv, row_base);
+        err = cudaGetLastError();
+    }
+
+    // B (b x ncol) := L^-1 B, L unit lower b x b (b arbitrary): 64-row blocks + GEMM
+    void trsm_lower(const T* L, int64_t ldl, int b, T* B, int64_t ldb, int ncol)
+    {
+        for (int d = 0; d < b && ok(); d += 64) {
+            const int db = b - d < 64 ? b - d : 64;
+            trsm_diag_kernel<T, false><<<(ncol + 31) / 32, 128, 0, st>>>(L + d + d * ldl, ldl, db, B + d, ldb, ncol);
+            err = cudaGetLastError();
+            if (d + db < b && ok())
+                berr = gemm_sub(h, b - d - db, ncol, db, L + (d + db) + d * ldl, ldl, B + d, ldb, B + d + db, ldb);
+        }
+    }
+
+    template <int W, int RPT>
+    void leaf_launch(T* A, int64_t lda, int m, int w, int* piv, int piv_base, int col_base)
+    {
+        const int C = (m + kLeafThreads * RPT - 1) / (kLeafThreads * RPT);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(kLeafThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        err = cudaLaunchKernelEx(&cfg, leaf_lu_kernel<T, W, RPT>, A, lda, m, w, piv, piv_base, info, col_base);
+    }
+
+    void leaf(T* A, int64_t lda, int m, int w, int* piv, int piv_base, int col_base)
+    {
+        if (!ok()) return;
+        switch (leaf_rpt(m)) {
+            case 1: leaf_launch<32, 1>(A, lda, m, w, piv, piv_base, col_base); break;
+            case 2: leaf_launch<16, 2>(A, lda, m, w, piv, piv_base, col_base); break;
+            case 4: leaf_launch<8, 4>(A, lda, m, w, piv, piv_base, col_base); break;
+            default: leaf_launch<4, 8>(A, lda, m, w, piv, piv_base, col_base); break;
+        }
+    }
+
+    // m x w panel at A; its pivots (relative to the panel top, + piv_base) go to piv[0..w)
+    void panel(T* A, int64_t lda, int m, int w, int* piv, int piv_base, int col_base)
+    {
+        if (!ok()) return;
+        const int lw = leaf_width(m);
+        if (w <= lw) {
+            leaf(A, lda, m, w, piv, piv_base, col_base);
+            return;
+        }
+        int w1 = w / 2;
+        w1 = (w1 + lw - 1) / lw * lw;
+        if (w1 >= w) w1 = w - lw;
+        panel(A, lda, m, w1, piv, piv_base, col_base);
+        laswp(piv, w1, piv_base, A + w1 * lda, w - w1, nullptr, 0, lda);
+        trsm_lower(A, lda, w1, A + w1 * lda, lda, w - w1);
+        if (m > w1 && ok())
+            berr = gemm_sub(h, m - w1, w - w1, w1, A + w1, lda, A + w1 * lda, lda, A + w1 + w1 * lda, lda);
+        panel(A + w1 + w1 * lda, lda, m - w1, w - w1, piv + w1, piv_base + w1, col_base + w1);
+        // the right half's pivots (rows w1.. of the panel) applied to the left half's columns
+        laswp(piv + w1, w - w1, piv_base + w1, A + w1, w1, nullptr, 0, lda);
+    }
+
+    void use(bool side)
+    {
+        st = side ? side_st : main_st;
+        h = side ? side_h : main_h;
+    }
+
+    // Right-looking blocked LU with a look-ahead of one block column.  Block
+    // b's update is split: the main stream swaps, solves and updates block
+    // column b + 1 only, then factorises it as the next panel; the side stream
+    // meanwhile swaps, solves and updates the remaining columns.  The panel is
+    // latency-bound on a few SMs, the trailing GEMM fills the rest.  Events:
+    // panel[b] (block column b factorised; its pivots exist), rest[b] (side
+    // work of block b done -- the main stream waits for it before touching
+    // block column b + 2 or swapping rows of the L columns the side GEMM reads).
+    void factor(T* A, int64_t n, int64_t lda, int nb)
+    {
+        use(false);
+        set_int_kernel<<<1, 1, 0, st>>>(info, INT_MAX);
+        err = cudaGetLastError();
+        const int nblk = (int)((n + nb - 1) / nb);
+        if (nblk == 0 || !ok()) return;
+        std::vector<cudaEvent_t> ev_panel(nblk, nullptr), ev_rest(nblk, nullptr);
+        for (int b = 0; b < nblk && ok(); ++b) {
+            err = cudaEventCreateWithFlags(&ev_panel[b], cudaEventDisableTiming);
+            if (ok()) err = cudaEventCreateWithFlags(&ev_rest[b], cudaEventDisableTiming);
+        }
+        if (ok()) {
+            const int kb0 = (int)(n < nb ? n : nb);
+            panel(A, lda, (int)n, kb0, ipiv, 0, 0);
+            if (ok()) err = cudaEventRecord(ev_panel[0], main_st);
+        }
+        for (int b = 0; b < nblk && ok(); ++b) {
+            const int64_t k = (int64_t)b * nb;
+            const int kb = (int)(n - k < nb ? n - k : nb);
+            const int64_t k1 = k + kb;                                  // next block column
+            const int kb1 = (int)(n - k1 < nb ? n - k1 : nb);
+            const int64_t k2 = k1 + kb1;                                // the rest
+            const int nr2 = (int)(n - k2);
+            T* Akk = A + k + k * lda;
+            // main: swaps left of the panel and in the next block column, its
+            // solve and update, then the next panel
+            use(false);
+            if (b > 0) err = cudaStreamWaitEvent(main_st, ev_rest[b - 1], 0);
+            laswp(ipiv + k, kb, (int)k, A + k, (int)k, A + k + k1 * lda, kb1, lda);
+            if (kb1 > 0) {
+                trsm_lower(Akk, lda, kb, A + k + k1 * lda, lda, kb1);
+                if (ok())
+                    berr = gemm_sub(h, (int)(n - k1), kb1, kb, A + k1 + k * lda, lda, A + k + k1 * lda, lda,
+                                    A + k1 + k1 * lda, lda);
+                panel(A + k1 + k1 * lda, lda, (int)(n - k1), kb1, ipiv + k1, (int)k1, (int)k1);
+                if (ok()) err = cudaEventRecord(ev_panel[b + 1], main_st);
+            }
+            // side: the same for the remaining block columns
+            use(true);
+            if (nr2 > 0 && ok()) {
+                err = cudaStreamWaitEvent(side_st, ev_panel[b], 0);
+                laswp(ipiv + k, kb, (int)k, A + k + k2 * lda, nr2, nullptr, 0, lda);
+                trsm_lower(Akk, lda, kb, A + k + k2 * lda, lda, nr2);
+                if (ok())
+                    berr = gemm_sub(h, (int)(n - k1), nr2, kb, A + k1 + k * lda, lda, A + k + k2 * lda, lda,
+                                    A + k1 + k2 * lda, lda);
+            }
+            if (ok()) err = cudaEventRecord(ev_rest[b], side_st);
+        }
+        use(false);
+        if (ok()) err = cudaStreamWaitEvent(main_st, ev_rest[nblk - 1], 0);
+        for (int b = 0; b < nblk; ++b) {
+            if (ev_panel[b]) cudaEventDestroy(ev_panel[b]);
+            if (ev_rest[b]) cudaEventDestroy(ev_rest[b]);
+        }
+    }
+
+    // X (n x nrhs) := A^-1 B with the factors in A; perm: n ints
+    void solve(const T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X, int64_t ldx, int* perm)
+    {
+        if (!ok()) return;
+        const size_t psmem = (size_t)n * sizeof(int);
+        err = cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+        if (!ok()) return;
+        pivots_to_perm_kernel<<<1, 1024, psmem, st>>>(ipiv, (int)n, perm);
+        err = cudaGetLastError();
+        if (!ok()) return;
+        permute_rows_kernel<T><<<dim3((unsigned)((n + 255) / 256), nrhs), 256, 0, st>>>(B, ldb, perm, (int)n, nrhs, X,
+                                                                                        ldx);
+        err = cudaGetLastError();
+        // forward: L y = P b (unit lower), 64-row blocks
+        for (int64_t d = 0; d < n && ok(); d += 64) {
+            const int db = (int)(n - d < 64 ? n - d : 64);
+            trsm_diag_kernel<T, false><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
+            err = cudaGetLastError();
+            if (d + db < n && ok())
+                berr = gemm_sub(h, (int)(n - d - db), nrhs, db, A + (d + db) + d * lda, lda, X + d, ldx, X + d + db, ldx);
+        }
+        // backward: U x = y, 64-row blocks from the bottom
+        for (int64_t e = n; e > 0 && ok(); e -= 64) {
+            const int64_t d = e - 64 > 0 ? e - 64 : 0;
+            const int db = (int)(e - d);
+            trsm_diag_kernel<T, true><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
+            err = cudaGetLastError();
+            if (d > 0 && ok()) berr = gemm_sub(h, (int)d, nrhs, db, A + d * lda, lda, X + d, ldx, X, ldx);
+        }
+    }
+};
+
+template <typename T, int W, int RPT>
+void allow_wide_clusters()
+{
+    cudaFuncSetAttribute(leaf_lu_kernel<T, W, RPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+// largest leaf cluster the device co-schedules: 16 CTAs (non-portable) or 8
+template <typename T>
+int configure(Lu<T>& lu)
+{
+    allow_wide_clusters<T, 32, 1>();
+    allow_wide_clusters<T, 16, 2>();
+    allow_wide_clusters<T, 8, 4>();
+    allow_wide_clusters<T, 4, 8>();
+    lu.cluster = 16;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kLeafThreads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, leaf_lu_kernel<T, 32, 1>, &cfg) != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        lu.cluster = 8;
+    }
+    return 0;
+}
+
+}  // namespace
+
+template <typename T>
+int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X,
+                    int64_t ldx, int* ipiv, int* perm, int* info, int nb, bool factor, bool solve)
+{
+    Lu<T> lu;
+    lu.main_h = s.main_blas;
+    lu.main_st = s.main;
+    // without a side stream the look-ahead degenerates to one in-order stream
+    lu.side_h = s.side_blas ? s.side_blas : s.main_blas;
+    lu.side_st = s.side_blas ? s.side : s.main;
+    lu.use(false);
+    lu.ipiv = ipiv;
+    lu.info = info;
+    configure(lu);
+    // nb bounds the pivots one row-swap launch applies; a leaf cluster holds
+    // at most cluster * 512 * 8 rows; the pivot-to-permutation kernel keeps n
+    // ints in shared memory
+    int dev = 0, smem_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (nb < 1 || nb > kMaxSwaps || n > (int64_t)lu.cluster * kLeafThreads * 8 ||
+        n * (int64_t)sizeof(int) > smem_optin)
+        return LU_TOO_LARGE;
+    if (cublasSetStream(lu.main_h, lu.main_st) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetStream(lu.side_h, lu.side_st) != CUBLAS_STATUS_SUCCESS)
+        return LU_BLAS_ERROR;
+    if (factor) lu.factor(A, n, lda, nb);
+    lu.use(false);
+    if (solve && nrhs > 0) lu.solve(A, n, lda, B, ldb, nrhs, X, ldx, perm);
+    if (lu.err != cudaSuccess) return LU_CUDA_ERROR;
+    if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;
+    return LU_OK;
+}
+
+template int lu_factor_solve<double>(const LuStreams&, double*, int64_t, int64_t, const double*, int64_t, int, double*,
+                                     int64_t, int*, int*, int*, int, bool, bool);
+template int lu_factor_solve<float>(const LuStreams&, float*, int64_t, int64_t, const float*, int64_t, int, float*,
+                                    int64_t, int*, int*, int*, int, bool, bool);
+
+}  // namespace cad

@@ -1,0 +1,33 @@
+// Dense LU with partial pivoting + solve (csrc/lu.cu).
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace cad {
+
+enum { LU_OK = 0, LU_CUDA_ERROR = 1, LU_BLAS_ERROR = 2, LU_TOO_LARGE = 3 };
+
+// Where the factorisation runs: the caller's stream (and a cuBLAS handle for
+// it), plus an optional side stream with its own handle for the look-ahead's
+// trailing updates (side_blas null: everything on the main stream).  The
+// result is ordered on the main stream.
+struct LuStreams {
+    cudaStream_t main;
+    cublasHandle_t main_blas;
+    cudaStream_t side;
+    cublasHandle_t side_blas;
+};
+
+// Factorise A (n x n, lda, column-major) in place (if factor) and / or solve
+// A X = B with the factors (if solve).  ipiv (n ints), perm (n ints) and info
+// (1 int) are device memory; info ends as INT_MAX when every pivot is
+// non-zero, else the 1-based column of the first zero pivot.  nb: outer block
+// width (1..256).
+// The single-precision variant runs its GEMMs on TF32 tensor cores.
+template <typename T>
+int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X,
+                    int64_t ldx, int* ipiv, int* perm, int* info, int nb, bool factor, bool solve);
+
+}  // namespace cad

@@ -187,3 +187,23 @@ def test_solve_matches_lapack(cad):
     B = rng.standard_normal((300, 4))
     X = cad.solve(A, B)
     assert np.max(np.abs(X - np.linalg.solve(A, B))) <= 1e-12 * np.max(np.abs(X))
+
+
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (37, 2), (700, 3), (2111, 1)])
+def test_solve_with_pivoting_matches_lapack(cad, n, nrhs):
+    # general matrices (no diagonal dominance): partial pivoting is exercised
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, nrhs))
+    X = cad.solve(A, B)
+    Xo = np.linalg.solve(A, B)
+    cond = np.linalg.cond(A)
+    assert np.max(np.abs(X - Xo)) <= 1e-14 * cond * np.max(np.abs(Xo)) + 1e-300
+    assert np.linalg.norm(A @ X - B) <= 1e-12 * np.linalg.norm(A) * np.linalg.norm(X)
+
+
+def test_solve_singular_raises(cad):
+    A = np.eye(50)
+    A[:, 7] = 0.0
+    with pytest.raises(cad.CadError, match="singular"):
+        cad.solve(A, np.ones(50))
