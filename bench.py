@@ -40,6 +40,9 @@ FALG_ASSEMBLY_FS = 2960.0 + 288.0
 # Half-space strain of all three unit modes (43867 on the dipping-crack
 # collocation pairs) plus the same traction epilogue.
 FALG_ASSEMBLY_HS = 43867.0 + 288.0
+# DRAM bytes (read + write) of one assembly launch from the committed ncu captures
+# (profiles/td_pair_kernel_*.md): (triangles captured, bytes).  Output scales as N^2.
+PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 77.27e6 + 2627.06e6)}
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
@@ -221,6 +224,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    launches0 = L.cad_kernel_launches(ctx)
     t_start.record(stream)
     for k in range(args.steps):
         step(evs[k])
@@ -229,6 +233,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
+    launches = L.cad_kernel_launches(ctx) - launches0
     ms_total = t_start.elapsed_time(t_end)
     asm_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
     sol_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
@@ -306,14 +311,20 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "api": "cad_slip_calculator (host C ABI, pinned host buffers)"},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": int(launches),
         "roofline": {"kernel": "td_pair_kernel<%s, strain, A-matrix>" % ("HS" if hs else "FS"), "bound": "fp64",
                      "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak_tflops,
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
-                     "falg_per_pair": falg, "traffic": None,
+                     "falg_per_pair": falg,
+                     "traffic": PAIR_TRAFFIC[args.workload][1] * (n / PAIR_TRAFFIC[args.workload][0]) ** 2,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                                       "N=%d, scaled by (N/%d)^2" % (PAIR_TRAFFIC[args.workload][0],
+                                                                      PAIR_TRAFFIC[args.workload][0]),
                      "step_share": asm_ms / ms_step},
-        "roofline_solve": {"kernel": "dense LU (cusolverDnDgetrf + getrs)", "bound": "fp64",
+        "roofline_solve": {"kernel": "blocked LU with look-ahead (cluster leaf_lu_kernel, own row-swap and "
+                                     "triangular kernels, cuBLAS DGEMM trailing update) + triangular solves",
+                           "bound": "fp64",
                            "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                            "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
         "cpu_baseline": cpu,

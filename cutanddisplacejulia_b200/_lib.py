@@ -27,7 +27,7 @@ CAD_ERR_TOO_LARGE = 10
 # Every symbol include/cad_td.h declares (checked by the tests).
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
-    "cad_version", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
+    "cad_version", "cad_kernel_launches", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
     "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
     "cad_solve_dev", "cad_td_sum_eval_noalloc",
 ]
@@ -69,6 +69,8 @@ def load():
     L.cad_last_time_ms.argtypes = [P, INT]
     L.cad_last_time_ms.restype = D
     L.cad_version.restype = ctypes.c_char_p
+    L.cad_kernel_launches.argtypes = [P]
+    L.cad_kernel_launches.restype = I64
     L.cad_fp64_fma_probe.argtypes = [P, I64, ctypes.POINTER(D)]
     td = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, D, INT, INT, INT, P, P]
     L.cad_td_inf.argtypes = td

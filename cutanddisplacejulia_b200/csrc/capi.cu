@@ -46,6 +46,7 @@ struct cad_ctx {
     DevBuf buf[S_COUNT];
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed[2] = {false, false};
+    int64_t launches = 0;   // own kernel launches issued through this context
     std::string err;
 };
 
@@ -115,6 +116,7 @@ int hs_check(cad_ctx* ctx, const double* Z, int64_t M, const double* P1, const d
 {
     void* flag;
     if (int r = ensure(ctx, S_FLAG, sizeof(int), &flag)) return r;
+    ++ctx->launches;
     CK(launch_hs_check(Z, M, P1, P2, P3, N, (int*)flag, ctx->stream));
     int h = 0;
     CK(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -137,6 +139,7 @@ int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, i
     }
     void* tri;
     if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    ++ctx->launches;
     CK(launch_td_setup(P1, P2, P3, N, Dss, Dds, Dn, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
     PairArgs a{};
     a.X = X; a.Y = Y; a.Z = Z; a.M = M; a.tri = (const TriDev*)tri; a.N = N;
@@ -149,12 +152,14 @@ int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, i
         a.partial = (double*)part;
     }
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    ++ctx->launches;
     CK(launch_td_pairs(a, out_kind, hs == 1, strain == 1, disp == 1, ctx->stream));
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     ctx->timed[0] = true;
     if (out_kind == OUT_SUM) {
         const int mask = (strain == 1 ? 0x3f : 0) | (disp == 1 ? 0x1c0 : 0);
-        CK(launch_sum_chunks(a.partial, nchunk, M, mask, sum_out, ctx->stream));
+        ++ctx->launches;
+    CK(launch_sum_chunks(a.partial, nchunk, M, mask, sum_out, ctx->stream));
     }
     return CAD_OK;
 }
@@ -168,12 +173,14 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
     if (int r = ensure(ctx, S_OBS, (size_t)3 * N * sizeof(double), &obs)) return r;
     if (int r = ensure(ctx, S_DIRS, (size_t)9 * N * sizeof(double), &dirs)) return r;
     double* X = (double*)obs;
+    ++ctx->launches;
     CK(launch_colloc(normals, mid, N, X, X + N, X + 2 * N, (double*)dirs, ctx->stream));
     if (hs == 1 && N > 0)
         if (int r = hs_check(ctx, X + 2 * N, N, P1, P2, P3, N)) return r;
     if (N == 0) return CAD_OK;
     void* tri;
     if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    ++ctx->launches;
     CK(launch_td_setup(P1, P2, P3, N, nullptr, nullptr, nullptr, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
     PairArgs a{};
     a.X = X; a.Y = X + N; a.Z = X + 2 * N; a.M = N; a.tri = (const TriDev*)tri; a.N = N;
@@ -181,6 +188,7 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
     a.lambda = lambda; a.G = G; a.dirs = (const double*)dirs;
     a.trac = trac_out; a.A = A; a.lda = lda;
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    ++ctx->launches;
     CK(launch_td_pairs(a, out_kind, hs == 1, true, false, ctx->stream));
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     ctx->timed[0] = true;
@@ -198,7 +206,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas};
+    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches};
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
                                            (int*)info, kLuBlock, true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
@@ -294,6 +302,8 @@ int cad_destroy(cad_ctx* ctx)
 }
 
 const char* cad_last_error(const cad_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t cad_kernel_launches(const cad_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int cad_set_stream(cad_ctx* ctx, void* stream)
 {
@@ -398,7 +408,8 @@ int cad_td_sum(cad_ctx* ctx, int64_t M, int64_t N, const double* const* strain_i
         if (int r = ensure(ctx, S_OUT, (size_t)nf * M * sizeof(double), &dev_out)) return r;
         for (int f = 0; f < 3 * nf; ++f)
             if (int r = upload(ctx, (double*)dev_in + f * MN, in[f], MN)) return r;
-        CK(launch_td_sum((const double*)dev_in, M, N, nf, (double*)dev_out, ctx->stream));
+        ++ctx->launches;
+    CK(launch_td_sum((const double*)dev_in, M, N, nf, (double*)dev_out, ctx->stream));
         if (int r = copy_fields_out(ctx, (const double*)dev_out, nf, M, out)) return r;
         CK(cudaStreamSynchronize(ctx->stream));
     }

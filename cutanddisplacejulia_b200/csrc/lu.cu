@@ -479,6 +479,7 @@ struct Lu {
     int* ipiv;    // absolute pivots, device
     int* info;
     int cluster;  // largest leaf cluster (16 where the device co-schedules it, else 8)
+    int64_t launches = 0;   // own kernels launched (cuBLAS calls not counted)
     cudaError_t err = cudaSuccess;
     cublasStatus_t berr = CUBLAS_STATUS_SUCCESS;
 
@@ -501,6 +502,7 @@ struct Lu {
         const int ncol = ncol1 + ncol2;
         const int blocks = (ncol + 7) / 8 < 148 * 2 ? (ncol + 7) / 8 : 148 * 2;
         laswp_kernel<T><<<blocks, 256, 0, st>>>(A1, ncol1, A2, ncol2, lda, piv, npiv, row_base);
+        ++launches;
         err = cudaGetLastError();
     }
 
@@ -510,6 +512,7 @@ struct Lu {
         for (int d = 0; d < b && ok(); d += 64) {
             const int db = b - d < 64 ? b - d : 64;
             trsm_diag_kernel<T, false><<<(ncol + 31) / 32, 128, 0, st>>>(L + d + d * ldl, ldl, db, B + d, ldb, ncol);
+            ++launches;
             err = cudaGetLastError();
             if (d + db < b && ok())
                 berr = gemm_sub(h, b - d - db, ncol, db, L + (d + db) + d * ldl, ldl, B + d, ldb, B + d + db, ldb);
@@ -533,6 +536,7 @@ struct Lu {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         err = cudaLaunchKernelEx(&cfg, leaf_lu_kernel<T, W, RPT>, A, lda, m, w, piv, piv_base, info, col_base);
+        ++launches;
     }
 
     void leaf(T* A, int64_t lda, int m, int w, int* piv, int piv_base, int col_base)
@@ -586,6 +590,7 @@ struct Lu {
     {
         use(false);
         set_int_kernel<<<1, 1, 0, st>>>(info, INT_MAX);
+        ++launches;
         err = cudaGetLastError();
         const int nblk = (int)((n + nb - 1) / nb);
         if (nblk == 0 || !ok()) return;
@@ -648,15 +653,18 @@ struct Lu {
         err = cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
         if (!ok()) return;
         pivots_to_perm_kernel<<<1, 1024, psmem, st>>>(ipiv, (int)n, perm);
+        ++launches;
         err = cudaGetLastError();
         if (!ok()) return;
         permute_rows_kernel<T><<<dim3((unsigned)((n + 255) / 256), nrhs), 256, 0, st>>>(B, ldb, perm, (int)n, nrhs, X,
                                                                                         ldx);
+        ++launches;
         err = cudaGetLastError();
         // forward: L y = P b (unit lower), 64-row blocks
         for (int64_t d = 0; d < n && ok(); d += 64) {
             const int db = (int)(n - d < 64 ? n - d : 64);
             trsm_diag_kernel<T, false><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
+            ++launches;
             err = cudaGetLastError();
             if (d + db < n && ok())
                 berr = gemm_sub(h, (int)(n - d - db), nrhs, db, A + (d + db) + d * lda, lda, X + d, ldx, X + d + db, ldx);
@@ -666,6 +674,7 @@ struct Lu {
             const int64_t d = e - 64 > 0 ? e - 64 : 0;
             const int db = (int)(e - d);
             trsm_diag_kernel<T, true><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
+            ++launches;
             err = cudaGetLastError();
             if (d > 0 && ok()) berr = gemm_sub(h, (int)d, nrhs, db, A + d * lda, lda, X + d, ldx, X, ldx);
         }
@@ -736,6 +745,7 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     if (factor) lu.factor(A, n, lda, nb);
     lu.use(false);
     if (solve && nrhs > 0) lu.solve(A, n, lda, B, ldb, nrhs, X, ldx, perm);
+    if (s.launches) *s.launches += lu.launches;
     if (lu.err != cudaSuccess) return LU_CUDA_ERROR;
     if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;
     return LU_OK;

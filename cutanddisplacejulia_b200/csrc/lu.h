@@ -18,6 +18,7 @@ struct LuStreams {
     cublasHandle_t main_blas;
     cudaStream_t side;
     cublasHandle_t side_blas;
+    int64_t* launches;   // if set, incremented by the number of own kernel launches
 };
 
 // Factorise A (n x n, lda, column-major) in place (if factor) and / or solve

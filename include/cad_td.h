@@ -65,6 +65,10 @@ void* cad_get_stream(const cad_ctx* ctx);
 double cad_last_time_ms(const cad_ctx* ctx, int which);
 /* Library version string. */
 const char* cad_version(void);
+/* Number of the library's own CUDA kernels launched through this context so
+ * far (cuBLAS calls not included).  No counterpart in the reference (an
+ * accounting utility). */
+int64_t cad_kernel_launches(const cad_ctx* ctx);
 /* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 flops
  * per FMA), the denominator of the TD kernels' roofline.  No counterpart in
  * the reference (a measurement utility). */

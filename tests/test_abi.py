@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "cad_td.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|double|void\*|const char\*)\s+(cad_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|double|void\*|const char\*)\s+(cad_\w+)\(", text, re.M)))
 
 
 def test_header_matches_binding_list():
