@@ -23,11 +23,13 @@ CAD_ERR_NOT_CONVERGED = 7
 CAD_ERR_SINGULAR = 8
 CAD_ERR_ARG = 9
 CAD_ERR_TOO_LARGE = 10
+CAD_SOLVER_LU64 = 0
+CAD_SOLVER_MIXED = 1
 
 # Every symbol include/cad_td.h declares (checked by the tests).
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
-    "cad_version", "cad_kernel_launches", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
+    "cad_version", "cad_kernel_launches", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
     "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
     "cad_solve_dev", "cad_td_sum_eval_noalloc",
 ]
@@ -71,6 +73,8 @@ def load():
     L.cad_version.restype = ctypes.c_char_p
     L.cad_kernel_launches.argtypes = [P]
     L.cad_kernel_launches.restype = I64
+    L.cad_set_solver.argtypes = [P, INT, D, INT]
+    L.cad_last_solve_stats.argtypes = [P, ctypes.POINTER(INT), ctypes.POINTER(D)]
     L.cad_fp64_fma_probe.argtypes = [P, I64, ctypes.POINTER(D)]
     td = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, D, INT, INT, INT, P, P]
     L.cad_td_inf.argtypes = td
@@ -114,3 +118,30 @@ def ptr_array(arrays):
     for k, a in enumerate(arrays):
         arr[k] = None if a is None else a.ctypes.data
     return arr
+
+
+class solver_mode:
+    """Context manager selecting the dense solver of `ctx` for the calls inside it
+    ("lu64": FP64 LU as the reference's A\\b; "mixed": FP32/TF32 LU preconditioning
+    FP64 GMRES to relative residual `tol`), restoring the FP64 LU afterwards."""
+
+    def __init__(self, ctx, solver="lu64", tol=1e-10, max_iter=200):
+        modes = {"lu64": CAD_SOLVER_LU64, "mixed": CAD_SOLVER_MIXED}
+        if solver not in modes:
+            raise ValueError("solver must be 'lu64' or 'mixed'")
+        self.ctx, self.mode, self.tol, self.max_iter = ctx, modes[solver], float(tol), int(max_iter)
+
+    def __enter__(self):
+        check(load().cad_set_solver(self.ctx, self.mode, self.tol, self.max_iter), self.ctx)
+        return self
+
+    def __exit__(self, *exc):
+        load().cad_set_solver(self.ctx, CAD_SOLVER_LU64, 1e-10, 200)
+        return False
+
+
+def last_solve_stats(ctx):
+    """(GMRES iterations, final relative residual) of the last mixed solve on `ctx`."""
+    it, rr = ctypes.c_int(0), ctypes.c_double(0.0)
+    check(load().cad_last_solve_stats(ctx, ctypes.byref(it), ctypes.byref(rr)), ctx)
+    return it.value, rr.value

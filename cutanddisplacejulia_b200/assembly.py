@@ -91,8 +91,11 @@ def CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, nu, G, 
 
 
 def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag, BoundaryConditions, FixedEls,
-                     device=0):
-    """Plain (frictionless) slip solve: returns (Dn, Dss, Dds, A, b)."""
+                     device=0, solver="lu64", tol=1e-10, max_iter=200):
+    """Plain (frictionless) slip solve: returns (Dn, Dss, Dds, A, b).
+
+    solver="lu64" solves A \\ b by FP64 LU as src/SlipCalculator3D.jl:22 does;
+    solver="mixed" uses the FP32/TF32 LU + FP64 GMRES path to relative residual tol."""
     P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
     N = P1.shape[0]
     nrm = _tri(FaceNormalVector)
@@ -107,16 +110,18 @@ def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
     A = np.zeros((3 * N, 3 * N), order="F")
     b = np.zeros(3 * N)
     ctx = _lib.context(device)
-    rc = _lib.load().cad_slip_calculator(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu), float(G),
-                                         float(lam), mid.ctypes.data, nrm.ctypes.data, int(HSFlag), Tn.ctypes.data,
-                                         Tss.ctypes.data, Tds.ctypes.data, Dn.ctypes.data, Dss.ctypes.data,
-                                         Dds.ctypes.data, A.ctypes.data, b.ctypes.data)
-    _lib.check(rc, ctx)
+    with _lib.solver_mode(ctx, solver, tol, max_iter):
+        rc = _lib.load().cad_slip_calculator(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu),
+                                             float(G), float(lam), mid.ctypes.data, nrm.ctypes.data, int(HSFlag),
+                                             Tn.ctypes.data, Tss.ctypes.data, Tds.ctypes.data, Dn.ctypes.data,
+                                             Dss.ctypes.data, Dds.ctypes.data, A.ctypes.data, b.ctypes.data)
+        _lib.check(rc, ctx)
     return Dn, Dss, Dds, A, b
 
 
-def solve(A, B, device=0):
-    """Dense A \\ B by LU with partial pivoting on the GPU."""
+def solve(A, B, device=0, solver="lu64", tol=1e-10, max_iter=200):
+    """Dense A \\ B on the GPU: FP64 LU with partial pivoting ("lu64"), or the
+    FP32/TF32 LU + FP64 GMRES path ("mixed", relative residual tol)."""
     A = np.asfortranarray(A, dtype=np.float64)
     B = np.asarray(B, dtype=np.float64)
     vec = B.ndim == 1
@@ -124,6 +129,7 @@ def solve(A, B, device=0):
     n, nrhs = A.shape[0], Bf.shape[1]
     X = np.zeros((n, nrhs), order="F")
     ctx = _lib.context(device)
-    rc = _lib.load().cad_solve(ctx, n, A.ctypes.data, Bf.ctypes.data, nrhs, X.ctypes.data)
-    _lib.check(rc, ctx)
+    with _lib.solver_mode(ctx, solver, tol, max_iter):
+        rc = _lib.load().cad_solve(ctx, n, A.ctypes.data, Bf.ctypes.data, nrhs, X.ctypes.data)
+        _lib.check(rc, ctx)
     return X[:, 0] if vec else X

@@ -8,8 +8,9 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcad_td.so")
-SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu", "noalloc.cu", "lu.cu"]
-HEADERS = ["td_device.cuh", "tde_closed_form.cuh", "td_kernels.h", "lu.h", os.path.join("..", "..", "include", "cad_td.h")]
+SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu", "noalloc.cu", "lu.cu", "mixed.cu"]
+HEADERS = ["td_device.cuh", "tde_closed_form.cuh", "td_kernels.h", "lu.h", "mixed.h",
+           os.path.join("..", "..", "include", "cad_td.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -14,6 +14,7 @@
 
 #include "../../include/cad_td.h"
 #include "lu.h"
+#include "mixed.h"
 #include "td_device.cuh"
 #include "td_kernels.h"
 
@@ -25,7 +26,10 @@ size_t tri_record_bytes() { return sizeof(TriDev); }
 
 namespace {
 
-enum Slot { S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM, S_COUNT };
+enum Slot {
+    S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
+    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_COUNT
+};
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
 
@@ -47,6 +51,11 @@ struct cad_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed[2] = {false, false};
     int64_t launches = 0;   // own kernel launches issued through this context
+    int solver = CAD_SOLVER_LU64;   // cad_set_solver
+    double tol = 1e-10;
+    int max_iter = 200;
+    int last_iters = 0;           // of the last mixed solve (all right-hand sides)
+    double last_relres = 0.0;     // largest over its right-hand sides
     std::string err;
 };
 
@@ -195,9 +204,89 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
     return CAD_OK;
 }
 
+constexpr int kRestart = 30;   // Krylov dimension of a GMRES cycle
+
+int read_info(cad_ctx* ctx, int* info);
+
+// FP32/TF32 LU + FP64 GMRES: B := A^-1 B, A left unchanged.  Sets *info from
+// the FP32 factorisation's pivots (0: all non-zero).
+int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs,
+                       int* info_out)
+{
+    void *a32, *dinv, *piv, *perm, *info, *kry, *v32, *sync, *work;
+    if (int r = ensure(ctx, S_A32, (size_t)n * n * sizeof(float), &a32)) return r;
+    if (int r = ensure(ctx, S_DINV, mixed_dinv_floats(n) * sizeof(float), &dinv)) return r;
+    if (int r = ensure(ctx, S_PIV, (size_t)n * sizeof(int), &piv)) return r;
+    if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
+    if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
+    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (kRestart + 1) + 3 * (size_t)n + 2 * (kRestart + 1)) * sizeof(double),
+                       &kry))
+        return r;
+    if (int r = ensure(ctx, S_VEC32, 2 * (size_t)n * sizeof(float), &v32)) return r;
+    if (int r = ensure(ctx, S_SYNC, mixed_sync_ints(n) * sizeof(int), &sync)) return r;
+    if (int r = ensure(ctx, S_WORK, (size_t)n * sizeof(double), &work)) return r;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches};
+    int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
+    if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
+    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
+    if (int r = read_info(ctx, info_out)) return r;
+    if (*info_out > 0) return CAD_OK;
+    double* V = (double*)kry;
+    double* w = V + (size_t)n * (kRestart + 1);
+    GmresArgs g{};
+    g.blas = ctx->blas;
+    g.stream = ctx->stream;
+    g.n = n;
+    g.A = A;
+    g.lda = lda;
+    g.A32 = (const float*)a32;
+    g.Dinv = (const float*)dinv;
+    g.perm = (const int*)perm;
+    g.tol = ctx->tol;
+    g.max_iter = ctx->max_iter;
+    g.restart = kRestart;
+    g.V = V;
+    g.w = w;
+    g.z = w + n;
+    g.r = w + 2 * n;
+    g.hd = w + 3 * n;
+    g.y32 = (float*)v32;
+    g.x32 = (float*)v32 + n;
+    g.sync = (int*)sync;
+    g.launches = &ctx->launches;
+    ctx->last_iters = 0;
+    ctx->last_relres = 0.0;
+    bool converged = true;
+    for (int64_t c = 0; c < nrhs; ++c) {
+        g.b = B + c * ldb;
+        g.x = (double*)work;
+        GmresResult res{};
+        const int st = gmres_ir_solve(g, &res);
+        if (st == GMRES_TIMEOUT) return fail(ctx, CAD_ERR_TIMEOUT, "mixed solve: a triangular-solve wait ran out");
+        if (st == GMRES_CUDA_ERROR || st == GMRES_BLAS_ERROR)
+            return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA or cuBLAS error in GMRES");
+        converged = converged && st == GMRES_OK;
+        ctx->last_iters += res.iterations;
+        ctx->last_relres = res.rel_residual > ctx->last_relres ? res.rel_residual : ctx->last_relres;
+        CK(cudaMemcpyAsync(B + c * ldb, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    ctx->timed[1] = true;
+    if (!converged)
+        return fail(ctx, CAD_ERR_NOT_CONVERGED, "mixed solve: GMRES did not reach the residual tolerance");
+    return CAD_OK;
+}
+
 int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
 {
     if (n == 0 || nrhs == 0) return CAD_OK;
+    if (ctx->solver == CAD_SOLVER_MIXED) {
+        if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
+            return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
+        int info = 0;
+        return solve_mixed_device(ctx, n, A, lda, B, ldb, nrhs, &info);
+    }
     if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
         return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
     void *work, *piv, *info, *perm;
@@ -304,6 +393,25 @@ int cad_destroy(cad_ctx* ctx)
 const char* cad_last_error(const cad_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int64_t cad_kernel_launches(const cad_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if ((mode != CAD_SOLVER_LU64 && mode != CAD_SOLVER_MIXED) || !(tol > 0.0) || max_iter < 1)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->solver = mode;
+    ctx->tol = tol;
+    ctx->max_iter = max_iter;
+    return CAD_OK;
+}
+
+int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (iterations) *iterations = ctx->last_iters;
+    if (rel_residual) *rel_residual = ctx->last_relres;
+    return CAD_OK;
+}
 
 int cad_set_stream(cad_ctx* ctx, void* stream)
 {

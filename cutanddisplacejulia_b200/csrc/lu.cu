@@ -751,6 +751,19 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     return LU_OK;
 }
 
+int lu_pivots_to_perm(const LuStreams& s, const int* ipiv, int64_t n, int* perm)
+{
+    if (n <= 0) return LU_OK;
+    const size_t psmem = (size_t)n * sizeof(int);
+    if (cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) !=
+        cudaSuccess)
+        return LU_TOO_LARGE;
+    pivots_to_perm_kernel<<<1, 1024, psmem, s.main>>>(ipiv, (int)n, perm);
+    if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
+    if (s.launches) ++*s.launches;
+    return LU_OK;
+}
+
 template int lu_factor_solve<double>(const LuStreams&, double*, int64_t, int64_t, const double*, int64_t, int, double*,
                                      int64_t, int*, int*, int*, int, bool, bool);
 template int lu_factor_solve<float>(const LuStreams&, float*, int64_t, int64_t, const float*, int64_t, int, float*,

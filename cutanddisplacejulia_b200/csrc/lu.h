@@ -31,4 +31,8 @@ template <typename T>
 int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X,
                     int64_t ldx, int* ipiv, int* perm, int* info, int nb, bool factor, bool solve);
 
+// perm[i] = row of the original matrix that the factorisation's row i came
+// from (the pivots applied in order); perm: n ints, device.
+int lu_pivots_to_perm(const LuStreams& s, const int* ipiv, int64_t n, int* perm);
+
 }  // namespace cad

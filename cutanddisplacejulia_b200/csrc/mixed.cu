@@ -1,0 +1,375 @@
+// Mixed-precision solve of the 3N x 3N influence system (an addition to the
+// reference's `A\b`, src/SlipCalculator3D.jl:22): the FP64 matrix is cast to
+// FP32 and factorised by the blocked LU of csrc/lu.cu (TF32 tensor-core
+// trailing updates), and restarted GMRES in FP64, right-preconditioned by that
+// factorisation, drives the FP64 residual b - A x down to the requested
+// relative tolerance.  FP64 is kept for the matrix-vector product, the Krylov
+// basis and the solution; FP32 only inside the preconditioner.
+//
+// The preconditioner's triangular solves are one launch per triangle: each
+// CTA owns a 128-row block, takes its place in the dependency order from an
+// atomic ticket (so every block it waits for has already started), streams
+// its off-diagonal blocks against the solved pieces as they are published
+// (flag per block, release/acquire), and finishes with a GEMV against the
+// explicitly inverted diagonal block.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "lu.h"
+#include "mixed.h"
+
+namespace cad {
+
+namespace {
+
+constexpr int kRB = 128;            // row block of the triangular solves
+constexpr int kChainThreads = 256;  // two threads per row: halves of each 128-column block
+constexpr long kSpinLimit = 1L << 22;
+
+// B (n x n, leading dimension n) = (float) A (n x n, lda); columns strided over grid.y
+__global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64_t n, float* __restrict__ B)
+{
+    for (int64_t c = blockIdx.y; c < n; c += gridDim.y)
+        for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+            B[r + c * n] = (float)A[r + c * lda];
+}
+
+// Inverse of diagonal block i (kRB x kRB, zero-padded to the identity past n)
+// of the unit lower (UPPER false) or the non-unit upper triangle of the LU
+// factors, column-major into D + i * kRB * kRB.  Thread j computes column j of
+// the inverse by substitution; the block and the inverse sit in shared memory
+// (the inverse row-major with a pad, so the threads' columns are conflict-free).
+template <bool UPPER>
+__global__ void __launch_bounds__(kRB) invert_diag_kernel(const float* __restrict__ A, int64_t lda, int n,
+                                                         float* __restrict__ D)
+{
+    extern __shared__ float sm[];
+    float* s_a = sm;                  // [kRB][kRB] column-major
+    float* s_x = sm + kRB * kRB;      // [kRB][kRB + 1] row-major: s_x[r * (kRB + 1) + j]
+    const int i = blockIdx.x, j = threadIdx.x;
+    const int r0 = i * kRB;
+    const int b = n - r0 < kRB ? n - r0 : kRB;
+    for (int e = j; e < kRB * kRB; e += kRB) {
+        const int r = e % kRB, c = e / kRB;
+        float v = (r < b && c < b) ? A[(int64_t)(r0 + r) + (int64_t)(r0 + c) * lda] : 0.f;
+        if (r == c && r >= b) v = 1.f;
+        s_a[e] = v;
+    }
+    __syncthreads();
+    if (!UPPER) {
+        for (int r = 0; r < kRB; ++r) {
+            float v;
+            if (r < j) v = 0.f;
+            else if (r == j) v = 1.f;
+            else {
+                float s = 0.f;
+                for (int k = j; k < r; ++k) s = fmaf(s_a[r + k * kRB], s_x[k * (kRB + 1) + j], s);
+                v = -s;
+            }
+            s_x[r * (kRB + 1) + j] = v;
+        }
+    } else {
+        for (int r = kRB - 1; r >= 0; --r) {
+            float v;
+            if (r > j) v = 0.f;
+            else if (r == j) v = 1.f / s_a[r + r * kRB];
+            else {
+                float s = 0.f;
+                for (int k = r + 1; k <= j; ++k) s = fmaf(s_a[r + k * kRB], s_x[k * (kRB + 1) + j], s);
+                v = -s / s_a[r + r * kRB];
+            }
+            s_x[r * (kRB + 1) + j] = v;
+        }
+    }
+    __syncthreads();
+    float* out = D + (int64_t)i * kRB * kRB;
+    for (int e = j; e < kRB * kRB; e += kRB) {
+        const int r = e % kRB, c = e / kRB;
+        out[e] = s_x[r * (kRB + 1) + c];
+    }
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Partial product of this thread's row with half hh of a kRB-column block.
+__device__ __forceinline__ float row_half_dot(const float* __restrict__ a, int64_t lda, int ncols,
+                                              const float* __restrict__ s_x)
+{
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+    int c = 0;
+    for (; c + 4 <= ncols; c += 4) {
+        p0 = fmaf(a[(int64_t)c * lda], s_x[c], p0);
+        p1 = fmaf(a[(int64_t)(c + 1) * lda], s_x[c + 1], p1);
+        p2 = fmaf(a[(int64_t)(c + 2) * lda], s_x[c + 2], p2);
+        p3 = fmaf(a[(int64_t)(c + 3) * lda], s_x[c + 3], p3);
+    }
+    for (; c < ncols; ++c) p0 = fmaf(a[(int64_t)c * lda], s_x[c], p0);
+    return (p0 + p1) + (p2 + p3);
+}
+
+// One triangle of M^-1 v with M = P^T L U in FP32.  Lower (UPPER false):
+// y = L^-1 (P v), v FP64 gathered through perm.  Upper: x = U^-1 y, written
+// as FP64 to out.  x32 holds the solved blocks for the other CTAs; flags[i]
+// is set once block i is published; ticket orders the CTAs.
+template <bool UPPER>
+__global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
+    const float* __restrict__ A, int64_t lda, int n, int nblk, const float* __restrict__ Dinv,
+    const double* __restrict__ v_in, const int* __restrict__ perm, const float* y_in, float* x32,
+    double* __restrict__ out, int* flags, int* ticket, int* fail)
+{
+    __shared__ float s_x[kRB];
+    __shared__ float s_part[2][kRB];
+    __shared__ int s_t;
+    const int tid = threadIdx.x, rr = tid & (kRB - 1), hh = tid >> 7;
+    if (tid == 0) s_t = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int t = s_t;
+    const int i = UPPER ? nblk - 1 - t : t;
+    const int r0 = i * kRB;
+    const int rows = n - r0 < kRB ? n - r0 : kRB;
+    const int row = r0 + rr;
+    float acc = 0.f;
+    if (hh == 0 && rr < rows) acc = UPPER ? __ldcg(y_in + row) : (float)v_in[perm[row]];
+    for (int s = 0; s < t; ++s) {
+        const int j = UPPER ? nblk - 1 - s : s;
+        if (tid == 0) {
+            long spins = 0;
+            while (ld_acquire(flags + j) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicExch(fail, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __syncthreads();
+        const int c0 = j * kRB;
+        const int ncb = n - c0 < kRB ? n - c0 : kRB;
+        if (tid < kRB) s_x[tid] = tid < ncb ? __ldcg(x32 + c0 + tid) : 0.f;
+        __syncthreads();
+        const int half0 = hh * (kRB / 2);
+        int nc = ncb - half0;
+        nc = nc < 0 ? 0 : (nc > kRB / 2 ? kRB / 2 : nc);
+        if (rr < rows && nc > 0) acc -= row_half_dot(A + row + (int64_t)(c0 + half0) * lda, lda, nc, s_x + half0);
+    }
+    // right-hand side of the diagonal block, then its explicit inverse
+    s_part[hh][rr] = acc;
+    __syncthreads();
+    if (tid < kRB) s_x[tid] = s_part[0][tid] + s_part[1][tid];
+    __syncthreads();
+    const float* d = Dinv + (int64_t)i * kRB * kRB + rr + (int64_t)(hh * (kRB / 2)) * kRB;
+    const float p = row_half_dot(d, kRB, kRB / 2, s_x + hh * (kRB / 2));
+    s_part[hh][rr] = p;
+    __syncthreads();
+    if (tid < rows) {
+        const float x = s_part[0][tid] + s_part[1][tid];
+        x32[r0 + tid] = x;
+        if (UPPER) out[r0 + tid] = (double)x;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        st_release(flags + i, 1);
+    }
+}
+
+}  // namespace
+
+int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, float* A32, float* Dinv, int* ipiv,
+                  int* perm, int* info, int nb)
+{
+    if (n <= 0) return LU_OK;
+    const int64_t rb = (n + 255) / 256;
+    cast_f32_kernel<<<dim3((unsigned)(rb < 8 ? rb : 8), (unsigned)(n < 4096 ? n : 4096)), 256, 0, ls.main>>>(A, lda, n,
+                                                                                                     A32);
+    if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
+    if (ls.launches) ++*ls.launches;
+    int rc = lu_factor_solve<float>(ls, A32, n, n, nullptr, 0, 0, nullptr, 0, ipiv, perm, info, nb, true, false);
+    if (rc != LU_OK) return rc;
+    rc = lu_pivots_to_perm(ls, ipiv, n, perm);
+    if (rc != LU_OK) return rc;
+    const int nblk = (int)((n + kRB - 1) / kRB);
+    const size_t smem = (size_t)(kRB * kRB + kRB * (kRB + 1)) * sizeof(float);
+    if (cudaFuncSetAttribute(invert_diag_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(invert_diag_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return LU_CUDA_ERROR;
+    invert_diag_kernel<false><<<nblk, kRB, smem, ls.main>>>(A32, n, (int)n, Dinv);
+    invert_diag_kernel<true><<<nblk, kRB, smem, ls.main>>>(A32, n, (int)n, Dinv + (int64_t)nblk * kRB * kRB);
+    if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
+    if (ls.launches) *ls.launches += 2;
+    return LU_OK;
+}
+
+size_t mixed_dinv_floats(int64_t n) { return (size_t)2 * ((n + kRB - 1) / kRB) * kRB * kRB; }
+size_t mixed_sync_ints(int64_t n) { return (size_t)2 * ((n + kRB - 1) / kRB) + 4; }
+
+namespace {
+
+struct Precond {
+    const float* A32;
+    const float* Dinv;
+    const int* perm;
+    int n, nblk;
+    float* y32;
+    float* x32;
+    int* sync;   // [2 * nblk flags][2 tickets][fail]
+    cudaStream_t st;
+    int64_t* launches;
+
+    // z = M^-1 v (FP64 in and out, FP32 inside)
+    bool apply(const double* v, double* z) const
+    {
+        if (cudaMemsetAsync(sync, 0, (size_t)(2 * nblk + 2) * sizeof(int), st) != cudaSuccess) return false;
+        int* fl = sync;
+        int* fu = sync + nblk;
+        int* tk = sync + 2 * nblk;
+        int* fail = sync + 2 * nblk + 2;
+        const float* DL = Dinv;
+        const float* DU = Dinv + (int64_t)nblk * kRB * kRB;
+        trsv_chain_kernel<false><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DL, v, perm, nullptr, y32, nullptr,
+                                                                 fl, tk, fail);
+        trsv_chain_kernel<true><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DU, nullptr, nullptr, y32, x32, z, fu,
+                                                                tk + 1, fail);
+        if (launches) *launches += 2;
+        return cudaGetLastError() == cudaSuccess;
+    }
+};
+
+}  // namespace
+
+int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
+{
+    const int64_t n = a.n;
+    const int m = a.restart;
+    cublasHandle_t h = a.blas;
+    cudaStream_t st = a.stream;
+    res->iterations = 0;
+    res->rel_residual = 0.0;
+    res->status = GMRES_OK;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
+    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
+    const int nblk = (int)((n + kRB - 1) / kRB);
+    Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.y32, a.x32, a.sync, st, a.launches};
+    double* V = a.V;        // n x (m + 1)
+    double* w = a.w;
+    double* z = a.z;
+    double* r = a.r;
+    double* hd = a.hd;      // 2 (m + 1) device scratch
+    double* x = a.x;
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    bool ok = true;
+    auto B = [&](cublasStatus_t s) { ok = ok && s == CUBLAS_STATUS_SUCCESS; };
+
+    if (cudaMemsetAsync(a.sync + 2 * nblk + 2, 0, sizeof(int), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+    double bnorm = 0.0;
+    B(cublasDnrm2(h, (int)n, a.b, 1, &bnorm));
+    if (!ok) return GMRES_BLAS_ERROR;
+    if (cudaMemsetAsync(x, 0, n * sizeof(double), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+    if (bnorm == 0.0) return GMRES_OK;
+
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hcol(2 * (m + 1)), y(m);
+    int total = 0;
+    while (true) {
+        // true residual r = b - A x
+        if (cudaMemcpyAsync(r, a.b, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        B(cublasDgemv(h, CUBLAS_OP_N, (int)n, (int)n, &mone, a.A, (int)a.lda, x, 1, &one, r, 1));
+        double beta = 0.0;
+        B(cublasDnrm2(h, (int)n, r, 1, &beta));
+        if (!ok) return GMRES_BLAS_ERROR;
+        res->rel_residual = beta / bnorm;
+        res->iterations = total;
+        if (res->rel_residual <= a.tol) return GMRES_OK;
+        if (total >= a.max_iter) {
+            res->status = GMRES_NOT_CONVERGED;
+            return GMRES_NOT_CONVERGED;
+        }
+        const double ib = 1.0 / beta;
+        if (cudaMemcpyAsync(V, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        B(cublasDscal(h, (int)n, &ib, V, 1));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int kend = 0;
+        for (int k = 0; k < m; ++k) {
+            double* vk = V + (int64_t)k * n;
+            if (!M.apply(vk, z)) return GMRES_CUDA_ERROR;
+            B(cublasDgemv(h, CUBLAS_OP_N, (int)n, (int)n, &one, a.A, (int)a.lda, z, 1, &zero, w, 1));
+            // classical Gram-Schmidt, twice
+            for (int pass = 0; pass < 2; ++pass) {
+                B(cublasDgemv(h, CUBLAS_OP_T, (int)n, k + 1, &one, V, (int)n, w, 1, &zero, hd + pass * (m + 1), 1));
+                B(cublasDgemv(h, CUBLAS_OP_N, (int)n, k + 1, &mone, V, (int)n, hd + pass * (m + 1), 1, &one, w, 1));
+            }
+            double hn = 0.0;
+            B(cublasDnrm2(h, (int)n, w, 1, &hn));
+            if (!ok) return GMRES_BLAS_ERROR;
+            if (cudaMemcpyAsync(hcol.data(), hd, 2 * (m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return GMRES_CUDA_ERROR;
+            double* Hk = H.data() + (size_t)k * (m + 1);
+            for (int q = 0; q <= k; ++q) Hk[q] = hcol[q] + hcol[(m + 1) + q];
+            Hk[k + 1] = hn;
+            if (hn > 0.0 && k + 1 < m + 1) {
+                const double ih = 1.0 / hn;
+                double* vn = V + (int64_t)(k + 1) * n;
+                if (cudaMemcpyAsync(vn, w, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                    return GMRES_CUDA_ERROR;
+                B(cublasDscal(h, (int)n, &ih, vn, 1));
+            }
+            // previous rotations, then a new one zeroing H[k+1][k]
+            for (int q = 0; q < k; ++q) {
+                const double t0 = cs[q] * Hk[q] + sn[q] * Hk[q + 1];
+                Hk[q + 1] = -sn[q] * Hk[q] + cs[q] * Hk[q + 1];
+                Hk[q] = t0;
+            }
+            const double den = std::hypot(Hk[k], Hk[k + 1]);
+            cs[k] = den > 0.0 ? Hk[k] / den : 1.0;
+            sn[k] = den > 0.0 ? Hk[k + 1] / den : 0.0;
+            Hk[k] = den;
+            Hk[k + 1] = 0.0;
+            g[k + 1] = -sn[k] * g[k];
+            g[k] = cs[k] * g[k];
+            ++total;
+            kend = k + 1;
+            // the rotated g estimates the residual; stop a little below the
+            // tolerance so the true residual checked next is within it
+            if (std::fabs(g[k + 1]) <= 0.5 * a.tol * bnorm || total >= a.max_iter || hn == 0.0) break;
+        }
+        // y = H^-1 g (upper triangular kend x kend), x += M^-1 (V y)
+        for (int q = kend - 1; q >= 0; --q) {
+            double s = g[q];
+            for (int c = q + 1; c < kend; ++c) s -= H[(size_t)c * (m + 1) + q] * y[c];
+            y[q] = s / H[(size_t)q * (m + 1) + q];
+        }
+        if (cudaMemcpyAsync(hd, y.data(), kend * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        B(cublasDgemv(h, CUBLAS_OP_N, (int)n, kend, &one, V, (int)n, hd, 1, &zero, w, 1));
+        if (!M.apply(w, z)) return GMRES_CUDA_ERROR;
+        B(cublasDaxpy(h, (int)n, &one, z, 1, x, 1));
+        if (!ok) return GMRES_BLAS_ERROR;
+        int fail = 0;
+        if (cudaMemcpyAsync(&fail, a.sync + 2 * nblk + 2, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        if (fail) return GMRES_TIMEOUT;
+    }
+}
+
+}  // namespace cad

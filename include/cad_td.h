@@ -48,6 +48,10 @@ extern "C" {
 #define CAD_ERR_ARG 9
 #define CAD_ERR_TOO_LARGE 10
 
+/* Solvers for the dense system (cad_set_solver). */
+#define CAD_SOLVER_LU64 0  /* FP64 LU with partial pivoting: the reference's A\b (default) */
+#define CAD_SOLVER_MIXED 1 /* FP32 LU (TF32 tensor-core updates) preconditioning FP64 GMRES */
+
 typedef struct cad_ctx cad_ctx;
 
 /* Context: one device, one stream, its own workspace.  A context is used by
@@ -69,6 +73,19 @@ const char* cad_version(void);
  * far (cuBLAS calls not included).  No counterpart in the reference (an
  * accounting utility). */
 int64_t cad_kernel_launches(const cad_ctx* ctx);
+/* Solver of the dense 3N x 3N system used by cad_slip_calculator, cad_solve and
+ * cad_solve_dev from now on.  CAD_SOLVER_LU64 (default) factorises in FP64 as
+ * the reference's A\b (src/SlipCalculator3D.jl:22) does.  CAD_SOLVER_MIXED has
+ * no counterpart in the reference: A is cast to FP32 and factorised with
+ * TF32 tensor-core trailing updates; restarted GMRES in FP64, right-
+ * preconditioned by that factorisation, iterates until ||b - A x|| / ||b|| <=
+ * tol (computed in FP64) or max_iter iterations (then CAD_ERR_NOT_CONVERGED,
+ * with the last iterate returned).  In mixed mode cad_solve_dev leaves A
+ * unchanged. */
+int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter);
+/* GMRES iterations (summed over right-hand sides) and the largest final
+ * relative residual of the last mixed solve. */
+int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual);
 /* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 flops
  * per FMA), the denominator of the TD kernels' roofline.  No counterpart in
  * the reference (a measurement utility). */

@@ -1,0 +1,108 @@
+"""GPU tests of the mixed-precision solve (FP32 LU with TF32 tensor-core
+updates preconditioning FP64 GMRES): the solution must reach the requested
+FP64 relative residual and agree with the FP64 LU solution (the plain path,
+src/SlipCalculator3D.jl:22) to 1e-8 relative, on general matrices and on the
+influence systems of a full-space penny crack and a half-space dipping crack."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SLIP_TOL = 1e-8   # relative slip error vs the FP64 LU solution
+RESID_TOL = 1e-10
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("n,nrhs", [(37, 1), (129, 2), (700, 3), (1500, 1)])
+def test_mixed_solve_general_matrix(cad, n, nrhs):
+    from cutanddisplacejulia_b200 import _lib
+    rng = np.random.default_rng(1000 + n)
+    A = rng.standard_normal((n, n)) + 2.0 * np.sqrt(n) * np.eye(n)
+    B = rng.standard_normal((n, nrhs))
+    X = cad.solve(A, B, solver="mixed", tol=RESID_TOL)
+    Xo = np.linalg.solve(A, B)
+    assert _rel(X, Xo) <= SLIP_TOL
+    for c in range(nrhs):
+        assert np.linalg.norm(A @ X[:, c] - B[:, c]) <= 2 * RESID_TOL * np.linalg.norm(B[:, c])
+    it, rr = _lib.last_solve_stats(_lib.context(0))
+    assert 1 <= it <= 200 and rr <= RESID_TOL
+
+
+def _geom(P1, P2, P3):
+    from oracle import geometry as g
+    nrm, mid = g.face_normal_and_midpoint(P1, P2, P3)
+    _, _, lam, nu, G = g.elastic_constants(1.0, 0.25)
+    return nrm, mid, lam, nu, G
+
+
+def test_mixed_slip_calculator_penny_matches_fp64(cad):
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.penny(seed=3, spacing=0.12)
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    bc = cad.Tractions(np.full(n, -1e-3), np.zeros(n), np.zeros(n))
+    ref = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 0, bc, np.zeros(n))
+    mix = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 0, bc, np.zeros(n), solver="mixed", tol=RESID_TOL)
+    D, Dm = np.concatenate(ref[:3]), np.concatenate(mix[:3])
+    assert _rel(Dm, D) <= SLIP_TOL
+    A, b = mix[3], mix[4]
+    assert np.linalg.norm(A @ Dm - b) <= 2 * RESID_TOL * np.linalg.norm(b)
+
+
+def test_mixed_slip_calculator_halfspace_dipping_matches_fp64(cad):
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=5, ntri=400)
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    s = workloads.remote_stress(seed=5)
+    bc = cad.Stresses(*[np.full(n, v) for v in s])
+    ref = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n))
+    mix = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n), solver="mixed", tol=RESID_TOL)
+    D, Dm = np.concatenate(ref[:3]), np.concatenate(mix[:3])
+    assert _rel(Dm, D) <= SLIP_TOL
+
+
+def test_mixed_solve_dev_leaves_matrix_unchanged(cad):
+    torch = pytest.importorskip("torch")
+    from cutanddisplacejulia_b200 import _lib
+    L = _lib.load()
+    ctx = _lib.context(0)
+    n = 300
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((n, n)) + 40.0 * np.eye(n)
+    b = rng.standard_normal(n)
+    dev = torch.device("cuda", 0)
+    Ad = torch.tensor(A.T.copy(), dtype=torch.float64, device=dev)   # row-major A^T = column-major A
+    bd = torch.tensor(b, dtype=torch.float64, device=dev)
+    with _lib.solver_mode(ctx, "mixed", RESID_TOL):
+        _lib.check(L.cad_solve_dev(ctx, n, Ad.data_ptr(), n, bd.data_ptr(), n, 1), ctx)
+    torch.cuda.synchronize()
+    assert np.array_equal(Ad.cpu().numpy(), A.T)
+    assert _rel(bd.cpu().numpy(), np.linalg.solve(A, b)) <= SLIP_TOL
+
+
+def test_mixed_reports_not_converged(cad):
+    from cutanddisplacejulia_b200 import _lib
+    rng = np.random.default_rng(11)
+    n = 200
+    A = rng.standard_normal((n, n)) + 3.0 * np.eye(n)
+    with pytest.raises(_lib.CadError) as e:
+        cad.solve(A, rng.standard_normal(n), solver="mixed", tol=1e-30, max_iter=1)
+    assert e.value.args and "GMRES" in str(e.value)
+
+
+def test_set_solver_rejects_bad_arguments(cad):
+    from cutanddisplacejulia_b200 import _lib
+    L = _lib.load()
+    ctx = _lib.context(0)
+    assert L.cad_set_solver(ctx, 7, 1e-10, 10) == _lib.CAD_ERR_ARG
+    assert L.cad_set_solver(ctx, _lib.CAD_SOLVER_MIXED, 0.0, 10) == _lib.CAD_ERR_ARG
+    assert L.cad_set_solver(ctx, _lib.CAD_SOLVER_MIXED, 1e-10, 0) == _lib.CAD_ERR_ARG
+    assert L.cad_set_solver(ctx, _lib.CAD_SOLVER_LU64, 1e-10, 200) == _lib.CAD_OK
+    it, rr = ctypes.c_int(-1), ctypes.c_double(-1.0)
+    assert L.cad_last_solve_stats(ctx, ctypes.byref(it), ctypes.byref(rr)) == _lib.CAD_OK
