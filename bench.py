@@ -46,6 +46,7 @@ PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 77.27e6 + 
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
+MIXED_TOL = 1e-10       # relative residual the mixed-precision solve iterates to
 
 UNIT = "pair-evals/s"
 WORKLOADS = {
@@ -167,6 +168,68 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def mixed_solve_timing(args, ctx, L, stream, step_asm_args, A, b0, x64, ms_fp64, world, dev):
+    """The mixed-precision step on the same system: FP64 assembly of A, then
+    FP32 LU (TF32 tensor-core updates) preconditioning FP64 GMRES to relative
+    residual 1e-10 (A is left unchanged).  Timed like the FP64 step (CUDA
+    events on the context stream, warm-up first); reports the solve time, the
+    iterations and the slip error against the FP64 LU solution x64."""
+    import torch
+    import torch.distributed as dist
+
+    from cutanddisplacejulia_b200 import _lib
+    dN, dM, dP1, dP2, dP3, n, lam, hs = step_asm_args
+    n3 = 3 * n
+    xm = torch.empty_like(x64)
+
+    def assemble():
+        _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
+                                      dP3.data_ptr(), n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
+
+    def step(evs=None):
+        if evs:
+            evs[0].record(stream)
+        assemble()
+        if evs:
+            evs[1].record(stream)
+        xm.copy_(b0)
+        _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, xm.data_ptr(), n3, 1), ctx)
+        if evs:
+            evs[2].record(stream)
+
+    with _lib.solver_mode(ctx, "mixed", tol=MIXED_TOL, max_iter=200):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize()
+        iters, relres = _lib.last_solve_stats(ctx)
+    ms = t0.elapsed_time(t1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    asm_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    sol_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    Am = A.view(n3, n3).t()
+    resid = float(torch.linalg.vector_norm(Am @ xm - b0) / torch.linalg.vector_norm(b0))
+    slip_err = float(torch.linalg.vector_norm(xm - x64) / torch.linalg.vector_norm(x64))
+    return {"solver": "FP32 LU (TF32 tensor-core trailing updates) preconditioning FP64 restarted GMRES",
+            "assembly": "FP64", "tol": MIXED_TOL, "ms_per_step": ms, "breakdown_ms": {"assembly": asm_ms,
+                                                                                      "solve": sol_ms},
+            "gmres_iterations": iters, "rel_residual": resid, "slip_rel_err_vs_fp64_lu": slip_err,
+            "step_speedup_vs_fp64": ms_fp64 / ms}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -250,6 +313,9 @@ def run_ours(args, rank, world, local_rank):
     Am = A.view(n3, n3).t()      # column-major storage
     resid = float(torch.linalg.vector_norm(Am @ x - b0) / torch.linalg.vector_norm(b0))
 
+    mixed = None if args.no_mixed else mixed_solve_timing(args, ctx, L, stream, step_asm_args=(
+        dN, dM, dP1, dP2, dP3, n, lam, hs), A=A, b0=b0, x64=x, ms_fp64=ms_step, world=world, dev=dev)
+
     # end to end through the host C ABI: pinned host inputs, slips back to host
     def pinned(a):
         t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
@@ -328,6 +394,7 @@ def run_ours(args, rank, world, local_rank):
                            "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                            "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
         "cpu_baseline": cpu,
+        "mixed": mixed,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -340,6 +407,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the same system")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="penny",
                     help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
     ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")

@@ -47,6 +47,7 @@ struct cad_ctx {
     cublasHandle_t blas = nullptr;
     cudaStream_t side_stream = nullptr;   // the LU's look-ahead trailing updates
     cublasHandle_t side_blas = nullptr;
+    LuGraphCache* graphs = nullptr;       // captured LU factorisations, replayed for repeated calls
     DevBuf buf[S_COUNT];
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed[2] = {false, false};
@@ -226,7 +227,8 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     if (int r = ensure(ctx, S_SYNC, mixed_sync_ints(n) * sizeof(int), &sync)) return r;
     if (int r = ensure(ctx, S_WORK, (size_t)n * sizeof(double), &work)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches};
+    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
+                        ctx->graphs};
     int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
@@ -295,7 +297,8 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches};
+    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
+                        ctx->graphs};
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
                                            (int*)info, kLuBlock, true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
@@ -368,6 +371,7 @@ int cad_init(int device, cad_ctx** out)
         cad_destroy(ctx);
         return CAD_ERR_CUDA;
     }
+    ctx->graphs = lu_graph_cache_create();
     *out = ctx;
     return CAD_OK;
 }
@@ -382,6 +386,7 @@ int cad_destroy(cad_ctx* ctx)
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
+    lu_graph_cache_destroy(ctx->graphs);
     if (ctx->blas) cublasDestroy(ctx->blas);
     if (ctx->side_blas) cublasDestroy(ctx->side_blas);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);

@@ -18,6 +18,7 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <vector>
@@ -34,7 +35,8 @@ constexpr int kLeafThreads = 512;
 constexpr int kLeafWarps = kLeafThreads / 32;
 constexpr int kMaxCluster = 16;
 constexpr int kLeafRegs = 32;   // row values one leaf thread keeps in registers (RPT * W)
-constexpr int kMaxSwaps = 256;  // pivots one row-swap launch applies (outer block width bound)
+constexpr int kMaxSwaps = 256;
+constexpr int kMaxDevices = 64;  // devices whose leaf cluster size is remembered  // pivots one row-swap launch applies (outer block width bound)
 
 // A pivot candidate as integers: |value| orders like the bit pattern of the
 // non-negative double, so hi = 1 + its high word (0: no candidate), lo = its
@@ -687,10 +689,21 @@ void allow_wide_clusters()
     cudaFuncSetAttribute(leaf_lu_kernel<T, W, RPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
-// largest leaf cluster the device co-schedules: 16 CTAs (non-portable) or 8
+// largest leaf cluster the device co-schedules: 16 CTAs (non-portable) or 8;
+// worked out once per device and precision
 template <typename T>
 int configure(Lu<T>& lu)
 {
+    static std::atomic<int> known[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = -1;
+    if (dev >= 0) {
+        const int c = known[dev].load();
+        if (c) {
+            lu.cluster = c;
+            return 0;
+        }
+    }
     allow_wide_clusters<T, 32, 1>();
     allow_wide_clusters<T, 16, 2>();
     allow_wide_clusters<T, 8, 4>();
@@ -711,7 +724,129 @@ int configure(Lu<T>& lu)
         cudaGetLastError();
         lu.cluster = 8;
     }
+    if (dev >= 0) known[dev].store(lu.cluster);
     return 0;
+}
+
+// ------------------------------------------------------------ graph cache
+struct LuGraphKey {
+    int type;   // sizeof(T)
+    const void *A, *B, *X;
+    int64_t n, lda, ldb, ldx;
+    int nrhs, nb;
+    const int *ipiv, *perm, *info;
+    bool factor, solve;
+    cudaStream_t main, side;
+    cublasHandle_t main_blas, side_blas;
+    bool same(const LuGraphKey& o) const
+    {
+        return type == o.type && A == o.A && B == o.B && X == o.X && n == o.n && lda == o.lda && ldb == o.ldb &&
+               ldx == o.ldx && nrhs == o.nrhs && nb == o.nb && ipiv == o.ipiv && perm == o.perm && info == o.info &&
+               factor == o.factor && solve == o.solve && main == o.main && side == o.side &&
+               main_blas == o.main_blas && side_blas == o.side_blas;
+    }
+};
+
+struct LuGraphEntry {
+    LuGraphKey key;
+    cudaGraphExec_t exec = nullptr;   // null: seen once, not captured yet
+    int64_t launches = 0;             // own kernels inside the graph
+    uint64_t stamp = 0;
+};
+
+}  // namespace
+
+struct LuGraphCache {
+    static constexpr int kMax = 8;
+    std::vector<LuGraphEntry> entries;
+    uint64_t clock = 0;
+
+    LuGraphEntry* find(const LuGraphKey& k)
+    {
+        for (auto& e : entries)
+            if (e.key.same(k)) {
+                e.stamp = ++clock;
+                return &e;
+            }
+        return nullptr;
+    }
+    LuGraphEntry* insert(const LuGraphKey& k)
+    {
+        if ((int)entries.size() >= kMax) {
+            size_t old = 0;
+            for (size_t i = 1; i < entries.size(); ++i)
+                if (entries[i].stamp < entries[old].stamp) old = i;
+            if (entries[old].exec) cudaGraphExecDestroy(entries[old].exec);
+            entries.erase(entries.begin() + (long)old);
+        }
+        LuGraphEntry e;
+        e.key = k;
+        e.stamp = ++clock;
+        entries.push_back(e);
+        return &entries.back();
+    }
+    ~LuGraphCache()
+    {
+        for (auto& e : entries)
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+    }
+};
+
+LuGraphCache* lu_graph_cache_create() { return new LuGraphCache(); }
+void lu_graph_cache_destroy(LuGraphCache* c) { delete c; }
+
+namespace {
+
+template <typename T>
+void lu_body(Lu<T>& lu, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X, int64_t ldx,
+             int* perm, int nb, bool factor, bool solve)
+{
+    if (factor) lu.factor(A, n, lda, nb);
+    lu.use(false);
+    if (solve && nrhs > 0) lu.solve(A, n, lda, B, ldb, nrhs, X, ldx, perm);
+}
+
+// Captures lu_body on the main stream (the side stream joins through a fork
+// event and is joined back before the capture ends) and instantiates it.
+template <typename T>
+cudaError_t lu_capture(Lu<T>& lu, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X, int64_t ldx,
+                       int* perm, int nb, bool factor, bool solve, cudaGraphExec_t* exec)
+{
+    *exec = nullptr;
+    const bool two = lu.side_st != lu.main_st;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (fork) cudaEventDestroy(fork);
+        return e;
+    }
+    e = cudaStreamBeginCapture(lu.main_st, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        if (two) {
+            lu.err = cudaEventRecord(fork, lu.main_st);
+            if (lu.ok()) lu.err = cudaStreamWaitEvent(lu.side_st, fork, 0);
+        }
+        if (lu.ok()) lu_body(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve);
+        if (two) {
+            const cudaError_t e1 = cudaEventRecord(join, lu.side_st);
+            const cudaError_t e2 = cudaStreamWaitEvent(lu.main_st, join, 0);
+            if (lu.err == cudaSuccess) lu.err = e1 != cudaSuccess ? e1 : e2;
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(lu.main_st, &graph);
+        if (lu.err == cudaSuccess) lu.err = ee;
+        if (lu.ok() && graph) lu.err = cudaGraphInstantiate(exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        e = lu.err;
+        if (!lu.ok() && *exec) {
+            cudaGraphExecDestroy(*exec);
+            *exec = nullptr;
+        }
+    }
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
+    return e;
 }
 
 }  // namespace
@@ -742,9 +877,33 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     if (cublasSetStream(lu.main_h, lu.main_st) != CUBLAS_STATUS_SUCCESS ||
         cublasSetStream(lu.side_h, lu.side_st) != CUBLAS_STATUS_SUCCESS)
         return LU_BLAS_ERROR;
-    if (factor) lu.factor(A, n, lda, nb);
-    lu.use(false);
-    if (solve && nrhs > 0) lu.solve(A, n, lda, B, ldb, nrhs, X, ldx, perm);
+    LuGraphEntry* entry = nullptr;
+    if (s.graphs && n > 0) {
+        const LuGraphKey key{(int)sizeof(T), A, B, X, n, lda, ldb, ldx, nrhs, nb, ipiv, perm, info, factor, solve,
+                             lu.main_st, lu.side_st, lu.main_h, lu.side_h};
+        entry = s.graphs->find(key);
+        if (entry && entry->exec) {   // replay
+            if (cudaGraphLaunch(entry->exec, lu.main_st) != cudaSuccess) return LU_CUDA_ERROR;
+            if (s.launches) *s.launches += entry->launches;
+            return LU_OK;
+        }
+        if (!entry) {                 // first sighting: eager, remembered
+            s.graphs->insert(key);
+            entry = nullptr;
+        }
+    }
+    if (entry) {                      // second sighting: capture, then launch
+        cudaGraphExec_t exec = nullptr;
+        lu_capture(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve, &exec);
+        if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;
+        if (lu.err != cudaSuccess || !exec) return LU_CUDA_ERROR;
+        entry->exec = exec;
+        entry->launches = lu.launches;
+        if (cudaGraphLaunch(exec, lu.main_st) != cudaSuccess) return LU_CUDA_ERROR;
+        if (s.launches) *s.launches += lu.launches;
+        return LU_OK;
+    }
+    lu_body(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve);
     if (s.launches) *s.launches += lu.launches;
     if (lu.err != cudaSuccess) return LU_CUDA_ERROR;
     if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;

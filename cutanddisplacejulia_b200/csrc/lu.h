@@ -9,6 +9,17 @@ namespace cad {
 
 enum { LU_OK = 0, LU_CUDA_ERROR = 1, LU_BLAS_ERROR = 2, LU_TOO_LARGE = 3 };
 
+// Executable CUDA graphs of lu_factor_solve calls, one per call signature
+// (precision, sizes, every pointer, streams and handles).  The factorisation
+// is thousands of dependent launches -- leaves, row swaps, triangular blocks,
+// GEMMs -- whose launch gaps dominate at moderate n; a signature seen a second
+// time is captured once and replayed from then on as a single graph launch.
+// The first call of a signature runs eagerly (no capture cost for one-off
+// calls).  Owned by one context (not thread-safe).
+struct LuGraphCache;
+LuGraphCache* lu_graph_cache_create();
+void lu_graph_cache_destroy(LuGraphCache* c);
+
 // Where the factorisation runs: the caller's stream (and a cuBLAS handle for
 // it), plus an optional side stream with its own handle for the look-ahead's
 // trailing updates (side_blas null: everything on the main stream).  The
@@ -18,7 +29,8 @@ struct LuStreams {
     cublasHandle_t main_blas;
     cudaStream_t side;
     cublasHandle_t side_blas;
-    int64_t* launches;   // if set, incremented by the number of own kernel launches
+    int64_t* launches;       // if set, incremented by the number of own kernel launches
+    LuGraphCache* graphs;    // if set, repeated call signatures replay a captured graph
 };
 
 // Factorise A (n x n, lda, column-major) in place (if factor) and / or solve

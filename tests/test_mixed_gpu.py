@@ -106,3 +106,15 @@ def test_set_solver_rejects_bad_arguments(cad):
     assert L.cad_set_solver(ctx, _lib.CAD_SOLVER_LU64, 1e-10, 200) == _lib.CAD_OK
     it, rr = ctypes.c_int(-1), ctypes.c_double(-1.0)
     assert L.cad_last_solve_stats(ctx, ctypes.byref(it), ctypes.byref(rr)) == _lib.CAD_OK
+
+
+def test_mixed_repeated_solves_same_size(cad):
+    # the FP32 factorisation of one call signature runs eagerly, then is
+    # captured as a CUDA graph and replayed; new contents on every call
+    rng = np.random.default_rng(77)
+    n = 900
+    for rep in range(4):
+        A = rng.standard_normal((n, n)) + 2.0 * np.sqrt(n) * np.eye(n)
+        B = rng.standard_normal((n, 1))
+        X = cad.solve(A, B, solver="mixed", tol=RESID_TOL)
+        assert _rel(X, np.linalg.solve(A, B)) <= SLIP_TOL, rep

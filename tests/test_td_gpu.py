@@ -207,3 +207,17 @@ def test_solve_singular_raises(cad):
     A[:, 7] = 0.0
     with pytest.raises(cad.CadError, match="singular"):
         cad.solve(A, np.ones(50))
+
+
+@pytest.mark.parametrize("n", [700, 2111])
+def test_repeated_solves_same_size(cad, n):
+    # one call signature four times (first eager, then captured as a CUDA
+    # graph, then replayed), with new matrix contents on every call
+    rng = np.random.default_rng(7 * n)
+    for rep in range(4):
+        A = rng.standard_normal((n, n))
+        B = rng.standard_normal((n, 2))
+        X = cad.solve(A, B)
+        Xo = np.linalg.solve(A, B)
+        cond = np.linalg.cond(A)
+        assert np.max(np.abs(X - Xo)) <= 1e-14 * cond * np.max(np.abs(Xo)), rep
