@@ -25,11 +25,13 @@ CAD_ERR_ARG = 9
 CAD_ERR_TOO_LARGE = 10
 CAD_SOLVER_LU64 = 0
 CAD_SOLVER_MIXED = 1
+CAD_ASSEMBLY_FP64 = 0
+CAD_ASSEMBLY_MIXED = 1
 
 # Every symbol include/cad_td.h declares (checked by the tests).
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
-    "cad_version", "cad_kernel_launches", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
+    "cad_version", "cad_kernel_launches", "cad_set_assembly", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
     "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
     "cad_solve_dev", "cad_td_sum_eval_noalloc",
 ]
@@ -74,6 +76,7 @@ def load():
     L.cad_kernel_launches.argtypes = [P]
     L.cad_kernel_launches.restype = I64
     L.cad_set_solver.argtypes = [P, INT, D, INT]
+    L.cad_set_assembly.argtypes = [P, INT, D]
     L.cad_last_solve_stats.argtypes = [P, ctypes.POINTER(INT), ctypes.POINTER(D)]
     L.cad_fp64_fma_probe.argtypes = [P, I64, ctypes.POINTER(D)]
     td = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, D, INT, INT, INT, P, P]
@@ -137,6 +140,26 @@ class solver_mode:
 
     def __exit__(self, *exc):
         load().cad_set_solver(self.ctx, CAD_SOLVER_LU64, 1e-10, 200)
+        return False
+
+
+class assembly_mode:
+    """Context manager selecting the system-matrix assembly precision of `ctx`
+    ("fp64": every pair in FP64; "mixed": far-field pairs in FP32, pairs within
+    `near_factor` mean edge lengths in FP64), restoring FP64 afterwards."""
+
+    def __init__(self, ctx, assembly="fp64", near_factor=3.0):
+        modes = {"fp64": CAD_ASSEMBLY_FP64, "mixed": CAD_ASSEMBLY_MIXED}
+        if assembly not in modes:
+            raise ValueError("assembly must be 'fp64' or 'mixed'")
+        self.ctx, self.mode, self.near_factor = ctx, modes[assembly], float(near_factor)
+
+    def __enter__(self):
+        check(load().cad_set_assembly(self.ctx, self.mode, self.near_factor), self.ctx)
+        return self
+
+    def __exit__(self, *exc):
+        load().cad_set_assembly(self.ctx, CAD_ASSEMBLY_FP64, 3.0)
         return False
 
 

@@ -91,11 +91,13 @@ def CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, nu, G, 
 
 
 def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag, BoundaryConditions, FixedEls,
-                     device=0, solver="lu64", tol=1e-10, max_iter=200):
+                     device=0, solver="lu64", tol=1e-10, max_iter=200, assembly="fp64", near_factor=3.0):
     """Plain (frictionless) slip solve: returns (Dn, Dss, Dds, A, b).
 
     solver="lu64" solves A \\ b by FP64 LU as src/SlipCalculator3D.jl:22 does;
-    solver="mixed" uses the FP32/TF32 LU + FP64 GMRES path to relative residual tol."""
+    solver="mixed" uses the FP32/TF32 LU + FP64 GMRES path to relative residual tol.
+    assembly="mixed" evaluates far-field pairs in FP32 and pairs within
+    near_factor mean edge lengths in FP64 (assembly="fp64": all in FP64)."""
     P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
     N = P1.shape[0]
     nrm = _tri(FaceNormalVector)
@@ -110,7 +112,7 @@ def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
     A = np.zeros((3 * N, 3 * N), order="F")
     b = np.zeros(3 * N)
     ctx = _lib.context(device)
-    with _lib.solver_mode(ctx, solver, tol, max_iter):
+    with _lib.solver_mode(ctx, solver, tol, max_iter), _lib.assembly_mode(ctx, assembly, near_factor):
         rc = _lib.load().cad_slip_calculator(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu),
                                              float(G), float(lam), mid.ctypes.data, nrm.ctypes.data, int(HSFlag),
                                              Tn.ctypes.data, Tss.ctypes.data, Tds.ctypes.data, Dn.ctypes.data,

@@ -28,7 +28,7 @@ namespace {
 
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
-    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_COUNT
+    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -49,10 +49,14 @@ struct cad_ctx {
     cublasHandle_t side_blas = nullptr;
     LuGraphCache* graphs = nullptr;       // captured LU factorisations, replayed for repeated calls
     DevBuf buf[S_COUNT];
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    bool timed[2] = {false, false};
+    // event pairs: [0,1] TD pair kernel, [2,3] dense solve, [2,4] its
+    // factorisation (mixed solver: cast + FP32 LU + block inverses)
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool timed[3] = {false, false, false};
     int64_t launches = 0;   // own kernel launches issued through this context
     int solver = CAD_SOLVER_LU64;   // cad_set_solver
+    int assembly = CAD_ASSEMBLY_FP64;   // cad_set_assembly
+    double near_factor = 3.0;
     double tol = 1e-10;
     int max_iter = 200;
     int last_iters = 0;           // of the last mixed solve (all right-hand sides)
@@ -197,6 +201,17 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
     a.tri_chunk = pick_chunk(N, N, false);
     a.lambda = lambda; a.G = G; a.dirs = (const double*)dirs;
     a.trac = trac_out; a.A = A; a.lda = lda;
+    if (out_kind == OUT_AMAT && ctx->assembly == CAD_ASSEMBLY_MIXED) {
+        void *tri32, *near;
+        if (int r = ensure(ctx, S_TRI32, (size_t)N * tri_record_bytes_f32(), &tri32)) return r;
+        if (int r = ensure(ctx, S_NEAR, (size_t)(3 * N + 1) * sizeof(double), &near)) return r;
+        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        CK(launch_assemble_mixed(a, hs == 1, P1, P2, P3, ctx->near_factor, tri32, (double*)near, ctx->stream,
+                                 &ctx->launches));
+        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        ctx->timed[0] = true;
+        return CAD_OK;
+    }
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     ++ctx->launches;
     CK(launch_td_pairs(a, out_kind, hs == 1, true, false, ctx->stream));
@@ -229,9 +244,12 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
                         ctx->graphs};
+    ctx->timed[1] = ctx->timed[2] = false;
     int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
+    CK(cudaEventRecord(ctx->ev[4], ctx->stream));
+    ctx->timed[2] = true;
     if (int r = read_info(ctx, info_out)) return r;
     if (*info_out > 0) return CAD_OK;
     double* V = (double*)kry;
@@ -297,6 +315,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    ctx->timed[1] = ctx->timed[2] = false;
     const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
                         ctx->graphs};
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
@@ -352,8 +371,12 @@ int cad_init(int device, cad_ctx** out)
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return CAD_ERR_CUDA;
     cad_ctx* ctx = new cad_ctx();
     ctx->device = device;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) !=
-                                                   cudaSuccess) {
+    // the context stream carries the LU's latency-bound panel chain: highest
+    // priority, so its small launches get SMs ahead of the side stream's
+    // trailing-update GEMMs (lowest priority)
+    int prio_low = 0, prio_high = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->own_stream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
         delete ctx;
         return CAD_ERR_CUDA;
     }
@@ -365,7 +388,7 @@ int cad_init(int device, cad_ctx** out)
         }
     if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS ||
         cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
-        cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
         cublasCreate(&ctx->side_blas) != CUBLAS_STATUS_SUCCESS ||
         cublasSetStream(ctx->side_blas, ctx->side_stream) != CUBLAS_STATUS_SUCCESS) {
         cad_destroy(ctx);
@@ -399,6 +422,16 @@ const char* cad_last_error(const cad_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 int64_t cad_kernel_launches(const cad_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if ((mode != CAD_ASSEMBLY_FP64 && mode != CAD_ASSEMBLY_MIXED) || !(near_factor >= 0.0))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->assembly = mode;
+    ctx->near_factor = near_factor;
+    return CAD_OK;
+}
+
 int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
 {
     if (!ctx) return CAD_ERR_ARG;
@@ -431,11 +464,12 @@ void* cad_get_stream(const cad_ctx* ctx) { return ctx ? (void*)ctx->stream : nul
 
 double cad_last_time_ms(const cad_ctx* ctx, int which)
 {
-    if (!ctx || which < 0 || which > 1 || !ctx->timed[which]) return -1.0;
+    if (!ctx || which < 0 || which > 2 || !ctx->timed[which]) return -1.0;
+    static const int from[3] = {0, 2, 2}, to[3] = {1, 3, 4};
     float ms = 0.f;
-    if (cudaEventSynchronize(ctx->ev[2 * which + 1]) != cudaSuccess) return -1.0;
-    if (cudaEventElapsedTime(&ms, ctx->ev[2 * which], ctx->ev[2 * which + 1]) != cudaSuccess) return -1.0;
-    return (double)ms;
+    if (cudaEventSynchronize(ctx->ev[to[which]]) != cudaSuccess) return -1.0;
+    if (cudaEventElapsedTime(&ms, ctx->ev[from[which]], ctx->ev[to[which]]) != cudaSuccess) return -1.0;
+    return ms;
 }
 
 // ------------------------------------------------------------------- TD

@@ -9,7 +9,10 @@ What the generator does to each function:
   3. replaces x**-k by (1/x)**k with one reciprocal per distinct denominator
      (a reciprocal square root where the denominator is a square root);
   4. runs sympy common-subexpression elimination over all outputs together;
-  5. prints straight-line FP64 code (integer powers as products).
+  5. prints straight-line code (integer powers as products): the
+     per-dislocation setup in FP64, the per-pair body as a template on its
+     arithmetic type R (FP64, or FP32 for far-field pairs), with every literal
+     and math function in R.
 
 The result computes the same closed-form mathematics as the reference; only
 the association of operations differs.  Usage:
@@ -143,28 +146,31 @@ def reciprocals(exprs, sqrt_defs):
 
 class Printer(C99CodePrinter):
     struct_syms = set()
+    pair = False   # printing a per-pair body (literals and functions in R)
+
+    def lit(self, v):
+        return ("R(%r)" % v) if self.pair else repr(v)
 
     def _print_Symbol(self, s):
         if s == PI:
-            return "M_PI"
+            return "R(M_PI)" if self.pair else "M_PI"
         if s in self.struct_syms:
             return "k." + s.name
         return s.name
 
     def _print_Float(self, f):
-        v = float(f)
-        return repr(v)
+        return self.lit(float(f))
 
     def _print_Rational(self, r):
-        return repr(float(r))
+        return self.lit(float(r))
 
     def _print_Integer(self, i):
-        return repr(float(i))
+        return self.lit(float(i))
 
     def _print_Pow(self, e):
         b, n = e.base, e.exp
         if n == sp.Rational(1, 2):
-            return "sqrt(%s)" % self._print(b)
+            return ("cad_sqrt(%s)" if self.pair else "sqrt(%s)") % self._print(b)
         assert n.is_Integer, e
         if n < 0:   # only in per-dislocation setup code
             return "(1.0/%s)" % self._print(sp.Pow(b, -n, evaluate=False))
@@ -179,16 +185,16 @@ class Printer(C99CodePrinter):
         return "((%s > %s) ? (%s) : (%s))" % (a, b, b, a)
 
     def _print_rcp(self, e):
-        return "(1.0/(%s))" % self._print(e.args[0])
+        return "(%s/(%s))" % (self.lit(1.0), self._print(e.args[0]))
 
     def _print_rsq(self, e):
-        return "rsqrt(%s)" % self._print(e.args[0])
+        return "cad_rsqrt(%s)" % self._print(e.args[0])
 
     def _print_log(self, e):
-        return "log(%s)" % self._print(e.args[0])
+        return ("cad_log(%s)" if self.pair else "log(%s)") % self._print(e.args[0])
 
     def _print_atan(self, e):
-        return "atan(%s)" % self._print(e.args[0])
+        return ("cad_atan(%s)" if self.pair else "atan(%s)") % self._print(e.args[0])
 
 
 def count_ops(exprs):
@@ -285,13 +291,14 @@ def emit(fname, groups, P, suffixes):
     setup_stmts = list(g0["setup_rep"]) + list(zip(g0["setup_syms"], g0["setup_red"]))
     kname = fname + "_k"
     L.append("// %s: generated from the %s table (reference %s)." % (fname, fname, T["src"]))
+    L.append("template <typename T>")
     L.append("struct %s {" % kname)
     for s_ in used_consts:
-        L.append("    double %s;" % s_.name)
+        L.append("    T %s;" % s_.name)
     L.append("};")
     L.append("")
     args = ", ".join("double %s" % n for n in g0["const_in"])
-    L.append("CAD_HD void %s_setup(%s, %s& k)" % (fname, args, kname))
+    L.append("CAD_HD void %s_setup(%s, %s<double>& k)" % (fname, args, kname))
     L.append("{")
     deps = {s_: e_.free_symbols for s_, e_ in setup_stmts}
     live = set()
@@ -309,19 +316,22 @@ def emit(fname, groups, P, suffixes):
     L.append("}")
     L.append("")
     for g, suf in zip(groups, suffixes):
-        pargs = ", ".join("double %s" % n for n in g["pair_in"])
+        pargs = ", ".join("R %s" % n for n in g["pair_in"])
         idx = g["out_idx"] or list(range(len(g["outs"])))
         L.append("// outputs %s of %s" % (list(idx), fname))
-        L.append("CAD_HD void %s%s(const %s& k, %s, double* __restrict__ o)" % (
+        L.append("template <typename R>")
+        L.append("CAD_HD void %s%s(const %s<R>& k, %s, R* __restrict__ o)" % (
             fname, suf, kname, pargs))
         L.append("{")
         P.struct_syms = set(used_consts)
+        P.pair = True
         pair_in = {sp.Symbol(n, real=True) for n in g["pair_in"]}
         for s_, e_ in topo(pair_statements(g), set(used_consts) | pair_in | {PI}):
-            L.append("    const double %s = %s;" % (s_.name, P.doprint(e_)))
+            L.append("    const R %s = %s;" % (s_.name, P.doprint(e_)))
         for i, o in enumerate(g["outs"]):
             L.append("    o[%d] = %s;" % (i, P.doprint(o)))
         P.struct_syms = set()
+        P.pair = False
         L.append("}")
         L.append("")
     return L
@@ -341,14 +351,15 @@ def main():
     out = [
         "// GENERATED by csrc/gen/gen_device.py from csrc/gen/tde_formulas.py -- do not edit.",
         "//",
-        "// FP64 device code for the closed-form angular-dislocation terms of the",
+        "// Device code for the closed-form angular-dislocation terms of the",
         "// triangular dislocation solution (Nikkhoo & Walter 2015):",
         "//   ang_dis_disp, ang_dis_strain            full-space angular dislocation",
         "//   ang_dis_disp_fsc, ang_dis_strain_fsc    half-space free-surface correction",
         "// Each function is split into a per-dislocation setup (constants reused for",
         "// every observation point) and a per-pair body with one reciprocal per",
-        "// distinct denominator.  Output order equals the return order of the",
-        "// reference functions.",
+        "// distinct denominator.  Setup is FP64; the per-pair bodies are templates",
+        "// on their arithmetic type R (double, or float for far-field pairs).",
+        "// Output order equals the return order of the reference functions.",
         "#pragma once",
         "#include <math.h>",
         "#ifdef __CUDACC__",
@@ -363,7 +374,18 @@ def main():
         "#ifndef __CUDACC__",
         "// plain C++ build of the device code (used only to test it on a CPU)",
         "inline double rsqrt(double x) { return 1.0 / sqrt(x); }",
+        "inline float rsqrtf(float x) { return 1.0f / sqrtf(x); }",
         "#endif",
+        "",
+        "// math functions in the pair bodies' arithmetic type",
+        "CAD_HD double cad_sqrt(double x) { return sqrt(x); }",
+        "CAD_HD float cad_sqrt(float x) { return sqrtf(x); }",
+        "CAD_HD double cad_rsqrt(double x) { return rsqrt(x); }",
+        "CAD_HD float cad_rsqrt(float x) { return rsqrtf(x); }",
+        "CAD_HD double cad_log(double x) { return log(x); }",
+        "CAD_HD float cad_log(float x) { return logf(x); }",
+        "CAD_HD double cad_atan(double x) { return atan(x); }",
+        "CAD_HD float cad_atan(float x) { return atanf(x); }",
         "",
     ]
     stats = {}

@@ -28,7 +28,7 @@ namespace cad {
 namespace {
 
 constexpr int kRB = 128;            // row block of the triangular solves
-constexpr int kChainThreads = 256;  // two threads per row: halves of each 128-column block
+constexpr int kChainThreads = 512;  // four threads per row: quarters of each 128-column block
 constexpr long kSpinLimit = 1L << 22;
 
 // B (n x n, leading dimension n) = (float) A (n x n, lda); columns strided over grid.y
@@ -105,36 +105,26 @@ __device__ __forceinline__ void st_release(int* p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Partial product of this thread's row with half hh of a kRB-column block.
-__device__ __forceinline__ float row_half_dot(const float* __restrict__ a, int64_t lda, int ncols,
-                                              const float* __restrict__ s_x)
-{
-    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-    int c = 0;
-    for (; c + 4 <= ncols; c += 4) {
-        p0 = fmaf(a[(int64_t)c * lda], s_x[c], p0);
-        p1 = fmaf(a[(int64_t)(c + 1) * lda], s_x[c + 1], p1);
-        p2 = fmaf(a[(int64_t)(c + 2) * lda], s_x[c + 2], p2);
-        p3 = fmaf(a[(int64_t)(c + 3) * lda], s_x[c + 3], p3);
-    }
-    for (; c < ncols; ++c) p0 = fmaf(a[(int64_t)c * lda], s_x[c], p0);
-    return (p0 + p1) + (p2 + p3);
-}
-
 // One triangle of M^-1 v with M = P^T L U in FP32.  Lower (UPPER false):
 // y = L^-1 (P v), v FP64 gathered through perm.  Upper: x = U^-1 y, written
 // as FP64 to out.  x32 holds the solved blocks for the other CTAs; flags[i]
-// is set once block i is published; ticket orders the CTAs.
+// is set once block i is published; ticket orders the CTAs (a CTA waits only
+// on blocks whose CTAs took earlier tickets, so they are running).
+// Thread (q, r): row r of the CTA's 128-row block, column quarter q of every
+// 128-column block.  The quarter's 32 values of the next block are loaded
+// before its flag is awaited, so the memory latency overlaps the wait.
 template <bool UPPER>
 __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
     const float* __restrict__ A, int64_t lda, int n, int nblk, const float* __restrict__ Dinv,
     const double* __restrict__ v_in, const int* __restrict__ perm, const float* y_in, float* x32,
     double* __restrict__ out, int* flags, int* ticket, int* fail)
 {
+    constexpr int kQ = kChainThreads / kRB;   // column quarters
+    constexpr int kC = kRB / kQ;              // columns per quarter
     __shared__ float s_x[kRB];
-    __shared__ float s_part[2][kRB];
+    __shared__ float s_part[kQ][kRB];
     __shared__ int s_t;
-    const int tid = threadIdx.x, rr = tid & (kRB - 1), hh = tid >> 7;
+    const int tid = threadIdx.x, rr = tid % kRB, q = tid / kRB;
     if (tid == 0) s_t = atomicAdd(ticket, 1);
     __syncthreads();
     const int t = s_t;
@@ -142,10 +132,15 @@ __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
     const int r0 = i * kRB;
     const int rows = n - r0 < kRB ? n - r0 : kRB;
     const int row = r0 + rr;
+    const bool rok = rr < rows;
     float acc = 0.f;
-    if (hh == 0 && rr < rows) acc = UPPER ? __ldcg(y_in + row) : (float)v_in[perm[row]];
+    if (q == 0 && rok) acc = UPPER ? __ldcg(y_in + row) : (float)v_in[perm[row]];
     for (int s = 0; s < t; ++s) {
         const int j = UPPER ? nblk - 1 - s : s;
+        const int c0 = j * kRB + q * kC;
+        float a[kC];
+#pragma unroll
+        for (int c = 0; c < kC; ++c) a[c] = (rok && c0 + c < n) ? __ldg(A + row + (int64_t)(c0 + c) * lda) : 0.f;
         if (tid == 0) {
             long spins = 0;
             while (ld_acquire(flags + j) == 0) {
@@ -153,30 +148,43 @@ __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
                     atomicExch(fail, 1);
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         __syncthreads();
-        const int c0 = j * kRB;
-        const int ncb = n - c0 < kRB ? n - c0 : kRB;
-        if (tid < kRB) s_x[tid] = tid < ncb ? __ldcg(x32 + c0 + tid) : 0.f;
+        if (tid < kRB) s_x[tid] = j * kRB + tid < n ? __ldcg(x32 + j * kRB + tid) : 0.f;
         __syncthreads();
-        const int half0 = hh * (kRB / 2);
-        int nc = ncb - half0;
-        nc = nc < 0 ? 0 : (nc > kRB / 2 ? kRB / 2 : nc);
-        if (rr < rows && nc > 0) acc -= row_half_dot(A + row + (int64_t)(c0 + half0) * lda, lda, nc, s_x + half0);
+        float p0 = 0.f, p1 = 0.f;
+#pragma unroll
+        for (int c = 0; c < kC; c += 2) {
+            p0 = fmaf(a[c], s_x[q * kC + c], p0);
+            p1 = fmaf(a[c + 1], s_x[q * kC + c + 1], p1);
+        }
+        acc -= p0 + p1;
     }
     // right-hand side of the diagonal block, then its explicit inverse
-    s_part[hh][rr] = acc;
+    s_part[q][rr] = acc;
     __syncthreads();
-    if (tid < kRB) s_x[tid] = s_part[0][tid] + s_part[1][tid];
+    if (tid < kRB) {
+        float sum = 0.f;
+#pragma unroll
+        for (int k = 0; k < kQ; ++k) sum += s_part[k][tid];
+        s_x[tid] = sum;
+    }
     __syncthreads();
-    const float* d = Dinv + (int64_t)i * kRB * kRB + rr + (int64_t)(hh * (kRB / 2)) * kRB;
-    const float p = row_half_dot(d, kRB, kRB / 2, s_x + hh * (kRB / 2));
-    s_part[hh][rr] = p;
+    const float* d = Dinv + (int64_t)i * kRB * kRB + rr + (int64_t)(q * kC) * kRB;
+    float p0 = 0.f, p1 = 0.f;
+#pragma unroll
+    for (int c = 0; c < kC; c += 2) {
+        p0 = fmaf(d[(int64_t)c * kRB], s_x[q * kC + c], p0);
+        p1 = fmaf(d[(int64_t)(c + 1) * kRB], s_x[q * kC + c + 1], p1);
+    }
+    s_part[q][rr] = p0 + p1;
     __syncthreads();
     if (tid < rows) {
-        const float x = s_part[0][tid] + s_part[1][tid];
+        float x = 0.f;
+#pragma unroll
+        for (int k = 0; k < kQ; ++k) x += s_part[k][tid];
         x32[r0 + tid] = x;
         if (UPPER) out[r0 + tid] = (double)x;
     }

@@ -27,56 +27,70 @@
 namespace cad {
 
 // ------------------------------------------------------------------ records
-struct AngDis {          // one angular dislocation of a TD frame (configuration I)
-    double cosT, sinT;   // side-vector z and y components; configuration II negates both
-    double tv1, tv2;     // vertex y, z in TDCS
-    double sinADE1;      // sin(alpha - pi) / (8 pi (1 - nu))
-    ang_dis_strain_k ks;
-    ang_dis_disp_k kd;
+// Every field of a record has the record's type T, so a record is a plain
+// array of T: the FP32 copy used for far-field pairs is an element-wise
+// conversion of the FP64 record (flags are stored as 0 / 1 values).
+template <typename T>
+struct AngDisT {         // one angular dislocation of a TD frame (configuration I)
+    T cosT, sinT;        // side-vector z and y components; configuration II negates both
+    T tv1, tv2;          // vertex y, z in TDCS
+    T sinADE1;           // sin(alpha - pi) / (8 pi (1 - nu))
+    ang_dis_strain_k<T> ks;
+    ang_dis_disp_k<T> kd;
 };
 
-struct Frame {           // a TD (real or image) in its own coordinate system
-    double P2[3];
-    double Vn[3], Vs[3], Vd[3];
-    double p1y, p1z, p3y, p3z;          // TDCS (y, z) of P1 and P3; P2 is the origin
-    double t23y, t32x, t31y, t13x, base; // configuration-test constants
-    AngDis v[3];                         // at P1 (side -e13), P2 (e12), P3 (e23)
-    int flat;                            // all vertex z exactly 0
-    int pad_;
+template <typename T>
+struct FrameT {          // a TD (real or image) in its own coordinate system
+    T P2[3];
+    T P2lo[3];           // FP32 records: P2 - (double)(float)P2 (0 in FP64 records)
+    T Vn[3], Vs[3], Vd[3];
+    T p1y, p1z, p3y, p3z;           // TDCS (y, z) of P1 and P3; P2 is the origin
+    T t23y, t32x, t31y, t13x, base; // configuration-test constants
+    AngDisT<T> v[3];                // at P1 (side -e13), P2 (e12), P3 (e23)
+    T flat;                         // 1: all vertex z exactly 0
 };
 
-struct FscSide {         // one TD side PA -> PB of the free-surface correction
-    int skip;
-    int pad_;
-    double ey1[3], ey2[3], ey3[3];
-    double PA[3];
-    double y1B, y2B, y3B;
-    double beta;
-    double cs[3][3];     // ADCS slip of each unit mode m (Dn, Dss, Dds), component g
-    double cd[3][3];     // the same scaled by 1 / (4 pi (1 - nu)) for displacements
-    ang_dis_strain_fsc_k ks[2][2];   // [0: beta, 1: pi - beta][0: at PA, 1: at PB]
-    ang_dis_disp_fsc_k kd[2][2];     // [0: beta, 1: beta - pi][0: at PA, 1: at PB]
+template <typename T>
+struct FscSideT {        // one TD side PA -> PB of the free-surface correction
+    T skip;              // 1: the side adds nothing (beta test)
+    T ey1[3], ey2[3], ey3[3];
+    T PA[3];
+    T PAlo[3];           // as P2lo
+    T y1B, y2B, y3B;
+    T beta;
+    T cs[3][3];          // ADCS slip of each unit mode m (Dn, Dss, Dds), component g
+    T cd[3][3];          // the same scaled by 1 / (4 pi (1 - nu)) for displacements
+    ang_dis_strain_fsc_k<T> ks[2][2];   // [0: beta, 1: pi - beta][0: at PA, 1: at PB]
+    ang_dis_disp_fsc_k<T> kd[2][2];     // [0: beta, 1: beta - pi][0: at PA, 1: at PB]
 };
 
-struct TriDev {
-    double Dss, Dds, Dn;
-    double K8;           // 1 / (8 pi (1 - nu))
-    Frame real;
-    Frame image;
-    FscSide side[3];
+template <typename T>
+struct TriDevT {
+    T Dss, Dds, Dn;
+    T K8;                // 1 / (8 pi (1 - nu))
+    FrameT<T> real;
+    FrameT<T> image;
+    FscSideT<T> side[3];
 };
 
-// Number of doubles of a TriDev needed by a full-space-only kernel.
+using AngDis = AngDisT<double>;
+using Frame = FrameT<double>;
+using FscSide = FscSideT<double>;
+using TriDev = TriDevT<double>;
+static_assert(sizeof(TriDevT<float>) * 2 == sizeof(TriDevT<double>), "records are plain arrays of their type");
+
+// Number of values of a record needed by a full-space-only kernel / in all.
 constexpr int kTriWordsFS = (int)(offsetof(TriDev, image) / sizeof(double));
 constexpr int kTriWordsHS = (int)(sizeof(TriDev) / sizeof(double));
 
 // ------------------------------------------------------------------ helpers
-CAD_HD double qnan()
+template <typename R>
+CAD_HD R qnan()
 {
 #ifdef __CUDA_ARCH__
-    return __longlong_as_double(0x7ff8000000000000LL);
+    return (R)__longlong_as_double(0x7ff8000000000000LL);
 #else
-    return __builtin_nan("");
+    return (R)__builtin_nan("");
 #endif
 }
 
@@ -111,21 +125,71 @@ CAD_HD double sub_rn(double a, double b)
     return a - b;
 #endif
 }
-CAD_HD double dot3_rn(double a0, double a1, double a2, double b0, double b1, double b2)
+CAD_HD float mul_rn(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    float r = a * b;
+#if !defined(__CUDACC__) && defined(__GNUC__) && defined(__x86_64__)
+    asm("" : "+x"(r));
+#endif
+    return r;
+#endif
+}
+CAD_HD float add_rn(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+CAD_HD float sub_rn(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+template <typename R>
+CAD_HD R dot3_rn(R a0, R a1, R a2, R b0, R b1, R b2)
 {
     return add_rn(add_rn(mul_rn(a0, b0), mul_rn(a1, b1)), mul_rn(a2, b2));
+}
+CAD_HD double cad_atan2(double y, double x) { return atan2(y, x); }
+CAD_HD float cad_atan2(float y, float x) { return atan2f(y, x); }
+
+// Observation point minus a record origin, in R.  FP64 records subtract
+// unfused; FP32 records subtract their origin's two float parts in FP64 and
+// round the difference once.
+template <typename R>
+CAD_HD void rel_origin(const R* o, const R* olo, double X, double Y, double Z, R& dX, R& dY, R& dZ)
+{
+    if constexpr (sizeof(R) == sizeof(double)) {
+        dX = sub_rn(X, (double)o[0]);
+        dY = sub_rn(Y, (double)o[1]);
+        dZ = sub_rn(Z, (double)o[2]);
+    } else {
+        dX = (R)((X - (double)o[0]) - (double)olo[0]);
+        dY = (R)((Y - (double)o[1]) - (double)olo[1]);
+        dZ = (R)((Z - (double)o[2]) - (double)olo[2]);
+    }
 }
 
 // Symmetric tensor t (xx,yy,zz,xy,xz,yz) -> A-rotated, A column-major 3x3
 // (TensorTransformation3D! form).
-CAD_HD void tensor_rot(double t[6], const double* A)
+template <typename R>
+CAD_HD void tensor_rot(R t[6], const R* A)
 {
-    const double Txx = t[0], Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
-    t[0] = A[0] * A[0] * Txx + 2.0 * A[0] * A[3] * Txy + 2.0 * A[0] * A[6] * Txz + 2.0 * A[3] * A[6] * Tyz +
+    const R two = R(2.0);
+    const R Txx = t[0], Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
+    t[0] = A[0] * A[0] * Txx + two * A[0] * A[3] * Txy + two * A[0] * A[6] * Txz + two * A[3] * A[6] * Tyz +
            A[3] * A[3] * Tyy + A[6] * A[6] * Tzz;
-    t[1] = A[1] * A[1] * Txx + 2.0 * A[1] * A[4] * Txy + 2.0 * A[1] * A[7] * Txz + 2.0 * A[4] * A[7] * Tyz +
+    t[1] = A[1] * A[1] * Txx + two * A[1] * A[4] * Txy + two * A[1] * A[7] * Txz + two * A[4] * A[7] * Tyz +
            A[4] * A[4] * Tyy + A[7] * A[7] * Tzz;
-    t[2] = A[2] * A[2] * Txx + 2.0 * A[2] * A[5] * Txy + 2.0 * A[2] * A[8] * Txz + 2.0 * A[5] * A[8] * Tyz +
+    t[2] = A[2] * A[2] * Txx + two * A[2] * A[5] * Txy + two * A[2] * A[8] * Txz + two * A[5] * A[8] * Tyz +
            A[5] * A[5] * Tyy + A[8] * A[8] * Tzz;
     t[3] = A[0] * A[1] * Txx + (A[0] * A[4] + A[1] * A[3]) * Txy + (A[0] * A[7] + A[1] * A[6]) * Txz +
            (A[3] * A[7] + A[4] * A[6]) * Tyz + A[3] * A[4] * Tyy + A[6] * A[7] * Tzz;
@@ -137,34 +201,37 @@ CAD_HD void tensor_rot(double t[6], const double* A)
 
 // Rotation of a tensor about the TDCS x axis by the side angle (the B matrix
 // [1 0 0; 0 c -s; 0 s c] of TDSetupS, stored column-major), written out.
-CAD_HD void tensor_rot_x(double t[6], double c, double s)
+template <typename R>
+CAD_HD void tensor_rot_x(R t[6], R c, R s)
 {
-    const double Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
-    const double cc = c * c, ss = s * s, cs = c * s;
-    t[1] = 2.0 * cs * Tyz + cc * Tyy + ss * Tzz;
-    t[2] = -2.0 * cs * Tyz + ss * Tyy + cc * Tzz;
+    const R Tyy = t[1], Tzz = t[2], Txy = t[3], Txz = t[4], Tyz = t[5];
+    const R cc = c * c, ss = s * s, cs = c * s;
+    t[1] = R(2.0) * cs * Tyz + cc * Tyy + ss * Tzz;
+    t[2] = R(-2.0) * cs * Tyz + ss * Tyy + cc * Tzz;
     t[3] = c * Txy + s * Txz;
     t[4] = -s * Txy + c * Txz;
     t[5] = (cc - ss) * Tyz + cs * (Tzz - Tyy);
 }
 
 // Observation point -> TDCS of frame f.
-CAD_HD void to_tdcs(const Frame& f, double X, double Y, double Z, double& x, double& y,
-                                        double& z)
+template <typename R>
+CAD_HD void to_tdcs(const FrameT<R>& f, double X, double Y, double Z, R& x, R& y, R& z)
 {
-    const double dX = sub_rn(X, f.P2[0]), dY = sub_rn(Y, f.P2[1]), dZ = sub_rn(Z, f.P2[2]);
+    R dX, dY, dZ;
+    rel_origin(f.P2, f.P2lo, X, Y, Z, dX, dY, dZ);
     x = dot3_rn(f.Vn[0], f.Vn[1], f.Vn[2], dX, dY, dZ);
     y = dot3_rn(f.Vs[0], f.Vs[1], f.Vs[2], dX, dY, dZ);
     z = dot3_rn(f.Vd[0], f.Vd[1], f.Vd[2], dX, dY, dZ);
 }
 
 // Artefact-free configuration: +1 (I), -1 (II), 0 (on a side, in the TD plane).
-CAD_HD int trimode(const Frame& f, double x, double y, double z)
+template <typename R>
+CAD_HD int trimode(const FrameT<R>& f, R x, R y, R z)
 {
-    const double dy = sub_rn(y, f.p3y), dz = sub_rn(z, f.p3z);
-    const double a = add_rn(mul_rn(f.t23y, dy), mul_rn(f.t32x, dz)) / f.base;
-    const double b = add_rn(mul_rn(f.t31y, dy), mul_rn(f.t13x, dz)) / f.base;
-    const double c = sub_rn(sub_rn(1.0, a), b);
+    const R dy = sub_rn(y, f.p3y), dz = sub_rn(z, f.p3z);
+    const R a = add_rn(mul_rn(f.t23y, dy), mul_rn(f.t32x, dz)) / f.base;
+    const R b = add_rn(mul_rn(f.t31y, dy), mul_rn(f.t13x, dz)) / f.base;
+    const R c = sub_rn(sub_rn(R(1.0), a), b);
     bool casen = false, casez = false;
     if (a <= 0.0 && b > c && c > a) casen = true;
     else if (b <= 0.0 && c > a && a > b) casen = true;
@@ -179,31 +246,31 @@ CAD_HD int trimode(const Frame& f, double x, double y, double z)
 // ------------------------------------------------------ full-space strain
 // One angular dislocation's contribution for all three unit modes, added to
 // E[m][k] (TDCS).  sgn = +1 for configuration I, -1 for II.
-CAD_HD void ad_strain(const AngDis& v, double sgn, double x, double y, double z, double Dss,
-                                          double Dds, double Dn, double K8, double E[3][6])
+template <typename R>
+CAD_HD void ad_strain(const AngDisT<R>& v, R sgn, R x, R y, R z, R Dss, R Dds, R Dn, R K8, R E[3][6])
 {
-    const double CosT = sgn * v.cosT, SinT = sgn * v.sinT;
-    const double dy = y - v.tv1, dz = z - v.tv2;
-    const double Yr = CosT * dy - SinT * dz;
-    const double Zr = SinT * dy + CosT * dz;
-    double o[21];
+    const R CosT = sgn * v.cosT, SinT = sgn * v.sinT;
+    const R dy = y - v.tv1, dz = z - v.tv2;
+    const R Yr = CosT * dy - SinT * dz;
+    const R Zr = SinT * dy + CosT * dz;
+    R o[21];
     ang_dis_strain(v.ks, x, Yr, Zr, o);
-    const double exxBx = o[0], exxBy = o[1], exxBz = o[2];
-    const double eyyBx = o[3], eyyBy = o[4], eyyBz = o[5];
-    const double ezzBx = o[6], ezzBy = o[7], ezzBz = o[8];
-    const double exyBx = o[9], exyBy = o[10], exyBz = o[11];
-    const double exzBx = o[12], exzBy = o[13], exzBz = o[14];
-    const double eyzBx = o[15], eyzBy = o[16], eyzBz = o[17];
-    const double rFx = o[18], rFy = o[19], rFz = o[20];
-    const double sinADE1 = v.sinADE1;
+    const R exxBx = o[0], exxBy = o[1], exxBz = o[2];
+    const R eyyBx = o[3], eyyBy = o[4], eyyBz = o[5];
+    const R ezzBx = o[6], ezzBy = o[7], ezzBz = o[8];
+    const R exyBx = o[9], exyBy = o[10], exyBz = o[11];
+    const R exzBx = o[12], exzBy = o[13], exzBz = o[14];
+    const R eyzBx = o[15], eyzBy = o[16], eyzBz = o[17];
+    const R rFx = o[18], rFy = o[19], rFz = o[20];
+    const R sinADE1 = v.sinADE1;
     if (Dn != 0.0) {
-        const double E3 = Dn * K8;
-        double t[6];
+        const R E3 = Dn * K8;
+        R t[6];
         t[0] = Dn * rFx + E3 * exxBx;
         t[1] = E3 * eyyBx;
         t[2] = E3 * ezzBx;
-        t[3] = 0.5 * Dn * rFy - E3 * exyBx;
-        t[4] = 0.5 * Dn * rFz - E3 * exzBx;
+        t[3] = R(0.5) * Dn * rFy - E3 * exyBx;
+        t[4] = R(0.5) * Dn * rFz - E3 * exzBx;
         t[5] = E3 * eyzBx;
         tensor_rot_x(t, CosT, SinT);
 #pragma unroll
@@ -211,22 +278,22 @@ CAD_HD void ad_strain(const AngDis& v, double sgn, double x, double y, double z,
     }
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const double slip = q == 0 ? Dss : Dds;
+        const R slip = q == 0 ? Dss : Dds;
         if (!(slip != 0.0)) continue;
         // in-plane slip (strike, dip) of this mode in ADCS
-        const double Ds = q == 0 ? CosT * Dss : -SinT * Dds;
-        const double Dd = q == 0 ? SinT * Dss : CosT * Dds;
-        const double E5 = Ds * K8;
-        const double E4 = E5 * x;
-        const double dsa = Dd * sinADE1;
-        const double dsax = dsa * x;
-        double t[6];
+        const R Ds = q == 0 ? CosT * Dss : -SinT * Dds;
+        const R Dd = q == 0 ? SinT * Dss : CosT * Dds;
+        const R E5 = Ds * K8;
+        const R E4 = E5 * x;
+        const R dsa = Dd * sinADE1;
+        const R dsax = dsa * x;
+        R t[6];
         t[0] = -E4 * exxBy + dsax * exxBz;
         t[1] = Ds * rFy - E4 * eyyBy + dsax * eyyBz;
         t[2] = -E4 * ezzBy + Dd * rFz + dsax * ezzBz;
-        t[3] = 0.5 * Ds * rFx + E5 * exyBy - dsa * exyBz;
-        t[4] = E5 * exzBy + 0.5 * Dd * rFx - dsa * exzBz;
-        t[5] = 0.5 * Ds * rFz - E4 * eyzBy + 0.5 * Dd * rFy - dsax * eyzBz;
+        t[3] = R(0.5) * Ds * rFx + E5 * exyBy - dsa * exyBz;
+        t[4] = E5 * exzBy + R(0.5) * Dd * rFx - dsa * exzBz;
+        t[5] = R(0.5) * Ds * rFz - E4 * eyzBy + R(0.5) * Dd * rFy - dsax * eyzBz;
         tensor_rot_x(t, CosT, SinT);
 #pragma unroll
         for (int k = 0; k < 6; ++k) E[1 + q][k] += t[k];
@@ -237,17 +304,16 @@ CAD_HD void ad_strain(const AngDis& v, double sgn, double x, double y, double z,
 // image frame the accumulated value is first carried into the image TDCS and
 // the result carried back, as the reference does; a flat (z = 0) image
 // triangle keeps the reference's detached xz / yz components.
-template <bool IMAGE>
-CAD_HD void strain_fs(const Frame& f, double X, double Y, double Z, double Dss, double Dds,
-                                          double Dn, double K8, double E[3][6])
+template <bool IMAGE, typename R>
+CAD_HD void strain_fs(const FrameT<R>& f, double X, double Y, double Z, R Dss, R Dds, R Dn, R K8, R E[3][6])
 {
-    double x, y, z;
+    R x, y, z;
     to_tdcs(f, X, Y, Z, x, y, z);
     const int mode = trimode(f, x, y, z);
-    double keep_xz[3], keep_yz[3];
-    const bool detach = IMAGE && f.flat;
+    R keep_xz[3], keep_yz[3];
+    const bool detach = IMAGE && f.flat != R(0);
     if (IMAGE) {
-        const double RotInv[9] = {f.Vn[0], f.Vs[0], f.Vd[0], f.Vn[1], f.Vs[1], f.Vd[1], f.Vn[2], f.Vs[2], f.Vd[2]};
+        const R RotInv[9] = {f.Vn[0], f.Vs[0], f.Vd[0], f.Vn[1], f.Vs[1], f.Vd[1], f.Vn[2], f.Vs[2], f.Vd[2]};
 #pragma unroll
         for (int m = 0; m < 3; ++m) tensor_rot(E[m], RotInv);
         if (detach) {
@@ -260,16 +326,16 @@ CAD_HD void strain_fs(const Frame& f, double X, double Y, double Z, double Dss, 
             }
         }
     }
-    const double sgn = mode == -1 ? -1.0 : 1.0;
+    const R sgn = mode == -1 ? R(-1.0) : R(1.0);
 #pragma unroll 1
     for (int a = 0; a < 3; ++a) ad_strain(f.v[a], sgn, x, y, z, Dss, Dds, Dn, K8, E);
     if (mode == 0) {
 #pragma unroll
         for (int m = 0; m < 3; ++m)
 #pragma unroll
-            for (int k = 0; k < 6; ++k) E[m][k] = qnan();
+            for (int k = 0; k < 6; ++k) E[m][k] = qnan<R>();
     }
-    const double Rot[9] = {f.Vn[0], f.Vn[1], f.Vn[2], f.Vs[0], f.Vs[1], f.Vs[2], f.Vd[0], f.Vd[1], f.Vd[2]};
+    const R Rot[9] = {f.Vn[0], f.Vn[1], f.Vn[2], f.Vs[0], f.Vs[1], f.Vs[2], f.Vd[0], f.Vd[1], f.Vd[2]};
 #pragma unroll
     for (int m = 0; m < 3; ++m) tensor_rot(E[m], Rot);
     if (detach) {
@@ -282,53 +348,52 @@ CAD_HD void strain_fs(const Frame& f, double X, double Y, double Z, double Dss, 
 }
 
 // -------------------------------------------------- full-space displacement
-CAD_HD void ad_disp(const AngDis& v, double sgn, double x, double y, double z, double Dss,
-                                        double Dds, double Dn, double K8, double U[3][3])
+template <typename R>
+CAD_HD void ad_disp(const AngDisT<R>& v, R sgn, R x, R y, R z, R Dss, R Dds, R Dn, R K8, R U[3][3])
 {
-    const double CosT = sgn * v.cosT, SinT = sgn * v.sinT;
-    const double dy = y - v.tv1, dz = z - v.tv2;
-    const double Yr = CosT * dy - SinT * dz;
-    const double Zr = SinT * dy + CosT * dz;
-    double o[9];
+    const R CosT = sgn * v.cosT, SinT = sgn * v.sinT;
+    const R dy = y - v.tv1, dz = z - v.tv2;
+    const R Yr = CosT * dy - SinT * dz;
+    const R Zr = SinT * dy + CosT * dz;
+    R o[9];
     ang_dis_disp(v.kd, x, Yr, Zr, o);
-    const double ux = o[0], uy = o[1], uz = o[2], vx = o[3], vy = o[4], vz = o[5], wx = o[6], wy = o[7], wz = o[8];
-    const double sinADE1 = v.sinADE1;
+    const R ux = o[0], uy = o[1], uz = o[2], vx = o[3], vy = o[4], vz = o[5], wx = o[6], wy = o[7], wz = o[8];
+    const R sinADE1 = v.sinADE1;
     // back-rotation of (y, z) components: (c u + s w, -s u + c w)
     if (Dn != 0.0) {
-        const double c = Dn * K8;
-        const double a = c * vx, b = c * wx;
+        const R c = Dn * K8;
+        const R a = c * vx, b = c * wx;
         U[0][0] += c * ux;
         U[0][1] += CosT * a + SinT * b;
         U[0][2] += -SinT * a + CosT * b;
     }
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const double slip = q == 0 ? Dss : Dds;
+        const R slip = q == 0 ? Dss : Dds;
         if (!(slip != 0.0)) continue;
-        const double Ds = q == 0 ? CosT * Dss : -SinT * Dds;
-        const double Dd = q == 0 ? SinT * Dss : CosT * Dds;
-        const double cs = Ds * K8, cd = Dd * sinADE1;
-        const double a = x * (cs * vy + cd * vz);
-        const double b = x * (cs * wy + cd * wz);
+        const R Ds = q == 0 ? CosT * Dss : -SinT * Dds;
+        const R Dd = q == 0 ? SinT * Dss : CosT * Dds;
+        const R cs = Ds * K8, cd = Dd * sinADE1;
+        const R a = x * (cs * vy + cd * vz);
+        const R b = x * (cs * wy + cd * wz);
         U[1 + q][0] += cs * uy + cd * uz;
         U[1 + q][1] += CosT * a + SinT * b;
         U[1 + q][2] += -SinT * a + CosT * b;
     }
 }
 
-template <bool IMAGE>
-CAD_HD void disp_fs(const Frame& f, double X, double Y, double Z, double Dss, double Dds,
-                                        double Dn, double K8, double U[3][3])
+template <bool IMAGE, typename R>
+CAD_HD void disp_fs(const FrameT<R>& f, double X, double Y, double Z, R Dss, R Dds, R Dn, R K8, R U[3][3])
 {
-    double x, y, z;
+    R x, y, z;
     to_tdcs(f, X, Y, Z, x, y, z);
     const int mode = trimode(f, x, y, z);
-    const bool detach = IMAGE && f.flat;
-    double keep_z[3];
+    const bool detach = IMAGE && f.flat != R(0);
+    R keep_z[3];
     if (IMAGE) {
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const double a = U[m][0], b = U[m][1], c = U[m][2];
+            const R a = U[m][0], b = U[m][1], c = U[m][2];
             U[m][0] = f.Vn[0] * a + f.Vn[1] * b + f.Vn[2] * c;
             U[m][1] = f.Vs[0] * a + f.Vs[1] * b + f.Vs[2] * c;
             U[m][2] = f.Vd[0] * a + f.Vd[1] * b + f.Vd[2] * c;
@@ -341,36 +406,36 @@ CAD_HD void disp_fs(const Frame& f, double X, double Y, double Z, double Dss, do
             }
         }
     }
-    const double sgn = mode == -1 ? -1.0 : 1.0;
+    const R sgn = mode == -1 ? R(-1.0) : R(1.0);
 #pragma unroll 1
     for (int a = 0; a < 3; ++a) ad_disp(f.v[a], sgn, x, y, z, Dss, Dds, Dn, K8, U);
     if (mode == 0) {
 #pragma unroll
         for (int m = 0; m < 3; ++m)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) U[m][c] = qnan();
+            for (int c = 0; c < 3; ++c) U[m][c] = qnan<R>();
     }
     {   // Burgers' function (solid angle of the TD seen from the point)
-        const double a1 = -x, a2 = f.p1y - y, a3 = f.p1z - z;
-        const double b2 = -y, b3 = -z;
-        const double c2 = f.p3y - y, c3 = f.p3z - z;
-        const double a12 = a1 * a1;
-        const double na = sqrt(a12 + a2 * a2 + a3 * a3);
-        const double nb = sqrt(a12 + b2 * b2 + b3 * b3);
-        const double nc = sqrt(a12 + c2 * c2 + c3 * c3);
-        const double one = a1 * (b2 * c3 - b3 * c2) - a2 * (a1 * c3 - b3 * a1) + a3 * (a1 * c2 - b2 * a1);
-        const double ab = a1 * a1 + a2 * b2 + a3 * b3;
-        const double ac = a1 * a1 + a2 * c2 + a3 * c3;
-        const double bc = a1 * a1 + b2 * c2 + b3 * c3;
-        const double two = na * nb * nc + ab * nc + ac * nb + bc * na;
-        const double Fi = -0.5 * M_1_PI * atan2(one, two);
+        const R a1 = -x, a2 = f.p1y - y, a3 = f.p1z - z;
+        const R b2 = -y, b3 = -z;
+        const R c2 = f.p3y - y, c3 = f.p3z - z;
+        const R a12 = a1 * a1;
+        const R na = cad_sqrt(a12 + a2 * a2 + a3 * a3);
+        const R nb = cad_sqrt(a12 + b2 * b2 + b3 * b3);
+        const R nc = cad_sqrt(a12 + c2 * c2 + c3 * c3);
+        const R one = a1 * (b2 * c3 - b3 * c2) - a2 * (a1 * c3 - b3 * a1) + a3 * (a1 * c2 - b2 * a1);
+        const R ab = a1 * a1 + a2 * b2 + a3 * b3;
+        const R ac = a1 * a1 + a2 * c2 + a3 * c3;
+        const R bc = a1 * a1 + b2 * c2 + b3 * c3;
+        const R two = na * nb * nc + ab * nc + ac * nb + bc * na;
+        const R Fi = R(-0.5) * R(M_1_PI) * cad_atan2(one, two);
         U[0][0] += Dn * Fi;
         U[1][1] += Dss * Fi;
         U[2][2] += Dds * Fi;
     }
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-        const double a = U[m][0], b = U[m][1], c = U[m][2];
+        const R a = U[m][0], b = U[m][1], c = U[m][2];
         U[m][0] = f.Vn[0] * a + f.Vs[0] * b + f.Vd[0] * c;
         U[m][1] = f.Vn[1] * a + f.Vs[1] * b + f.Vd[1] * c;
         U[m][2] = f.Vn[2] * a + f.Vs[2] * b + f.Vd[2] * c;
@@ -383,60 +448,88 @@ CAD_HD void disp_fs(const Frame& f, double X, double Y, double Z, double Dss, do
 
 // --------------------------------------------------- free-surface correction
 // Observation point -> ADCS of a side, relative to PA.
-CAD_HD void to_adcs(const FscSide& s, double X, double Y, double Z, double& x, double& y,
-                                        double& z)
+template <typename R>
+CAD_HD void to_adcs(const FscSideT<R>& s, double X, double Y, double Z, R& x, R& y, R& z)
 {
-    const double dX = sub_rn(X, s.PA[0]), dY = sub_rn(Y, s.PA[1]), dZ = sub_rn(Z, s.PA[2]);
+    R dX, dY, dZ;
+    rel_origin(s.PA, s.PAlo, X, Y, Z, dX, dY, dZ);
     x = add_rn(add_rn(mul_rn(s.ey1[0], dX), mul_rn(s.ey2[0], dY)), mul_rn(s.ey3[0], dZ));
     y = add_rn(add_rn(mul_rn(s.ey1[1], dX), mul_rn(s.ey2[1], dY)), mul_rn(s.ey3[1], dZ));
     z = add_rn(add_rn(mul_rn(s.ey1[2], dX), mul_rn(s.ey2[2], dY)), mul_rn(s.ey3[2], dZ));
 }
 
-CAD_HD void fsc_strain_eval(const ang_dis_strain_fsc_k& k, double y1, double y2, double y3,
-                                                double v[18])
+// The FP64 free-surface strain groups are called out of line: each then gets
+// the whole register file, which spills far less than one inlined body (the
+// FP32 groups fit inline).
+#ifdef __CUDACC__
+#define CAD_OUTLINE static __host__ __device__ __noinline__
+#else
+#define CAD_OUTLINE static inline
+#endif
+CAD_OUTLINE void fsc_strain_g0_f64(const ang_dis_strain_fsc_k<double>& k, double y1, double y2, double y3, double* v)
 {
     ang_dis_strain_fsc_g0(k, y1, y2, y3, v);
-    ang_dis_strain_fsc_g1(k, y1, y2, y3, v + 6);
-    ang_dis_strain_fsc_g2(k, y1, y2, y3, v + 12);
+}
+CAD_OUTLINE void fsc_strain_g1_f64(const ang_dis_strain_fsc_k<double>& k, double y1, double y2, double y3, double* v)
+{
+    ang_dis_strain_fsc_g1(k, y1, y2, y3, v);
+}
+CAD_OUTLINE void fsc_strain_g2_f64(const ang_dis_strain_fsc_k<double>& k, double y1, double y2, double y3, double* v)
+{
+    ang_dis_strain_fsc_g2(k, y1, y2, y3, v);
+}
+
+template <typename R>
+CAD_HD void fsc_strain_eval(const ang_dis_strain_fsc_k<R>& k, R y1, R y2, R y3, R v[18])
+{
+    if constexpr (sizeof(R) == sizeof(double)) {
+        fsc_strain_g0_f64(k, y1, y2, y3, v);
+        fsc_strain_g1_f64(k, y1, y2, y3, v + 6);
+        fsc_strain_g2_f64(k, y1, y2, y3, v + 12);
+    } else {
+        ang_dis_strain_fsc_g0(k, y1, y2, y3, v);
+        ang_dis_strain_fsc_g1(k, y1, y2, y3, v + 6);
+        ang_dis_strain_fsc_g2(k, y1, y2, y3, v + 12);
+    }
 }
 
 // One side's harmonic correction to the strain, added into E (EFCS).
-CAD_HD void fsc_strain(const FscSide& s, double X, double Y, double Z, double Dss, double Dds,
-                                           double Dn, double E[3][6])
+template <typename R>
+CAD_HD void fsc_strain(const FscSideT<R>& s, double X, double Y, double Z, R Dss, R Dds, R Dn, R E[3][6])
 {
-    double x, y, z;
+    R x, y, z;
     to_adcs(s, X, Y, Z, x, y, z);
     const bool flip = mul_rn(s.beta, x) >= 0.0;
     const int c = flip ? 1 : 0;
-    const double f = flip ? -1.0 : 1.0;
+    const R f = flip ? R(-1.0) : R(1.0);
     // d = (term at PB) - (term at PA), formed before any slip product: far
     // from the side the two terms nearly cancel, and differencing them first
     // keeps the products from rounding the two halves differently.
-    double d[18];
+    R d[18];
     fsc_strain_eval(s.ks[c][0], f * x, f * y, z, d);
 #pragma unroll
     for (int q = 0; q < 18; ++q) d[q] = -d[q];
     {
-        double v[18];
+        R v[18];
         fsc_strain_eval(s.ks[c][1], f * (x - s.y1B), f * (y - s.y2B), z - s.y3B, v);
 #pragma unroll
         for (int q = 0; q < 18; ++q) d[q] += v[q];
     }
-    double T[3][6];
+    R T[3][6];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
         // configuration flip negates the first two ADCS slip components and
         // the 13 / 23 strain components
-        const double c0 = f * s.cs[m][0], c1 = f * s.cs[m][1], c2 = s.cs[m][2];
+        const R c0 = f * s.cs[m][0], c1 = f * s.cs[m][1], c2 = s.cs[m][2];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const double fk = (k >= 4) ? f : 1.0;
-            const double h = (k >= 3) ? 0.5 : 1.0;
+            const R fk = (k >= 4) ? f : R(1.0);
+            const R h = (k >= 3) ? R(0.5) : R(1.0);
             T[m][k] = h * fk * (c0 * d[k] + c1 * d[6 + k] + c2 * d[12 + k]);
         }
     }
-    const double AFlip[9] = {s.ey1[0], s.ey1[1], s.ey1[2], s.ey2[0], s.ey2[1], s.ey2[2], s.ey3[0], s.ey3[1], s.ey3[2]};
-    const double slip[3] = {Dn, Dss, Dds};
+    const R AFlip[9] = {s.ey1[0], s.ey1[1], s.ey1[2], s.ey2[0], s.ey2[1], s.ey2[2], s.ey3[0], s.ey3[1], s.ey3[2]};
+    const R slip[3] = {Dn, Dss, Dds};
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
         if (!(slip[m] != 0.0)) continue;
@@ -447,20 +540,20 @@ CAD_HD void fsc_strain(const FscSide& s, double X, double Y, double Z, double Ds
 }
 
 // One side's harmonic correction to the displacement, added into U (EFCS).
-CAD_HD void fsc_disp(const FscSide& s, double X, double Y, double Z, double Dss, double Dds,
-                                         double Dn, double U[3][3])
+template <typename R>
+CAD_HD void fsc_disp(const FscSideT<R>& s, double X, double Y, double Z, R Dss, R Dds, R Dn, R U[3][3])
 {
-    double x, y, z;
+    R x, y, z;
     to_adcs(s, X, Y, Z, x, y, z);
     const int c = mul_rn(s.beta, x) >= 0.0 ? 1 : 0;
-    double uA[9], uB[9];
+    R uA[9], uB[9];
     ang_dis_disp_fsc(s.kd[c][0], x, y, z, uA);
     ang_dis_disp_fsc(s.kd[c][1], x - s.y1B, y - s.y2B, z - s.y3B, uB);
-    const double slip[3] = {Dn, Dss, Dds};
+    const R slip[3] = {Dn, Dss, Dds};
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
         if (!(slip[m] != 0.0)) continue;
-        double u[3];
+        R u[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d)
             u[d] = s.cd[m][0] * (uB[3 * d] - uA[3 * d]) + s.cd[m][1] * (uB[3 * d + 1] - uA[3 * d + 1]) +
@@ -553,8 +646,8 @@ CAD_HD void build_frame(const double P1[3], const double P2[3], const double P3[
         ang_dis_disp_setup(cosA, sinA, sub_rn(1.0, nu), sub_rn(1.0, mul_rn(2.0, nu)), mul_rn(cosA, cosA), d.sinADE1,
                            d.kd);
     }
-    f.flat = (P1[2] == 0.0 && P2[2] == 0.0 && P3[2] == 0.0) ? 1 : 0;
-    f.pad_ = 0;
+    f.flat = (P1[2] == 0.0 && P2[2] == 0.0 && P3[2] == 0.0) ? 1.0 : 0.0;
+    for (int i = 0; i < 3; ++i) f.P2lo[i] = 0.0;
 }
 
 CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real, double Dss, double Dds,
@@ -564,10 +657,9 @@ CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real
     const double Sv = norm3_rn(S[0], S[1], S[2]);
     const double beta = acos(-S[2] / Sv);
     s.beta = beta;
-    s.skip = (fabs(beta) < DBL_EPSILON) || (fabs(M_PI - beta) < DBL_EPSILON) || (fabs(1.0 / tan(beta)) > 5e3);
-    s.pad_ = 0;
-    for (int i = 0; i < 3; ++i) s.PA[i] = PA[i];
-    if (s.skip) return;
+    s.skip = ((fabs(beta) < DBL_EPSILON) || (fabs(M_PI - beta) < DBL_EPSILON) || (fabs(1.0 / tan(beta)) > 5e3)) ? 1.0 : 0.0;
+    for (int i = 0; i < 3; ++i) { s.PA[i] = PA[i]; s.PAlo[i] = 0.0; }
+    if (s.skip != 0.0) return;
     const double n1 = norm3_rn(S[0], S[1], 0.0);
     const double e1[3] = {S[0] / n1, S[1] / n1, 0.0 / n1};
     const double e3[3] = {-0.0, -0.0, -1.0};
@@ -601,34 +693,34 @@ CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real
 }
 
 // ------------------------------------------------------------ pair drivers
-template <bool HS>
-CAD_HD void pair_strain(const TriDev& t, double X, double Y, double Z, double E[3][6])
+template <bool HS, typename R>
+CAD_HD void pair_strain(const TriDevT<R>& t, double X, double Y, double Z, R E[3][6])
 {
 #pragma unroll
     for (int m = 0; m < 3; ++m)
 #pragma unroll
-        for (int k = 0; k < 6; ++k) E[m][k] = 0.0;
+        for (int k = 0; k < 6; ++k) E[m][k] = R(0.0);
     strain_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
     if (HS) {
 #pragma unroll 1
         for (int sd = 0; sd < 3; ++sd)
-            if (!t.side[sd].skip) fsc_strain(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, E);
+            if (t.side[sd].skip == R(0)) fsc_strain(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, E);
         strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
     }
 }
 
-template <bool HS>
-CAD_HD void pair_disp(const TriDev& t, double X, double Y, double Z, double U[3][3])
+template <bool HS, typename R>
+CAD_HD void pair_disp(const TriDevT<R>& t, double X, double Y, double Z, R U[3][3])
 {
 #pragma unroll
     for (int m = 0; m < 3; ++m)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) U[m][c] = 0.0;
+        for (int c = 0; c < 3; ++c) U[m][c] = R(0.0);
     disp_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
     if (HS) {
 #pragma unroll 1
         for (int sd = 0; sd < 3; ++sd)
-            if (!t.side[sd].skip) fsc_disp(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, U);
+            if (t.side[sd].skip == R(0)) fsc_disp(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, U);
         disp_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
     }
 }

@@ -91,27 +91,31 @@ __global__ void colloc_kernel(const double* __restrict__ normals, const double* 
 // Unit-mode strain -> (Tn, Tss, Tds) on the element with normal n, strike ss,
 // dip ds (Hooke, CalculateNormalTraction3D!, TractionVectorCartesianComponents3D!,
 // CalculateTractionInChosenDirection3D!).
-__device__ __forceinline__ void strain_to_traction(const double e[6], double lam, double G2, const double n[3],
-                                                   const double ss[3], const double ds[3], double out[3])
+template <typename R>
+__device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, const R n[3], const R ss[3],
+                                                   const R ds[3], R out[3])
 {
-    const double cons = lam * (e[0] + e[1] + e[2]);
-    const double Sxx = G2 * e[0] + cons, Syy = G2 * e[1] + cons, Szz = G2 * e[2] + cons;
-    const double Sxy = G2 * e[3], Sxz = G2 * e[4], Syz = G2 * e[5];
-    const double cx = n[0], cy = n[1], cz = n[2];
-    out[0] = Sxx * (cx * cx) + Syy * (cy * cy) + Szz * (cz * cz) + 2.0 * Sxy * (cx * cy) + 2.0 * Syz * (cy * cz) +
-             2.0 * Sxz * (cz * cx);
-    const double Tx = Sxx * cx + Sxy * cy + Sxz * cz;
-    const double Ty = Sxy * cx + Syy * cy + Syz * cz;
-    const double Tz = Sxz * cx + Syz * cy + Szz * cz;
+    const R cons = lam * (e[0] + e[1] + e[2]);
+    const R Sxx = G2 * e[0] + cons, Syy = G2 * e[1] + cons, Szz = G2 * e[2] + cons;
+    const R Sxy = G2 * e[3], Sxz = G2 * e[4], Syz = G2 * e[5];
+    const R cx = n[0], cy = n[1], cz = n[2];
+    const R two = R(2.0);
+    out[0] = Sxx * (cx * cx) + Syy * (cy * cy) + Szz * (cz * cz) + two * Sxy * (cx * cy) + two * Syz * (cy * cz) +
+             two * Sxz * (cz * cx);
+    const R Tx = Sxx * cx + Sxy * cy + Sxz * cz;
+    const R Ty = Sxy * cx + Syy * cy + Syz * cz;
+    const R Tz = Sxz * cx + Syz * cy + Szz * cz;
     // traction projected onto the plane: t - (t.n) n
-    const double tn = Tx * cx + Ty * cy + Tz * cz;
-    const double px = Tx - tn * cx, py = Ty - tn * cy, pz = Tz - tn * cz;
+    const R tn = Tx * cx + Ty * cy + Tz * cz;
+    const R px = Tx - tn * cx, py = Ty - tn * cy, pz = Tz - tn * cz;
     out[1] = px * ss[0] + py * ss[1] + pz * ss[2];
     out[2] = px * ds[0] + py * ds[1] + pz * ds[2];
 }
 
 // ------------------------------------------------------------- pair kernel
-template <bool HS, bool STRAIN, bool DISP, int OUT>
+// NEAR: rewrite only the triangles whose centroid lies within the near
+// radius of some point of the block (the FP64 pass of the mixed assembly).
+template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false>
 __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
 {
     extern __shared__ double smem[];
@@ -133,8 +137,18 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
             ds[k] = a.dirs[i + (6 + k) * a.M];
         }
     }
+    const double near_r2 = NEAR ? a.near[3 * a.N] : 0.0;
     for (int64_t j = j0; j < j1; ++j) {
-        __syncthreads();
+        if (NEAR) {
+            bool nr = false;
+            if (active) {
+                const double dx = X - a.near[j], dy = Y - a.near[j + a.N], dz = Z - a.near[j + 2 * a.N];
+                nr = dx * dx + dy * dy + dz * dz < near_r2;
+            }
+            if (!__syncthreads_or(nr)) continue;   // also the barrier before restaging
+        } else {
+            __syncthreads();
+        }
         const double* src = reinterpret_cast<const double*>(a.tri + j);
         for (int w = threadIdx.x; w < words; w += kPairThreads) smem[w] = src[w];
         __syncthreads();
@@ -232,6 +246,107 @@ __global__ void td_sum_kernel(const double* __restrict__ in, int64_t M, int64_t 
     out[f * M + i] = s;
 }
 
+// ----------------------------------------------- mixed-precision assembly
+// Centroids of the triangles (near + [0, 3N)) and the squared near-field
+// radius (near[3N]) = (factor x mean edge length)^2; one block, fixed
+// summation order.
+__global__ void __launch_bounds__(1024) near_setup_kernel(const double* __restrict__ P1, const double* __restrict__ P2,
+                                                          const double* __restrict__ P3, int64_t N, double factor,
+                                                          double* __restrict__ near)
+{
+    __shared__ double s_sum[1024];
+    double acc = 0.0;
+    for (int64_t j = threadIdx.x; j < N; j += blockDim.x) {
+        double e = 0.0;
+        for (int c = 0; c < 3; ++c) near[j + c * N] = (P1[j + c * N] + P2[j + c * N] + P3[j + c * N]) / 3.0;
+        const double* P[3] = {P1, P2, P3};
+        for (int v = 0; v < 3; ++v) {
+            const double* p = P[v];
+            const double* q = P[(v + 1) % 3];
+            const double dx = q[j] - p[j], dy = q[j + N] - p[j + N], dz = q[j + 2 * N] - p[j + 2 * N];
+            e += sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        acc += e;
+    }
+    s_sum[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s_sum[threadIdx.x] += s_sum[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double r = factor * (N > 0 ? s_sum[0] / (3.0 * (double)N) : 0.0);
+        near[3 * N] = r * r;
+    }
+}
+
+// FP32 copy of the first `words` values of each triangle record (records
+// `stride` values apart in both copies): element-wise, then the origins' low
+// parts (an FP32 record keeps each origin as hi + lo).
+__global__ void tri_to_f32_kernel(const double* __restrict__ in, int64_t N, int words, int stride,
+                                  float* __restrict__ out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N * words) return;
+    const int64_t j = i / words;
+    const int w = (int)(i - j * words);
+    const int64_t at = j * stride + w;
+    constexpr int kReal = (int)((offsetof(TriDev, real) + offsetof(Frame, P2lo)) / sizeof(double));
+    constexpr int kImage = (int)((offsetof(TriDev, image) + offsetof(Frame, P2lo)) / sizeof(double));
+    constexpr int kSide0 = (int)((offsetof(TriDev, side) + offsetof(FscSide, PAlo)) / sizeof(double));
+    constexpr int kSideW = (int)(sizeof(FscSide) / sizeof(double));
+    bool lo = (w >= kReal && w < kReal + 3) || (w >= kImage && w < kImage + 3);
+    for (int sd = 0; sd < 3; ++sd) lo = lo || (w >= kSide0 + sd * kSideW && w < kSide0 + sd * kSideW + 3);
+    if (lo) {
+        const double hi = in[at - 3];
+        out[at] = (float)(hi - (double)(float)hi);
+    } else {
+        out[at] = (float)in[at];
+    }
+}
+
+// Far-field pass: the system-matrix kernel with FP32 records and FP32
+// arithmetic (coordinates relative to each origin formed in FP64).
+template <bool HS>
+__global__ void __launch_bounds__(kPairThreads) td_pair_f32_kernel(PairArgs a)
+{
+    extern __shared__ float smem32[];
+    constexpr int words = HS ? kTriWordsHS : kTriWordsFS;
+    const TriDevT<float>& t = *reinterpret_cast<const TriDevT<float>*>(smem32);
+    const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
+    const bool active = i < a.M;
+    double X = 0.0, Y = 0.0, Z = 0.0;
+    if (active) { X = a.X[i]; Y = a.Y[i]; Z = a.Z[i]; }
+    const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
+    const int64_t j1 = min(a.N, j0 + a.tri_chunk);
+    float n[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, ds[3] = {0, 0, 0};
+    if (active) {
+        for (int k = 0; k < 3; ++k) {
+            n[k] = (float)a.dirs[i + k * a.M];
+            ss[k] = (float)a.dirs[i + (3 + k) * a.M];
+            ds[k] = (float)a.dirs[i + (6 + k) * a.M];
+        }
+    }
+    const float* recs = reinterpret_cast<const float*>(a.tri32);
+    const float lam = (float)a.lambda, G2 = (float)(2.0 * a.G);
+    for (int64_t j = j0; j < j1; ++j) {
+        __syncthreads();
+        const float* src = recs + j * (int64_t)kTriWordsHS;   // records keep the FP64 stride
+        for (int w = threadIdx.x; w < words; w += kPairThreads) smem32[w] = src[w];
+        __syncthreads();
+        if (!active) continue;
+        float E[3][6];
+        pair_strain<HS>(t, X, Y, Z, E);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            float tr[3];
+            strain_to_traction(E[m], lam, G2, n, ss, ds, tr);
+#pragma unroll
+            for (int r = 0; r < 3; ++r) a.A[(int64_t)(r * a.N + i) + a.lda * (int64_t)(m * a.N + j)] = -(double)tr[r];
+        }
+    }
+}
+
 // ------------------------------------------------------------ launchers
 template <bool HS, bool STRAIN, bool DISP, int OUT>
 static cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
@@ -274,6 +389,47 @@ cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bo
     }
     return cudaErrorInvalidValue;
 }
+
+cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const double* P2, const double* P3,
+                                  double near_factor, void* tri32, double* near, cudaStream_t st, int64_t* launches)
+{
+    if (a.N == 0 || a.M == 0) return cudaSuccess;
+    near_setup_kernel<<<1, 1024, 0, st>>>(P1, P2, P3, a.N, near_factor, near);
+    const int words = hs ? kTriWordsHS : kTriWordsFS;
+    const int64_t total = a.N * words;
+    tri_to_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(reinterpret_cast<const double*>(a.tri), a.N,
+                                                                         words, kTriWordsHS, (float*)tri32);
+    *launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    a.tri32 = tri32;
+    a.near = near;
+    const int64_t ntile = (a.M + kPairThreads - 1) / kPairThreads;
+    const int64_t nchunk = (a.N + a.tri_chunk - 1) / a.tri_chunk;
+    dim3 grid((unsigned)ntile, (unsigned)nchunk);
+    {
+        auto kern = hs ? td_pair_f32_kernel<true> : td_pair_f32_kernel<false>;
+        const size_t smem = (size_t)words * sizeof(float);
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, kPairThreads, smem, st>>>(a);
+        ++*launches;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    {
+        auto kern = hs ? td_pair_kernel<true, true, false, OUT_AMAT, true>
+                       : td_pair_kernel<false, true, false, OUT_AMAT, true>;
+        const size_t smem = (size_t)words * sizeof(double);
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, kPairThreads, smem, st>>>(a);
+        ++*launches;
+    }
+    return cudaGetLastError();
+}
+
+size_t tri_record_bytes_f32() { return sizeof(TriDevT<float>); }
 
 cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
                             const double* Dds, const double* Dn, int64_t slip_stride, double nu, bool hs,

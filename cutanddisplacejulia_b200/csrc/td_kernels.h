@@ -6,7 +6,9 @@
 
 namespace cad {
 
-struct TriDev;
+template <typename T>
+struct TriDevT;
+using TriDev = TriDevT<double>;
 
 constexpr int kPairThreads = 128;
 
@@ -28,7 +30,18 @@ struct PairArgs {
     double* A;           // OUT_AMAT: 3N x 3N column-major, leading dimension lda
     int64_t lda;
     const double* dirs;  // OUT_TRAC / OUT_AMAT: 9 x M (normal, strike, dip of each observed element)
+    // mixed-precision assembly (OUT_AMAT): FP32 records of the triangles, and
+    // the near field -- centroids (3 x N) followed by the squared radius
+    const void* tri32;
+    const double* near;
 };
+
+// Mixed-precision system matrix: every pair in FP32 (far field), then the
+// pairs of every 128-point tile that has a point within the near radius of
+// the source centroid again in FP64.  near_factor: radius in mean edge lengths.
+cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const double* P2, const double* P3,
+                                  double near_factor, void* tri32, double* near, cudaStream_t st, int64_t* launches);
+size_t tri_record_bytes_f32();
 
 size_t tri_record_bytes();
 

@@ -52,6 +52,10 @@ extern "C" {
 #define CAD_SOLVER_LU64 0  /* FP64 LU with partial pivoting: the reference's A\b (default) */
 #define CAD_SOLVER_MIXED 1 /* FP32 LU (TF32 tensor-core updates) preconditioning FP64 GMRES */
 
+/* Precision of the system-matrix assembly (cad_set_assembly). */
+#define CAD_ASSEMBLY_FP64 0  /* every pair in FP64, as the reference (default) */
+#define CAD_ASSEMBLY_MIXED 1 /* far-field pairs in FP32, near-field pairs in FP64 */
+
 typedef struct cad_ctx cad_ctx;
 
 /* Context: one device, one stream, its own workspace.  A context is used by
@@ -65,7 +69,9 @@ const char* cad_last_error(const cad_ctx* ctx);
 int cad_set_stream(cad_ctx* ctx, void* stream);
 void* cad_get_stream(const cad_ctx* ctx);
 /* Device time (ms, CUDA events on the context stream) of the most recent
- * launch of: 0 = TD pair kernel, 1 = dense factorisation + solve. */
+ * launch of: 0 = TD pair kernel, 1 = dense factorisation + solve, 2 = the
+ * factorisation part of the last mixed-precision solve (cast to FP32, FP32 LU,
+ * diagonal-block inverses; -1 after an FP64 LU solve). */
 double cad_last_time_ms(const cad_ctx* ctx, int which);
 /* Library version string. */
 const char* cad_version(void);
@@ -83,6 +89,17 @@ int64_t cad_kernel_launches(const cad_ctx* ctx);
  * with the last iterate returned).  In mixed mode cad_solve_dev leaves A
  * unchanged. */
 int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter);
+/* Precision of the 3N x 3N system matrix built by cad_assemble_dev and
+ * cad_slip_calculator from now on.  CAD_ASSEMBLY_FP64 (default) evaluates
+ * every pair in FP64 like the reference (src/CalculateInfluenceMatrices3D.jl).
+ * CAD_ASSEMBLY_MIXED has no counterpart in the reference: pairs are evaluated
+ * in FP32 (coordinates relative to each triangle origin formed in FP64), then
+ * every 128-element tile that holds a collocation point within near_factor
+ * mean edge lengths of a source triangle's centroid is evaluated again in
+ * FP64 for that triangle (the near field, where the log and atan terms
+ * cancel).  The matrix is stored in FP64 either way.  The traction influence
+ * matrices of cad_influence_traction are always FP64. */
+int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor);
 /* GMRES iterations (summed over right-hand sides) and the largest final
  * relative residual of the last mixed solve. */
 int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual);

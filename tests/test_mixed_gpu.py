@@ -118,3 +118,62 @@ def test_mixed_repeated_solves_same_size(cad):
         B = rng.standard_normal((n, 1))
         X = cad.solve(A, B, solver="mixed", tol=RESID_TOL)
         assert _rel(X, np.linalg.solve(A, B)) <= SLIP_TOL, rep
+
+
+def _near_pairs(P1, P2, P3, mid, nrm, factor=3.0, tile=128):
+    """(i, j) pairs the mixed assembly evaluates in FP64: every point i of a
+    128-element tile holding some point within factor x mean edge length of
+    triangle j's centroid."""
+    cen = (P1 + P2 + P3) / 3.0
+    edges = (np.linalg.norm(P2 - P1, axis=1) + np.linalg.norm(P3 - P2, axis=1) + np.linalg.norm(P1 - P3, axis=1))
+    r = factor * edges.sum() / (3.0 * len(P1))
+    obs = mid - 1e-12 * nrm
+    d2 = ((obs[:, None, :] - cen[None, :, :]) ** 2).sum(-1)
+    near = d2 < r * r
+    n = len(P1)
+    tiles = np.zeros_like(near)
+    for t0 in range(0, n, tile):
+        tiles[t0:t0 + tile] = near[t0:t0 + tile].any(axis=0)[None, :]
+    return tiles
+
+
+@pytest.mark.parametrize("kind", ["penny", "dipping"])
+def test_mixed_assembly_matrix(cad, kind):
+    from cutanddisplacejulia_b200 import workloads
+    from oracle import oracle
+    if kind == "penny":
+        P1, P2, P3 = workloads.penny(seed=3, spacing=0.12)
+        hs = 0
+    else:
+        P1, P2, P3 = workloads.dipping_rect(seed=5, ntri=500)
+        hs = 1
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    bc = cad.Tractions(np.full(n, -1e-3), np.zeros(n), np.zeros(n))
+    Am = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, hs, bc, np.zeros(n), assembly="mixed")[3]
+    Ao = oracle.influence_traction(nrm, mid, P1, P2, P3, nu, G, lam, hs, want_A=True)
+    near = np.tile(_near_pairs(P1, P2, P3, mid, nrm), (3, 3))
+    scale = np.max(np.abs(Ao))
+    assert near.any() and (~near).any()
+    # near-field pairs: FP64, as the plain path (normwise 1e-12)
+    assert np.max(np.abs(Am[near] - Ao[near])) <= 1e-12 * scale
+    # far-field pairs: FP32 arithmetic (normwise 1e-6 of the matrix)
+    assert np.max(np.abs(Am[~near] - Ao[~near])) <= 1e-6 * scale
+
+
+def test_mixed_assembly_and_solve_slip_error(cad):
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=5, ntri=800)
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    s = workloads.remote_stress(seed=0)
+    bc = cad.Stresses(*s)
+    ref = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n))
+    mix = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n), solver="mixed", tol=RESID_TOL,
+                               assembly="mixed")
+    D, Dm = np.concatenate(ref[:3]), np.concatenate(mix[:3])
+    # the system itself differs from the FP64 one by the far field's FP32
+    # rounding; the slip follows it to about that level
+    assert np.linalg.norm(Dm - D) / np.linalg.norm(D) <= 1e-5
+    Am, b = mix[3], mix[4]
+    assert np.linalg.norm(Am @ Dm - b) <= 2 * RESID_TOL * np.linalg.norm(b)
