@@ -130,3 +130,17 @@ def read_off(path):
         k += 1 + c
     Points = np.column_stack([np.arange(1, nv + 1, dtype=np.float64), pts])
     return Points, np.asarray(tris, dtype=np.int64)
+
+
+def HookesLaw3DStrain2Stress(*args):
+    """Hooke's law, strain -> stress (src/HookesLaw3DStrain2Stress.jl:1-57):
+    sigma = 2 G eps + lambda tr(eps) I.  Either (Exx, Eyy, Ezz, Exy, Exz, Eyz,
+    lam, G) -> the six components, or (Strains, lam, G) -> Stresses."""
+    from .structs import Strains, Stresses
+    if len(args) == 3 and isinstance(args[0], Strains):
+        S, lam, G = args
+        return Stresses(*HookesLaw3DStrain2Stress(*list(S), lam, G))
+    Exx, Eyy, Ezz, Exy, Exz, Eyz, lam, G = (np.asarray(a, dtype=np.float64) if k < 6 else a
+                                            for k, a in enumerate(args))
+    tr = lam * (Exx + Eyy + Ezz)
+    return (2 * G * Exx + tr, 2 * G * Eyy + tr, 2 * G * Ezz + tr, 2 * G * Exy, 2 * G * Exz, 2 * G * Eyz)
