@@ -267,6 +267,52 @@ def mixed_solve_timing(args, ctx, L, stream, step_asm_args, A, b0, x64, ms_fp64,
             "step_speedup_vs_fp64": ms_fp64 / ms}
 
 
+def batch_rhs_timing(args, ctx, L, stream, asm_args, nrm, A, dev):
+    """K right-hand sides (seeded remote stress tensors, six components
+    U[-1e-3, 1e-3], resolved onto the element tractions) on the same system:
+    assembly + FP64 LU with K columns, and mixed assembly + FP32 LU + batched
+    FP64 refinement (GMRES for any column it leaves).  One timed pass each
+    after one warm-up pass; errors of the mixed solutions against the FP64 LU
+    ones (largest column relative L2)."""
+    import numpy as np
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib, assembly
+    dN, dM, dP1, dP2, dP3, n, lam, hs = asm_args
+    n3, K = 3 * n, args.batch_rhs
+    rng = np.random.default_rng(7)
+    B = np.empty((n3, K))
+    for c in range(K):
+        Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*rng.uniform(-1e-3, 1e-3, 6), nrm)
+        B[:, c] = np.concatenate([Tn, Tss, Tds])
+    B0 = torch.tensor(np.asfortranarray(B).ravel(order="F"), device=dev)
+    X = torch.empty_like(B0)
+
+    def run(mode):
+        with _lib.solver_mode(ctx, "lu64" if mode == "fp64" else "mixed", tol=MIXED_TOL, max_iter=400), \
+                _lib.assembly_mode(ctx, mode, NEAR_FACTOR):
+            ms = []
+            for rep in range(2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
+                                              dP3.data_ptr(), n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
+                X.copy_(B0)
+                _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, X.data_ptr(), n3, K), ctx)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            its = _lib.last_solve_stats(ctx)[0] if mode == "mixed" else 0
+        return ms[-1], X.view(K, n3).clone(), its
+    ms64, X64, _ = run("fp64")
+    msm, Xm, its = run("mixed")
+    err = float(((Xm - X64).norm(dim=1) / X64.norm(dim=1)).max())
+    return {"rhs": K, "fp64_ms": ms64, "mixed_ms": msm, "speedup": ms64 / msm, "mixed_iterations": its,
+            "max_col_slip_rel_err_vs_fp64": err,
+            "what": "assembly + factorisation + K-column solve; mixed = FP32 far field, FP32 LU, batched FP64 "
+                    "refinement to relative residual %g" % MIXED_TOL}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -353,6 +399,8 @@ def run_ours(args, rank, world, local_rank):
 
     mixed = None if args.no_mixed else mixed_solve_timing(args, ctx, L, stream, step_asm_args=(
         dN, dM, dP1, dP2, dP3, n, lam, hs), A=A, b0=b0, x64=x, ms_fp64=ms_step, world=world, dev=dev)
+    batch = None if args.batch_rhs <= 0 else batch_rhs_timing(args, ctx, L, stream, (dN, dM, dP1, dP2, dP3, n, lam,
+                                                                                      hs), nrm, A, dev)
 
     # end to end through the host C ABI: pinned host inputs, slips back to host
     def pinned(a):
@@ -433,6 +481,7 @@ def run_ours(args, rank, world, local_rank):
                            "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
         "cpu_baseline": cpu,
         "mixed": mixed,
+        "batch_rhs": batch,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -446,6 +495,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the same system")
+    ap.add_argument("--batch-rhs", type=int, default=0,
+                    help="also time K seeded remote-stress right-hand sides on the same system (FP64 LU and mixed)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="penny",
                     help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
     ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/cad_td.h"
 #include "lu.h"
@@ -28,7 +29,7 @@ namespace {
 
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
-    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_COUNT
+    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -221,6 +222,7 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
 }
 
 constexpr int kRestart = 30;   // Krylov dimension of a GMRES cycle
+constexpr int kIrMaxIter = 20; // refinement sweeps of a multi-column mixed solve before GMRES takes over
 
 int read_info(cad_ctx* ctx, int* info);
 
@@ -278,9 +280,32 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
     bool converged = true;
+    // several right-hand sides: batched refinement first; GMRES finishes the
+    // columns it leaves (their solutions go to the refinement's X, which is
+    // copied to B at the end, so GMRES still reads the original B)
+    std::vector<char> done((size_t)nrhs, 0);
+    double* X = nullptr;
+    if (nrhs > 1) {
+        void *ir, *ir32, *norms;
+        if (int r = ensure(ctx, S_IR, 2 * (size_t)n * nrhs * sizeof(double), &ir)) return r;
+        if (int r = ensure(ctx, S_IR32, 2 * (size_t)n * nrhs * sizeof(float), &ir32)) return r;
+        if (int r = ensure(ctx, S_NORMS, 2 * (size_t)nrhs * sizeof(double), &norms)) return r;
+        X = (double*)ir;
+        IrArgs ia{ls, n, A, lda, B, ldb, (int)nrhs, X, (float*)a32, (int*)piv, (int*)perm, (int*)info, kLuBlock,
+                  ctx->tol, kIrMaxIter, X + (size_t)n * nrhs, (float*)ir32, (float*)ir32 + (size_t)n * nrhs,
+                  (double*)norms};
+        IrResult res{};
+        const int st = ir_solve_batched(ia, &res, done);
+        if (st != GMRES_OK) return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA or cuBLAS error in the refinement");
+        ctx->last_iters += res.iterations;
+        for (int64_t c = 0; c < nrhs; ++c)
+            if (done[c]) ctx->last_relres = res.max_rel_residual > ctx->last_relres ? res.max_rel_residual
+                                                                                    : ctx->last_relres;
+    }
     for (int64_t c = 0; c < nrhs; ++c) {
+        if (done[c]) continue;
         g.b = B + c * ldb;
-        g.x = (double*)work;
+        g.x = X ? X + c * n : (double*)work;
         GmresResult res{};
         const int st = gmres_ir_solve(g, &res);
         if (st == GMRES_TIMEOUT) return fail(ctx, CAD_ERR_TIMEOUT, "mixed solve: a triangular-solve wait ran out");
@@ -289,8 +314,11 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
         converged = converged && st == GMRES_OK;
         ctx->last_iters += res.iterations;
         ctx->last_relres = res.rel_residual > ctx->last_relres ? res.rel_residual : ctx->last_relres;
-        CK(cudaMemcpyAsync(B + c * ldb, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if (!X) CK(cudaMemcpyAsync(B + c * ldb, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     }
+    if (X)
+        CK(cudaMemcpy2DAsync(B, ldb * sizeof(double), X, n * sizeof(double), n * sizeof(double), nrhs,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     ctx->timed[1] = true;
     if (!converged)

@@ -17,6 +17,7 @@
 
 #include <climits>
 #include <cmath>
+#include <math.h>
 #include <cstdint>
 #include <vector>
 
@@ -378,6 +379,110 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
             return GMRES_CUDA_ERROR;
         if (fail) return GMRES_TIMEOUT;
     }
+}
+
+
+// ------------------------------------------------- batched iterative refinement
+namespace {
+
+// Y (n x ncol, ldy) = (float) X (ldx)
+__global__ void d2f_kernel(const double* __restrict__ X, int64_t ldx, int64_t n, float* __restrict__ Y, int64_t ldy)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t c = blockIdx.y;
+    if (i < n) Y[i + c * ldy] = (float)X[i + c * ldx];
+}
+
+// X (ldx) += (double) Y (ldy)
+__global__ void add_f2d_kernel(const float* __restrict__ Y, int64_t ldy, int64_t n, double* __restrict__ X,
+                               int64_t ldx)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t c = blockIdx.y;
+    if (i < n) X[i + c * ldx] += (double)Y[i + c * ldy];
+}
+
+// out[c] = || X[:, c] ||_2, one block per column, fixed summation order
+__global__ void __launch_bounds__(256) col_norms_kernel(const double* __restrict__ X, int64_t ldx, int64_t n,
+                                                        double* __restrict__ out)
+{
+    __shared__ double s[256];
+    const int64_t c = blockIdx.x;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += 256) {
+        const double v = X[i + c * ldx];
+        acc = fma(v, v, acc);
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = sqrt(s[0]);
+}
+
+}  // namespace
+
+int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converged)
+{
+    const int64_t n = a.n;
+    const int nrhs = a.nrhs;
+    cudaStream_t st = a.ls.main;
+    cublasHandle_t h = a.ls.main_blas;
+    res->status = GMRES_OK;
+    res->iterations = 0;
+    res->max_rel_residual = 0.0;
+    converged.assign(nrhs, 0);
+    if (n == 0 || nrhs == 0) return GMRES_OK;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
+    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
+    int64_t* launches = a.ls.launches;
+    const dim3 g((unsigned)((n + 255) / 256), (unsigned)nrhs);
+    std::vector<double> hn(2 * (size_t)nrhs);
+    col_norms_kernel<<<nrhs, 256, 0, st>>>(a.B, a.ldb, n, a.norms);
+    if (cudaMemsetAsync(a.X, 0, (size_t)n * nrhs * sizeof(double), st) != cudaSuccess ||
+        cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return GMRES_CUDA_ERROR;
+    if (launches) ++*launches;
+    double prev = INFINITY;
+    const double one = 1.0, mone = -1.0;
+    for (int it = 1; it <= a.max_iter; ++it) {
+        d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
+        if (launches) ++*launches;
+        if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
+        const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
+                                              a.nb, false, true);
+        if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
+        add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
+        if (launches) ++*launches;
+        if (cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
+                              cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nrhs, (int)n, &mone, a.A, (int)a.lda, a.X, (int)n, &one,
+                        a.R, (int)n) != CUBLAS_STATUS_SUCCESS)
+            return GMRES_BLAS_ERROR;
+        col_norms_kernel<<<nrhs, 256, 0, st>>>(a.R, n, n, a.norms + nrhs);
+        if (launches) ++*launches;
+        if (cudaMemcpyAsync(hn.data(), a.norms, 2 * (size_t)nrhs * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        res->iterations = it;
+        double worst = 0.0;
+        bool all = true;
+        for (int c = 0; c < nrhs; ++c) {
+            const double rr = hn[c] > 0.0 ? hn[nrhs + c] / hn[c] : 0.0;
+            converged[c] = rr <= a.tol;
+            all = all && converged[c];
+            worst = rr > worst || rr != rr ? rr : worst;
+        }
+        res->max_rel_residual = worst;
+        if (all || !(worst < 0.5 * prev)) break;   // done, or refinement stopped converging (or NaN)
+        prev = worst;
+    }
+    return GMRES_OK;
 }
 
 }  // namespace cad

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "lu.h"
 
@@ -55,5 +56,42 @@ struct GmresResult {
 };
 
 int gmres_ir_solve(const GmresArgs& a, GmresResult* res);
+
+// Many right-hand sides at once: classical iterative refinement on the FP32
+// factors -- X += LU32 \ (float)(B - A X), the residual of every column from
+// one FP64 GEMM, the corrections from one multi-column FP32 triangular solve
+// -- until every column's ||b - A x|| / ||b|| <= tol, or until the largest
+// ratio stops halving or max_iter is reached.  converged[c] (host) tells
+// which columns made it; the caller finishes the others with GMRES.
+struct IrArgs {
+    LuStreams ls;
+    int64_t n;
+    const double* A;    // FP64 system matrix (n x n, lda)
+    int64_t lda;
+    const double* B;    // n x nrhs, ldb
+    int64_t ldb;
+    int nrhs;
+    double* X;          // n x nrhs (leading dimension n), the solution
+    float* A32;         // FP32 LU factors and pivots from mixed_prepare
+    int* ipiv;
+    int* perm;
+    int* info;
+    int nb;
+    double tol;
+    int max_iter;
+    // workspace
+    double* R;          // n x nrhs
+    float* R32;         // n x nrhs
+    float* X32;         // n x nrhs
+    double* norms;      // 2 nrhs
+};
+
+struct IrResult {
+    int status;         // GMRES_OK / GMRES_CUDA_ERROR / GMRES_BLAS_ERROR
+    int iterations;
+    double max_rel_residual;
+};
+
+int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converged);
 
 }  // namespace cad

@@ -86,8 +86,13 @@ int64_t cad_kernel_launches(const cad_ctx* ctx);
  * TF32 tensor-core trailing updates; restarted GMRES in FP64, right-
  * preconditioned by that factorisation, iterates until ||b - A x|| / ||b|| <=
  * tol (computed in FP64) or max_iter iterations (then CAD_ERR_NOT_CONVERGED,
- * with the last iterate returned).  In mixed mode cad_solve_dev leaves A
- * unchanged. */
+ * with the last iterate returned).  Several right-hand sides are first
+ * refined together (FP64 residuals of all columns from one GEMM, corrections
+ * from the FP32 factors); GMRES finishes any column the refinement leaves.
+ * The TF32 updates make the FP32 factors accurate to ~1e-3 relative, so the
+ * mixed solver suits condition numbers up to ~1e3-1e4 (the influence systems
+ * are ~1e2); take the FP64 LU for ill-conditioned systems.  In mixed mode
+ * cad_solve_dev leaves A unchanged. */
 int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter);
 /* Precision of the 3N x 3N system matrix built by cad_assemble_dev and
  * cad_slip_calculator from now on.  CAD_ASSEMBLY_FP64 (default) evaluates

@@ -177,3 +177,44 @@ def test_mixed_assembly_and_solve_slip_error(cad):
     assert np.linalg.norm(Dm - D) / np.linalg.norm(D) <= 1e-5
     Am, b = mix[3], mix[4]
     assert np.linalg.norm(Am @ Dm - b) <= 2 * RESID_TOL * np.linalg.norm(b)
+
+
+def test_mixed_many_rhs_influence_system(cad):
+    # 48 remote stress states on one half-space crack: batched refinement on
+    # the FP32 factors, every column to the residual tolerance
+    from cutanddisplacejulia_b200 import assembly, workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=9, ntri=600)
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    bc = cad.Tractions(np.full(n, -1e-3), np.zeros(n), np.zeros(n))
+    A = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n))[3]
+    rng = np.random.default_rng(4)
+    B = np.empty((3 * n, 48))
+    for c in range(48):
+        Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*rng.uniform(-1e-3, 1e-3, 6), nrm)
+        B[:, c] = np.concatenate([Tn, Tss, Tds])
+    X = cad.solve(A, B, solver="mixed", tol=RESID_TOL)
+    Xo = np.linalg.solve(A, B)
+    for c in range(48):
+        assert np.linalg.norm(A @ X[:, c] - B[:, c]) <= 2 * RESID_TOL * np.linalg.norm(B[:, c])
+        assert np.linalg.norm(X[:, c] - Xo[:, c]) <= SLIP_TOL * np.linalg.norm(Xo[:, c])
+
+
+def test_mixed_many_rhs_general_matrix(cad):
+    # condition number 1e3, no structure: every column must reach the residual
+    # tolerance (refinement, GMRES for any column it leaves).  The TF32
+    # trailing updates make the FP32 factors accurate to ~1e-3 relative, so
+    # the mixed solve is meant for condition numbers up to ~1e3-1e4 (the
+    # influence systems are ~1e2); ill-conditioned systems take the FP64 LU.
+    from cutanddisplacejulia_b200 import _lib
+    rng = np.random.default_rng(5)
+    n = 400
+    Q1, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    Q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = (Q1 * np.logspace(0, -3, n)) @ Q2.T
+    B = rng.standard_normal((n, 3))
+    X = cad.solve(A, B, solver="mixed", tol=RESID_TOL, max_iter=400)
+    for c in range(3):
+        assert np.linalg.norm(A @ X[:, c] - B[:, c]) <= 2 * RESID_TOL * np.linalg.norm(B[:, c])
+    it, rr = _lib.last_solve_stats(_lib.context(0))
+    assert rr <= RESID_TOL and it >= 1
