@@ -135,3 +135,46 @@ def solve(A, B, device=0, solver="lu64", tol=1e-10, max_iter=200):
         rc = _lib.load().cad_solve(ctx, n, A.ctypes.data, Bf.ctypes.data, nrhs, X.ctypes.data)
         _lib.check(rc, ctx)
     return X[:, 0] if vec else X
+
+
+def SlipCalculator3D_batched(cracks, nu, G, lam, HSFlag, BoundaryConditions, device=0, tol=1e-10,
+                             assembly="mixed", near_factor=3.0):
+    """SlipCalculator3D (src/SlipCalculator3D.jl:1-33) over many independent
+    cracks in one batched GPU call.  cracks: list of (P1, P2, P3); one
+    boundary condition per crack (or one for all).  Each crack is assembled
+    (assembly="mixed": FP32 far field, FP64 near field; "fp64": all FP64) and
+    solved by FP32 LU with FP64 refinement to relative residual tol.  Returns
+    a list of (Dn, Dss, Dds) and the final relative residuals."""
+    from .geometry import CreateFaceNormalAndMidPoint
+    bcs = BoundaryConditions if isinstance(BoundaryConditions, (list, tuple)) else [BoundaryConditions] * len(cracks)
+    if len(bcs) != len(cracks):
+        raise ValueError("one boundary condition per crack")
+    offs = [0]
+    blocks = {k: [] for k in ("P1", "P2", "P3", "nrm", "mid", "T")}
+    for (P1, P2, P3), bc in zip(cracks, bcs):
+        P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+        N = P1.shape[0]
+        nrm, mid = CreateFaceNormalAndMidPoint(P1, P2, P3)
+        Tn, Tds, Tss = SetupTractionVector(bc, nrm, N, G, lam)
+        for k, a in (("P1", P1), ("P2", P2), ("P3", P3), ("nrm", _tri(nrm)), ("mid", _tri(mid))):
+            blocks[k].append(a.ravel(order="F"))
+        blocks["T"].append(np.concatenate([_col(Tn, N), _col(Tss, N), _col(Tds, N)]))
+        offs.append(offs[-1] + N)
+    cat = {k: np.ascontiguousarray(np.concatenate(v)) if v else np.zeros(0) for k, v in blocks.items()}
+    offsets = np.asarray(offs, dtype=np.int64)
+    D = np.zeros(3 * offs[-1])
+    rel = np.zeros(len(cracks))
+    ctx = _lib.context(device)
+    with _lib.solver_mode(ctx, "mixed", tol, 400), _lib.assembly_mode(ctx, assembly, near_factor):
+        rc = _lib.load().cad_slip_calculator_batched(ctx, len(cracks), offsets.ctypes.data, cat["P1"].ctypes.data,
+                                                     cat["P2"].ctypes.data, cat["P3"].ctypes.data,
+                                                     cat["nrm"].ctypes.data, cat["mid"].ctypes.data, float(nu),
+                                                     float(G), float(lam), int(HSFlag), cat["T"].ctypes.data,
+                                                     D.ctypes.data, rel.ctypes.data)
+        _lib.check(rc, ctx)
+    out = []
+    for c in range(len(cracks)):
+        o, N = offs[c], offs[c + 1] - offs[c]
+        d = D[3 * o:3 * o + 3 * N]
+        out.append((d[:N], d[N:2 * N], d[2 * N:]))
+    return out, rel

@@ -8,6 +8,7 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -29,7 +30,7 @@ namespace {
 
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
-    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_COUNT
+    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -37,6 +38,30 @@ constexpr int kLuBlock = 256;   // outer block width of the LU
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+};
+
+// One lane of the batched solve: its own streams, cuBLAS handles and
+// workspaces, so cracks on different lanes run concurrently.
+enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS, L_BLASWS,
+                L_COUNT };
+struct Lane {
+    cudaStream_t main = nullptr, side = nullptr;
+    cublasHandle_t main_blas = nullptr, side_blas = nullptr;
+    cudaEvent_t done = nullptr;
+    DevBuf buf[L_COUNT];
+};
+constexpr int kLanes = 8;            // cracks of a batch in flight at once
+constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
+constexpr size_t kBlasWorkspace = 32u << 20;
+
+// The captured graph of the last batched call and what it was captured for.
+struct BatchGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int64_t> offsets;
+    const void* ptrs[8] = {};
+    double params[5] = {};
+    int flags[2] = {};
+    int64_t launches = 0;
 };
 
 }  // namespace
@@ -49,6 +74,8 @@ struct cad_ctx {
     cudaStream_t side_stream = nullptr;   // the LU's look-ahead trailing updates
     cublasHandle_t side_blas = nullptr;
     LuGraphCache* graphs = nullptr;       // captured LU factorisations, replayed for repeated calls
+    std::vector<Lane> lanes;              // batched solve (created on first use)
+    BatchGraph batch;
     DevBuf buf[S_COUNT];
     // event pairs: [0,1] TD pair kernel, [2,3] dense solve, [2,4] its
     // factorisation (mixed solver: cast + FP32 LU + block inverses)
@@ -387,6 +414,279 @@ bool bad_flag(int f) { return f != 0 && f != 1; }
 
 }  // namespace
 
+
+// ------------------------------------------------------------- batched solve
+int lane_ensure(cad_ctx* ctx, Lane& l, LaneSlot slot, size_t bytes, void** out)
+{
+    DevBuf& b = l.buf[slot];
+    if (bytes == 0) bytes = 16;
+    if (b.bytes < bytes) {
+        if (b.p) {
+            CK(cudaStreamSynchronize(l.main));
+            CK(cudaStreamSynchronize(l.side));
+            CK(cudaFree(b.p));
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        CK(cudaMalloc(&b.p, bytes));
+        b.bytes = bytes;
+    }
+    *out = b.p;
+    return CAD_OK;
+}
+
+int make_lanes(cad_ctx* ctx)
+{
+    if (!ctx->lanes.empty()) return CAD_OK;
+    int prio_low = 0, prio_high = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    ctx->lanes.resize(kLanes);
+    for (auto& l : ctx->lanes) {
+        CK(cudaStreamCreateWithPriority(&l.main, cudaStreamNonBlocking, prio_high));
+        CK(cudaStreamCreateWithPriority(&l.side, cudaStreamNonBlocking, prio_low));
+        CK(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming));
+        if (cublasCreate(&l.main_blas) != CUBLAS_STATUS_SUCCESS || cublasCreate(&l.side_blas) != CUBLAS_STATUS_SUCCESS)
+            return fail(ctx, CAD_ERR_CUDA, "cuBLAS handle creation failed");
+        // fixed workspaces: nothing is allocated while the batch is captured
+        void *w0, *w1;
+        if (int r = lane_ensure(ctx, l, L_BLASWS, 2 * kBlasWorkspace, &w0)) return r;
+        w1 = (char*)w0 + kBlasWorkspace;
+        if (cublasSetStream(l.main_blas, l.main) != CUBLAS_STATUS_SUCCESS ||
+            cublasSetStream(l.side_blas, l.side) != CUBLAS_STATUS_SUCCESS ||
+            cublasSetWorkspace(l.main_blas, w0, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS ||
+            cublasSetWorkspace(l.side_blas, w1, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS)
+            return fail(ctx, CAD_ERR_CUDA, "cuBLAS lane set-up failed");
+    }
+    return CAD_OK;
+}
+
+// One crack's system matrix on the lane's main stream with the lane's buffers.
+cudaError_t assemble_on_lane(Lane& l, int64_t* launches, const double* normals, const double* mid, const double* P1,
+                             const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                             int hs, bool mixed, double near_factor, double* A, int64_t lda)
+{
+    double* X = (double*)l.buf[L_OBS].p;
+    cudaError_t e = launch_colloc(normals, mid, N, X, X + N, X + 2 * N, (double*)l.buf[L_DIRS].p, l.main);
+    if (e != cudaSuccess) return e;
+    e = launch_td_setup(P1, P2, P3, N, nullptr, nullptr, nullptr, 1, nu, hs == 1, (TriDev*)l.buf[L_TRI].p, l.main);
+    if (e != cudaSuccess) return e;
+    *launches += 2;
+    PairArgs a{};
+    a.X = X; a.Y = X + N; a.Z = X + 2 * N; a.M = N; a.tri = (const TriDev*)l.buf[L_TRI].p; a.N = N;
+    a.tri_chunk = pick_chunk(N, N, false);
+    a.lambda = lambda; a.G = G; a.dirs = (const double*)l.buf[L_DIRS].p;
+    a.A = A; a.lda = lda;
+    if (mixed)
+        return launch_assemble_mixed(a, hs == 1, P1, P2, P3, near_factor, l.buf[L_TRI32].p, (double*)l.buf[L_NEAR].p,
+                                     l.main, launches);
+    ++*launches;
+    return launch_td_pairs(a, OUT_AMAT, hs == 1, true, false, l.main);
+}
+
+struct BatchArgs {
+    int64_t nbatch;
+    const int64_t* offsets;
+    const double *P1, *P2, *P3, *normals, *midpoints, *T;
+    double* D;
+    double nu, G, lambda;
+    int hs;
+    double* Aall;                   // every crack's 3N x 3N matrix, back to back
+    const std::vector<int64_t>* aoff;
+    const std::vector<int>* lane_of;
+    const std::vector<int64_t>* order;   // issue order
+    double* rel;                    // device, nbatch
+};
+
+// Issues the whole batch: fork the lanes off the context stream, every crack
+// (assembly, FP32 LU, fixed refinement sweeps) on its lane, join.
+int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
+{
+    CK(cudaEventRecord(fork, ctx->stream));
+    for (auto& l : ctx->lanes) {
+        CK(cudaStreamWaitEvent(l.main, fork, 0));
+        CK(cudaStreamWaitEvent(l.side, fork, 0));
+    }
+    const bool mixed = ctx->assembly == CAD_ASSEMBLY_MIXED;
+    for (int64_t c : *b.order) {
+        Lane& l = ctx->lanes[(*b.lane_of)[c]];
+        const int64_t o = b.offsets[c], N = b.offsets[c + 1] - o, n3 = 3 * N;
+        if (N == 0) continue;
+        double* A = b.Aall + (*b.aoff)[c];
+        CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
+                            b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
+        const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr};
+        int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, nullptr, (int*)l.buf[L_PIV].p,
+                               (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, false);
+        if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "batched solve: FP32 LU failed");
+        float* r32 = (float*)l.buf[L_IR32].p;
+        IrArgs ia{ls, n3, A, n3, b.T + 3 * o, n3, 1, b.D + 3 * o, (float*)l.buf[L_A32].p, (int*)l.buf[L_PIV].p,
+                  (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, ctx->tol, kBatchSweeps,
+                  (double*)l.buf[L_IR].p, r32, r32 + n3, (double*)l.buf[L_NORMS].p};
+        if (ir_solve_fixed(ia, kBatchSweeps, b.rel + c) != GMRES_OK)
+            return fail(ctx, CAD_ERR_CUDA, "batched solve: refinement launch failed");
+    }
+    for (auto& l : ctx->lanes) {
+        CK(cudaEventRecord(l.done, l.main));
+        CK(cudaStreamWaitEvent(ctx->stream, l.done, 0));
+    }
+    return CAD_OK;
+}
+
+int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1, const double* P2,
+                 const double* P3, const double* normals, const double* midpoints, double nu, double G, double lambda,
+                 int hs, const double* T, double* D, double* rel_host)
+{
+    if (nbatch == 0) return CAD_OK;
+    if (hs == 1) {   // every crack's vertices and collocation points at or below z = 0
+        void* flag;
+        if (int r = ensure(ctx, S_FLAG, sizeof(int), &flag)) return r;
+        CK(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+        for (int64_t c = 0; c < nbatch; ++c) {
+            const int64_t o = offsets[c], N = offsets[c + 1] - o;
+            CK(launch_hs_check(midpoints + 3 * o + 2 * N, N, P1 + 3 * o, P2 + 3 * o, P3 + 3 * o, N, (int*)flag,
+                               ctx->stream, normals + 3 * o + 2 * N, false));
+        }
+        ctx->launches += nbatch;
+        int h = 0;
+        CK(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (h) return fail(ctx, CAD_ERR_HS_ABOVE_SURFACE, "Half-space solution: Z coordinates must be negative!");
+    }
+    // sizes, matrix offsets, lanes (largest cracks first, each to the least
+    // loaded lane), issue order (round robin over lanes)
+    std::vector<int64_t> aoff((size_t)nbatch + 1, 0), byN((size_t)nbatch);
+    int64_t maxN = 0;
+    for (int64_t c = 0; c < nbatch; ++c) {
+        const int64_t N = offsets[c + 1] - offsets[c];
+        aoff[c + 1] = aoff[c] + 9 * N * N;
+        maxN = N > maxN ? N : maxN;
+        byN[c] = c;
+    }
+    std::sort(byN.begin(), byN.end(), [&](int64_t x, int64_t y) {
+        return offsets[x + 1] - offsets[x] > offsets[y + 1] - offsets[y];
+    });
+    if (int r = make_lanes(ctx)) return r;
+    std::vector<int> lane_of((size_t)nbatch, 0);
+    std::vector<double> load(kLanes, 0.0);
+    std::vector<std::vector<int64_t>> per_lane(kLanes);
+    std::vector<int64_t> laneN(kLanes, 0);
+    for (int64_t c : byN) {
+        int best = 0;
+        for (int k = 1; k < kLanes; ++k)
+            if (load[k] < load[best]) best = k;
+        const double N = (double)(offsets[c + 1] - offsets[c]);
+        load[best] += N * N * N;
+        lane_of[c] = best;
+        per_lane[best].push_back(c);
+        laneN[best] = std::max<int64_t>(laneN[best], offsets[c + 1] - offsets[c]);
+    }
+    std::vector<int64_t> order;
+    for (size_t i = 0;; ++i) {
+        bool any = false;
+        for (int k = 0; k < kLanes; ++k)
+            if (i < per_lane[k].size()) {
+                order.push_back(per_lane[k][i]);
+                any = true;
+            }
+        if (!any) break;
+    }
+    // workspaces sized before anything is captured
+    void *Aall, *rel, *p;
+    if (int r = ensure(ctx, S_A, (size_t)aoff[nbatch] * sizeof(double), &Aall)) return r;
+    if (int r = ensure(ctx, S_REL, (size_t)nbatch * sizeof(double), &rel)) return r;
+    for (int k = 0; k < kLanes; ++k) {
+        Lane& l = ctx->lanes[k];
+        const size_t N = (size_t)laneN[k], n3 = 3 * N;
+        if (N == 0) continue;
+        if (int r = lane_ensure(ctx, l, L_OBS, 3 * N * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_DIRS, 9 * N * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_TRI, N * tri_record_bytes(), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_TRI32, N * tri_record_bytes_f32(), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_NEAR, (3 * N + 1) * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_A32, n3 * n3 * sizeof(float), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_PIV, n3 * sizeof(int), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_PERM, n3 * sizeof(int), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_INFO, sizeof(int), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_IR, n3 * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_IR32, 2 * n3 * sizeof(float), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_NORMS, 2 * sizeof(double), &p)) return r;
+    }
+    BatchArgs b{nbatch, offsets, P1, P2, P3, normals, midpoints, T, D, nu, G, lambda, hs, (double*)Aall, &aoff,
+                &lane_of, &order, (double*)rel};
+    // the captured graph of an identical earlier call is replayed
+    BatchGraph& g = ctx->batch;
+    const void* ptrs[8] = {P1, P2, P3, normals, midpoints, T, D, Aall};
+    const double params[5] = {nu, G, lambda, ctx->tol, ctx->near_factor};
+    const int flags[2] = {hs, ctx->assembly};
+    const bool same = g.exec && g.offsets.size() == (size_t)nbatch + 1 &&
+                      std::equal(g.offsets.begin(), g.offsets.end(), offsets) &&
+                      std::equal(ptrs, ptrs + 8, g.ptrs) && std::equal(params, params + 5, g.params) &&
+                      std::equal(flags, flags + 2, g.flags);
+    cudaEvent_t fork = nullptr;
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    int rc = CAD_OK;
+    if (same) {
+        CK(cudaGraphLaunch(g.exec, ctx->stream));
+        ctx->launches += g.launches;
+    } else if (ctx->stream == nullptr) {   // the legacy default stream cannot be captured: run directly
+        rc = batch_body(ctx, b, fork);
+    } else {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        const int64_t l0 = ctx->launches;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(fork);
+            return cuda_fail(ctx, e, "batched solve: stream capture");
+        }
+        rc = batch_body(ctx, b, fork);
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc == CAD_OK && e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: stream capture");
+        if (rc == CAD_OK) {
+            e = cudaGraphInstantiate(&g.exec, graph, 0);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: graph instantiation");
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (rc == CAD_OK) {
+            g.offsets.assign(offsets, offsets + nbatch + 1);
+            std::copy(ptrs, ptrs + 8, g.ptrs);
+            std::copy(params, params + 5, g.params);
+            std::copy(flags, flags + 2, g.flags);
+            g.launches = ctx->launches - l0;
+            e = cudaGraphLaunch(g.exec, ctx->stream);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: graph launch");
+        } else if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+    }
+    cudaEventDestroy(fork);
+    if (rc != CAD_OK) return rc;
+    // every crack's residual; GMRES (on the context stream) for any crack the
+    // refinement sweeps left above the tolerance
+    std::vector<double> hrel((size_t)nbatch);
+    CK(cudaMemcpyAsync(hrel.data(), rel, (size_t)nbatch * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    bool converged = true;
+    for (int64_t c = 0; c < nbatch; ++c) {
+        if (hrel[c] <= ctx->tol) continue;
+        const int64_t o = offsets[c], n3 = 3 * (offsets[c + 1] - o);
+        CK(cudaMemcpyAsync(D + 3 * o, T + 3 * o, n3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        int info = 0;
+        const int r = solve_mixed_device(ctx, n3, (double*)Aall + aoff[c], n3, D + 3 * o, n3, 1, &info);
+        if (r == CAD_ERR_NOT_CONVERGED) converged = false;
+        else if (r != CAD_OK) return r;
+        if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "matrix is singular to working precision");
+        hrel[c] = ctx->last_relres;
+    }
+    if (rel_host) std::copy(hrel.begin(), hrel.end(), rel_host);
+    if (!converged) return fail(ctx, CAD_ERR_NOT_CONVERGED, "batched solve: a crack did not reach the tolerance");
+    return CAD_OK;
+}
+
 extern "C" {
 
 const char* cad_version(void) { return "cad_td 1.0 (sm_100a, FP64)"; }
@@ -438,6 +738,18 @@ int cad_destroy(cad_ctx* ctx)
         if (e) cudaEventDestroy(e);
     if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
     lu_graph_cache_destroy(ctx->graphs);
+    if (ctx->batch.exec) cudaGraphExecDestroy(ctx->batch.exec);
+    for (auto& l : ctx->lanes) {
+        if (l.main) cudaStreamSynchronize(l.main);
+        if (l.side) cudaStreamSynchronize(l.side);
+        for (auto& b : l.buf)
+            if (b.p) cudaFree(b.p);
+        if (l.main_blas) cublasDestroy(l.main_blas);
+        if (l.side_blas) cublasDestroy(l.side_blas);
+        if (l.main) cudaStreamDestroy(l.main);
+        if (l.side) cudaStreamDestroy(l.side);
+        if (l.done) cudaEventDestroy(l.done);
+    }
     if (ctx->blas) cublasDestroy(ctx->blas);
     if (ctx->side_blas) cublasDestroy(ctx->side_blas);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
@@ -735,6 +1047,52 @@ int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, in
     if (n > 0 && nrhs > 0)
         if (int r = read_info(ctx, &info)) return r;
     if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    return CAD_OK;
+}
+
+int cad_slip_calculator_batched_dev(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1,
+                                    const double* P2, const double* P3, const double* normals,
+                                    const double* midpoints, double nu, double G, double lambda, int hs_flag,
+                                    const double* T, double* D, double* rel_residual)
+{
+    if (int r = set_device(ctx)) return r;
+    if (nbatch < 0 || bad_flag(hs_flag) || (nbatch > 0 && !offsets)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (nbatch > 0 && offsets[0] != 0) return fail(ctx, CAD_ERR_ARG, "offsets[0] must be 0");
+    for (int64_t c = 0; c < nbatch; ++c)
+        if (offsets[c + 1] < offsets[c]) return fail(ctx, CAD_ERR_DIMS, "Element size inputs must be the same dimensions");
+    if (nbatch > 0 && offsets[nbatch] > 0 && (!P1 || !P2 || !P3 || !normals || !midpoints || !T || !D))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    return slip_batched(ctx, nbatch, offsets, P1, P2, P3, normals, midpoints, nu, G, lambda, hs_flag, T, D,
+                        rel_residual);
+}
+
+int cad_slip_calculator_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1,
+                                const double* P2, const double* P3, const double* normals, const double* midpoints,
+                                double nu, double G, double lambda, int hs_flag, const double* T, double* D,
+                                double* rel_residual)
+{
+    if (int r = set_device(ctx)) return r;
+    if (nbatch < 0 || (nbatch > 0 && !offsets)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    const int64_t ntot = nbatch > 0 ? offsets[nbatch] : 0;
+    if (ntot < 0) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (ntot > 0 && (!P1 || !P2 || !P3 || !normals || !midpoints || !T || !D))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    void *geom, *td;
+    if (int r = ensure(ctx, S_BGEOM, (size_t)15 * ntot * sizeof(double), &geom)) return r;
+    if (int r = ensure(ctx, S_BTD, (size_t)6 * ntot * sizeof(double), &td)) return r;
+    double* g = (double*)geom;
+    double* t = (double*)td;
+    const double* src[5] = {P1, P2, P3, normals, midpoints};
+    for (int k = 0; k < 5; ++k)
+        if (int r = upload(ctx, g + k * 3 * ntot, src[k], 3 * ntot)) return r;
+    if (int r = upload(ctx, t, T, 3 * ntot)) return r;
+    if (int r = cad_slip_calculator_batched_dev(ctx, nbatch, offsets, g, g + 3 * ntot, g + 6 * ntot, g + 9 * ntot,
+                                                g + 12 * ntot, nu, G, lambda, hs_flag, t, t + 3 * ntot, rel_residual))
+        return r;
+    if (ntot > 0) {
+        CK(cudaMemcpyAsync(D, t + 3 * ntot, (size_t)3 * ntot * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     return CAD_OK;
 }
 

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
 }  // namespace
 
 int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, float* A32, float* Dinv, int* ipiv,
-                  int* perm, int* info, int nb)
+                  int* perm, int* info, int nb, bool inverses)
 {
     if (n <= 0) return LU_OK;
     const int64_t rb = (n + 255) / 256;
@@ -210,7 +210,7 @@ int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, 
     int rc = lu_factor_solve<float>(ls, A32, n, n, nullptr, 0, 0, nullptr, 0, ipiv, perm, info, nb, true, false);
     if (rc != LU_OK) return rc;
     rc = lu_pivots_to_perm(ls, ipiv, n, perm);
-    if (rc != LU_OK) return rc;
+    if (rc != LU_OK || !inverses) return rc;
     const int nblk = (int)((n + kRB - 1) / kRB);
     const size_t smem = (size_t)(kRB * kRB + kRB * (kRB + 1)) * sizeof(float);
     if (cudaFuncSetAttribute(invert_diag_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -483,6 +483,60 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
         prev = worst;
     }
     return GMRES_OK;
+}
+
+
+namespace {
+// out[0] = max_c norms[nrhs + c] / norms[c] (0 where norms[c] == 0; NaN kept)
+__global__ void relres_kernel(const double* __restrict__ norms, int nrhs, double* __restrict__ out)
+{
+    double worst = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+        const double r = norms[c] > 0.0 ? norms[nrhs + c] / norms[c] : 0.0;
+        worst = (r > worst || r != r) ? r : worst;
+    }
+    out[0] = worst;
+}
+}  // namespace
+
+int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
+{
+    const int64_t n = a.n;
+    const int nrhs = a.nrhs;
+    cudaStream_t st = a.ls.main;
+    cublasHandle_t h = a.ls.main_blas;
+    if (n == 0 || nrhs == 0) return GMRES_OK;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
+    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
+    int64_t* launches = a.ls.launches;
+    const dim3 g((unsigned)((n + 255) / 256), (unsigned)nrhs);
+    col_norms_kernel<<<nrhs, 256, 0, st>>>(a.B, a.ldb, n, a.norms);
+    if (launches) ++*launches;
+    if (cudaMemsetAsync(a.X, 0, (size_t)n * nrhs * sizeof(double), st) != cudaSuccess ||
+        cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return GMRES_CUDA_ERROR;
+    const double one = 1.0, mone = -1.0;
+    for (int it = 0; it < iters; ++it) {
+        d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
+        if (launches) ++*launches;
+        if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
+        const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
+                                              a.nb, false, true);
+        if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
+        add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
+        if (launches) ++*launches;
+        if (cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
+                              cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return GMRES_CUDA_ERROR;
+        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nrhs, (int)n, &mone, a.A, (int)a.lda, a.X, (int)n, &one,
+                        a.R, (int)n) != CUBLAS_STATUS_SUCCESS)
+            return GMRES_BLAS_ERROR;
+    }
+    col_norms_kernel<<<nrhs, 256, 0, st>>>(a.R, n, n, a.norms + nrhs);
+    relres_kernel<<<1, 1, 0, st>>>(a.norms, nrhs, rel_out);
+    if (launches) *launches += 2;
+    return cudaGetLastError() == cudaSuccess ? GMRES_OK : GMRES_CUDA_ERROR;
 }
 
 }  // namespace cad

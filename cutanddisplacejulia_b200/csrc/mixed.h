@@ -17,7 +17,7 @@ namespace cad {
 // triangles into Dinv (mixed_dinv_floats(n) floats).  Returns an LU_* code;
 // info as lu_factor_solve.
 int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, float* A32, float* Dinv, int* ipiv,
-                  int* perm, int* info, int nb);
+                  int* perm, int* info, int nb, bool inverses = true);
 size_t mixed_dinv_floats(int64_t n);
 size_t mixed_sync_ints(int64_t n);   // flags, tickets and the failure word of one preconditioner apply
 
@@ -93,5 +93,10 @@ struct IrResult {
 };
 
 int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converged);
+
+// `iters` refinement sweeps with no host synchronisation (capturable in a
+// CUDA graph); rel_out (device, 1 double) = the largest final column ratio
+// ||b - A x|| / ||b||.  Returns a GMRES_* status (launch errors only).
+int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out);
 
 }  // namespace cad

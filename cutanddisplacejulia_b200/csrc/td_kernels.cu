@@ -44,13 +44,15 @@ __global__ void td_setup_kernel(const double* __restrict__ P1, const double* __r
 
 // ------------------------------------------------ half-space argument check
 // flag |= 1 when any vertex or observation z > 0 (src/TD.jl:606-619).
-__global__ void hs_check_kernel(const double* __restrict__ Z, int64_t M, const double* __restrict__ P1,
-                                const double* __restrict__ P2, const double* __restrict__ P3, int64_t N,
-                                int* __restrict__ flag)
+// With nz set, the observation z is Z - 1e-12 nz (collocation points from
+// midpoints and normals, as SetupCollationPoints forms them).
+__global__ void hs_check_kernel(const double* __restrict__ Z, const double* __restrict__ nz, int64_t M,
+                                const double* __restrict__ P1, const double* __restrict__ P2,
+                                const double* __restrict__ P3, int64_t N, int* __restrict__ flag)
 {
     int bad = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M + N; i += (int64_t)gridDim.x * blockDim.x) {
-        if (i < M) bad |= Z[i] > 0.0;
+        if (i < M) bad |= (nz ? Z[i] - nz[i] * 1e-12 : Z[i]) > 0.0;
         else {
             const int64_t j = i - M;
             bad |= (P1[j + 2 * N] > 0.0) | (P2[j + 2 * N] > 0.0) | (P3[j + 2 * N] > 0.0);
@@ -443,14 +445,14 @@ cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3
 }
 
 cudaError_t launch_hs_check(const double* Z, int64_t M, const double* P1, const double* P2, const double* P3,
-                            int64_t N, int* flag, cudaStream_t st)
+                            int64_t N, int* flag, cudaStream_t st, const double* nz, bool clear)
 {
-    cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+    cudaError_t e = clear ? cudaMemsetAsync(flag, 0, sizeof(int), st) : cudaSuccess;
     if (e != cudaSuccess || M + N == 0) return e;
     const int bs = 256;
     int64_t nb = (M + N + bs - 1) / bs;
     if (nb > 1184) nb = 1184;
-    hs_check_kernel<<<(unsigned)nb, bs, 0, st>>>(Z, M, P1, P2, P3, N, flag);
+    hs_check_kernel<<<(unsigned)nb, bs, 0, st>>>(Z, nz, M, P1, P2, P3, N, flag);
     return cudaGetLastError();
 }
 

@@ -49,8 +49,10 @@ cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3
                             const double* Dds, const double* Dn, int64_t slip_stride, double nu, bool hs,
                             TriDev* out, cudaStream_t st);
 cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bool disp, cudaStream_t st);
+// flag |= 1 when an observation z or a vertex z is above 0 (nz set: the
+// observation z is Z - 1e-12 nz); clear: zero the flag first.
 cudaError_t launch_hs_check(const double* Z, int64_t M, const double* P1, const double* P2, const double* P3,
-                            int64_t N, int* flag, cudaStream_t st);
+                            int64_t N, int* flag, cudaStream_t st, const double* nz = nullptr, bool clear = true);
 cudaError_t launch_colloc(const double* normals, const double* mid, int64_t N, double* X, double* Y, double* Z,
                           double* dirs, cudaStream_t st);
 cudaError_t launch_sum_chunks(const double* partial, int64_t nchunk, int64_t M, int fields_mask, double* out,

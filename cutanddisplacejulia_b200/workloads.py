@@ -125,3 +125,38 @@ def surface_grid(n=100, extent=4.0):
     X = gx.reshape(-1, order="F")
     Y = gy.reshape(-1, order="F")
     return X, Y, np.zeros_like(X)
+
+
+def ellipse_crack(seed=0, a=1.0, b=1.0, ntri=800, jitter=0.1):
+    """Elliptical crack with semi-axes a (x) and b (y) on z = 0, ~ntri triangles:
+    the unit penny mesh at the lattice spacing that gives ntri, stretched."""
+    # a penny of radius 1 at spacing s has ~ 2 pi / (sqrt(3) s^2 / 2) lattice
+    # points, about twice as many triangles
+    s = np.sqrt(4 * np.pi / (np.sqrt(3) * max(ntri, 8)))
+    P1, P2, P3 = penny(seed=seed, radius=1.0, spacing=s, jitter=jitter)
+    scale = np.array([a, b, 1.0])
+    return P1 * scale, P2 * scale, P3 * scale
+
+
+def crack_batch(seed=0, count=512, n_range=(200, 2000), radius_range=(0.5, 2.0), aspect_range=(0.3, 1.0)):
+    """`count` independent full-space cracks: semi-major axis U[radius_range],
+    aspect ratio U[aspect_range] (1: penny), random orientation (uniform on
+    the sphere) and centre, triangle count log-uniform in n_range.  Returns a
+    list of (P1, P2, P3) and the seeded remote stress (6 components) of each."""
+    rng = np.random.default_rng(seed)
+    out, stresses = [], []
+    for k in range(count):
+        n = int(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
+        a = rng.uniform(*radius_range)
+        b = a * rng.uniform(*aspect_range)
+        P1, P2, P3 = ellipse_crack(seed=int(rng.integers(1 << 30)), a=a, b=b, ntri=n)
+        q = rng.standard_normal(4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        c = rng.uniform(-5, 5, 3)
+        out.append(tuple(P @ R.T + c for P in (P1, P2, P3)))
+        stresses.append(rng.uniform(-1e-3, 1e-3, 6))
+    return out, stresses

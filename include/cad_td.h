@@ -185,6 +185,31 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
  * (n x nrhs, ldb) by the solution. */
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
 
+/* Batched SlipCalculator3D over independent cracks (no counterpart in the
+ * reference, which solves one crack per call; src/SlipCalculator3D.jl:1-33 per
+ * crack).  Device pointers; crack c has N_c = offsets[c+1] - offsets[c]
+ * triangles (offsets: host array of nbatch + 1, offsets[0] = 0) and its
+ * arrays start at 3 * offsets[c]: its N_c x 3 column-major P1, P2, P3,
+ * normals and midpoints, its traction vector [Tn; Tss; Tds] in T and its
+ * slip [Dn; Dss; Dds] in D.  Each crack is assembled at the context's
+ * assembly precision (cad_set_assembly) and solved by FP32 LU (TF32
+ * updates) with FP64 refinement to the context's tolerance (cad_set_solver),
+ * GMRES finishing any crack the refinement leaves.  The cracks run
+ * concurrently on 8 stream lanes inside one CUDA graph, captured on the first
+ * call with these arguments and replayed by identical calls.  Needs device
+ * memory for every crack's 3N_c x 3N_c matrix at once.  rel_residual (host,
+ * nbatch, may be NULL): each crack's final ||b - A D|| / ||b||. */
+int cad_slip_calculator_batched_dev(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1,
+                                    const double* P2, const double* P3, const double* normals,
+                                    const double* midpoints, double nu, double G, double lambda, int hs_flag,
+                                    const double* T, double* D, double* rel_residual);
+
+/* The same with host arrays (copied in and out by the library). */
+int cad_slip_calculator_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1,
+                                const double* P2, const double* P3, const double* normals, const double* midpoints,
+                                double nu, double G, double lambda, int hs_flag, const double* T, double* D,
+                                double* rel_residual);
+
 /* -------------------------------------------------- no-allocation variant ---
  * Summing-overload evaluation that allocates no device memory, for callers
  * that cannot allow a library to call cudaMalloc: hosts whose device memory is
