@@ -56,6 +56,9 @@ WORKLOADS = {
     "dipping": ("TD pair-evals/s (HS dipping crack: influence assembly + FP64 LU solve)",
                 "2x1 crack dipping 60 deg, top at depth 2, half space, %d triangles, 3N=%d unknowns, "
                 "FP64 assembly + LU"),
+    "batch": ("TD pair-evals/s (batch of independent FS cracks: assembly + solve)",
+              "%d full-space penny/elliptical cracks, semi-axis U[0.5,2], aspect U[0.3,1], random orientation, "
+              "200-2000 triangles each (log-uniform), %d triangles in all"),
 }
 METRIC = WORKLOADS["penny"][0]
 
@@ -313,6 +316,134 @@ def batch_rhs_timing(args, ctx, L, stream, asm_args, nrm, A, dev):
                     "refinement to relative residual %g" % MIXED_TOL}
 
 
+def run_batch(args, rank, world, local_rank):
+    """Many independent cracks (the batching configuration): every crack
+    assembled (FP32 far field / FP64 near field) and solved by FP32 LU with
+    FP64 refinement to relative residual 1e-10, all cracks in one captured
+    CUDA graph over 8 stream lanes (cad_slip_calculator_batched_dev).  Beside
+    it: the plain per-crack FP64 path (assembly + FP64 LU, one crack after the
+    other) on the same cracks, and the slip error against it."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cutanddisplacejulia_b200 import _lib, assembly, geometry, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cracks, stresses = workloads.crack_batch(seed=0, count=args.cracks)
+    _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
+    offs = [0]
+    blocks = {k: [] for k in ("P1", "P2", "P3", "nrm", "mid", "T")}
+    for (P1, P2, P3), st in zip(cracks, stresses):
+        N = len(P1)
+        nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+        Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*st, nrm)
+        for k, a in (("P1", P1), ("P2", P2), ("P3", P3), ("nrm", nrm), ("mid", mid)):
+            blocks[k].append(np.asfortranarray(a).ravel(order="F"))
+        blocks["T"].append(np.concatenate([Tn, Tss, Tds]))
+        offs.append(offs[-1] + N)
+    host = {k: np.ascontiguousarray(np.concatenate(v)) for k, v in blocks.items()}
+    d = {k: torch.tensor(v, device=dev) for k, v in host.items()}
+    ntot = offs[-1]
+    offsets = np.asarray(offs, dtype=np.int64)
+    pairs = float(sum((offs[c + 1] - offs[c]) ** 2 for c in range(len(cracks))))
+    D = torch.zeros(3 * ntot, dtype=torch.float64, device=dev)
+    rel = np.zeros(len(cracks))
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
+    torch.cuda.set_stream(stream)
+
+    def batched():
+        _lib.check(L.cad_slip_calculator_batched_dev(ctx, len(cracks), offsets.ctypes.data, d["P1"].data_ptr(),
+                                                     d["P2"].data_ptr(), d["P3"].data_ptr(), d["nrm"].data_ptr(),
+                                                     d["mid"].data_ptr(), NU, G, lam, 0, d["T"].data_ptr(),
+                                                     D.data_ptr(), rel.ctypes.data), ctx)
+
+    with _lib.solver_mode(ctx, "mixed", MIXED_TOL, 400), _lib.assembly_mode(ctx, "mixed", NEAR_FACTOR):
+        t0 = time.perf_counter()
+        batched()                                   # captures the batch graph
+        torch.cuda.synchronize()
+        capture_s = time.perf_counter() - t0
+        for _ in range(max(0, args.warmup - 1)):
+            batched()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        time.sleep(0.3)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = L.cad_kernel_launches(ctx)
+        e0.record(stream)
+        for _ in range(args.steps):
+            batched()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        launches = L.cad_kernel_launches(ctx) - l0
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    Dm = D.clone()
+    # plain per-crack FP64 path on the same cracks: assembly + FP64 LU
+    A = torch.empty(9 * max(offs[c + 1] - offs[c] for c in range(len(cracks))) ** 2, dtype=torch.float64,
+                    device=dev)
+    D64 = torch.empty_like(D)
+
+    def plain():
+        for c in range(len(cracks)):
+            o, N = offs[c], offs[c + 1] - offs[c]
+            n3 = 3 * N
+            _lib.check(L.cad_assemble_dev(ctx, d["nrm"].data_ptr() + 24 * o, d["mid"].data_ptr() + 24 * o,
+                                          d["P1"].data_ptr() + 24 * o, d["P2"].data_ptr() + 24 * o,
+                                          d["P3"].data_ptr() + 24 * o, N, NU, G, lam, 0, A.data_ptr(), n3), ctx)
+            D64[3 * o:3 * o + n3].copy_(d["T"][3 * o:3 * o + n3])
+            _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, D64.data_ptr() + 24 * o, n3, 1), ctx)
+    plain()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    errs = [float(torch.linalg.vector_norm(Dm[3 * offs[c]:3 * offs[c + 1]] - D64[3 * offs[c]:3 * offs[c + 1]]) /
+                  torch.linalg.vector_norm(D64[3 * offs[c]:3 * offs[c + 1]])) for c in range(len(cracks))]
+    # end to end through the host C ABI (host arrays in, slips back to the host)
+    Dh = np.zeros(3 * ntot)
+    with _lib.solver_mode(ctx, "mixed", MIXED_TOL, 400), _lib.assembly_mode(ctx, "mixed", NEAR_FACTOR):
+        def e2e_call():
+            _lib.check(L.cad_slip_calculator_batched(ctx, len(cracks), offsets.ctypes.data, host["P1"].ctypes.data,
+                                                     host["P2"].ctypes.data, host["P3"].ctypes.data,
+                                                     host["nrm"].ctypes.data, host["mid"].ctypes.data, NU, G, lam, 0,
+                                                     host["T"].ctypes.data, Dh.ctypes.data, rel.ctypes.data), ctx)
+        e2e_call()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_call()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    line = {
+        "metric": WORKLOADS["batch"][0], "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 + f64 refinement", "data": "synthetic",
+        "config": {"workload": WORKLOADS["batch"][1] % (len(cracks), ntot), "pairs_per_step": pairs,
+                   "system_matrices_gb": 9 * pairs * 8 / 1e9, "l2": "inputs larger than L2"},
+        "breakdown_ms": {"batched_graph": ms, "graph_capture_first_call_s": capture_s},
+        "plain_fp64_per_crack_ms": plain_ms, "speedup_vs_plain_fp64": plain_ms / ms,
+        "max_crack_slip_rel_err_vs_fp64": max(errs), "max_rel_residual": float(rel.max()),
+        "clocks": clk, "gpu_launches": int(launches),
+        "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(18 * ntot * 8),
+                "d2h_bytes_per_step": int(3 * ntot * 8), "ms_per_step": e2e_ms,
+                "api": "cad_slip_calculator_batched (host C ABI)"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -500,6 +631,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="penny",
                     help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
     ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")
+    ap.add_argument("--cracks", type=int, default=512, help="cracks of the batch workload")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -516,7 +648,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "batch":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
