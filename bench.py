@@ -56,6 +56,8 @@ WORKLOADS = {
     "dipping": ("TD pair-evals/s (HS dipping crack: influence assembly + FP64 LU solve)",
                 "2x1 crack dipping 60 deg, top at depth 2, half space, %d triangles, 3N=%d unknowns, "
                 "FP64 assembly + LU"),
+    "learned": ("TD pair-evals/s (HS dipping crack: FP64 assembly + learned-preconditioner GMRES to 1e-10)",
+                "3x1.5 crack dipping 45 deg, top at depth 2, half space, %d triangles, 3N=%d unknowns"),
     "batch": ("TD pair-evals/s (batch of independent FS cracks: assembly + solve)",
               "%d full-space penny/elliptical cracks, semi-axis U[0.5,2], aspect U[0.3,1], random orientation, "
               "200-2000 triangles each (log-uniform), %d triangles in all"),
@@ -444,6 +446,106 @@ def run_batch(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_learned(args, rank, world, local_rank):
+    """The learned-preconditioner configuration: a network trained (by the
+    library's BF16 kernels) on exact inverse blocks of small seeded meshes,
+    applied to a large half-space crack as a block-sparse right
+    preconditioner of FP64 GMRES; beside it block-Jacobi GMRES and the FP64
+    dense LU (the fallback, and the judge of the solution error)."""
+    import numpy as np
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib, assembly, geometry, precond, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
+    torch.cuda.set_stream(stream)
+    # training
+    t0 = time.perf_counter()
+    meshes = precond.training_meshes(seed=0, count=args.train_meshes, n_range=(300, 900))
+    X, T = precond.training_set(meshes, device=local_rank)
+    t1 = time.perf_counter()
+    net = precond.Network(seed=0, device=local_rank)
+    hist = net.train(X, T, steps=args.train_steps, batch=4096, lr=1e-3)
+    t2 = time.perf_counter()
+    # the system
+    P1, P2, P3 = workloads.dipping_rect(seed=0, ntri=args.ntri, length=3.0, width=1.5, dip=45.0, top_depth=2.0)
+    n = len(P1)
+    n3 = 3 * n
+    nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
+    Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*workloads.remote_stress(seed=0), nrm)
+    b = torch.tensor(np.concatenate([Tn, Tss, Tds]), device=dev)
+
+    def col(a):
+        return torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device=dev)
+    dP1, dP2, dP3, dN, dM = col(P1), col(P2), col(P3), col(nrm), col(mid)
+    A = torch.empty(n3 * n3, dtype=torch.float64, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1])
+
+    asm_ms = timed(lambda: _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(),
+                                                         dP2.data_ptr(), dP3.data_ptr(), n, NU, G, lam, 1,
+                                                         A.data_ptr(), n3), ctx))
+    solves = {}
+    xs = {}
+    nbr1 = torch.arange(n, dtype=torch.int32, device=dev)
+    bj = torch.empty((n, 9), dtype=torch.float32, device=dev)
+    setup_ms = {}
+    t3 = time.perf_counter()
+    M = precond.LearnedPreconditioner(net, P1, P2, P3, G)
+    torch.cuda.synchronize()
+    setup_ms["learned"] = (time.perf_counter() - t3) * 1e3
+    setup_ms["block_jacobi"] = timed(lambda: _lib.check(L.cad_block_jacobi_dev(ctx, n, A.data_ptr(), n3,
+                                                                               nbr1.data_ptr(), bj.data_ptr()), ctx))
+    for name in ("learned", "block_jacobi"):
+        if name == "learned":
+            M.install()
+        else:
+            _lib.check(L.cad_set_preconditioner(ctx, n, 1, nbr1.data_ptr(), bj.data_ptr()), ctx)
+        x = b.clone()
+        with _lib.solver_mode(ctx, "gmres_spai", MIXED_TOL, args.max_iter):
+            rc = []
+            ms = timed(lambda: rc.append(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, x.data_ptr(), n3, 1)))
+            its, rr = _lib.last_solve_stats(ctx)
+        L.cad_set_preconditioner(ctx, 0, 0, None, None)
+        xs[name] = x
+        solves[name] = {"ms": ms, "iterations": its, "rel_residual": rr, "converged": rc[0] == 0,
+                        "setup_ms": setup_ms[name]}
+    # FP64 dense LU (overwrites A)
+    x = b.clone()
+    with _lib.solver_mode(ctx, "lu64"):
+        lu_ms = timed(lambda: _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, x.data_ptr(), n3, 1), ctx))
+    solves["fp64_lu"] = {"ms": lu_ms}
+    for name in ("learned", "block_jacobi"):
+        solves[name]["slip_rel_err_vs_fp64_lu"] = float(torch.linalg.vector_norm(xs[name] - x) /
+                                                         torch.linalg.vector_norm(x))
+    pairs = float(n) * n
+    step_ms = asm_ms + solves["learned"]["ms"]
+    line = {
+        "metric": WORKLOADS["learned"][0], "value": world * pairs / (step_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": 1, "warmup": 0, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (network bf16)", "data": "synthetic",
+        "config": {"workload": WORKLOADS["learned"][1] % (n, n3), "pairs_per_step": pairs},
+        "breakdown_ms": {"assembly_fp64": asm_ms, "learned_gmres": solves["learned"]["ms"]},
+        "solves_to_rel_residual_1e-10": solves,
+        "speedup_learned_vs_fp64_lu": lu_ms / solves["learned"]["ms"],
+        "training": {"meshes": len(meshes), "samples": int(X.shape[0]), "data_generation_s": t1 - t0,
+                     "train_s": t2 - t1, "steps": args.train_steps, "loss_first_last": [hist[0], hist[-1]]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -632,6 +734,9 @@ def main():
                     help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
     ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")
     ap.add_argument("--cracks", type=int, default=512, help="cracks of the batch workload")
+    ap.add_argument("--train-meshes", type=int, default=32, help="training meshes of the learned workload")
+    ap.add_argument("--train-steps", type=int, default=3000, help="training steps of the learned workload")
+    ap.add_argument("--max-iter", type=int, default=3000, help="GMRES iteration cap of the learned workload")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -650,6 +755,8 @@ def main():
     try:
         if args.workload == "batch":
             run_batch(args, rank, world, local_rank)
+        elif args.workload == "learned":
+            run_learned(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

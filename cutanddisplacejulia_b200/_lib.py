@@ -25,6 +25,7 @@ CAD_ERR_ARG = 9
 CAD_ERR_TOO_LARGE = 10
 CAD_SOLVER_LU64 = 0
 CAD_SOLVER_MIXED = 1
+CAD_SOLVER_GMRES_SPAI = 2
 CAD_ASSEMBLY_FP64 = 0
 CAD_ASSEMBLY_MIXED = 1
 
@@ -33,7 +34,8 @@ EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
     "cad_version", "cad_kernel_launches", "cad_set_assembly", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
     "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
-    "cad_solve_dev", "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
+    "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
+    "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
 ]
 
 
@@ -93,6 +95,10 @@ def load():
     L.cad_solve_dev.argtypes = [P, I64, P, I64, P, I64, I64]
     L.cad_slip_calculator_batched_dev.argtypes = [P, I64, P, P, P, P, P, P, D, D, D, INT, P, P, P]
     L.cad_slip_calculator_batched.argtypes = [P, I64, P, P, P, P, P, P, D, D, D, INT, P, P, P]
+    L.cad_set_preconditioner.argtypes = [P, I64, INT, P, P]
+    L.cad_block_jacobi_dev.argtypes = [P, I64, P, I64, P, P]
+    L.cad_lpc_param_count.restype = I64
+    L.cad_lpc_step.argtypes = [P, P, P, P, I64, P, P, P, P, P, I64, ctypes.c_float]
     L.cad_td_sum_eval_noalloc.argtypes = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
     _lib = L
     return L
@@ -131,9 +137,9 @@ class solver_mode:
     FP64 GMRES to relative residual `tol`), restoring the FP64 LU afterwards."""
 
     def __init__(self, ctx, solver="lu64", tol=1e-10, max_iter=200):
-        modes = {"lu64": CAD_SOLVER_LU64, "mixed": CAD_SOLVER_MIXED}
+        modes = {"lu64": CAD_SOLVER_LU64, "mixed": CAD_SOLVER_MIXED, "gmres_spai": CAD_SOLVER_GMRES_SPAI}
         if solver not in modes:
-            raise ValueError("solver must be 'lu64' or 'mixed'")
+            raise ValueError("solver must be 'lu64', 'mixed' or 'gmres_spai'")
         self.ctx, self.mode, self.tol, self.max_iter = ctx, modes[solver], float(tol), int(max_iter)
 
     def __enter__(self):

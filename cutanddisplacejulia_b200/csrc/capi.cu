@@ -17,6 +17,7 @@
 #include "../../include/cad_td.h"
 #include "lu.h"
 #include "mixed.h"
+#include "mlp.h"
 #include "td_device.cuh"
 #include "td_kernels.h"
 
@@ -30,7 +31,8 @@ namespace {
 
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
-    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_COUNT
+    S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
+    S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -84,6 +86,10 @@ struct cad_ctx {
     int64_t launches = 0;   // own kernel launches issued through this context
     int solver = CAD_SOLVER_LU64;   // cad_set_solver
     int assembly = CAD_ASSEMBLY_FP64;   // cad_set_assembly
+    const int* spai_nbr = nullptr;      // cad_set_preconditioner (caller's device memory)
+    const float* spai_blocks = nullptr;
+    int64_t spai_N = 0;
+    int spai_k = 0;
     double near_factor = 3.0;
     double tol = 1e-10;
     int max_iter = 200;
@@ -353,9 +359,71 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     return CAD_OK;
 }
 
+// FP64 GMRES right-preconditioned by the block-sparse preconditioner of
+// cad_set_preconditioner (no factorisation); B := A^-1 B, A unchanged.
+int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
+{
+    if (!ctx->spai_nbr || 3 * ctx->spai_N != n)
+        return fail(ctx, CAD_ERR_ARG, "no preconditioner for this system size (cad_set_preconditioner)");
+    void *kry, *sync, *work;
+    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (kRestart + 1) + 3 * (size_t)n + 2 * (kRestart + 1)) * sizeof(double),
+                       &kry))
+        return r;
+    if (int r = ensure(ctx, S_SYNC, mixed_sync_ints(n) * sizeof(int), &sync)) return r;
+    if (int r = ensure(ctx, S_WORK, (size_t)n * sizeof(double), &work)) return r;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    ctx->timed[1] = ctx->timed[2] = false;
+    double* V = (double*)kry;
+    double* w = V + (size_t)n * (kRestart + 1);
+    GmresArgs g{};
+    g.blas = ctx->blas;
+    g.stream = ctx->stream;
+    g.n = n;
+    g.A = A;
+    g.lda = lda;
+    g.tol = ctx->tol;
+    g.max_iter = ctx->max_iter;
+    g.restart = kRestart;
+    g.V = V;
+    g.w = w;
+    g.z = w + n;
+    g.r = w + 2 * n;
+    g.hd = w + 3 * n;
+    g.sync = (int*)sync;
+    g.launches = &ctx->launches;
+    g.spai_nbr = ctx->spai_nbr;
+    g.spai_blocks = ctx->spai_blocks;
+    g.spai_k = ctx->spai_k;
+    ctx->last_iters = 0;
+    ctx->last_relres = 0.0;
+    bool converged = true;
+    for (int64_t c = 0; c < nrhs; ++c) {
+        g.b = B + c * ldb;
+        g.x = (double*)work;
+        GmresResult res{};
+        const int st = gmres_ir_solve(g, &res);
+        if (st == GMRES_CUDA_ERROR || st == GMRES_BLAS_ERROR || st == GMRES_TIMEOUT)
+            return fail(ctx, CAD_ERR_CUDA, "preconditioned GMRES: CUDA or cuBLAS error");
+        converged = converged && st == GMRES_OK;
+        ctx->last_iters += res.iterations;
+        ctx->last_relres = res.rel_residual > ctx->last_relres ? res.rel_residual : ctx->last_relres;
+        CK(cudaMemcpyAsync(B + c * ldb, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    ctx->timed[1] = true;
+    if (!converged)
+        return fail(ctx, CAD_ERR_NOT_CONVERGED, "preconditioned GMRES did not reach the residual tolerance");
+    return CAD_OK;
+}
+
 int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
 {
     if (n == 0 || nrhs == 0) return CAD_OK;
+    if (ctx->solver == CAD_SOLVER_GMRES_SPAI) {
+        if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
+            return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
+        return solve_spai_device(ctx, n, A, lda, B, ldb, nrhs);
+    }
     if (ctx->solver == CAD_SOLVER_MIXED) {
         if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
             return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
@@ -384,9 +452,12 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     return CAD_OK;
 }
 
-// info of the last factorisation: 0 when every pivot was non-zero
+// info of the last factorisation: 0 when every pivot was non-zero (and when
+// the solver factorises nothing)
 int read_info(cad_ctx* ctx, int* info)
 {
+    *info = 0;
+    if (ctx->solver == CAD_SOLVER_GMRES_SPAI || !ctx->buf[S_INFO].p) return CAD_OK;
     int h = 0;
     CK(cudaMemcpyAsync(&h, ctx->buf[S_INFO].p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -775,7 +846,8 @@ int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor)
 int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
 {
     if (!ctx) return CAD_ERR_ARG;
-    if ((mode != CAD_SOLVER_LU64 && mode != CAD_SOLVER_MIXED) || !(tol > 0.0) || max_iter < 1)
+    if ((mode != CAD_SOLVER_LU64 && mode != CAD_SOLVER_MIXED && mode != CAD_SOLVER_GMRES_SPAI) || !(tol > 0.0) ||
+        max_iter < 1)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->solver = mode;
     ctx->tol = tol;
@@ -1093,6 +1165,60 @@ int cad_slip_calculator_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* off
         CK(cudaMemcpyAsync(D, t + 3 * ntot, (size_t)3 * ntot * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    return CAD_OK;
+}
+
+int cad_set_preconditioner(cad_ctx* ctx, int64_t N, int k, const int* nbr, const float* blocks)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (N < 0 || k < 0 || (N > 0 && (k < 1 || !nbr || !blocks))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->spai_N = N;
+    ctx->spai_k = k;
+    ctx->spai_nbr = N > 0 ? nbr : nullptr;
+    ctx->spai_blocks = N > 0 ? blocks : nullptr;
+    return CAD_OK;
+}
+
+int cad_block_jacobi_dev(cad_ctx* ctx, int64_t N, const double* A, int64_t lda, int* nbr, float* blocks)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || lda < 3 * N || (N > 0 && (!A || !nbr || !blocks))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ++ctx->launches;
+    CK(block_jacobi(ctx->stream, A, lda, N, nbr, blocks));
+    return CAD_OK;
+}
+
+int64_t cad_lpc_param_count(void) { return (int64_t)mlp_param_count(); }
+
+int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, int64_t rows, float* out, float* grads,
+                 float* loss, float* adam_m, float* adam_v, int64_t t, float lr)
+{
+    if (int r = set_device(ctx)) return r;
+    if (rows < 0 || !params || (rows > 0 && !X) || (grads && !T) || ((adam_m || adam_v) && (!adam_m || !adam_v ||
+                                                                                             !grads || t < 1)))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (rows == 0) return CAD_OK;
+    if (rows > INT32_MAX) return fail(ctx, CAD_ERR_ARG, "too many rows");
+    void* ws;
+    if (int r = ensure(ctx, S_MLP, mlp_workspace_bytes(rows), &ws)) return r;
+    MlpStep st{};
+    st.stream = ctx->stream;
+    st.params = params;
+    st.X = X;
+    st.T = T;
+    st.rows = rows;
+    st.out = out;
+    st.grads = grads;
+    st.loss = loss;
+    st.adam_m = adam_m;
+    st.adam_v = adam_v;
+    st.lr = lr;
+    st.bias_c1 = 1.f - powf(0.9f, (float)t);
+    st.bias_c2 = 1.f - powf(0.999f, (float)t);
+    st.workspace = ws;
+    st.launches = &ctx->launches;
+    const int e = mlp_step(st);
+    if (e != 0) return cuda_fail(ctx, (cudaError_t)e, "learned-preconditioner network step");
     return CAD_OK;
 }
 

@@ -444,6 +444,39 @@ __global__ void pivots_to_perm_kernel(const int* __restrict__ ipiv, int n, int* 
     for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = s_perm[i];
 }
 
+// The same in global memory, for n beyond what shared memory holds.
+__global__ void pivots_to_perm_global_kernel(const int* __restrict__ ipiv, int n, int* __restrict__ perm)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < n; ++k) {
+            const int q = ipiv[k];
+            const int t = perm[k];
+            perm[k] = perm[q];
+            perm[q] = t;
+        }
+}
+
+// perm from ipiv on stream st (shared-memory kernel where n ints fit)
+cudaError_t launch_pivots_to_perm(cudaStream_t st, const int* ipiv, int64_t n, int* perm)
+{
+    if (n <= 0) return cudaSuccess;
+    int dev = 0, smem_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t psmem = (size_t)n * sizeof(int);
+    if (psmem <= (size_t)smem_optin) {
+        cudaError_t e = cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)psmem);
+        if (e != cudaSuccess) return e;
+        pivots_to_perm_kernel<<<1, 1024, psmem, st>>>(ipiv, (int)n, perm);
+    } else {
+        pivots_to_perm_global_kernel<<<1, 1024, 0, st>>>(ipiv, (int)n, perm);
+    }
+    return cudaGetLastError();
+}
+
 // Y[i, c] = X[perm[i], c]
 template <typename T>
 __global__ void permute_rows_kernel(const T* __restrict__ X, int64_t ldx, const int* __restrict__ perm, int n,
@@ -651,12 +684,8 @@ struct Lu {
     void solve(const T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X, int64_t ldx, int* perm)
     {
         if (!ok()) return;
-        const size_t psmem = (size_t)n * sizeof(int);
-        err = cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-        if (!ok()) return;
-        pivots_to_perm_kernel<<<1, 1024, psmem, st>>>(ipiv, (int)n, perm);
+        err = launch_pivots_to_perm(st, ipiv, n, perm);
         ++launches;
-        err = cudaGetLastError();
         if (!ok()) return;
         permute_rows_kernel<T><<<dim3((unsigned)((n + 255) / 256), nrhs), 256, 0, st>>>(B, ldb, perm, (int)n, nrhs, X,
                                                                                         ldx);
@@ -866,13 +895,8 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     lu.info = info;
     configure(lu);
     // nb bounds the pivots one row-swap launch applies; a leaf cluster holds
-    // at most cluster * 512 * 8 rows; the pivot-to-permutation kernel keeps n
-    // ints in shared memory
-    int dev = 0, smem_optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (nb < 1 || nb > kMaxSwaps || n > (int64_t)lu.cluster * kLeafThreads * 8 ||
-        n * (int64_t)sizeof(int) > smem_optin)
+    // at most cluster * 512 * 8 rows
+    if (nb < 1 || nb > kMaxSwaps || n > (int64_t)lu.cluster * kLeafThreads * 8 || n > INT32_MAX)
         return LU_TOO_LARGE;
     if (cublasSetStream(lu.main_h, lu.main_st) != CUBLAS_STATUS_SUCCESS ||
         cublasSetStream(lu.side_h, lu.side_st) != CUBLAS_STATUS_SUCCESS)
@@ -913,12 +937,7 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
 int lu_pivots_to_perm(const LuStreams& s, const int* ipiv, int64_t n, int* perm)
 {
     if (n <= 0) return LU_OK;
-    const size_t psmem = (size_t)n * sizeof(int);
-    if (cudaFuncSetAttribute(pivots_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) !=
-        cudaSuccess)
-        return LU_TOO_LARGE;
-    pivots_to_perm_kernel<<<1, 1024, psmem, s.main>>>(ipiv, (int)n, perm);
-    if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
+    if (launch_pivots_to_perm(s.main, ipiv, n, perm) != cudaSuccess) return LU_CUDA_ERROR;
     if (s.launches) ++*s.launches;
     return LU_OK;
 }

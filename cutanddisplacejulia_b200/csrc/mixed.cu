@@ -23,6 +23,7 @@
 
 #include "lu.h"
 #include "mixed.h"
+#include "mlp.h"
 
 namespace cad {
 
@@ -240,10 +241,17 @@ struct Precond {
     int* sync;   // [2 * nblk flags][2 tickets][fail]
     cudaStream_t st;
     int64_t* launches;
+    const int* spai_nbr;
+    const float* spai_blocks;
+    int spai_k;
 
     // z = M^-1 v (FP64 in and out, FP32 inside)
     bool apply(const double* v, double* z) const
     {
+        if (spai_nbr) {
+            if (launches) ++*launches;
+            return spai_apply(st, spai_nbr, spai_blocks, spai_k, v, n / 3, z) == cudaSuccess;
+        }
         if (cudaMemsetAsync(sync, 0, (size_t)(2 * nblk + 2) * sizeof(int), st) != cudaSuccess) return false;
         int* fl = sync;
         int* fu = sync + nblk;
@@ -274,7 +282,8 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
     cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
     const int nblk = (int)((n + kRB - 1) / kRB);
-    Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.y32, a.x32, a.sync, st, a.launches};
+    Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.y32, a.x32, a.sync, st, a.launches, a.spai_nbr, a.spai_blocks,
+              a.spai_k};
     double* V = a.V;        // n x (m + 1)
     double* w = a.w;
     double* z = a.z;

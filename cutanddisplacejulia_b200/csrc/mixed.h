@@ -47,6 +47,11 @@ struct GmresArgs {
     float* x32;        // n
     int* sync;         // mixed_sync_ints(n)
     int64_t* launches;
+    // block-sparse preconditioner instead of the FP32 factors (when set):
+    // n / 3 elements x spai_k 3 x 3 blocks at the neighbours spai_nbr
+    const int* spai_nbr = nullptr;
+    const float* spai_blocks = nullptr;
+    int spai_k = 0;
 };
 
 struct GmresResult {

@@ -51,6 +51,7 @@ extern "C" {
 /* Solvers for the dense system (cad_set_solver). */
 #define CAD_SOLVER_LU64 0  /* FP64 LU with partial pivoting: the reference's A\b (default) */
 #define CAD_SOLVER_MIXED 1 /* FP32 LU (TF32 tensor-core updates) preconditioning FP64 GMRES */
+#define CAD_SOLVER_GMRES_SPAI 2 /* FP64 GMRES, block-sparse preconditioner of cad_set_preconditioner */
 
 /* Precision of the system-matrix assembly (cad_set_assembly). */
 #define CAD_ASSEMBLY_FP64 0  /* every pair in FP64, as the reference (default) */
@@ -184,6 +185,31 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
 /* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
  * (n x nrhs, ldb) by the solution. */
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
+
+/* ---------------------------------------------- learned preconditioner ---
+ * No counterpart in the reference (its only solver is the dense A\b).  A
+ * block-sparse approximate inverse M (N elements x k blocks of 3 x 3, FP32,
+ * row-major; block q of element i acts on the unknowns of element
+ * nbr[i*k + q], unknown order [Dn; Dss; Dds] as in SlipCalculator3D)
+ * right-preconditions FP64 restarted GMRES when the solver is
+ * CAD_SOLVER_GMRES_SPAI.  The device arrays are used in place: keep them
+ * alive while the setting stands.  cad_block_jacobi_dev fills the k = 1
+ * block-Jacobi preconditioner (inverses of the 3 x 3 self blocks of A). */
+int cad_set_preconditioner(cad_ctx* ctx, int64_t N, int k, const int* nbr, const float* blocks);
+int cad_block_jacobi_dev(cad_ctx* ctx, int64_t N, const double* A, int64_t lda, int* nbr, float* blocks);
+/* The network that predicts M's blocks from each element's 16 nearest
+ * elements: 112 inputs (per neighbour: centroid offset and normal in the
+ * element's own frame, area ratio), two hidden layers of 256 (ReLU), 144
+ * outputs (16 blocks of 9), BF16 weights and activations, FP32 accumulation,
+ * FP32 master weights (cad_lpc_param_count floats: W1, b1, W2, b2, W3, b3,
+ * each W in x out, row-major).  cad_lpc_step runs one pass over `rows`
+ * samples (device X rows x 112, T rows x 144): the output to `out` if set;
+ * with grads set, the gradient of the mean squared error against T and, with
+ * loss set, the sum of squared errors (device float); with adam_m and adam_v
+ * set, one Adam step (step number t >= 1, step size lr) on params. */
+int64_t cad_lpc_param_count(void);
+int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, int64_t rows, float* out, float* grads,
+                 float* loss, float* adam_m, float* adam_v, int64_t t, float lr);
 
 /* Batched SlipCalculator3D over independent cracks (no counterpart in the
  * reference, which solves one crack per call; src/SlipCalculator3D.jl:1-33 per
