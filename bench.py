@@ -546,6 +546,70 @@ def run_learned(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def learned_solve_timing(args, ctx, L, stream, step_asm_args, P, A, b0, x64, ms_fp64, dev):
+    """FP64 assembly + FP64 GMRES right-preconditioned by the learned sparse
+    approximate inverse (network trained here, by the library's kernels, on
+    small seeded meshes): time against the FP64 step, slip error against the
+    FP64 LU solution x64."""
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib, precond
+    dN, dM, dP1, dP2, dP3, n, lam, hs = step_asm_args
+    n3 = 3 * n
+    t0 = time.perf_counter()
+    meshes = precond.training_meshes(seed=0, count=args.train_meshes, n_range=(300, 900))
+    X, T = precond.training_set(meshes, device=dev.index)
+    net = precond.Network(seed=0, device=dev.index)
+    net.train(X, T, steps=args.train_steps, batch=4096, lr=1e-3)
+    train_s = time.perf_counter() - t0
+    xl = torch.empty_like(x64)
+
+    def step(evs=None):
+        if evs:
+            evs[0].record(stream)
+        _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
+                                      dP3.data_ptr(), n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
+        if evs:
+            evs[1].record(stream)
+        M = precond.LearnedPreconditioner(net, *P, G).install()
+        if evs:
+            evs[2].record(stream)
+        xl.copy_(b0)
+        _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, xl.data_ptr(), n3, 1), ctx)
+        if evs:
+            evs[3].record(stream)
+        return M
+
+    with _lib.solver_mode(ctx, "gmres_spai", MIXED_TOL, args.max_iter):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+        t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        keep = []
+        t0e.record(stream)
+        for k in range(args.steps):
+            keep.append(step(evs[k]))
+        t1e.record(stream)
+        torch.cuda.synchronize()
+        its, rr = _lib.last_solve_stats(ctx)
+    L.cad_set_preconditioner(ctx, 0, 0, None, None)
+    ms = t0e.elapsed_time(t1e) / args.steps
+    Am = A.view(n3, n3).t()
+    resid = float(torch.linalg.vector_norm(Am @ xl - b0) / torch.linalg.vector_norm(b0))
+    return {"solver": "FP64 GMRES(30), right preconditioner: learned 16-neighbour block sparse approximate inverse",
+            "assembly": "FP64", "tol": MIXED_TOL, "ms_per_step": ms,
+            "breakdown_ms": {"assembly": statistics.mean(e[0].elapsed_time(e[1]) for e in evs),
+                             "preconditioner_setup (features on the host + network)":
+                                 statistics.mean(e[1].elapsed_time(e[2]) for e in evs),
+                             "gmres": statistics.mean(e[2].elapsed_time(e[3]) for e in evs)},
+            "gmres_iterations": its, "rel_residual": resid,
+            "slip_rel_err_vs_fp64_lu": float(torch.linalg.vector_norm(xl - x64) / torch.linalg.vector_norm(x64)),
+            "step_speedup_vs_fp64": ms_fp64 / ms,
+            "training": {"meshes": args.train_meshes, "steps": args.train_steps, "seconds": train_s,
+                         "note": "trained in this run; one-time cost, reusable for any mesh"}}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -632,6 +696,9 @@ def run_ours(args, rank, world, local_rank):
 
     mixed = None if args.no_mixed else mixed_solve_timing(args, ctx, L, stream, step_asm_args=(
         dN, dM, dP1, dP2, dP3, n, lam, hs), A=A, b0=b0, x64=x, ms_fp64=ms_step, world=world, dev=dev)
+    use_learned = args.learned if args.learned is not None else args.workload == "dipping"
+    learned = None if not use_learned else learned_solve_timing(
+        args, ctx, L, stream, (dN, dM, dP1, dP2, dP3, n, lam, hs), (P1, P2, P3), A, b0, x, ms_step, dev)
     batch = None if args.batch_rhs <= 0 else batch_rhs_timing(args, ctx, L, stream, (dN, dM, dP1, dP2, dP3, n, lam,
                                                                                       hs), nrm, A, dev)
 
@@ -714,6 +781,7 @@ def run_ours(args, rank, world, local_rank):
                            "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
         "cpu_baseline": cpu,
         "mixed": mixed,
+        "learned": learned,
         "batch_rhs": batch,
     }
     if rank == 0:
@@ -737,6 +805,9 @@ def main():
     ap.add_argument("--train-meshes", type=int, default=32, help="training meshes of the learned workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training steps of the learned workload")
     ap.add_argument("--max-iter", type=int, default=3000, help="GMRES iteration cap of the learned workload")
+    ap.add_argument("--learned", dest="learned", action="store_true", default=None,
+                    help="also time the learned-preconditioner GMRES solve (default: on for --workload dipping)")
+    ap.add_argument("--no-learned", dest="learned", action="store_false")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
