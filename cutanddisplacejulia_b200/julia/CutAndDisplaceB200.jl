@@ -123,4 +123,36 @@ function SlipCalculator3D(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSF
     return Dn, Dss, Dds, A, b
 end
 
+# Precision settings (no counterpart in the reference): solver 0 = FP64 LU
+# (default), 1 = FP32/TF32 LU + FP64 GMRES, 2 = FP64 GMRES with the block-sparse
+# preconditioner set below; assembly 0 = FP64, 1 = FP32 far field.
+set_solver(mode::Integer, tol::Real=1e-10, max_iter::Integer=200) =
+    check(ccall((:cad_set_solver, libcad), Cint, (Ptr{Cvoid}, Cint, Float64, Cint), ctx(), mode, tol, max_iter))
+set_assembly(mode::Integer, near_factor::Real=3.0) =
+    check(ccall((:cad_set_assembly, libcad), Cint, (Ptr{Cvoid}, Cint, Float64), ctx(), mode, near_factor))
+
+# SlipCalculator3D over many independent cracks in one call: cracks is a vector
+# of (P1, P2, P3, MidPoint, FaceNormalVector, Tn, Tss, Tds) tuples; returns a
+# vector of (Dn, Dss, Dds) and the final relative residuals.
+function SlipCalculator3D_batched(cracks, ν, G, λ, HSFlag)
+    offs = Int64[0]
+    for c in cracks
+        push!(offs, offs[end] + size(c[1], 1))
+    end
+    cat(k) = reduce(vcat, [vec(f64(c[k])) for c in cracks])
+    T = reduce(vcat, [vcat(vec(c[6]), vec(c[7]), vec(c[8])) for c in cracks])
+    D = zeros(3 * offs[end]); rel = zeros(length(cracks))
+    check(ccall((:cad_slip_calculator_batched, libcad), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Float64, Float64, Float64, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        ctx(), length(cracks), offs, cat(1), cat(2), cat(3), cat(5), cat(4), ν, G, λ, HSFlag, T, D, rel))
+    out = Vector{NTuple{3,Vector{Float64}}}()
+    for c in 1:length(cracks)
+        o = offs[c]; n = offs[c + 1] - o
+        d = D[3o+1:3o+3n]
+        push!(out, (d[1:n], d[n+1:2n], d[2n+1:3n]))
+    end
+    return out, rel
+end
+
 end # module
