@@ -41,8 +41,9 @@ FALG_ASSEMBLY_FS = 2960.0 + 288.0
 # collocation pairs) plus the same traction epilogue.
 FALG_ASSEMBLY_HS = 43867.0 + 288.0
 # DRAM bytes (read + write) of one assembly launch from the committed ncu captures
-# (profiles/td_pair_kernel_*.md): (triangles captured, bytes).  Output scales as N^2.
-PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 77.27e6 + 2627.06e6)}
+# (profiles/td_pair_kernel_*.md): (triangles captured, bytes; the half-space one
+# as dram__bytes.sum.per_second x duration).  Output scales as N^2.
+PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 144.824e9 * 5.114e-3)}
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
@@ -770,7 +771,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
                      "falg_per_pair": falg,
                      "traffic": PAIR_TRAFFIC[args.workload][1] * (n / PAIR_TRAFFIC[args.workload][0]) ** 2,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                     "traffic_source": "ncu DRAM bytes (read + write) of one launch at "
                                        "N=%d, scaled by (N/%d)^2" % (PAIR_TRAFFIC[args.workload][0],
                                                                       PAIR_TRAFFIC[args.workload][0]),
                      "step_share": asm_ms / ms_step},
