@@ -33,7 +33,7 @@ CAD_ASSEMBLY_MIXED = 1
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
     "cad_version", "cad_kernel_launches", "cad_set_assembly", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
-    "cad_slip_calculator", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
+    "cad_slip_calculator", "cad_slip_calculator_fixed", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
     "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
     "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
 ]
@@ -88,6 +88,7 @@ def load():
     L.cad_influence_traction.argtypes = [P, P, P, P, P, P, I64, D, D, D, P, INT, P]
     L.cad_slip_calculator.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, P, P, P]
     L.cad_solve.argtypes = [P, I64, P, P, I64, P]
+    L.cad_slip_calculator_fixed.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, P, P, P, P]
     tdd = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
     L.cad_td_inf_dev.argtypes = tdd
     L.cad_td_sum_eval_dev.argtypes = tdd

@@ -74,13 +74,16 @@ def KnockOutFixedRows(FixedEls, Tn, Tds, Tss):
 
 def CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, nu, G, lam, FixedEls, HSFlag, n,
                                  device=0):
-    """Traction influence matrices (TractionInf of nine n x n arrays)."""
+    """Traction influence matrices (TractionInf of nine n x n arrays; with
+    elements marked 1 in FixedEls, displacement-influence rows for them and
+    only the other elements' columns, n x n_free)."""
     P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
     N = P1.shape[0]
     nrm = _tri(FaceNormalVector)
     mid = _tri(MidPoint)
     fixed = None if FixedEls is None else np.ascontiguousarray(np.asarray(FixedEls, dtype=np.float64).reshape(-1))
-    out = [np.zeros((N, N), order="F") for _ in range(9)]
+    nf = N if fixed is None else int(np.sum(fixed != 1))
+    out = [np.zeros((N, nf), order="F") for _ in range(9)]
     ctx = _lib.context(device)
     rc = _lib.load().cad_influence_traction(ctx, nrm.ctypes.data, mid.ctypes.data, P1.ctypes.data, P2.ctypes.data,
                                             P3.ctypes.data, N, float(nu), float(G), float(lam),
@@ -103,11 +106,25 @@ def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
     nrm = _tri(FaceNormalVector)
     mid = _tri(MidPoint)
     Tn, Tds, Tss = SetupTractionVector(BoundaryConditions, nrm, N, G, lam)
-    if FixedEls is not None:
-        Tn, Tds, Tss = KnockOutFixedRows(FixedEls, Tn, Tds, Tss)
-        if np.any(np.asarray(FixedEls).reshape(-1) == 1):
-            raise _lib.CadError(_lib.CAD_ERR_UNSUPPORTED, "fixed elements are not supported by this entry point")
+    fixed = None
+    if FixedEls is not None and np.any(np.asarray(FixedEls).reshape(-1) == 1):
+        fixed = np.ascontiguousarray(np.asarray(FixedEls, dtype=np.float64).reshape(-1))
+        Tn, Tds, Tss = KnockOutFixedRows(FixedEls, _col(Tn, N), _col(Tds, N), _col(Tss, N))
     Tn, Tss, Tds = _col(Tn, N), _col(Tss, N), _col(Tds, N)
+    if fixed is not None:
+        # fixed elements: displacement rows, no columns, least squares
+        nf = int(np.sum(fixed != 1))
+        Dn, Dss, Dds = np.zeros(nf), np.zeros(nf), np.zeros(nf)
+        A = np.zeros((3 * N, 3 * nf), order="F")
+        b = np.zeros(3 * N)
+        ctx = _lib.context(device)
+        rc = _lib.load().cad_slip_calculator_fixed(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu),
+                                                   float(G), float(lam), mid.ctypes.data, nrm.ctypes.data,
+                                                   int(HSFlag), Tn.ctypes.data, Tss.ctypes.data, Tds.ctypes.data,
+                                                   fixed.ctypes.data, Dn.ctypes.data, Dss.ctypes.data,
+                                                   Dds.ctypes.data, A.ctypes.data, b.ctypes.data)
+        _lib.check(rc, ctx)
+        return Dn, Dss, Dds, A, b
     Dn, Dss, Dds = np.zeros(N), np.zeros(N), np.zeros(N)
     A = np.zeros((3 * N, 3 * N), order="F")
     b = np.zeros(3 * N)

@@ -32,7 +32,7 @@ namespace {
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
-    S_COUNT
+    S_FIX, S_FOBS, S_FDISP, S_ATA, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -990,18 +990,88 @@ static int upload_geometry(cad_ctx* ctx, const double* normals, const double* mi
     return CAD_OK;
 }
 
+// Fixed elements of a FixedEls vector (value 1): row map (fixed row index or
+// -1) and the kept columns.
+struct FixedSplit {
+    std::vector<int> fixrow, freecol, fixidx;
+};
+static FixedSplit split_fixed(const double* fixed_els, int64_t N)
+{
+    FixedSplit f;
+    f.fixrow.assign((size_t)N, -1);
+    for (int64_t i = 0; i < N; ++i) {
+        if (fixed_els && fixed_els[i] == 1.0) {
+            f.fixrow[i] = (int)f.fixidx.size();
+            f.fixidx.push_back((int)i);
+        } else {
+            f.freecol.push_back((int)i);
+        }
+    }
+    return f;
+}
+
+// CalculateInfluenceMatrices3D with fixed elements
+// (src/CalculateInfluenceMatrices3D.jl:10-33, :145-199) on the device: the
+// traction fields of every pair, the displacement fields at the fixed
+// elements' collocation points (unit slips), spliced -- either the nine
+// N x nf fields (amat false) or A = -[Atn; Atss; Atds] (3N x 3nf, lda).
+static int assemble_fixed_device(cad_ctx* ctx, const double* g, int64_t N, double nu, double G, double lambda, int hs,
+                                 const FixedSplit& fs, bool amat, double* out, int64_t lda)
+{
+    const int64_t nfix = (int64_t)fs.fixidx.size(), nf = (int64_t)fs.freecol.size();
+    void *trac, *idx, *fobs, *fdisp;
+    if (int r = ensure(ctx, S_OUT, (size_t)9 * N * N * sizeof(double), &trac)) return r;
+    if (int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs, OUT_TRAC,
+                                (double*)trac, nullptr, 0))
+        return r;
+    if (int r = ensure(ctx, S_FIX, (size_t)(N + nf + nfix) * sizeof(int), &idx)) return r;
+    if (int r = ensure(ctx, S_FOBS, (size_t)3 * nfix * sizeof(double), &fobs)) return r;
+    if (int r = ensure(ctx, S_FDISP, (size_t)9 * nfix * N * sizeof(double), &fdisp)) return r;
+    int* fixrow = (int*)idx;
+    int* freecol = fixrow + N;
+    int* fixidx = freecol + nf;
+    CK(cudaMemcpyAsync(fixrow, fs.fixrow.data(), N * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (nf) CK(cudaMemcpyAsync(freecol, fs.freecol.data(), nf * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (nfix) {
+        CK(cudaMemcpyAsync(fixidx, fs.fixidx.data(), nfix * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        const double* X = (const double*)ctx->buf[S_OBS].p;   // collocation points of assemble_device
+        ++ctx->launches;
+        CK(launch_gather_points(X, X + N, X + 2 * N, fixidx, nfix, (double*)fobs, ctx->stream));
+        PairArgs a{};
+        const double* fo = (const double*)fobs;
+        a.X = fo; a.Y = fo + nfix; a.Z = fo + 2 * nfix; a.M = nfix;
+        a.tri = (const TriDev*)ctx->buf[S_TRI].p; a.N = N;   // unit-slip records of assemble_device
+        a.tri_chunk = pick_chunk(nfix, N, false);
+        a.disp = (double*)fdisp;
+        ++ctx->launches;
+        CK(launch_td_pairs(a, OUT_INF, hs == 1, false, true, ctx->stream));
+    }
+    ++ctx->launches;
+    CK(launch_splice_fixed((const double*)trac, (const double*)fdisp, N, nfix, fixrow, freecol, nf, amat, out, lda,
+                           ctx->stream));
+    // the host vectors of fs are read by the copies above: finish before they go
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
 int cad_influence_traction(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
                            const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                            const double* fixed_els, int hs_flag, double* const* trac_out)
 {
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || !trac_out) return fail(ctx, CAD_ERR_ARG, "invalid argument");
-    if (fixed_els)
-        for (int64_t i = 0; i < N; ++i)
-            if (fixed_els[i] == 1.0)
-                return fail(ctx, CAD_ERR_UNSUPPORTED, "fixed elements are not supported by this entry point");
     double* g;
     if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    const FixedSplit fs = split_fixed(fixed_els, N);
+    if (!fs.fixidx.empty()) {
+        const int64_t nf = (int64_t)fs.freecol.size();
+        void* out;
+        if (int r = ensure(ctx, S_A, (size_t)9 * N * nf * sizeof(double) + 16, &out)) return r;
+        if (int r = assemble_fixed_device(ctx, g, N, nu, G, lambda, hs_flag, fs, false, (double*)out, 0)) return r;
+        if (int rr = copy_fields_out(ctx, (const double*)out, 9, N * nf, trac_out)) return rr;
+        CK(cudaStreamSynchronize(ctx->stream));
+        return CAD_OK;
+    }
     void* out;
     if (int r = ensure(ctx, S_OUT, (size_t)9 * N * N * sizeof(double), &out)) return r;
     int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_TRAC,
@@ -1219,6 +1289,64 @@ int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, in
     st.launches = &ctx->launches;
     const int e = mlp_step(st);
     if (e != 0) return cuda_fail(ctx, (cudaError_t)e, "learned-preconditioner network step");
+    return CAD_OK;
+}
+
+int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N,
+                              double nu, double G, double lambda, const double* midpoints, const double* normals,
+                              int hs_flag, const double* Tn, const double* Tss, const double* Tds,
+                              const double* fixed_els, double* Dn, double* Dss, double* Dds, double* A_out,
+                              double* b_out)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || !Tn || !Tss || !Tds || !Dn || !Dss || !Dds)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    const FixedSplit fs = split_fixed(fixed_els, N);
+    if (fs.fixidx.empty())
+        return cad_slip_calculator(ctx, P1, P2, P3, N, nu, G, lambda, midpoints, normals, hs_flag, Tn, Tss, Tds, Dn,
+                                   Dss, Dds, A_out, b_out);
+    const int64_t nf = (int64_t)fs.freecol.size(), n3 = 3 * N, m3 = 3 * nf;
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    // tractions with the fixed rows knocked out (src/KnockOutFixedRows.jl)
+    std::vector<double> hb((size_t)n3);
+    for (int64_t i = 0; i < N; ++i) {
+        const bool fx = fs.fixrow[i] >= 0;
+        hb[i] = fx ? 0.0 : Tn[i];
+        hb[N + i] = fx ? 0.0 : Tss[i];
+        hb[2 * N + i] = fx ? 0.0 : Tds[i];
+    }
+    void *A, *b, *ata;
+    if (int r = ensure(ctx, S_A, (size_t)n3 * m3 * sizeof(double) + 16, &A)) return r;
+    if (int r = ensure(ctx, S_B, (size_t)n3 * sizeof(double), &b)) return r;
+    if (int r = ensure(ctx, S_ATA, ((size_t)m3 * m3 + m3) * sizeof(double), &ata)) return r;
+    if (int r = upload(ctx, (double*)b, hb.data(), n3)) return r;
+    if (int r = assemble_fixed_device(ctx, g, N, nu, G, lambda, hs_flag, fs, true, (double*)A, n3)) return r;
+    if (A_out) CK(cudaMemcpyAsync(A_out, A, (size_t)n3 * m3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (b_out) CK(cudaMemcpyAsync(b_out, b, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // the tall system in the least-squares sense (Julia's backslash on a 3N x 3nf
+    // matrix): normal equations A^T A D = A^T b, solved by the FP64 LU
+    double* AtA = (double*)ata;
+    double* Atb = AtA + (size_t)m3 * m3;
+    const double one = 1.0, zero = 0.0;
+    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)m3, (int)m3, (int)n3, &one, (const double*)A, (int)n3,
+                    (const double*)A, (int)n3, &zero, AtA, (int)m3) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemv(ctx->blas, CUBLAS_OP_T, (int)n3, (int)m3, &one, (const double*)A, (int)n3, (const double*)b, 1,
+                    &zero, Atb, 1) != CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "normal equations: cuBLAS error");
+    const int solver = ctx->solver;
+    ctx->solver = CAD_SOLVER_LU64;
+    int r = solve_device(ctx, m3, AtA, m3, Atb, m3, 1);
+    int info = 0;
+    if (r == CAD_OK) r = read_info(ctx, &info);
+    ctx->solver = solver;
+    if (r) return r;
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is rank deficient");
+    CK(cudaMemcpyAsync(Dn, Atb, nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dss, Atb + nf, nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dds, Atb + 2 * nf, nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return CAD_OK;
 }
 

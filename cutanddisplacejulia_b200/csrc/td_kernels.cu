@@ -248,6 +248,46 @@ __global__ void td_sum_kernel(const double* __restrict__ in, int64_t M, int64_t 
     out[f * M + i] = s;
 }
 
+// ------------------------------------------------------- fixed elements
+// Splice of CalculateInfluenceMatrices3D with fixed elements (ConcatInfMats,
+// PutDispInfsIntoInfMat, src/CalculateInfluenceMatrices3D.jl:145-199): field
+// f's row i is the displacement influence disp[f] (nfix x N) of fixed row
+// fixrow[i] when i is fixed (fixrow[i] >= 0), else the traction influence
+// trac[f] (N x N); only the columns freecol[0..nf) are kept.  amat = 0:
+// out + f * N * nf holds field f (N x nf, column-major); amat = 1: out is the
+// system A (3N x 3nf, lda) = -[[F0 F3 F6]; [F1 F4 F7]; [F2 F5 F8]].
+__global__ void splice_fixed_kernel(const double* __restrict__ trac, const double* __restrict__ disp, int64_t N,
+                                    int64_t nfix, const int* __restrict__ fixrow, const int* __restrict__ freecol,
+                                    int64_t nf, int amat, double* __restrict__ out, int64_t lda)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t jf = blockIdx.y;
+    const int f = blockIdx.z;
+    if (i >= N || jf >= nf) return;
+    const int64_t j = freecol[jf];
+    const int fr = fixrow[i];
+    const double v = fr >= 0 ? disp[(int64_t)f * nfix * N + fr + nfix * j] : trac[(int64_t)f * N * N + i + N * j];
+    if (!amat) {
+        out[(int64_t)f * N * nf + i + N * jf] = v;
+    } else {
+        const int m = f / 3, r = f % 3;   // field 3m + r: slip mode m (column block), traction row r
+        out[(r * N + i) + lda * (m * nf + jf)] = -v;
+    }
+}
+
+// out[k] = (X, Y, Z)[idx[k]] as three SoA arrays of length n
+__global__ void gather_points_kernel(const double* __restrict__ X, const double* __restrict__ Y,
+                                     const double* __restrict__ Z, const int* __restrict__ idx, int64_t n,
+                                     double* __restrict__ out)
+{
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int64_t i = idx[k];
+    out[k] = X[i];
+    out[k + n] = Y[i];
+    out[k + 2 * n] = Z[i];
+}
+
 // ----------------------------------------------- mixed-precision assembly
 // Centroids of the triangles (near + [0, 3N)) and the squared near-field
 // radius (near[3N]) = (factor x mean edge length)^2; one block, fixed
@@ -390,6 +430,23 @@ cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bo
             return launch_pair<false, true, false, OUT_AMAT>(a, st);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_splice_fixed(const double* trac, const double* disp, int64_t N, int64_t nfix, const int* fixrow,
+                                const int* freecol, int64_t nf, bool amat, double* out, int64_t lda, cudaStream_t st)
+{
+    if (N == 0 || nf == 0) return cudaSuccess;
+    dim3 grid((unsigned)((N + 127) / 128), (unsigned)nf, 9);
+    splice_fixed_kernel<<<grid, 128, 0, st>>>(trac, disp, N, nfix, fixrow, freecol, nf, amat ? 1 : 0, out, lda);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_points(const double* X, const double* Y, const double* Z, const int* idx, int64_t n,
+                                 double* out, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    gather_points_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(X, Y, Z, idx, n, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const double* P2, const double* P3,

@@ -43,6 +43,12 @@ cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const d
                                   double near_factor, void* tri32, double* near, cudaStream_t st, int64_t* launches);
 size_t tri_record_bytes_f32();
 
+// Fixed-element splice (see td_kernels.cu) and a gather of points by index.
+cudaError_t launch_splice_fixed(const double* trac, const double* disp, int64_t N, int64_t nfix, const int* fixrow,
+                                const int* freecol, int64_t nf, bool amat, double* out, int64_t lda, cudaStream_t st);
+cudaError_t launch_gather_points(const double* X, const double* Y, const double* Z, const int* idx, int64_t n,
+                                 double* out, cudaStream_t st);
+
 size_t tri_record_bytes();
 
 cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,

@@ -123,6 +123,21 @@ function SlipCalculator3D(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSF
     return Dn, Dss, Dds, A, b
 end
 
+# SlipCalculator3D with fixed elements (FixedEls .== 1): Dn, Dss, Dds of the
+# other elements, A (3n x 3n_free), b
+function SlipCalculator3D(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSFlag, Tn, Tss, Tds, FixedEls)
+    n = size(P1, 1)
+    nf = count(!=(1), FixedEls)
+    Dn = zeros(nf); Dss = zeros(nf); Dds = zeros(nf); A = zeros(3n, 3nf); b = zeros(3n)
+    check(ccall((:cad_slip_calculator_fixed, libcad), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Float64, Float64, Ptr{Float64},
+         Ptr{Float64}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        ctx(), f64(P1), f64(P2), f64(P3), n, ν, G, λ, f64(MidPoint), f64(FaceNormalVector), HSFlag,
+        f64(vec(Tn)), f64(vec(Tss)), f64(vec(Tds)), f64(vec(FixedEls)), Dn, Dss, Dds, A, b))
+    return Dn, Dss, Dds, A, b
+end
+
 # Precision settings (no counterpart in the reference): solver 0 = FP64 LU
 # (default), 1 = FP32/TF32 LU + FP64 GMRES, 2 = FP64 GMRES with the block-sparse
 # preconditioner set below; assembly 0 = FP64, 1 = FP32 far field.

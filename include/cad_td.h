@@ -146,9 +146,13 @@ int cad_td_sum(cad_ctx* ctx, int64_t M, int64_t N, const double* const* strain_i
  * CalculateInfluenceMatrices3D (src/CalculateInfluenceMatrices3D.jl:2-48):
  * normals and midpoints N x 3 (FaceNormalVector, MidPoint), vertex lists
  * N x 3; trac_out: 9 pointers to N x N arrays in TractionInf order (DnTn,
- * DnTss, DnTds, DssTn, DssTss, DssTds, DdsTn, DdsTss, DdsTds).  fixed_els may
- * be NULL; a fixed element (value 1) is not supported in this version and
- * returns CAD_ERR_UNSUPPORTED. */
+ * DnTss, DnTds, DssTn, DssTss, DssTds, DdsTn, DdsTss, DdsTds).  fixed_els
+ * (N values, may be NULL): with elements marked 1, the rows of those elements
+ * hold the displacement influence at their collocation points (DnUx in DnTn,
+ * DnUy in DnTss, DnUz in DnTds, and so on by field) and only the columns of
+ * the other n_free elements are kept (ConcatInfMats / PutDispInfsIntoInfMat,
+ * src/CalculateInfluenceMatrices3D.jl:145-199): each trac_out field is then
+ * N x n_free. */
 int cad_influence_traction(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
                            const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                            const double* fixed_els, int hs_flag, double* const* trac_out);
@@ -161,6 +165,20 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
                         double G, double lambda, const double* midpoints, const double* normals, int hs_flag,
                         const double* Tn, const double* Tss, const double* Tds, double* Dn, double* Dss,
                         double* Dds, double* A_out, double* b_out);
+
+/* SlipCalculator3D with fixed elements (src/SlipCalculator3D.jl:1-33 with
+ * FixedEls, src/KnockOutFixedRows.jl): the tractions of fixed elements are set
+ * to zero, A (3N x 3 n_free) has displacement rows for them and no columns,
+ * and A D = b is solved in the least-squares sense (the reference's `\` on a
+ * tall matrix) through the normal equations and the FP64 LU.  Dn, Dss, Dds:
+ * n_free values each (elements not fixed, in order); A_out (3N x 3 n_free)
+ * and b_out (3N) may be NULL.  Without fixed elements this is
+ * cad_slip_calculator. */
+int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N,
+                              double nu, double G, double lambda, const double* midpoints, const double* normals,
+                              int hs_flag, const double* Tn, const double* Tss, const double* Tds,
+                              const double* fixed_els, double* Dn, double* Dss, double* Dds, double* A_out,
+                              double* b_out);
 
 /* Dense solve A X = B (the `\` of src/SlipCalculator3D.jl:22): A n x n, B n x
  * nrhs, both column-major host arrays; X n x nrhs. */

@@ -213,6 +213,63 @@ def slip_calculator(P1, P2, P3, nu, G, lam, midpoints, normals, hs, Tn, Tss, Tds
     return D[:n], D[n:2 * n], D[2 * n:], A, b
 
 
+def influence_traction_fixed(normals, midpoints, P1, P2, P3, nu, G, lam, fixed, hs, nthreads=None):
+    """CalculateInfluenceMatrices3D with fixed elements
+    (src/CalculateInfluenceMatrices3D.jl:10-33, ConcatInfMats and
+    PutDispInfsIntoInfMat :145-199): rows of fixed elements hold the
+    displacement influence at their collocation points (field f of DispInf in
+    place of field f of TractionInf: DnUx for DnTn, DnUy for DnTss, ...), rows
+    of the others the traction influence; only the columns of the elements
+    that are not fixed are kept.  Returns the (9, N, n_free) stack."""
+    fixed = np.asarray(fixed).reshape(-1) == 1
+    free = ~fixed
+    T = influence_traction(normals, midpoints, P1, P2, P3, nu, G, lam, hs, nthreads=nthreads)
+    out = T.copy()
+    if fixed.any():
+        obs = np.asarray(midpoints, dtype=np.float64) - 1e-12 * np.asarray(normals, dtype=np.float64)
+        N = obs.shape[0]
+        ones = np.ones(N)
+        _, U = td_inf(obs[fixed, 0], obs[fixed, 1], obs[fixed, 2], P1, P2, P3, ones, ones, ones, nu, G, 1, 0, hs,
+                      nthreads=nthreads)
+        out[:, fixed, :] = U
+    return out[:, :, free]
+
+
+def assemble_A_rect(trac):
+    """A = -[[DnTn DssTn DdsTn]; [DnTss DssTss DdsTss]; [DnTds DssTds DdsTds]]
+    from (9, N, n_free) fields: 3N x 3 n_free (src/SlipCalculator3D.jl:13-16)."""
+    N, nf = trac.shape[1], trac.shape[2]
+    A = np.empty((3 * N, 3 * nf), order="F")
+    for r in range(3):
+        for m in range(3):
+            A[r * N:(r + 1) * N, m * nf:(m + 1) * nf] = -trac[3 * m + r]
+    return A
+
+
+def slip_calculator_fixed(P1, P2, P3, nu, G, lam, midpoints, normals, hs, Tn, Tss, Tds, fixed, nthreads=None):
+    """SlipCalculator3D with fixed elements (src/SlipCalculator3D.jl:1-33):
+    tractions of fixed elements knocked out (src/KnockOutFixedRows.jl), the
+    3N x 3 n_free system solved in the least-squares sense as Julia's backslash does
+    for a tall matrix (numpy lstsq).  Returns Dn, Dss, Dds (n_free each), A, b."""
+    fixed = np.asarray(fixed).reshape(-1) == 1
+    Tn, Tss, Tds = (np.where(fixed, 0.0, _vec(t)) for t in (Tn, Tss, Tds))
+    A = assemble_A_rect(influence_traction_fixed(normals, midpoints, P1, P2, P3, nu, G, lam, fixed, hs,
+                                                 nthreads=nthreads))
+    b = np.concatenate([Tn, Tss, Tds])
+    D = np.linalg.lstsq(A, b, rcond=None)[0]
+    nf = int((~fixed).sum())
+    return D[:nf], D[nf:2 * nf], D[2 * nf:], A, b
+
+
+def mogi_spherical_cavity(D, X, Y, radius, P, nu, G):
+    """Surface displacement above a pressurised spherical cavity, Mogi (1958),
+    as src/Mogi1958_SphericalCavity.jl states it: returns (Ux, Uy, Uz)."""
+    X, Y = np.asarray(X, dtype=np.float64), np.asarray(Y, dtype=np.float64)
+    R = np.sqrt(D * D + X * X + Y * Y)
+    lsi = radius ** 3 * P * ((1 - nu) / G)
+    return X / R ** 3 * lsi, Y / R ** 3 * lsi, D / R ** 3 * lsi
+
+
 def opcount(X, Y, Z, P1, P2, P3, Dss, Dds, Dn, nu, kind, hs):
     """Literal operation counts per pair (kind 0 strain, 1 displacement)."""
     X, Y, Z = _vec(X), _vec(Y), _vec(Z)

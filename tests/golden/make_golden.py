@@ -4,6 +4,9 @@ GPU machines); the resulting .npz files are what the tests read.
 
   squaregrid.npz   test/SquareGrid.stl          (STLReader, src/STLReader.jl)
   circle581.npz    test/CircleMesh_1a_500Faces.ts (GoCadAsciiReader, src/GoCadAsciiReader.jl)
+  mogi.npz         test/SphereUniformDistributionON_46Faces.ts with test/SphereFix4.ts (scaled x3)
+                   appended as fixed elements (DataAppender3D), 50 below the surface, as
+                   test/test_TDvsMogi.jl:6-20 builds it; also holds FixedEls
 
 Each file holds P1, P2, P3 (N x 3 float64), built as CreateP1P2P3 does
 (src/CreateP1P2P3.jl): vertex k of triangle i is the point whose index the
@@ -70,6 +73,16 @@ def main(ref):
     np.savez_compressed(os.path.join(HERE, "circle581.npz"), P1=P1, P2=P2, P3=P3)
     print("wrote squaregrid.npz (%d tris), circle581.npz (%d tris)" % (len(read_stl_ascii(
         os.path.join(test_dir, "SquareGrid.stl"))[1]), len(tris)))
+    pts, tris = read_gocad_ts(os.path.join(test_dir, "SphereUniformDistributionON_46Faces.ts"))
+    ptsf, trisf = read_gocad_ts(os.path.join(test_dir, "SphereFix4.ts"))
+    ptsf = ptsf * 3.0
+    allp = np.vstack([pts, ptsf])
+    allt = np.vstack([tris, trisf + len(pts)])
+    fixed = np.concatenate([np.zeros(len(tris)), np.ones(len(trisf))])
+    allp[:, 2] -= 50.0
+    P1, P2, P3 = p1p2p3(allp, allt)
+    np.savez_compressed(os.path.join(HERE, "mogi.npz"), P1=P1, P2=P2, P3=P3, FixedEls=fixed)
+    print("wrote mogi.npz (%d tris, %d fixed)" % (len(allt), int(fixed.sum())))
 
 
 if __name__ == "__main__":

@@ -3,13 +3,16 @@
   Okada (1985) half-space surface field   test/test_TDvsOkada.jl (<= 1e-13)
   traction-free crack, 5 orientations      test/test_TractionFreeSurface.jl (<= 1e-8)
   Eshelby penny crack slip                 test/test_TDvsEshelbyPennyCrack.jl (<= 11 %)
+  Mogi cavity with fixed elements          test/test_TDvsMogi.jl (spread <= 0.05, <= 20 %)
 plus self-consistency of the oracle (influence matrices + TD_sum == summing
 overload; strain == symmetric gradient of displacement at depth, FS and HS).
 """
+import os
+
 import numpy as np
 import pytest
 
-from helpers import load_mesh, okada_case
+from helpers import GOLDEN, load_mesh, okada_case
 
 
 def test_okada_kat(oracle):
@@ -132,3 +135,30 @@ def test_dims_error(oracle):
     P = np.zeros((2, 3))
     with pytest.raises(oracle.OracleError, match="Element size inputs must be the same dimensions"):
         oracle.td_inf([0.0], [0.0], [-1.0], P, P, P, [1.0], [1.0, 1.0], [1.0, 1.0], 0.25, 1.0, 1, 1, 0)
+
+
+def test_mogi_kat(oracle):
+    # test/test_TDvsMogi.jl: a 46-face sphere 50 below the free surface, 6
+    # fixed elements (SphereFix4 scaled x3) appended, unit pressure; the
+    # opening must be near uniform (spread <= 0.05 / G) and the surface
+    # displacement within 20 % of Mogi (1958) at x = 0..100
+    from oracle import geometry as g
+    d = np.load(os.path.join(GOLDEN, "mogi.npz"))
+    P1, P2, P3, fixed = d["P1"], d["P2"], d["P3"], d["FixedEls"]
+    nrm, mid = g.face_normal_and_midpoint(P1, P2, P3)
+    _, _, lam, nu, G = g.elastic_constants(1.0, 0.25)
+    n = len(P1)
+    Dn, Dss, Dds, A, b = oracle.slip_calculator_fixed(P1, P2, P3, nu, G, lam, mid, nrm, 1, np.ones(n), np.zeros(n),
+                                                      np.zeros(n), fixed)
+    assert A.shape == (3 * n, 3 * int((fixed == 0).sum()))
+    assert Dn.max() - Dn.min() <= 0.05 / G
+    free = fixed == 0
+    X = np.arange(0.0, 101.0)
+    Y, Z = np.zeros_like(X), np.zeros_like(X)
+    _, U = oracle.td_sum_eval(X, Y, Z, P1[free], P2[free], P3[free], Dss, Dds, Dn, nu, G, 1, 0, 1)
+    An = oracle.mogi_spherical_cavity(50.0, X, Y, 1.0, 1.0, nu, G)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for a, u in zip(An, U):
+            pct = 100.0 / a * u
+            pct[np.isinf(pct)] = np.nan
+            assert not np.any(np.abs(pct - 100) > 20)
