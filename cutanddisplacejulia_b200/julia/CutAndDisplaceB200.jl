@@ -99,7 +99,8 @@ end
 
 # CalculateInfluenceMatrices3D -> nine n x n matrices in TractionInf field order
 function CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, ν, G, λ, FixedEls, HSFlag, n)
-    T = [zeros(n, n) for _ in 1:9]; tp = [pointer(a) for a in T]
+    nf = count(!=(1), FixedEls)     # fixed elements: their columns are dropped
+    T = [zeros(n, nf) for _ in 1:9]; tp = [pointer(a) for a in T]
     GC.@preserve T tp begin
         check(ccall((:cad_influence_traction, libcad), Cint,
             (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64,
