@@ -32,6 +32,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+from cutanddisplacejulia_b200 import dist as cdist  # noqa: E402
+
 # Algorithmic FP64 operations per pair-evaluation of the assembly kernel:
 # full-space strain of all three unit slip modes (2960, counted with the
 # oracle's counting scalar on this mesh's collocation pairs) plus the strain ->
@@ -234,10 +236,7 @@ def mixed_solve_timing(args, ctx, L, stream, step_asm_args, A, b0, x64, ms_fp64,
         iters, relres = _lib.last_solve_stats(ctx)
         factor_ms = L.cad_last_time_ms(ctx, 2)   # the last step's cast + FP32 LU + block inverses
     ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = cdist.max_over_ranks(ms, dev)
     asm_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
     sol_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
     Am = A.view(n3, n3).t()
@@ -387,10 +386,7 @@ def run_batch(args, rank, world, local_rank):
         clk = clocks.stop()
         launches = L.cad_kernel_launches(ctx) - l0
     ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = cdist.max_over_ranks(ms, dev)
     Dm = D.clone()
     # plain per-crack FP64 path on the same cracks: assembly + FP64 LU
     A = torch.empty(9 * max(offs[c + 1] - offs[c] for c in range(len(cracks))) ** 2, dtype=torch.float64,
@@ -684,10 +680,7 @@ def run_ours(args, rank, world, local_rank):
     sol_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
     pair_kernel_ms = L.cad_last_time_ms(ctx, 0)   # last pair-kernel launch alone (library events)
     ms_step = ms_total / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = cdist.max_over_ranks(ms_step, dev)
 
     # solution quality: relative residual of the last solve against a fresh A
     _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(),
@@ -727,10 +720,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.steps):
         e2e_call()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = cdist.max_over_ranks(e2e_ms, dev)
     h2d = (5 * 3 * n + 3 * n) * 8
     d2h = 3 * n * 8
 
@@ -752,7 +742,8 @@ def run_ours(args, rank, world, local_rank):
     lu_flops = (2.0 / 3.0) * n3 ** 3 + 2.0 * n3 * n3
     solve_tflops = lu_flops / (sol_ms * 1e-3) / 1e12
     line = {
-        "metric": WORKLOADS[args.workload][0], "value": world * pairs / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world,
+        "metric": WORKLOADS[args.workload][0], "value": cdist.replica_throughput(pairs, ms_step, world), "unit": UNIT,
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][1] % (n, n3),
