@@ -33,7 +33,7 @@ CAD_ASSEMBLY_MIXED = 1
 EXPORTS = [
     "cad_init", "cad_destroy", "cad_last_error", "cad_set_stream", "cad_get_stream", "cad_last_time_ms",
     "cad_version", "cad_kernel_launches", "cad_set_assembly", "cad_set_solver", "cad_last_solve_stats", "cad_fp64_fma_probe", "cad_td_inf", "cad_td_sum_eval", "cad_td_sum", "cad_influence_traction",
-    "cad_slip_calculator", "cad_slip_calculator_fixed", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev",
+    "cad_slip_calculator", "cad_slip_calculator_fixed", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev", "cad_assemble_update_dev",
     "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
     "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
 ]
@@ -93,6 +93,7 @@ def load():
     L.cad_td_inf_dev.argtypes = tdd
     L.cad_td_sum_eval_dev.argtypes = tdd
     L.cad_assemble_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, P, I64]
+    L.cad_assemble_update_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, P, I64, P, I64]
     L.cad_solve_dev.argtypes = [P, I64, P, I64, P, I64, I64]
     L.cad_slip_calculator_batched_dev.argtypes = [P, I64, P, P, P, P, P, P, D, D, D, INT, P, P, P]
     L.cad_slip_calculator_batched.argtypes = [P, I64, P, P, P, P, P, P, D, D, D, INT, P, P, P]

@@ -32,7 +32,7 @@ namespace {
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
-    S_FIX, S_FOBS, S_FDISP, S_ATA, S_COUNT
+    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -1347,6 +1347,44 @@ int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, 
     CK(cudaMemcpyAsync(Dss, Atb + nf, nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(Dds, Atb + 2 * nf, nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                            const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                            int hs_flag, const int64_t* changed, int64_t k, double* A, int64_t lda)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || k < 0 || bad_flag(hs_flag) || lda < 3 * N || (k > 0 && !changed) || N > INT32_MAX)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    std::vector<int> list((size_t)k);
+    for (int64_t q = 0; q < k; ++q) {
+        if (changed[q] < 0 || changed[q] >= N) return fail(ctx, CAD_ERR_ARG, "changed element index out of range");
+        list[q] = (int)changed[q];
+    }
+    if (k == 0 || N == 0) return CAD_OK;
+    void *obs, *dirs, *tri, *dl;
+    if (int r = ensure(ctx, S_OBS, (size_t)3 * N * sizeof(double), &obs)) return r;
+    if (int r = ensure(ctx, S_DIRS, (size_t)9 * N * sizeof(double), &dirs)) return r;
+    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    if (int r = ensure(ctx, S_LIST, (size_t)k * sizeof(int), &dl)) return r;
+    double* X = (double*)obs;
+    ++ctx->launches;
+    CK(launch_colloc(normals, midpoints, N, X, X + N, X + 2 * N, (double*)dirs, ctx->stream));
+    if (hs_flag == 1)
+        if (int r = hs_check(ctx, X + 2 * N, N, P1, P2, P3, N)) return r;
+    ++ctx->launches;
+    CK(launch_td_setup(P1, P2, P3, N, nullptr, nullptr, nullptr, 1, nu, hs_flag == 1, (TriDev*)tri, ctx->stream));
+    CK(cudaMemcpyAsync(dl, list.data(), k * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    PairArgs a{};
+    a.X = X; a.Y = X + N; a.Z = X + 2 * N; a.M = N; a.tri = (const TriDev*)tri; a.N = N;
+    a.lambda = lambda; a.G = G; a.dirs = (const double*)dirs;
+    a.A = A; a.lda = lda;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(launch_assemble_update(a, hs_flag == 1, (const int*)dl, k, ctx->stream, &ctx->launches));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->timed[0] = true;
+    CK(cudaStreamSynchronize(ctx->stream));   // the host list is read by the copy above
     return CAD_OK;
 }
 

@@ -117,7 +117,9 @@ __device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, co
 // ------------------------------------------------------------- pair kernel
 // NEAR: rewrite only the triangles whose centroid lies within the near
 // radius of some point of the block (the FP64 pass of the mixed assembly).
-template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false>
+// LIST (OUT_AMAT only): incremental re-assembly through a.tri_list /
+// a.obs_list into a system of a.Ntot elements.
+template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false>
 __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
 {
     extern __shared__ double smem[];
@@ -125,8 +127,12 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
     const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
     const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
     const bool active = i < a.M;
+    // LIST: this thread's point (system row) and the full system's size
+    const int64_t io = (LIST && a.obs_list && active) ? (int64_t)a.obs_list[i] : i;
+    const int64_t NS = LIST ? a.Ntot : a.N;
+    const int64_t MD = LIST ? a.Ntot : a.M;
     double X = 0.0, Y = 0.0, Z = 0.0;
-    if (active) { X = a.X[i]; Y = a.Y[i]; Z = a.Z[i]; }
+    if (active) { X = a.X[io]; Y = a.Y[io]; Z = a.Z[io]; }
     const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
     const int64_t j1 = min(a.N, j0 + a.tri_chunk);
     const int64_t MN = a.M * a.N;
@@ -134,9 +140,9 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
     double n[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, ds[3] = {0, 0, 0};
     if ((OUT == OUT_TRAC || OUT == OUT_AMAT) && active) {
         for (int k = 0; k < 3; ++k) {
-            n[k] = a.dirs[i + k * a.M];
-            ss[k] = a.dirs[i + (3 + k) * a.M];
-            ds[k] = a.dirs[i + (6 + k) * a.M];
+            n[k] = a.dirs[io + k * MD];
+            ss[k] = a.dirs[io + (3 + k) * MD];
+            ds[k] = a.dirs[io + (6 + k) * MD];
         }
     }
     const double near_r2 = NEAR ? a.near[3 * a.N] : 0.0;
@@ -151,7 +157,8 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
         } else {
             __syncthreads();
         }
-        const double* src = reinterpret_cast<const double*>(a.tri + j);
+        const int64_t jt = (LIST && a.tri_list) ? (int64_t)a.tri_list[j] : j;   // system column
+        const double* src = reinterpret_cast<const double*>(a.tri + jt);
         for (int w = threadIdx.x; w < words; w += kPairThreads) smem[w] = src[w];
         __syncthreads();
         if (!active) continue;
@@ -177,7 +184,7 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
                     } else {
 #pragma unroll
                         for (int r = 0; r < 3; ++r)
-                            a.A[(int64_t)(r * a.N + i) + a.lda * (int64_t)(m * a.N + j)] = -tr[r];
+                            a.A[(int64_t)(r * NS + io) + a.lda * (int64_t)(m * NS + jt)] = -tr[r];
                     }
                 }
             }
@@ -489,6 +496,40 @@ cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const d
 }
 
 size_t tri_record_bytes_f32() { return sizeof(TriDevT<float>); }
+
+cudaError_t launch_assemble_update(PairArgs a, bool hs, const int* list, int64_t k, cudaStream_t st,
+                                   int64_t* launches)
+{
+    if (k == 0 || a.N == 0) return cudaSuccess;
+    const int words = hs ? kTriWordsHS : kTriWordsFS;
+    const size_t smem = (size_t)words * sizeof(double);
+    auto kern = hs ? td_pair_kernel<true, true, false, OUT_AMAT, false, true>
+                   : td_pair_kernel<false, true, false, OUT_AMAT, false, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t Ntot = a.N;
+    a.Ntot = Ntot;
+    // columns of the listed triangles, every point
+    PairArgs c = a;
+    c.tri_list = list;
+    c.obs_list = nullptr;
+    c.M = Ntot;
+    c.N = k;
+    c.tri_chunk = k < 8 ? k : 8;
+    dim3 gc((unsigned)((Ntot + kPairThreads - 1) / kPairThreads), (unsigned)((k + c.tri_chunk - 1) / c.tri_chunk));
+    kern<<<gc, kPairThreads, smem, st>>>(c);
+    // rows of the listed points, every triangle
+    PairArgs r = a;
+    r.tri_list = nullptr;
+    r.obs_list = list;
+    r.M = k;
+    r.N = Ntot;
+    r.tri_chunk = 8;
+    dim3 gr((unsigned)((k + kPairThreads - 1) / kPairThreads), (unsigned)((Ntot + 7) / 8));
+    kern<<<gr, kPairThreads, smem, st>>>(r);
+    *launches += 2;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_td_setup(const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
                             const double* Dds, const double* Dn, int64_t slip_stride, double nu, bool hs,

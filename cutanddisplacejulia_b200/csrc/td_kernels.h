@@ -34,6 +34,12 @@ struct PairArgs {
     // the near field -- centroids (3 x N) followed by the squared radius
     const void* tri32;
     const double* near;
+    // incremental re-assembly (OUT_AMAT): only the triangles tri_list[0..N)
+    // (columns) or only the points obs_list[0..M) (rows) of a system of Ntot
+    // elements; X, Y, Z, dirs and tri then cover all Ntot elements
+    const int* tri_list;
+    const int* obs_list;
+    int64_t Ntot;
 };
 
 // Mixed-precision system matrix: every pair in FP32 (far field), then the
@@ -42,6 +48,12 @@ struct PairArgs {
 cudaError_t launch_assemble_mixed(PairArgs a, bool hs, const double* P1, const double* P2, const double* P3,
                                   double near_factor, void* tri32, double* near, cudaStream_t st, int64_t* launches);
 size_t tri_record_bytes_f32();
+
+// Rows and columns of the k elements `list` (device) of an assembled system
+// matrix recomputed in FP64 (a: the full system's points, directions and
+// triangle records; a.N = a.M = the full size).
+cudaError_t launch_assemble_update(PairArgs a, bool hs, const int* list, int64_t k, cudaStream_t st,
+                                   int64_t* launches);
 
 // Fixed-element splice (see td_kernels.cu) and a gather of points by index.
 cudaError_t launch_splice_fixed(const double* trac, const double* disp, int64_t N, int64_t nfix, const int* fixrow,

@@ -200,6 +200,15 @@ int cad_td_sum_eval_dev(cad_ctx* ctx, const double* X, const double* Y, const do
 int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
                      const double* P2, const double* P3, int64_t N, double nu, double G, double lambda, int hs_flag,
                      double* A, int64_t lda);
+/* Incremental re-assembly (no counterpart in the reference, whose
+ * propagation loop re-assembles the whole system every step,
+ * test/test_PropagationTest.jl:398): after the geometry of the k elements
+ * `changed` (host, indices < N) changed, recompute their rows and columns of
+ * an A built by cad_assemble_dev for the same N (FP64, every other entry kept);
+ * the arguments are the updated geometry. */
+int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                            const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                            int hs_flag, const int64_t* changed, int64_t k, double* A, int64_t lda);
 /* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
  * (n x nrhs, ldb) by the solution. */
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
