@@ -32,7 +32,7 @@ namespace {
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
-    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_COUNT
+    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -441,6 +441,23 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     ctx->timed[1] = ctx->timed[2] = false;
     const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
                         ctx->graphs};
+    if (nrhs == 1) {   // one right-hand side: factorise, then the two chain launches
+        void* chain;
+        if (int r = ensure(ctx, S_CHAIN, (size_t)n * sizeof(double) + lu_chain_sync_ints(n) * sizeof(int), &chain))
+            return r;
+        int rc = lu_factor_solve<double>(ls, A, n, lda, nullptr, 0, 0, nullptr, 0, (int*)piv, (int*)perm, (int*)info,
+                                         kLuBlock, true, false);
+        if (rc == LU_OK) rc = lu_pivots_to_perm(ls, (const int*)piv, n, (int*)perm);
+        if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
+        if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
+        double* y = (double*)chain;
+        CK(lu_solve_chain_f64(ctx->stream, A, lda, n, (const int*)perm, B, y, (double*)work, (int*)(y + n),
+                              (int*)info, &ctx->launches));
+        CK(cudaMemcpyAsync(B, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+        ctx->timed[1] = true;
+        return CAD_OK;
+    }
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
                                            (int*)info, kLuBlock, true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");

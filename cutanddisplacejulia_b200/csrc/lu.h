@@ -43,6 +43,14 @@ template <typename T>
 int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X,
                     int64_t ldx, int* ipiv, int* perm, int* info, int nb, bool factor, bool solve);
 
+// x = U^-1 L^-1 P b for one right-hand side with the FP64 factors in A
+// (lda), perm from lu_pivots_to_perm: two ticket-ordered chain launches
+// (csrc/trsv.cu).  y: n doubles of workspace; sync: lu_chain_sync_ints(n)
+// ints; a dependency wait that runs out sets *info to -1.
+cudaError_t lu_solve_chain_f64(cudaStream_t st, const double* A, int64_t lda, int64_t n, const int* perm,
+                               const double* b, double* y, double* x, int* sync, int* info, int64_t* launches);
+size_t lu_chain_sync_ints(int64_t n);
+
 // perm[i] = row of the original matrix that the factorisation's row i came
 // from (the pivots applied in order); perm: n ints, device.
 int lu_pivots_to_perm(const LuStreams& s, const int* ipiv, int64_t n, int* perm);

@@ -209,7 +209,7 @@ def test_solve_singular_raises(cad):
         cad.solve(A, np.ones(50))
 
 
-@pytest.mark.parametrize("n", [700, 2111])
+@pytest.mark.parametrize("n", [700, 1149, 2111])
 def test_repeated_solves_same_size(cad, n):
     # one call signature four times (first eager, then captured as a CUDA
     # graph, then replayed), with new matrix contents on every call
