@@ -46,6 +46,9 @@ FALG_ASSEMBLY_HS = 43867.0 + 288.0
 # (profiles/td_pair_kernel_*.md): (triangles captured, bytes; the half-space one
 # as dram__bytes.sum.per_second x duration).  Output scales as N^2.
 PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 144.824e9 * 5.114e-3)}
+# share of the step's (serialised) device time taken by the LU panel leaf, from
+# the committed launch list (profiles/launches_penny2013_fp64_and_mixed_step.md)
+DOMINANT_SHARE = {"penny": 0.534}
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
@@ -756,21 +759,31 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "api": "cad_slip_calculator (host C ABI, pinned host buffers)"},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "td_pair_kernel<%s, strain, A-matrix>" % ("HS" if hs else "FS"), "bound": "fp64",
-                     "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak_tflops,
+        # the step's dominant phase is the dense solve (its largest kernel, the
+        # LU panel leaf, is latency-bound: one cluster-wide pivot exchange per
+        # column); the TD pair kernel is the assembly's
+        "roofline": {"kernel": "dense FP64 solve: blocked LU with look-ahead (cluster leaf_lu_kernel, own row-swap "
+                               "and triangular kernels, cuBLAS DGEMM trailing updates) + chained triangular solves",
+                     "bound": "fp64", "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
+                     "frac": solve_tflops / fp64_peak_tflops,
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
-                     "falg_per_pair": falg,
-                     "traffic": PAIR_TRAFFIC[args.workload][1] * (n / PAIR_TRAFFIC[args.workload][0]) ** 2,
-                     "traffic_source": "ncu DRAM bytes (read + write) of one launch at "
-                                       "N=%d, scaled by (N/%d)^2" % (PAIR_TRAFFIC[args.workload][0],
-                                                                      PAIR_TRAFFIC[args.workload][0]),
-                     "step_share": asm_ms / ms_step},
-        "roofline_solve": {"kernel": "blocked LU with look-ahead (cluster leaf_lu_kernel, own row-swap and "
-                                     "triangular kernels, cuBLAS DGEMM trailing update) + triangular solves",
-                           "bound": "fp64",
-                           "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
-                           "frac": solve_tflops / fp64_peak_tflops, "step_share": sol_ms / ms_step},
+                     "work": "(2/3)(3N)^3 + 2(3N)^2 flops per solve", "traffic": None,
+                     "step_share": sol_ms / ms_step},
+        "dominant_kernel": {"name": "leaf_lu_kernel<double, 32, 1>",
+                            "share_of_step_ncu": DOMINANT_SHARE.get(args.workload),
+                            "bound": "latency: one pivot search and row exchange across a 12-16 CTA cluster per "
+                                     "column (about 1.7 us per column)",
+                            "source": "profiles/launches_penny2013_fp64_and_mixed_step.md"},
+        "roofline_assembly": {"kernel": "td_pair_kernel<%s, strain, A-matrix>" % ("HS" if hs else "FS"),
+                              "bound": "fp64", "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
+                              "frac": achieved / fp64_peak_tflops,
+                              "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
+                              "falg_per_pair": falg,
+                              "traffic": PAIR_TRAFFIC[args.workload][1] * (n / PAIR_TRAFFIC[args.workload][0]) ** 2,
+                              "traffic_source": "ncu DRAM bytes (read + write) of one launch at "
+                                                "N=%d, scaled by (N/%d)^2" % (PAIR_TRAFFIC[args.workload][0],
+                                                                               PAIR_TRAFFIC[args.workload][0]),
+                              "step_share": asm_ms / ms_step},
         "cpu_baseline": cpu,
         "mixed": mixed,
         "learned": learned,
