@@ -48,7 +48,7 @@ FALG_ASSEMBLY_HS = 43867.0 + 288.0
 PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 144.824e9 * 5.114e-3)}
 # share of the step's (serialised) device time taken by the LU panel leaf, from
 # the committed launch list (profiles/launches_penny2013_fp64_and_mixed_step.md)
-DOMINANT_SHARE = {"penny": 0.534}
+DOMINANT_SHARE = {"penny": 0.571}
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
@@ -64,6 +64,9 @@ WORKLOADS = {
                 "FP64 assembly + LU"),
     "learned": ("TD pair-evals/s (HS dipping crack: FP64 assembly + learned-preconditioner GMRES to 1e-10)",
                 "3x1.5 crack dipping 45 deg, top at depth 2, half space, %d triangles, 3N=%d unknowns"),
+    "friction": ("frictional slip solve time (assembly + inverse + Fischer-Newton LCP), FS penny crack",
+                 "penny crack, full space, %d triangles, 5N=%d LCP unknowns, Tn=-2e-3 Tss=1e-3, mu=0.3, "
+                 "cohesion 2e-4 r/R, Fischer-Newton to max|Phi| <= 1e-10 max|q|"),
     "batch": ("TD pair-evals/s (batch of independent FS cracks: assembly + solve)",
               "%d full-space penny/elliptical cracks, semi-axis U[0.5,2], aspect U[0.3,1], random orientation, "
               "200-2000 triangles each (log-uniform), %d triangles in all"),
@@ -793,6 +796,114 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+FRICTION_SPACINGS = (0.12, 0.06)   # 496 and 2013 triangles
+
+
+def friction_case(spacing):
+    """Penny crack under compression and shear with friction: host arrays of
+    the C-ABI call (P1, P2, P3, normals, midpoints column-major; Tn, Tss, Tds,
+    mu, Sf per element)."""
+    import numpy as np
+
+    from cutanddisplacejulia_b200 import geometry, workloads
+    P1, P2, P3 = workloads.penny(seed=0, spacing=spacing)
+    nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
+    n = len(P1)
+    r = np.hypot(mid[:, 0], mid[:, 1])
+    return dict(n=n, lam=lam, P1=P1, P2=P2, P3=P3, nrm=nrm, mid=mid, Tn=np.full(n, -2e-3), Tss=np.full(n, 1e-3),
+                Tds=np.zeros(n), mu=np.full(n, 0.3), Sf=2e-4 * r)
+
+
+def friction_call(L, ctx, c, out):
+    import numpy as np
+
+    def f(a):
+        return np.asfortranarray(a, dtype=np.float64)
+    keep = [f(c[k]) for k in ("P1", "P2", "P3", "mid", "nrm")] + \
+        [np.ascontiguousarray(c[k], dtype=np.float64) for k in ("Tn", "Tss", "Tds", "mu", "Sf")]
+    P1, P2, P3, mid, nrm, Tn, Tss, Tds, mu, Sf = keep
+    n = c["n"]
+    return L.cad_slip_calculator_friction(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, n, NU, G, c["lam"],
+                                          mid.ctypes.data, nrm.ctypes.data, 0, Tn.ctypes.data, Tss.ctypes.data,
+                                          Tds.ctypes.data, mu.ctypes.data, Sf.ctypes.data, 1e-10, 100,
+                                          out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data)
+
+
+def run_friction(args, rank, world, local_rank):
+    """Frictional slip (src/SlipCalculator3D.jl:36-238) through the C ABI with
+    host buffers: one step = assembly of A, C = inv(A Scl) by the FP64 LU,
+    the 5N LCP by Fischer-Burmeister Newton (one FP64 LU of the 5N x 5N
+    Newton matrix per step).  Two sizes: 496 triangles (the size of the
+    reference's friction test) and 2013 (the penny workload); the CPU
+    baseline (oracle + numpy, all threads) on the 496-triangle case."""
+    import numpy as np
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    sizes = []
+    for sp in args.friction_spacing:
+        c = friction_case(sp)
+        n = c["n"]
+        out = [np.zeros(n), np.zeros(n), np.zeros(n)]
+        for _ in range(args.warmup):
+            _lib.check(friction_call(L, ctx, c, out), ctx)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=torch.device("cuda", local_rank))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        l0 = L.cad_kernel_launches(ctx)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            _lib.check(friction_call(L, ctx, c, out), ctx)
+        wall = time.perf_counter() - t0
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        launches = (L.cad_kernel_launches(ctx) - l0) // args.steps
+        its, rel = _lib.last_solve_stats(ctx)
+        dev = torch.device("cuda", local_rank)
+        ms = cdist.max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps, dev)
+        wall_ms = cdist.max_over_ranks(1e3 * wall / args.steps, dev)
+        n3, n5 = 3 * n, 5 * n
+        flops = (8.0 / 3.0) * n3 ** 3 + its * (2.0 / 3.0) * n5 ** 3
+        sizes.append({"triangles": n, "lcp_unknowns": n5, "ms_per_solve": ms, "e2e_wall_ms": wall_ms,
+                      "newton_steps": its, "gpu_launches_per_solve": launches,
+                      "final_rel_phi": rel, "slip_max": [float(np.abs(o).max()) for o in out],
+                      "fp64_lu_tflops": flops / (ms * 1e-3) / 1e12})
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import friction as F
+        from oracle import oracle as O
+        O.build()
+        c = friction_case(max(args.friction_spacing))
+        t0 = time.perf_counter()
+        F.slip_calculator_friction(c["P1"], c["P2"], c["P3"], NU, G, c["lam"], c["mid"], c["nrm"], 0, c["Tn"],
+                                   c["Tss"], c["Tds"], c["mu"], c["Sf"])
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": cpu_s * 1e3, "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+               "sample": "the %d-triangle case, one full solve: oracle assembly + numpy inv + numpy "
+                         "Fischer-Newton (LAPACK, all threads)" % c["n"]}
+    head = sizes[0]
+    line = {
+        "metric": WORKLOADS["friction"][0], "value": head["ms_per_solve"], "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_solve"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS["friction"][1] % (head["triangles"], head["lcp_unknowns"]),
+                   "inputs": "host memory (C ABI, copies inside the timed region)"},
+        "sizes": sizes, "cpu_baseline": cpu, "gpu_launches": head["gpu_launches_per_solve"] * args.steps,
+        "e2e": {"value": head["e2e_wall_ms"], "unit": "ms", "h2d_bytes_per_step": 8 * 25 * head["triangles"],
+                "d2h_bytes_per_step": 8 * 3 * head["triangles"]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -806,6 +917,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="penny",
                     help="penny: the default full-space penny crack (N~2000); dipping: half-space dipping crack")
     ap.add_argument("--ntri", type=int, default=10000, help="triangles of the dipping crack")
+    ap.add_argument("--friction-spacing", type=float, nargs="+", default=list(FRICTION_SPACINGS),
+                    help="lattice spacings of the friction workload's penny cracks (0.12: 496 triangles)")
     ap.add_argument("--cracks", type=int, default=512, help="cracks of the batch workload")
     ap.add_argument("--train-meshes", type=int, default=32, help="training meshes of the learned workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training steps of the learned workload")
@@ -833,6 +946,8 @@ def main():
             run_batch(args, rank, world, local_rank)
         elif args.workload == "learned":
             run_learned(args, rank, world, local_rank)
+        elif args.workload == "friction":
+            run_friction(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -9,11 +9,12 @@ orders and error messages); julia/CutAndDisplaceB200.jl is the Julia one.
 """
 from ._lib import CadError, context, load  # noqa: F401
 from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTractions3D,  # noqa: F401
-                       KnockOutFixedRows, SetupTractionVector, SlipCalculator3D, SlipCalculator3D_batched, solve)
+                       KnockOutFixedRows, SetupTractionVector, SlipCalculator3D, SlipCalculator3D_batched, fischer_newton,
+                       solve)
 from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint, HookesLaw3DStrain2Stress,  # noqa: F401
                        CreateP1P2P3, ElasticConstantsCheck)
-from .structs import (DispInf, Disps, MixedBoundaryConditions, StrainInf, Strains, Stresses,  # noqa: F401
-                      TractionInf, Tractions)
+from .structs import (DispInf, Disps, FrictionParameters, MixedBoundaryConditions,  # noqa: F401
+                      MixedBoundaryConditionsFriction, StrainInf, Strains, Stresses, TractionInf, Tractions)
 from .td import TD, TD_sum  # noqa: F401
 
 __version__ = "1.0.0"

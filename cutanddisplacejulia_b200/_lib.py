@@ -36,6 +36,7 @@ EXPORTS = [
     "cad_slip_calculator", "cad_slip_calculator_fixed", "cad_solve", "cad_td_inf_dev", "cad_td_sum_eval_dev", "cad_assemble_dev", "cad_assemble_update_dev",
     "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
     "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
+    "cad_slip_calculator_friction", "cad_fischer_newton",
 ]
 
 
@@ -102,6 +103,8 @@ def load():
     L.cad_lpc_param_count.restype = I64
     L.cad_lpc_step.argtypes = [P, P, P, P, I64, P, P, P, P, P, I64, ctypes.c_float]
     L.cad_td_sum_eval_noalloc.argtypes = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
+    L.cad_slip_calculator_friction.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, D, INT, P, P, P]
+    L.cad_fischer_newton.argtypes = [P, I64, P, P, D, INT, P]
     _lib = L
     return L
 

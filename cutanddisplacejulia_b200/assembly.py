@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from .geometry import ss_ds_dirs
-from .structs import MixedBoundaryConditions, Stresses, TractionInf, Tractions
+from .structs import MixedBoundaryConditions, MixedBoundaryConditionsFriction, Stresses, TractionInf, Tractions
 
 
 def _tri(P):
@@ -100,7 +100,14 @@ def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
     solver="lu64" solves A \\ b by FP64 LU as src/SlipCalculator3D.jl:22 does;
     solver="mixed" uses the FP32/TF32 LU + FP64 GMRES path to relative residual tol.
     assembly="mixed" evaluates far-field pairs in FP32 and pairs within
-    near_factor mean edge lengths in FP64 (assembly="fp64": all in FP64)."""
+    near_factor mean edge lengths in FP64 (assembly="fp64": all in FP64).
+
+    With MixedBoundaryConditionsFriction boundary conditions this is the
+    frictional solve of src/SlipCalculator3D.jl:36-87 and returns
+    (Dn, Dss, Dds) only, as the reference does (see SlipCalculator3D_friction)."""
+    if isinstance(BoundaryConditions, MixedBoundaryConditionsFriction):
+        return SlipCalculator3D_friction(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
+                                         BoundaryConditions, FixedEls, device=device)
     P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
     N = P1.shape[0]
     nrm = _tri(FaceNormalVector)
@@ -136,6 +143,61 @@ def SlipCalculator3D(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag,
                                              Dss.ctypes.data, Dds.ctypes.data, A.ctypes.data, b.ctypes.data)
         _lib.check(rc, ctx)
     return Dn, Dss, Dds, A, b
+
+
+def SlipCalculator3D_friction(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag, BoundaryConditions,
+                              FixedEls, device=0, tol=1e-10, max_iter=100):
+    """Slip with frictional contact (src/SlipCalculator3D.jl:36-238): returns
+    (Dn, Dss, Dds).  BoundaryConditions: MixedBoundaryConditionsFriction (the
+    remote stress and tractions of its MixedBoundaryConditions, mu and Sf of
+    its FrictionParameters, scalars broadcast to every element).  The
+    influence matrix is inverted after scaling by Scl = mean half-perimeter / G
+    and the 5N-variable complementarity problem is solved by a
+    Fischer-Burmeister Newton method on the GPU to max|Phi| <= tol max|q|.
+    Prints "Cant overcome frictional strength" and returns zero slip when no
+    element can slip, as the reference does.  The reference inverts the square
+    influence matrix, so fixed elements are not supported (Julia's inv raises
+    on the tall matrix they produce)."""
+    if FixedEls is not None and np.any(np.asarray(FixedEls).reshape(-1) == 1):
+        raise ValueError("DimensionMismatch: matrix is not square: the frictional solve takes no fixed elements")
+    P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+    N = P1.shape[0]
+    nrm = _tri(FaceNormalVector)
+    mid = _tri(MidPoint)
+    fp = BoundaryConditions.FrictionParameters
+    Tn, Tds, Tss = SetupTractionVector(BoundaryConditions.MixedBoundaryConditions, nrm, N, G, lam)
+    Tn, Tss, Tds = _col(Tn, N), _col(Tss, N), _col(Tds, N)
+    mu, Sf = _col(fp.mu, N), _col(fp.Sf, N)
+    if np.all(-np.abs(Tss) > Tn * mu) and np.all(-np.abs(Tds) > Tn * mu):
+        print("Cant overcome frictional strength")
+        return np.zeros(N), np.zeros(N), np.zeros(N)
+    Dn, Dss, Dds = np.zeros(N), np.zeros(N), np.zeros(N)
+    ctx = _lib.context(device)
+    rc = _lib.load().cad_slip_calculator_friction(ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, N, float(nu),
+                                                  float(G), float(lam), mid.ctypes.data, nrm.ctypes.data,
+                                                  int(HSFlag), Tn.ctypes.data, Tss.ctypes.data, Tds.ctypes.data,
+                                                  mu.ctypes.data, Sf.ctypes.data, float(tol), int(max_iter),
+                                                  Dn.ctypes.data, Dss.ctypes.data, Dds.ctypes.data)
+    _lib.check(rc, ctx)
+    return Dn, Dss, Dds
+
+
+def fischer_newton(A, b, device=0, tol=1e-10, max_iter=100):
+    """x solving the linear complementarity problem x >= 0, A x + b >= 0,
+    x'(A x + b) = 0 -- the FischerNewton.fischer_newton(A, b) call of
+    src/SlipCalculator3D.jl:196 -- by the GPU Fischer-Burmeister Newton method
+    from x = 0, to max|Phi| <= tol max|b|."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.float64).reshape(-1))
+    n = b.shape[0]
+    if A.shape != (n, n):
+        raise ValueError("DimensionMismatch: A must be %d x %d" % (n, n))
+    x = np.zeros(n)
+    ctx = _lib.context(device)
+    rc = _lib.load().cad_fischer_newton(ctx, n, A.ctypes.data, b.ctypes.data, float(tol), int(max_iter),
+                                        x.ctypes.data)
+    _lib.check(rc, ctx)
+    return x
 
 
 def solve(A, B, device=0, solver="lu64", tol=1e-10, max_iter=200):

@@ -9,12 +9,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/cad_td.h"
+#include "lcp.h"
 #include "lu.h"
 #include "mixed.h"
 #include "mlp.h"
@@ -32,7 +34,7 @@ namespace {
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
-    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_COUNT
+    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -1403,6 +1405,254 @@ int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* m
     ctx->timed[0] = true;
     CK(cudaStreamSynchronize(ctx->stream));   // the host list is read by the copy above
     return CAD_OK;
+}
+
+
+// ---------------------------------------------------------------- LCP solve ---
+
+namespace {
+
+// Fischer-Burmeister Newton method for the LCP x >= 0, y = M x + q >= 0,
+// x'y = 0 (the job of FischerNewton.fischer_newton, src/SlipCalculator3D.jl:196):
+// from x = 0, Newton steps on Phi(x) = FB(x, M x + q) = 0 with the generalized
+// Jacobian diag(Da) + diag(Db) M (rows with x_i = y_i = 0 taken along
+// z = e_beta), each solved by the FP64 LU and chain solve, and an Armijo
+// backtracking line search on psi = |Phi|^2 / 2 (all kLsSteps trial steps in
+// one launch).  A singular Newton matrix or a non-finite direction falls back
+// to steepest descent on psi.  Stops when max|Phi| <= tol max|q|, after
+// max_iter steps, or when no trial step decreases psi.  x (device, n) is the
+// solution; y (device, n) holds M x + q at exit; rel = max|Phi| / max|q|.
+int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, double* x, double* y, double tol,
+                      int max_iter, int* iters_out, double* rel_out)
+{
+    const int64_t n = op.n;
+    constexpr double kSigma = 1e-4;
+    void *jv, *vv;
+    if (int r = ensure(ctx, S_LCPJ, (size_t)n * n * sizeof(double), &jv)) return r;
+    if (int r = ensure(ctx, S_LCPV, ((size_t)9 * n + lcp_partial_doubles()) * sizeof(double), &vv)) return r;
+    double* J = (double*)jv;
+    double* V = (double*)vv;
+    double *phi = V, *z = V + n, *w = V + 2 * n, *Da = V + 3 * n, *Db = V + 4 * n, *d = V + 5 * n, *Md = V + 6 * n,
+           *u = V + 7 * n, *part = V + 8 * n;
+    double* stats = part + (size_t)kRedBlocks * (kLsSteps + 1);
+    double* psi_dev = stats + 8;
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(x, 0, n * sizeof(double), st));
+    CK(cudaMemsetAsync(w, 0, n * sizeof(double), st));
+    double hs[kLsSteps + 1];
+    CK(lcp_max_abs(q, n, part, stats, st, &ctx->launches));
+    CK(cudaMemcpyAsync(hs, stats, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double qscale = hs[0] > 0.0 ? hs[0] : 1.0;
+    const int saved_solver = ctx->solver;
+    struct Restore {
+        cad_ctx* c;
+        int s;
+        ~Restore() { c->solver = s; }
+    } restore{ctx, saved_solver};
+    ctx->solver = CAD_SOLVER_LU64;
+    int it = 0;
+    bool stalled = false;
+    double rel = 0.0;
+    for (;;) {
+        if (lcp_matvec(op, ctx->blas, st, x, q, y, u, &ctx->launches))
+            return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+        CK(lcp_fb_eval(x, y, n, phi, z, part, stats, st, &ctx->launches));
+        CK(cudaMemcpyAsync(hs, stats, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        rel = hs[0] / qscale;
+        const double psi = 0.5 * hs[1];
+        if (!(rel > tol) || it >= max_iter || stalled) break;
+        if (hs[2] > 0.0)   // rows with x_i = y_i = 0: w = M z
+            if (lcp_matvec(op, ctx->blas, st, z, nullptr, w, u, &ctx->launches))
+                return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+        CK(lcp_fb_diag(x, y, z, w, phi, n, Da, Db, d, st, &ctx->launches));
+        CK(lcp_build_jacobian(op, Da, Db, J, n, st));
+        ++ctx->launches;
+        int info = 0;
+        if (int r = solve_device(ctx, n, J, n, d, n, 1)) return r;
+        if (int r = read_info(ctx, &info)) return r;
+        double slope = -2.0 * psi;
+        bool newton = info == 0;
+        if (newton) {
+            if (lcp_matvec(op, ctx->blas, st, d, nullptr, Md, u, &ctx->launches))
+                return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+            CK(lcp_line_search(x, d, y, Md, n, part, psi_dev, st, &ctx->launches));
+            CK(cudaMemcpyAsync(hs, psi_dev, (kLsSteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (hs[kLsSteps] > 0.0) newton = false;   // a non-finite direction
+        }
+        if (!newton) {   // steepest descent: d = -(Da phi + M^T (Db phi))
+            CK(lcp_scale(Db, phi, n, Md, st, &ctx->launches));
+            if (lcp_matvec_t(op, ctx->blas, st, Md, d, u, &ctx->launches))
+                return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+            CK(lcp_grad_dir(Da, phi, n, d, part, stats, st, &ctx->launches));
+            CK(cudaMemcpyAsync(hs, stats + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            slope = -hs[0];
+            if (lcp_matvec(op, ctx->blas, st, d, nullptr, Md, u, &ctx->launches))
+                return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+            CK(lcp_line_search(x, d, y, Md, n, part, psi_dev, st, &ctx->launches));
+            CK(cudaMemcpyAsync(hs, psi_dev, (kLsSteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        double step = 0.0, t = 1.0;
+        for (int k = 0; k < kLsSteps; ++k) {
+            if (hs[k] <= psi + kSigma * t * slope) {
+                step = t;
+                break;
+            }
+            t *= 0.5;
+        }
+        ++it;
+        if (step == 0.0) {
+            stalled = true;   // no decrease left at rounding level: re-evaluate and stop
+            continue;
+        }
+        CK(lcp_step(x, d, step, n, st, &ctx->launches));
+    }
+    ctx->last_iters = it;
+    ctx->last_relres = rel;
+    *iters_out = it;
+    *rel_out = rel;
+    return CAD_OK;
+}
+
+int lcp_status(cad_ctx* ctx, int iters, double rel, double tol)
+{
+    if (rel > tol || !(rel == rel)) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "Fischer-Newton stopped at max|Phi|/max|q| = %.3e after %d iterations", rel,
+                      iters);
+        return fail(ctx, CAD_ERR_NOT_CONVERGED, msg);
+    }
+    return CAD_OK;
+}
+
+}  // namespace
+
+int cad_fischer_newton(cad_ctx* ctx, int64_t n, const double* A, const double* b, double tol, int max_iter,
+                       double* x)
+{
+    if (int r = set_device(ctx)) return r;
+    if (n < 0 || !(tol > 0.0) || max_iter < 0 || (n > 0 && (!A || !b || !x)) || n > INT32_MAX)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (n == 0) return CAD_OK;
+    void *Mv, *pv;
+    if (int r = ensure(ctx, S_LCPC, (size_t)n * n * sizeof(double), &Mv)) return r;
+    if (int r = ensure(ctx, S_LCPP, (size_t)3 * n * sizeof(double), &pv)) return r;
+    double* P = (double*)pv;
+    double *q = P, *xd = P + n, *y = P + 2 * n;
+    if (int r = upload(ctx, (double*)Mv, A, n * n)) return r;
+    if (int r = upload(ctx, q, b, n)) return r;
+    LcpOperator op;
+    op.n = n;
+    op.M = (const double*)Mv;
+    op.ldm = n;
+    int iters = 0;
+    double rel = 0.0;
+    if (int r = lcp_newton_device(ctx, op, q, xd, y, tol, max_iter, &iters, &rel)) return r;
+    CK(cudaMemcpyAsync(x, xd, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return lcp_status(ctx, iters, rel, tol);
+}
+
+int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N,
+                                 double nu, double G, double lambda, const double* midpoints, const double* normals,
+                                 int hs_flag, const double* Tn, const double* Tss, const double* Tds,
+                                 const double* mu, const double* Sf, double tol, int max_iter, double* Dn,
+                                 double* Dss, double* Dds)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || !(tol > 0.0) || max_iter < 0 || !(G != 0.0) ||
+        (N > 0 && (!P1 || !P2 || !P3 || !midpoints || !normals || !Tn || !Tss || !Tds || !mu || !Sf || !Dn ||
+                   !Dss || !Dds)) ||
+        5 * N > INT32_MAX)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->last_iters = 0;
+    ctx->last_relres = 0.0;
+    if (N == 0) return CAD_OK;
+    // no element can overcome its frictional resistance: no slip
+    // (src/SlipCalculator3D.jl:46-55; FricRes = Tn mu, negative is compression)
+    bool all_ss = true, all_ds = true;
+    for (int64_t i = 0; i < N; ++i) {
+        const double fr = Tn[i] * mu[i];
+        all_ss = all_ss && (-std::fabs(Tss[i]) > fr);
+        all_ds = all_ds && (-std::fabs(Tds[i]) > fr);
+    }
+    if (all_ss && all_ds) {
+        std::fill(Dn, Dn + N, 0.0);
+        std::fill(Dss, Dss + N, 0.0);
+        std::fill(Dds, Dds + N, 0.0);
+        return CAD_OK;
+    }
+    // Scl = mean(HalfPerimeter) / G (src/SlipCalculator3D.jl:58-59, AreaOfTriangle3D)
+    double hp = 0.0;
+    for (int64_t i = 0; i < N; ++i) {
+        double e[3];
+        const double* V[4] = {P1, P2, P3, P1};
+        for (int k = 0; k < 3; ++k) {
+            const double dx = V[k][i] - V[k + 1][i], dy = V[k][i + N] - V[k + 1][i + N],
+                         dz = V[k][i + 2 * N] - V[k + 1][i + 2 * N];
+            e[k] = std::sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        hp += (e[0] + e[1] + e[2]) / 2.0;
+    }
+    const double scl = (hp / (double)N) / G;
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    const int64_t n3 = 3 * N, n5 = 5 * N;
+    void *A, *Cv, *pv;
+    if (int r = ensure(ctx, S_A, (size_t)n3 * n3 * sizeof(double), &A)) return r;
+    if (int r = ensure(ctx, S_LCPC, (size_t)n3 * n3 * sizeof(double), &Cv)) return r;
+    if (int r = ensure(ctx, S_LCPP, ((size_t)2 * N + n3 + n3 + 3 * n5) * sizeof(double), &pv)) return r;
+    double* P = (double*)pv;
+    double *dmu = P, *dsf = P + N, *b = P + 2 * N, *rr = b + n3, *q = rr + n3, *xd = q + n5, *y = xd + n5;
+    double* slip = rr;   // r is dead once q is formed
+    if (int r = upload(ctx, dmu, mu, N)) return r;
+    if (int r = upload(ctx, dsf, Sf, N)) return r;
+    if (int r = upload(ctx, b, Tn, N)) return r;
+    if (int r = upload(ctx, b + N, Tss, N)) return r;
+    if (int r = upload(ctx, b + 2 * N, Tds, N)) return r;
+    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
+                            nullptr, (double*)A, n3);
+    if (r) return r;
+    // C = inv(A Scl): the FP64 LU of A Scl solved against the identity
+    double* C = (double*)Cv;
+    CK(scale_and_identity((double*)A, n3, n3, scl, C, ctx->stream, &ctx->launches));
+    {
+        const int solver = ctx->solver;
+        ctx->solver = CAD_SOLVER_LU64;
+        r = solve_device(ctx, n3, (double*)A, n3, C, n3, n3);
+        int info = 0;
+        if (r == CAD_OK) r = read_info(ctx, &info);
+        ctx->solver = solver;
+        if (r) return r;
+        if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    }
+    // q = [C (b - [0; Sf; Sf]); 2 Sf; 2 Sf] (src/SlipCalculator3D.jl:158-163, :190-193)
+    CK(friction_rhs(b, dsf, N, rr, q, ctx->stream, &ctx->launches));
+    const double one = 1.0, zero = 0.0;
+    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)n3, (int)n3, &one, C, (int)n3, rr, 1, &zero, q, 1) !=
+            CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "friction right-hand side: cuBLAS error");
+    LcpOperator op;
+    op.friction = true;
+    op.n = n5;
+    op.C = C;
+    op.ldc = n3;
+    op.mu = dmu;
+    op.m = N;
+    int iters = 0;
+    double rel = 0.0;
+    if ((r = lcp_newton_device(ctx, op, q, xd, y, tol, max_iter, &iters, &rel))) return r;
+    CK(friction_slip(xd, y, N, scl, slip, ctx->stream, &ctx->launches));
+    CK(cudaMemcpyAsync(Dn, slip, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dss, slip + N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dds, slip + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return lcp_status(ctx, iters, rel, tol);
 }
 
 }  // extern "C"

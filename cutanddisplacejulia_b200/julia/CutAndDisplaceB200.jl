@@ -139,6 +139,43 @@ function SlipCalculator3D(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSF
     return Dn, Dss, Dds, A, b
 end
 
+# Frictional slip (src/SlipCalculator3D.jl:36-87): Tn, Tss, Tds are the element
+# tractions of the MixedBoundaryConditions (remote stress resolved plus applied
+# tractions), μ and Sf the FrictionParameters (one value or one per element).
+# The reference's early exit (no element can overcome its frictional strength)
+# is taken here as there.  The LCP is solved on the GPU (Fischer-Burmeister
+# Newton in place of FischerNewton.fischer_newton, :196).
+function SlipCalculator3D_friction(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSFlag, Tn, Tss, Tds, μ, Sf;
+                                   tol::Real=1e-10, max_iter::Integer=100)
+    n = size(P1, 1)
+    μv = zeros(n) .+ μ
+    Sfv = zeros(n) .+ Sf
+    FricRes = vec(Tn) .* μv
+    if all(-abs.(vec(Tss)) .> FricRes) && all(-abs.(vec(Tds)) .> FricRes)
+        println("Cant overcome frictional strength")
+        return zeros(n), zeros(n), zeros(n)
+    end
+    Dn = zeros(n); Dss = zeros(n); Dds = zeros(n)
+    check(ccall((:cad_slip_calculator_friction, libcad), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Float64, Float64, Ptr{Float64},
+         Ptr{Float64}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Float64, Cint,
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        ctx(), f64(P1), f64(P2), f64(P3), n, ν, G, λ, f64(MidPoint), f64(FaceNormalVector), HSFlag,
+        f64(vec(Tn)), f64(vec(Tss)), f64(vec(Tds)), μv, Sfv, tol, max_iter, Dn, Dss, Dds))
+    return Dn, Dss, Dds
+end
+
+# The LCP x ≥ 0, A x + b ≥ 0, x'(A x + b) = 0 (FischerNewton.fischer_newton(A, b)).
+function fischer_newton(A, b; tol::Real=1e-10, max_iter::Integer=100)
+    n = length(b)
+    size(A) == (n, n) || error("DimensionMismatch: A must be $n x $n")
+    x = zeros(n)
+    check(ccall((:cad_fischer_newton, libcad), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Cint, Ptr{Float64}),
+        ctx(), n, f64(A), f64(vec(b)), tol, max_iter, x))
+    return x
+end
+
 # Precision settings (no counterpart in the reference): solver 0 = FP64 LU
 # (default), 1 = FP32/TF32 LU + FP64 GMRES, 2 = FP64 GMRES with the block-sparse
 # preconditioner set below; assembly 0 = FP64, 1 = FP32 far field.

@@ -57,6 +57,20 @@ class MixedBoundaryConditions(_Record):
 
 
 @dataclass
+class FrictionParameters(_Record):
+    """Friction coefficient mu (the reference's µ) and cohesion Sf, per
+    element or one value for all."""
+    mu: object = None
+    Sf: object = None
+
+
+@dataclass
+class MixedBoundaryConditionsFriction(_Record):
+    MixedBoundaryConditions: MixedBoundaryConditions = None
+    FrictionParameters: FrictionParameters = None
+
+
+@dataclass
 class StrainInf(_Record):
     exxDn: object = None
     eyyDn: object = None

@@ -180,6 +180,35 @@ int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, 
                               const double* fixed_els, double* Dn, double* Dss, double* Dds, double* A_out,
                               double* b_out);
 
+/* SlipCalculator3D with friction (MixedBoundaryConditionsFriction,
+ * src/SlipCalculator3D.jl:36-238).  Tn, Tss, Tds: element tractions of the
+ * boundary conditions (remote stress resolved on the elements plus applied
+ * tractions, as the frictionless call takes them); mu, Sf: friction
+ * coefficient and cohesion per element (N each).  When no element can
+ * overcome its frictional resistance Tn*mu on both shear components
+ * (:46-55) the slip is zero.  Otherwise A (3N x 3N, as cad_slip_calculator)
+ * is scaled by Scl = mean half-perimeter / G, C = inv(A Scl), and the 5N x 5N
+ * linear complementarity problem of :90-175 is solved by a Fischer-Burmeister
+ * Newton method (the reference calls FischerNewton.fischer_newton, :196) to
+ * max|Phi| <= tol max|q| within max_iter Newton steps; Dn = y1 Scl,
+ * Dss = (y2 - x4) Scl, Dds = (y3 - x5) Scl (:197-237).  The results are
+ * written also when the tolerance is not met, which returns
+ * CAD_ERR_NOT_CONVERGED; cad_last_solve_stats() gives the Newton steps and
+ * the final max|Phi| / max|q|. */
+int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N,
+                                 double nu, double G, double lambda, const double* midpoints, const double* normals,
+                                 int hs_flag, const double* Tn, const double* Tss, const double* Tds,
+                                 const double* mu, const double* Sf, double tol, int max_iter, double* Dn,
+                                 double* Dss, double* Dds);
+
+/* Linear complementarity problem x >= 0, y = A x + b >= 0, x'y = 0 for a dense
+ * A (n x n, column-major) and b (n): the call FischerNewton.fischer_newton(A, b)
+ * makes at src/SlipCalculator3D.jl:196, solved by the same Fischer-Burmeister
+ * Newton method as cad_slip_calculator_friction, from x = 0.  x: n values
+ * (written also when CAD_ERR_NOT_CONVERGED is returned). */
+int cad_fischer_newton(cad_ctx* ctx, int64_t n, const double* A, const double* b, double tol, int max_iter,
+                       double* x);
+
 /* Dense solve A X = B (the `\` of src/SlipCalculator3D.jl:22): A n x n, B n x
  * nrhs, both column-major host arrays; X n x nrhs. */
 int cad_solve(cad_ctx* ctx, int64_t n, const double* A, const double* B, int64_t nrhs, double* X);

@@ -7,6 +7,8 @@ GPU machines); the resulting .npz files are what the tests read.
   mogi.npz         test/SphereUniformDistributionON_46Faces.ts with test/SphereFix4.ts (scaled x3)
                    appended as fixed elements (DataAppender3D), 50 below the surface, as
                    test/test_TDvsMogi.jl:6-20 builds it; also holds FixedEls
+  blade500.npz     test/BladeFaultShort_500Tris_Vertical_NorthDip_0.5.ts (GoCadAsciiReader), as read;
+                   test/test_TDvsBurgmannLinearFrictionCrack.jl flattens and scales it itself
 
 Each file holds P1, P2, P3 (N x 3 float64), built as CreateP1P2P3 does
 (src/CreateP1P2P3.jl): vertex k of triangle i is the point whose index the
@@ -83,6 +85,10 @@ def main(ref):
     P1, P2, P3 = p1p2p3(allp, allt)
     np.savez_compressed(os.path.join(HERE, "mogi.npz"), P1=P1, P2=P2, P3=P3, FixedEls=fixed)
     print("wrote mogi.npz (%d tris, %d fixed)" % (len(allt), int(fixed.sum())))
+    pts, tris = read_gocad_ts(os.path.join(test_dir, "BladeFaultShort_500Tris_Vertical_NorthDip_0.5.ts"))
+    P1, P2, P3 = p1p2p3(pts, tris)
+    np.savez_compressed(os.path.join(HERE, "blade500.npz"), P1=P1, P2=P2, P3=P3)
+    print("wrote blade500.npz (%d tris)" % len(tris))
 
 
 if __name__ == "__main__":

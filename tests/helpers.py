@@ -105,3 +105,67 @@ def rel_inf_err(a, b):
     if scale == 0:
         return float(np.max(np.abs(a[m])))
     return float(np.max(np.abs(a[m] - b[m])) / scale)
+
+
+def burgmann_case(half):
+    """The two cracks of test/test_TDvsBurgmannLinearFrictionCrack.jl: the 497
+    triangle blade fault flattened to y = 0 and scaled to half length 1e-4
+    (half 1, driven by sxy, closed by syy) or turned into the z = 0 plane at
+    half length 1e4 (half 2, driven by sxz, closed by szz); mu = 0 and
+    cohesion Sf = |x| of each collocation point."""
+    from oracle.geometry import elastic_constants, face_normal_and_midpoint
+    P1, P2, P3 = load_mesh("blade500")
+    for P in (P1, P2, P3):
+        if half == 1:
+            P[:, 1] = 0.0
+        else:
+            P[:, 1] = P[:, 2]
+            P[:, 2] = 0.0
+    S = 1e-4 if half == 1 else 1e4
+    P1, P2, P3 = P1 * S, P2 * S, P3 * S
+    nrm, mid = face_normal_and_midpoint(P1, P2, P3)
+    n = len(P1)
+    _, _, lam, nu, G = elastic_constants(1.0, 0.25)
+    z = np.zeros(n)
+    if half == 1:
+        sig = (z, np.full(n, -0.05 * S), z, np.full(n, S), z, z)
+    else:
+        sig = (z, z, np.full(n, -0.05 * S), z, np.full(n, S), z)
+    return dict(P1=P1, P2=P2, P3=P3, nrm=nrm, mid=mid, nu=nu, G=G, lam=lam, sig=sig, mu=0.0,
+                Sf=np.abs(mid[:, 0]), S=S, n=n)
+
+
+def burgmann_check(case, half, D_plain, D_fric):
+    """The reference's acceptance of test/test_TDvsBurgmannLinearFrictionCrack.jl:
+    near the crack centre line, slip within 36 % of the analytic profile on
+    |x| < 0.9 a, and the summed percentage deviation at most 1400.  D_*: the
+    shear component the case drives (Dss for half 1, Dds for half 2)."""
+    from oracle import friction as F
+    mid, S, G, nu = case["mid"], case["S"], case["G"], case["nu"]
+    good = np.abs(mid[:, 2 if half == 1 else 1]) < S
+    x = mid[good, 0]
+    ana_u = F.pollard_segall1987_slip(G, nu, 0.0, S, x, S)
+    ana_f = F.burgmann1994_slip(G, nu, S, x, S)
+    pu = 100.0 / ana_u * np.abs(D_plain[good])
+    pf = 100.0 / ana_f * np.abs(D_fric[good])
+    pu[np.isinf(pu)] = np.nan
+    pf[np.isinf(pf)] = np.nan
+    assert np.sum(pu - 100) <= 1400 and np.sum(pf - 100) <= 1400, (np.sum(pu - 100), np.sum(pf - 100))
+    inner = np.abs(x) < 0.9 * S
+    assert not np.any(np.abs(pu[inner] - 100) > 36), np.nanmax(np.abs(pu[inner] - 100))
+    assert not np.any(np.abs(pf[inner] - 100) > 36), np.nanmax(np.abs(pf[inner] - 100))
+
+
+def random_lcp(rng, n, frac_active=0.5, frac_degenerate=0.0):
+    """LCP (M, q) with a known unique solution x*: M = R R^T / n + I is
+    positive definite; x* > 0 on a random subset, y* = M x* + q > 0 off it,
+    both zero on a further fraction of rows (degenerate)."""
+    R = rng.standard_normal((n, n))
+    M = R @ R.T / n + np.eye(n)
+    u = rng.uniform(size=n)
+    act = u < frac_active
+    deg = (u >= frac_active) & (u < frac_active + frac_degenerate)
+    x = np.where(act, rng.uniform(0.5, 2.0, n), 0.0)
+    y = np.where(act | deg, 0.0, rng.uniform(0.5, 2.0, n))
+    q = y - M @ x
+    return np.asfortranarray(M), q, x
