@@ -833,8 +833,8 @@ def friction_call(L, ctx, c, out):
 def run_friction(args, rank, world, local_rank):
     """Frictional slip (src/SlipCalculator3D.jl:36-238) through the C ABI with
     host buffers: one step = assembly of A, C = inv(A Scl) by the FP64 LU,
-    the 5N LCP by Fischer-Burmeister Newton (one FP64 LU of the 5N x 5N
-    Newton matrix per step).  Two sizes: 496 triangles (the size of the
+    the 5N LCP by Fischer-Burmeister Newton (one FP64 LU of the Newton
+    system, reduced to 3N unknowns, per step).  Two sizes: 496 triangles (the size of the
     reference's friction test) and 2013 (the penny workload); the CPU
     baseline (oracle + numpy, all threads) on the 496-triangle case."""
     import numpy as np
@@ -871,7 +871,8 @@ def run_friction(args, rank, world, local_rank):
         ms = cdist.max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps, dev)
         wall_ms = cdist.max_over_ranks(1e3 * wall / args.steps, dev)
         n3, n5 = 3 * n, 5 * n
-        flops = (8.0 / 3.0) * n3 ** 3 + its * (2.0 / 3.0) * n5 ** 3
+        # inverse (LU + 3N-column solve) and one LU of the reduced 3N x 3N Newton system per step
+        flops = (8.0 / 3.0) * n3 ** 3 + its * (2.0 / 3.0) * n3 ** 3
         sizes.append({"triangles": n, "lcp_unknowns": n5, "ms_per_solve": ms, "e2e_wall_ms": wall_ms,
                       "newton_steps": its, "gpu_launches_per_solve": launches,
                       "final_rel_phi": rel, "slip_max": [float(np.abs(o).max()) for o in out],

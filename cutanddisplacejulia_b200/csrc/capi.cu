@@ -1427,13 +1427,17 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
 {
     const int64_t n = op.n;
     constexpr double kSigma = 1e-4;
+    // the friction problem's Newton systems are solved in reduced form (3m unknowns)
+    const int64_t nj = op.friction ? 3 * op.m : n;
     void *jv, *vv;
-    if (int r = ensure(ctx, S_LCPJ, (size_t)n * n * sizeof(double), &jv)) return r;
-    if (int r = ensure(ctx, S_LCPV, ((size_t)9 * n + lcp_partial_doubles()) * sizeof(double), &vv)) return r;
+    if (int r = ensure(ctx, S_LCPJ, (size_t)nj * nj * sizeof(double), &jv)) return r;
+    if (int r = ensure(ctx, S_LCPV, ((size_t)13 * n + lcp_partial_doubles()) * sizeof(double), &vv)) return r;
     double* J = (double*)jv;
     double* V = (double*)vv;
     double *phi = V, *z = V + n, *w = V + 2 * n, *Da = V + 3 * n, *Db = V + 4 * n, *d = V + 5 * n, *Md = V + 6 * n,
-           *u = V + 7 * n, *part = V + 8 * n;
+           *u = V + 7 * n, *part = V + 13 * n;
+    // friction: coef (16m), u0 (3m), C u0 (3m), reduced right-hand side (3m) = 5n doubles
+    double *coef = V + 8 * n, *u0 = coef + 16 * op.m, *cu0 = u0 + 3 * op.m, *rhs = cu0 + 3 * op.m;
     double* stats = part + (size_t)kRedBlocks * (kLsSteps + 1);
     double* psi_dev = stats + 8;
     cudaStream_t st = ctx->stream;
@@ -1467,11 +1471,27 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
             if (lcp_matvec(op, ctx->blas, st, z, nullptr, w, u, &ctx->launches))
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
         CK(lcp_fb_diag(x, y, z, w, phi, n, Da, Db, d, st, &ctx->launches));
-        CK(lcp_build_jacobian(op, Da, Db, J, n, st));
-        ++ctx->launches;
         int info = 0;
-        if (int r = solve_device(ctx, n, J, n, d, n, 1)) return r;
-        if (int r = read_info(ctx, &info)) return r;
+        if (op.friction) {   // J d = -phi through the 3m x 3m reduced system
+            const int64_t m = op.m, m3 = 3 * m;
+            const double one = 1.0, zero = 0.0;
+            CK(friction_reduce_prep(Da, Db, d, op.mu, m, coef, u0, st, &ctx->launches));
+            if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS ||
+                cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)m3, (int)m3, &one, op.C, (int)op.ldc, u0, 1, &zero, cu0,
+                            1) != CUBLAS_STATUS_SUCCESS)
+                return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
+            CK(friction_reduced_rhs(d, Da, Db, cu0, coef, m, rhs, st, &ctx->launches));
+            CK(friction_reduced_jacobian(op.C, op.ldc, op.mu, Da, Db, coef, m, J, m3, st));
+            ++ctx->launches;
+            if (int r = solve_device(ctx, m3, J, m3, rhs, m3, 1)) return r;
+            if (int r = read_info(ctx, &info)) return r;
+            CK(friction_recover(rhs, coef, m, d, st, &ctx->launches));
+        } else {
+            CK(lcp_build_jacobian(op, Da, Db, J, n, st));
+            ++ctx->launches;
+            if (int r = solve_device(ctx, n, J, n, d, n, 1)) return r;
+            if (int r = read_info(ctx, &info)) return r;
+        }
         double slope = -2.0 * psi;
         bool newton = info == 0;
         if (newton) {

@@ -342,6 +342,113 @@ __global__ void scale_identity_kernel(double* __restrict__ A, int64_t lda, int64
     }
 }
 
+// coef layout: field f of element r at coef[f * m + r]
+enum { CF_A2, CF_B2, CF_C2, CF_A4, CF_B4, CF_C4, CF_A3, CF_B3, CF_C3, CF_A5, CF_B5, CF_C5, CF_L21, CF_L22, CF_L31,
+       CF_L33, CF_COUNT };
+
+__global__ void reduce_prep_kernel(const double* __restrict__ Da, const double* __restrict__ Db,
+                                   const double* __restrict__ r, const double* __restrict__ mu, int64_t m,
+                                   double* __restrict__ coef, double* __restrict__ u0)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const double w2 = __dmul_rn(2.0, mu[e]);
+        u0[e] = 0.0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {   // h = 0: blocks 2 / 4, h = 1: blocks 3 / 5
+            const int64_t s = (1 + h) * m + e, t = (3 + h) * m + e;
+            const double da = Da[t], db = Db[t], rt = r[t];
+            double as, bs, cs, at, bt, ct;
+            if (fabs(da) >= fabs(db)) {   // row t solved for d_t
+                as = 0.0; bs = 0.0; cs = 1.0;
+                at = __ddiv_rn(rt, da);
+                bt = -__ddiv_rn(__dmul_rn(w2, db), da);
+                ct = __ddiv_rn(db, da);
+            } else {                      // row t solved for d_s; d_t becomes the unknown
+                as = -__ddiv_rn(rt, db);
+                bs = w2;
+                cs = __ddiv_rn(da, db);
+                at = 0.0; bt = 0.0; ct = 1.0;
+            }
+            double* c = coef + (int64_t)(6 * h) * m + e;
+            c[0 * m] = as; c[1 * m] = bs; c[2 * m] = cs;
+            c[3 * m] = at; c[4 * m] = bt; c[5 * m] = ct;
+            const double das = Da[s], dbs = Db[s];
+            coef[(int64_t)(CF_L21 + 2 * h) * m + e] = __dadd_rn(__dmul_rn(das, bs), __dmul_rn(dbs, bt));
+            coef[(int64_t)(CF_L22 + 2 * h) * m + e] = __dadd_rn(__dmul_rn(das, cs), __dmul_rn(dbs, ct));
+            u0[(1 + h) * m + e] = as;
+        }
+    }
+}
+
+__global__ void reduced_rhs_kernel(const double* __restrict__ r, const double* __restrict__ Da,
+                                   const double* __restrict__ Db, const double* __restrict__ cu0,
+                                   const double* __restrict__ coef, int64_t m, double* __restrict__ rhs)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double v = __dsub_rn(r[i], __dmul_rn(Db[i], cu0[i]));
+        if (i >= m) {
+            const int64_t h = i / m - 1, e = i - (1 + h) * m;
+            const double as = coef[(int64_t)(CF_A2 + 6 * h) * m + e], at = coef[(int64_t)(CF_A4 + 6 * h) * m + e];
+            v = __dsub_rn(v, __dadd_rn(__dmul_rn(Da[i], as), __dmul_rn(Db[i], at)));
+        }
+        rhs[i] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) reduced_jacobian_kernel(const double* __restrict__ C, int64_t ldc,
+                                                                   const double* __restrict__ mu,
+                                                                   const double* __restrict__ Da,
+                                                                   const double* __restrict__ Db,
+                                                                   const double* __restrict__ coef, int64_t m,
+                                                                   double* __restrict__ R, int64_t ldr)
+{
+    const int64_t n3 = 3 * m;
+    const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+    if (i >= n3) return;
+    const double db = Db[i];
+    const int64_t rb = i / m, ri = i - rb * m;
+    for (int64_t col = blockIdx.y; col < n3; col += gridDim.y) {
+        const int64_t cb = col / m, e = col - cb * m;
+        double v;
+        if (cb == 0) {
+            const double g2 = __dsub_rn(coef[(int64_t)CF_B2 * m + e], mu[e]);
+            const double g3 = __dsub_rn(coef[(int64_t)CF_B3 * m + e], mu[e]);
+            v = __dadd_rn(__dadd_rn(C[i + e * ldc], __dmul_rn(g2, C[i + (m + e) * ldc])),
+                          __dmul_rn(g3, C[i + (2 * m + e) * ldc]));
+        } else {
+            v = __dmul_rn(coef[(int64_t)(cb == 1 ? CF_C2 : CF_C3) * m + e], C[i + col * ldc]);
+        }
+        double out = __dmul_rn(db, v);
+        if (ri == e) {
+            double loc = 0.0;
+            if (rb == 0 && cb == 0) loc = Da[i];
+            else if (rb == 1 && cb == 0) loc = coef[(int64_t)CF_L21 * m + e];
+            else if (rb == 1 && cb == 1) loc = coef[(int64_t)CF_L22 * m + e];
+            else if (rb == 2 && cb == 0) loc = coef[(int64_t)CF_L31 * m + e];
+            else if (rb == 2 && cb == 2) loc = coef[(int64_t)CF_L33 * m + e];
+            out = __dadd_rn(out, loc);
+        }
+        R[i + col * ldr] = out;
+    }
+}
+
+__global__ void recover_kernel(const double* __restrict__ v, const double* __restrict__ coef, int64_t m,
+                               double* __restrict__ d)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const double v1 = v[e];
+        d[e] = v1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const double vs = v[(1 + h) * m + e];
+            const double* c = coef + (int64_t)(6 * h) * m + e;
+            d[(1 + h) * m + e] = __dadd_rn(__dadd_rn(c[0 * m], __dmul_rn(c[1 * m], v1)), __dmul_rn(c[2 * m], vs));
+            d[(3 + h) * m + e] = __dadd_rn(__dadd_rn(c[3 * m], __dmul_rn(c[4 * m], v1)), __dmul_rn(c[5 * m], vs));
+        }
+    }
+}
+
 int grid_for(int64_t n)
 {
     const int64_t g = (n + kThreads - 1) / kThreads;
@@ -479,6 +586,40 @@ cudaError_t friction_slip(const double* x, const double* y, int64_t m, double sc
                           int64_t* launches)
 {
     friction_slip_kernel<<<grid_for(m), kThreads, 0, st>>>(x, y, m, scl, out);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t friction_reduce_prep(const double* Da, const double* Db, const double* r, const double* mu, int64_t m,
+                                 double* coef, double* u0, cudaStream_t st, int64_t* launches)
+{
+    reduce_prep_kernel<<<grid_for(m), kThreads, 0, st>>>(Da, Db, r, mu, m, coef, u0);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t friction_reduced_rhs(const double* r, const double* Da, const double* Db, const double* cu0,
+                                 const double* coef, int64_t m, double* rhs, cudaStream_t st, int64_t* launches)
+{
+    reduced_rhs_kernel<<<grid_for(3 * m), kThreads, 0, st>>>(r, Da, Db, cu0, coef, m, rhs);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t friction_reduced_jacobian(const double* C, int64_t ldc, const double* mu, const double* Da,
+                                      const double* Db, const double* coef, int64_t m, double* R, int64_t ldr,
+                                      cudaStream_t st)
+{
+    if (m <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)((3 * m + kThreads - 1) / kThreads), cols_grid(3 * m));
+    reduced_jacobian_kernel<<<grid, kThreads, 0, st>>>(C, ldc, mu, Da, Db, coef, m, R, ldr);
+    return cudaGetLastError();
+}
+
+cudaError_t friction_recover(const double* v, const double* coef, int64_t m, double* d, cudaStream_t st,
+                             int64_t* launches)
+{
+    recover_kernel<<<grid_for(m), kThreads, 0, st>>>(v, coef, m, d);
     if (launches) ++*launches;
     return cudaGetLastError();
 }

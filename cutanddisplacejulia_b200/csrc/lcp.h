@@ -78,6 +78,28 @@ cudaError_t friction_rhs(const double* b, const double* Sf, int64_t m, double* r
 // Dn = y1 Scl, Dss = (y2 - x4) Scl, Dds = (y3 - x5) Scl into out (3m).
 cudaError_t friction_slip(const double* x, const double* y, int64_t m, double scl, double* out, cudaStream_t st,
                           int64_t* launches);
+// Newton direction of the friction LCP through a 3m x 3m system instead of
+// the 5m x 5m one.  Rows L4 / L5 of J = diag(Da) + diag(Db) M couple only d4
+// (d5), d2 (d3) and d1 of the same element; each such row is solved for d4_r
+// when |Da4_r| >= |Db4_r|, else for d2_r (Da, Db lie on the circle
+// (Da+1)^2 + (Db+1)^2 = 1, so the divisor is at least 1 - 1/sqrt(2)), and the
+// result substituted into rows L1..L3.  The unknowns of the reduced system
+// are v = [d1; d2 or d4; d3 or d5] per element; coef (16m) holds, per
+// element, d2 = a2 + b2 v1 + c2 v2, d4 = a4 + b4 v1 + c4 v2, the same for
+// 3 / 5, and the four local diagonal entries.  u0 (3m) = [0; a2; a3].
+cudaError_t friction_reduce_prep(const double* Da, const double* Db, const double* r, const double* mu, int64_t m,
+                                 double* coef, double* u0, cudaStream_t st, int64_t* launches);
+// rhs (3m) = r_top - Db_top (C u0) - the local constants; cu0 = C u0.
+cudaError_t friction_reduced_rhs(const double* r, const double* Da, const double* Db, const double* cu0,
+                                 const double* coef, int64_t m, double* rhs, cudaStream_t st, int64_t* launches);
+// R (3m x 3m, ldr): the reduced Newton matrix, entry by entry from C.
+cudaError_t friction_reduced_jacobian(const double* C, int64_t ldc, const double* mu, const double* Da,
+                                      const double* Db, const double* coef, int64_t m, double* R, int64_t ldr,
+                                      cudaStream_t st);
+// d (5m) from the reduced solution v (3m).
+cudaError_t friction_recover(const double* v, const double* coef, int64_t m, double* d, cudaStream_t st,
+                             int64_t* launches);
+
 // A *= s (n x n, lda); I = identity (n x n, n).
 cudaError_t scale_and_identity(double* A, int64_t lda, int64_t n, double s, double* I, cudaStream_t st,
                                int64_t* launches);
