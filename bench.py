@@ -37,7 +37,8 @@ from cutanddisplacejulia_b200 import dist as cdist  # noqa: E402
 # Algorithmic FP64 operations per pair-evaluation of the assembly kernel:
 # full-space strain of all three unit slip modes (2960, counted with the
 # oracle's counting scalar on this mesh's collocation pairs) plus the strain ->
-# traction epilogue (288 = 3 modes x 96).  Frozen values, see DESIGN.md.
+# traction epilogue (288 = 3 modes x 96).  Frozen values: kernel-side common
+# subexpressions count as speed-up, not as fewer operations.
 FALG_ASSEMBLY_FS = 2960.0 + 288.0
 # Half-space strain of all three unit modes (43867 on the dipping-crack
 # collocation pairs) plus the same traction epilogue.
@@ -454,7 +455,7 @@ def run_learned(args, rank, world, local_rank):
     library's BF16 kernels) on exact inverse blocks of small seeded meshes,
     applied to a large half-space crack as a block-sparse right
     preconditioner of FP64 GMRES; beside it block-Jacobi GMRES and the FP64
-    dense LU (the fallback, and the judge of the solution error)."""
+    dense LU (the fallback, and the reference for the solution error)."""
     import numpy as np
     import torch
 
