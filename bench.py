@@ -777,7 +777,8 @@ def run_ours(args, rank, world, local_rank):
                             "share_of_step_ncu": DOMINANT_SHARE.get(args.workload),
                             "bound": "latency: one pivot search and row exchange across a 12-16 CTA cluster per "
                                      "column (about 1.7 us per column)",
-                            "source": "profiles/launches_penny2013_fp64_and_mixed_step.md"},
+                            "source": "profiles/launches_penny2013_fp64_and_mixed_step.md",
+                            "ncu_full": "profiles/leaf_lu_kernel_penny2013.md"},
         "roofline_assembly": {"kernel": "td_pair_kernel<%s, strain, A-matrix>" % ("HS" if hs else "FS"),
                               "bound": "fp64", "achieved": achieved, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                               "frac": achieved / fp64_peak_tflops,
