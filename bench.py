@@ -153,15 +153,92 @@ def cpu_reference_step(wl, nthreads):
     return t1 - t0, t2 - t1
 
 
+def reference_line(args, metric, value, unit, higher, ms, workload_desc, sample, nthreads, extra=None):
+    line = {
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": higher,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_desc, "inputs": "host memory"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line.update(extra or {})
+    return line
+
+
+def run_reference_friction(args, nthreads):
+    """Reference arm of the friction workload: the oracle's frictional solve
+    (assembly, numpy inverse, numpy Fischer-Newton on the full 5N system) of
+    the first (smallest) penny crack, per step."""
+    from oracle import friction as F
+    c = friction_case(max(args.friction_spacing))
+
+    def step():
+        t0 = time.perf_counter()
+        F.slip_calculator_friction(c["P1"], c["P2"], c["P3"], NU, G, c["lam"], c["mid"], c["nrm"], 0, c["Tn"],
+                                   c["Tss"], c["Tds"], c["mu"], c["Sf"])
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    ms = 1e3 * sum(step() for _ in range(args.steps)) / args.steps
+    return reference_line(args, WORKLOADS["friction"][0], ms, "ms", False, ms,
+                          WORKLOADS["friction"][1] % (c["n"], 5 * c["n"]),
+                          "one full frictional solve of the %d-triangle crack per step: oracle assembly, numpy "
+                          "inverse and Fischer-Newton (LAPACK, %d threads)" % (c["n"], nthreads), nthreads)
+
+
+def run_reference_batch(args, nthreads, sample=8):
+    """Reference arm of the batch workload on a bounded sample: the first
+    `sample` cracks of the same seeded batch, each assembled by the oracle and
+    solved by numpy LAPACK, one after the other; pairs per second of the
+    sample."""
+    import numpy as np
+    from oracle import oracle as O
+
+    from cutanddisplacejulia_b200 import assembly, geometry, workloads
+    cracks, stresses = workloads.crack_batch(seed=0, count=args.cracks)
+    _, _, lam, _, _ = geometry.ElasticConstantsCheck(G, NU)
+    wls = []
+    for (P1, P2, P3), st in list(zip(cracks, stresses))[:sample]:
+        nrm, mid = geometry.CreateFaceNormalAndMidPoint(P1, P2, P3)
+        Tn, Tds, Tss = assembly.CalculateNormalAndShearTractions3D(*st, nrm)
+        wls.append((P1, P2, P3, nrm, mid, lam, 0, (Tn, Tss, Tds)))
+    pairs = float(sum(len(w[0]) ** 2 for w in wls))
+
+    def step():
+        t = 0.0
+        for wl in wls:
+            a, b = cpu_reference_step(wl, nthreads)
+            t += a + b
+        return t
+    for _ in range(args.warmup):
+        step()
+    step_s = sum(step() for _ in range(args.steps)) / args.steps
+    ntot = sum(len(w[0]) for w in wls)
+    return reference_line(args, WORKLOADS["batch"][0], pairs / step_s, UNIT, True, step_s * 1e3,
+                          WORKLOADS["batch"][1] % (args.cracks, sum(len(c[0]) for c in cracks)),
+                          "the first %d cracks of the batch (%d triangles, %.3g pairs) per step: oracle assembly "
+                          "+ numpy LAPACK gesv, %d threads" % (len(wls), ntot, pairs, nthreads), nthreads)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
     import numpy as np  # noqa: F401
     from oracle import oracle as O
     O.build()
+    nthreads = os.cpu_count() or 1
+    if args.workload in ("friction", "batch"):
+        fn = run_reference_friction if args.workload == "friction" else run_reference_batch
+        print(json.dumps(fn(args, nthreads)), flush=True)
+        return
+    if args.workload == "learned":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement needs well over an hour per "
+                          "step at N = 20000 in half space; the reference arm covers penny, dipping, friction and "
+                          "batch"}), flush=True)
+        return
     wl = workload(args.workload, args.ntri)
     n = len(wl[0])
-    nthreads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_reference_step(wl, nthreads)
     ta, ts = 0.0, 0.0
