@@ -105,3 +105,35 @@ def test_fischer_newton_not_converged(cad):
         cad.fischer_newton(M, q, tol=1e-14, max_iter=1)
     assert e.value.code == cad._lib.CAD_ERR_NOT_CONVERGED
     assert "Fischer-Newton" in str(e.value)
+
+
+def test_friction_half_space_dipping_crack(cad, oracle):
+    """Friction in half space: a 60-degree dipping crack 1 below the surface
+    under a compressive remote stress with shear, mu = 0.7 and cohesion
+    growing with depth (about 45 % of the elements slip, the rest stick);
+    slip against the oracle's frictional solve (the half-space influence
+    matrix on both sides)."""
+    from oracle import friction as F
+
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=4, ntri=320, top_depth=1.0)
+    nrm, mid = cad.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
+    n = len(P1)
+    sig = (-2e-3, -1e-3, -3e-3, 1e-3, 1.5e-3, -0.5e-3)
+    Sf = 2e-4 * np.abs(mid[:, 2])
+    bc = cad.MixedBoundaryConditionsFriction(
+        cad.MixedBoundaryConditions(cad.Stresses(*sig), cad.Tractions(0.0, 0.0, 0.0)),
+        cad.FrictionParameters(0.7, Sf))
+    args = (P1, P2, P3, nu, G, lam, mid, nrm, 1)
+    DnF, DssF, DdsF = cad.SlipCalculator3D(*args, bc, None)
+    it, rel = cad._lib.last_solve_stats(cad.context(0))
+    assert rel <= 1e-10
+    Tn, Tds, Tss = oracle.normal_and_shear_tractions(*[np.full(n, s) for s in sig], nrm)
+    Dno, Dsso, Ddso, info = F.slip_calculator_friction(*args, Tn, Tss, Tds, 0.7, Sf)
+    ref = np.concatenate([Dno, Dsso, Ddso])
+    got = np.concatenate([DnF, DssF, DdsF])
+    slipping = np.abs(Dsso) > 1e-9
+    assert 0 < slipping.sum() < n
+    assert np.linalg.norm(got - ref) <= SLIP_TOL * np.linalg.norm(ref)
+    assert np.array_equal(np.abs(DssF) > 1e-9, slipping)
