@@ -406,7 +406,7 @@ def run_batch(args, rank, world, local_rank):
     """Many independent cracks (the batching configuration): every crack
     assembled (FP32 far field / FP64 near field) and solved by FP32 LU with
     FP64 refinement to relative residual 1e-10, all cracks in one captured
-    CUDA graph over 8 stream lanes (cad_slip_calculator_batched_dev).  Beside
+    CUDA graph over 32 stream lanes (cad_slip_calculator_batched_dev).  Beside
     it: the plain per-crack FP64 path (assembly + FP64 LU, one crack after the
     other) on the same cracks, and the slip error against it."""
     import numpy as np

@@ -54,7 +54,7 @@ struct Lane {
     cudaEvent_t done = nullptr;
     DevBuf buf[L_COUNT];
 };
-constexpr int kLanes = 8;            // cracks of a batch in flight at once
+constexpr int kLanes = 32;           // cracks of a batch in flight at once
 constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
 constexpr size_t kBlasWorkspace = 32u << 20;
 

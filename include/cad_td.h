@@ -277,7 +277,7 @@ int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, in
  * assembly precision (cad_set_assembly) and solved by FP32 LU (TF32
  * updates) with FP64 refinement to the context's tolerance (cad_set_solver),
  * GMRES finishing any crack the refinement leaves.  The cracks run
- * concurrently on 8 stream lanes inside one CUDA graph, captured on the first
+ * concurrently on 32 stream lanes inside one CUDA graph, captured on the first
  * call with these arguments and replayed by identical calls.  Needs device
  * memory for every crack's 3N_c x 3N_c matrix at once.  rel_residual (host,
  * nbatch, may be NULL): each crack's final ||b - A D|| / ||b||. */
