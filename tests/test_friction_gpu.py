@@ -137,3 +137,21 @@ def test_friction_half_space_dipping_crack(cad, oracle):
     assert 0 < slipping.sum() < n
     assert np.linalg.norm(got - ref) <= SLIP_TOL * np.linalg.norm(ref)
     assert np.array_equal(np.abs(DssF) > 1e-9, slipping)
+
+
+def test_fischer_newton_rank_deficient_complementarity(cad):
+    """A positive semi-definite, rank-deficient M (solutions not unique): the
+    returned x must satisfy the complementarity conditions x >= 0,
+    y = M x + q >= 0, x'y = 0 to the tolerance's scale."""
+    rng = np.random.default_rng(0)
+    n = 400
+    B = rng.standard_normal((n, 120))
+    M = np.asfortranarray(B @ B.T / 120)
+    xs = np.where(rng.uniform(size=n) < 0.3, rng.uniform(0.5, 1.0, n), 0.0)
+    ys = np.where(xs > 0, 0.0, rng.uniform(0.5, 1.0, n))
+    q = ys - M @ xs
+    x = cad.fischer_newton(M, q, tol=1e-12, max_iter=200)
+    y = M @ x + q
+    s = np.abs(q).max()
+    assert x.min() >= -1e-10 * s and y.min() >= -1e-10 * s
+    assert np.abs(x * y).max() <= 1e-10 * s * max(1.0, np.abs(x).max())
