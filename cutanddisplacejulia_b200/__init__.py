@@ -9,8 +9,8 @@ orders and error messages); julia/CutAndDisplaceB200.jl is the Julia one.
 """
 from ._lib import CadError, context, load  # noqa: F401
 from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTractions3D,  # noqa: F401
-                       KnockOutFixedRows, SetupTractionVector, SlipCalculator3D, SlipCalculator3D_batched, fischer_newton,
-                       solve)
+                       FrictionSolver, KnockOutFixedRows, SetupTractionVector, SlipCalculator3D,
+                       SlipCalculator3D_batched, fischer_newton, solve)
 from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint, HookesLaw3DStrain2Stress,  # noqa: F401
                        CreateP1P2P3, ElasticConstantsCheck)
 from .structs import (DispInf, Disps, FrictionParameters, MixedBoundaryConditions,  # noqa: F401

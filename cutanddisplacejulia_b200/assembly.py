@@ -182,6 +182,43 @@ def SlipCalculator3D_friction(P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector
     return Dn, Dss, Dds
 
 
+class FrictionSolver:
+    """Frictional slip for many loads on one geometry: the set-up of
+    src/SlipCalculator3D.jl:56-61 and :90-175 (A assembled, C = inv(A Scl)
+    kept on the GPU) once, then `solve` per load (:177-238).  One prepared
+    system per device context: preparing another, calling
+    SlipCalculator3D_friction or fischer_newton on the same device replaces
+    it (solve then raises)."""
+
+    def __init__(self, P1, P2, P3, nu, G, lam, MidPoint, FaceNormalVector, HSFlag, device=0):
+        P1, P2, P3 = _tri(P1), _tri(P2), _tri(P3)
+        self.N = P1.shape[0]
+        self.nrm = _tri(FaceNormalVector)
+        self.G, self.lam = float(G), float(lam)
+        mid = _tri(MidPoint)
+        self.ctx = _lib.context(device)
+        rc = _lib.load().cad_friction_prepare(self.ctx, P1.ctypes.data, P2.ctypes.data, P3.ctypes.data, self.N,
+                                              float(nu), float(G), float(lam), mid.ctypes.data,
+                                              self.nrm.ctypes.data, int(HSFlag))
+        _lib.check(rc, self.ctx)
+
+    def solve(self, BoundaryConditions, tol=1e-10, max_iter=100):
+        """(Dn, Dss, Dds) for MixedBoundaryConditionsFriction boundary
+        conditions (no early exit here: the reference's prepared solve has
+        none)."""
+        N = self.N
+        fp = BoundaryConditions.FrictionParameters
+        Tn, Tds, Tss = SetupTractionVector(BoundaryConditions.MixedBoundaryConditions, self.nrm, N, self.G, self.lam)
+        Tn, Tss, Tds = _col(Tn, N), _col(Tss, N), _col(Tds, N)
+        mu, Sf = _col(fp.mu, N), _col(fp.Sf, N)
+        Dn, Dss, Dds = np.zeros(N), np.zeros(N), np.zeros(N)
+        rc = _lib.load().cad_friction_solve(self.ctx, N, Tn.ctypes.data, Tss.ctypes.data, Tds.ctypes.data,
+                                            mu.ctypes.data, Sf.ctypes.data, float(tol), int(max_iter),
+                                            Dn.ctypes.data, Dss.ctypes.data, Dds.ctypes.data)
+        _lib.check(rc, self.ctx)
+        return Dn, Dss, Dds
+
+
 def fischer_newton(A, b, device=0, tol=1e-10, max_iter=100):
     """x solving the linear complementarity problem x >= 0, A x + b >= 0,
     x'(A x + b) = 0 -- the FischerNewton.fischer_newton(A, b) call of

@@ -95,6 +95,9 @@ struct cad_ctx {
     double near_factor = 3.0;
     double tol = 1e-10;
     int max_iter = 200;
+    bool fric_ready = false;      // cad_friction_prepare: C = inv(A Scl) of fric_N elements in S_LCPC
+    int64_t fric_N = 0;
+    double fric_scl = 0.0;
     int last_iters = 0;           // of the last mixed solve (all right-hand sides)
     double last_relres = 0.0;     // largest over its right-hand sides
     std::string err;
@@ -1559,6 +1562,7 @@ int cad_fischer_newton(cad_ctx* ctx, int64_t n, const double* A, const double* b
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
     if (n == 0) return CAD_OK;
     void *Mv, *pv;
+    ctx->fric_ready = false;   // the dense matrix takes the prepared frictional system's place
     if (int r = ensure(ctx, S_LCPC, (size_t)n * n * sizeof(double), &Mv)) return r;
     if (int r = ensure(ctx, S_LCPP, (size_t)3 * n * sizeof(double), &pv)) return r;
     double* P = (double*)pv;
@@ -1577,6 +1581,117 @@ int cad_fischer_newton(cad_ctx* ctx, int64_t n, const double* A, const double* b
     return lcp_status(ctx, iters, rel, tol);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The set-up half of the frictional solve (src/SlipCalculator3D.jl:56-61 and
+// :90-92): A assembled as the plain path does, Scl = mean(HalfPerimeter) / G
+// (AreaOfTriangle3D), C = inv(A Scl) from the FP64 LU solved against the
+// identity, kept in the context for friction_solve_device.
+int friction_prepare_device(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                            double G, double lambda, const double* midpoints, const double* normals, int hs_flag)
+{
+    ctx->fric_ready = false;
+    double hp = 0.0;
+    for (int64_t i = 0; i < N; ++i) {
+        double e[3];
+        const double* V[4] = {P1, P2, P3, P1};
+        for (int k = 0; k < 3; ++k) {
+            const double dx = V[k][i] - V[k + 1][i], dy = V[k][i + N] - V[k + 1][i + N],
+                         dz = V[k][i + 2 * N] - V[k + 1][i + 2 * N];
+            e[k] = std::sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        hp += (e[0] + e[1] + e[2]) / 2.0;
+    }
+    const double scl = (hp / (double)N) / G;
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    const int64_t n3 = 3 * N;
+    void *A, *Cv;
+    if (int r = ensure(ctx, S_A, (size_t)n3 * n3 * sizeof(double), &A)) return r;
+    if (int r = ensure(ctx, S_LCPC, (size_t)n3 * n3 * sizeof(double), &Cv)) return r;
+    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
+                            nullptr, (double*)A, n3);
+    if (r) return r;
+    double* C = (double*)Cv;
+    CK(scale_and_identity((double*)A, n3, n3, scl, C, ctx->stream, &ctx->launches));
+    const int solver = ctx->solver;
+    ctx->solver = CAD_SOLVER_LU64;
+    r = solve_device(ctx, n3, (double*)A, n3, C, n3, n3);
+    int info = 0;
+    if (r == CAD_OK) r = read_info(ctx, &info);
+    ctx->solver = solver;
+    if (r) return r;
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    ctx->fric_ready = true;
+    ctx->fric_N = N;
+    ctx->fric_scl = scl;
+    return CAD_OK;
+}
+
+// The solve half (src/SlipCalculator3D.jl:90-175 for q, :177-237 for the
+// solve and the read-out) with the prepared C: q = [C (b - [0; Sf; Sf]); 2 Sf;
+// 2 Sf], the LCP by the Fischer-Burmeister Newton method, slip from x and y.
+int friction_solve_device(cad_ctx* ctx, const double* Tn, const double* Tss, const double* Tds, const double* mu,
+                          const double* Sf, double tol, int max_iter, double* Dn, double* Dss, double* Dds)
+{
+    const int64_t N = ctx->fric_N, n3 = 3 * N, n5 = 5 * N;
+    const double scl = ctx->fric_scl;
+    double* C = (double*)ctx->buf[S_LCPC].p;
+    void* pv;
+    if (int r = ensure(ctx, S_LCPP, ((size_t)2 * N + n3 + n3 + 3 * n5) * sizeof(double), &pv)) return r;
+    double* P = (double*)pv;
+    double *dmu = P, *dsf = P + N, *b = P + 2 * N, *rr = b + n3, *q = rr + n3, *xd = q + n5, *y = xd + n5;
+    double* slip = rr;   // r is dead once q is formed
+    if (int r = upload(ctx, dmu, mu, N)) return r;
+    if (int r = upload(ctx, dsf, Sf, N)) return r;
+    if (int r = upload(ctx, b, Tn, N)) return r;
+    if (int r = upload(ctx, b + N, Tss, N)) return r;
+    if (int r = upload(ctx, b + 2 * N, Tds, N)) return r;
+    // q = [C (b - [0; Sf; Sf]); 2 Sf; 2 Sf] (src/SlipCalculator3D.jl:158-163, :190-193)
+    CK(friction_rhs(b, dsf, N, rr, q, ctx->stream, &ctx->launches));
+    const double one = 1.0, zero = 0.0;
+    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)n3, (int)n3, &one, C, (int)n3, rr, 1, &zero, q, 1) !=
+            CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, CAD_ERR_CUDA, "friction right-hand side: cuBLAS error");
+    LcpOperator op;
+    op.friction = true;
+    op.n = n5;
+    op.C = C;
+    op.ldc = n3;
+    op.mu = dmu;
+    op.m = N;
+    int iters = 0;
+    double rel = 0.0;
+    if (int r = lcp_newton_device(ctx, op, q, xd, y, tol, max_iter, &iters, &rel)) return r;
+    CK(friction_slip(xd, y, N, scl, slip, ctx->stream, &ctx->launches));
+    CK(cudaMemcpyAsync(Dn, slip, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dss, slip + N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Dds, slip + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return lcp_status(ctx, iters, rel, tol);
+}
+
+bool friction_geometry_args_ok(int64_t N, int hs_flag, double G, const double* P1, const double* P2,
+                               const double* P3, const double* midpoints, const double* normals)
+{
+    return N >= 0 && !bad_flag(hs_flag) && G != 0.0 && 5 * N <= INT32_MAX &&
+           (N == 0 || (P1 && P2 && P3 && midpoints && normals));
+}
+
+bool friction_load_args_ok(int64_t N, double tol, int max_iter, const double* Tn, const double* Tss,
+                           const double* Tds, const double* mu, const double* Sf, const double* Dn, const double* Dss,
+                           const double* Dds)
+{
+    return tol > 0.0 && max_iter >= 0 && (N == 0 || (Tn && Tss && Tds && mu && Sf && Dn && Dss && Dds));
+}
+
+}  // namespace
+
+extern "C" {
+
 int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N,
                                  double nu, double G, double lambda, const double* midpoints, const double* normals,
                                  int hs_flag, const double* Tn, const double* Tss, const double* Tds,
@@ -1584,10 +1699,8 @@ int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P
                                  double* Dss, double* Dds)
 {
     if (int r = set_device(ctx)) return r;
-    if (N < 0 || bad_flag(hs_flag) || !(tol > 0.0) || max_iter < 0 || !(G != 0.0) ||
-        (N > 0 && (!P1 || !P2 || !P3 || !midpoints || !normals || !Tn || !Tss || !Tds || !mu || !Sf || !Dn ||
-                   !Dss || !Dds)) ||
-        5 * N > INT32_MAX)
+    if (!friction_geometry_args_ok(N, hs_flag, G, P1, P2, P3, midpoints, normals) ||
+        !friction_load_args_ok(N, tol, max_iter, Tn, Tss, Tds, mu, Sf, Dn, Dss, Dds))
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
@@ -1606,73 +1719,35 @@ int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P
         std::fill(Dds, Dds + N, 0.0);
         return CAD_OK;
     }
-    // Scl = mean(HalfPerimeter) / G (src/SlipCalculator3D.jl:58-59, AreaOfTriangle3D)
-    double hp = 0.0;
-    for (int64_t i = 0; i < N; ++i) {
-        double e[3];
-        const double* V[4] = {P1, P2, P3, P1};
-        for (int k = 0; k < 3; ++k) {
-            const double dx = V[k][i] - V[k + 1][i], dy = V[k][i + N] - V[k + 1][i + N],
-                         dz = V[k][i + 2 * N] - V[k + 1][i + 2 * N];
-            e[k] = std::sqrt(dx * dx + dy * dy + dz * dz);
-        }
-        hp += (e[0] + e[1] + e[2]) / 2.0;
-    }
-    const double scl = (hp / (double)N) / G;
-    double* g;
-    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
-    const int64_t n3 = 3 * N, n5 = 5 * N;
-    void *A, *Cv, *pv;
-    if (int r = ensure(ctx, S_A, (size_t)n3 * n3 * sizeof(double), &A)) return r;
-    if (int r = ensure(ctx, S_LCPC, (size_t)n3 * n3 * sizeof(double), &Cv)) return r;
-    if (int r = ensure(ctx, S_LCPP, ((size_t)2 * N + n3 + n3 + 3 * n5) * sizeof(double), &pv)) return r;
-    double* P = (double*)pv;
-    double *dmu = P, *dsf = P + N, *b = P + 2 * N, *rr = b + n3, *q = rr + n3, *xd = q + n5, *y = xd + n5;
-    double* slip = rr;   // r is dead once q is formed
-    if (int r = upload(ctx, dmu, mu, N)) return r;
-    if (int r = upload(ctx, dsf, Sf, N)) return r;
-    if (int r = upload(ctx, b, Tn, N)) return r;
-    if (int r = upload(ctx, b + N, Tss, N)) return r;
-    if (int r = upload(ctx, b + 2 * N, Tds, N)) return r;
-    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
-                            nullptr, (double*)A, n3);
-    if (r) return r;
-    // C = inv(A Scl): the FP64 LU of A Scl solved against the identity
-    double* C = (double*)Cv;
-    CK(scale_and_identity((double*)A, n3, n3, scl, C, ctx->stream, &ctx->launches));
-    {
-        const int solver = ctx->solver;
-        ctx->solver = CAD_SOLVER_LU64;
-        r = solve_device(ctx, n3, (double*)A, n3, C, n3, n3);
-        int info = 0;
-        if (r == CAD_OK) r = read_info(ctx, &info);
-        ctx->solver = solver;
-        if (r) return r;
-        if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
-    }
-    // q = [C (b - [0; Sf; Sf]); 2 Sf; 2 Sf] (src/SlipCalculator3D.jl:158-163, :190-193)
-    CK(friction_rhs(b, dsf, N, rr, q, ctx->stream, &ctx->launches));
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)n3, (int)n3, &one, C, (int)n3, rr, 1, &zero, q, 1) !=
-            CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "friction right-hand side: cuBLAS error");
-    LcpOperator op;
-    op.friction = true;
-    op.n = n5;
-    op.C = C;
-    op.ldc = n3;
-    op.mu = dmu;
-    op.m = N;
-    int iters = 0;
-    double rel = 0.0;
-    if ((r = lcp_newton_device(ctx, op, q, xd, y, tol, max_iter, &iters, &rel))) return r;
-    CK(friction_slip(xd, y, N, scl, slip, ctx->stream, &ctx->launches));
-    CK(cudaMemcpyAsync(Dn, slip, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(Dss, slip + N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(Dds, slip + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    return lcp_status(ctx, iters, rel, tol);
+    if (int r = friction_prepare_device(ctx, P1, P2, P3, N, nu, G, lambda, midpoints, normals, hs_flag)) return r;
+    return friction_solve_device(ctx, Tn, Tss, Tds, mu, Sf, tol, max_iter, Dn, Dss, Dds);
+}
+
+int cad_friction_prepare(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                         double G, double lambda, const double* midpoints, const double* normals, int hs_flag)
+{
+    if (int r = set_device(ctx)) return r;
+    if (!friction_geometry_args_ok(N, hs_flag, G, P1, P2, P3, midpoints, normals))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->fric_ready = false;
+    if (N == 0) return CAD_OK;
+    return friction_prepare_device(ctx, P1, P2, P3, N, nu, G, lambda, midpoints, normals, hs_flag);
+}
+
+int cad_friction_solve(cad_ctx* ctx, int64_t N, const double* Tn, const double* Tss, const double* Tds,
+                       const double* mu, const double* Sf, double tol, int max_iter, double* Dn, double* Dss,
+                       double* Dds)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || !friction_load_args_ok(N, tol, max_iter, Tn, Tss, Tds, mu, Sf, Dn, Dss, Dds))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->last_iters = 0;
+    ctx->last_relres = 0.0;
+    if (N == 0) return CAD_OK;
+    if (!ctx->fric_ready || ctx->fric_N != N)
+        return fail(ctx, CAD_ERR_ARG, "cad_friction_solve: no prepared frictional system of this size "
+                                      "(call cad_friction_prepare first)");
+    return friction_solve_device(ctx, Tn, Tss, Tds, mu, Sf, tol, max_iter, Dn, Dss, Dds);
 }
 
 }  // extern "C"

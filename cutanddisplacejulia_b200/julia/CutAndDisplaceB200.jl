@@ -165,6 +165,26 @@ function SlipCalculator3D_friction(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVe
     return Dn, Dss, Dds
 end
 
+# Prepared frictional system (src/SlipCalculator3D.jl:90-175 once, :177-238 per
+# load): friction_prepare keeps C = inv(A Scl) on the GPU, friction_solve runs
+# one load on it (no early exit, as in the reference's prepared overloads).
+friction_prepare(P1, P2, P3, ν, G, λ, MidPoint, FaceNormalVector, HSFlag) =
+    check(ccall((:cad_friction_prepare, libcad), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int64, Float64, Float64, Float64, Ptr{Float64},
+         Ptr{Float64}, Cint),
+        ctx(), f64(P1), f64(P2), f64(P3), size(P1, 1), ν, G, λ, f64(MidPoint), f64(FaceNormalVector), HSFlag))
+
+function friction_solve(Tn, Tss, Tds, μ, Sf; tol::Real=1e-10, max_iter::Integer=100)
+    n = length(Tn)
+    Dn = zeros(n); Dss = zeros(n); Dds = zeros(n)
+    check(ccall((:cad_friction_solve, libcad), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Float64, Cint,
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        ctx(), n, f64(vec(Tn)), f64(vec(Tss)), f64(vec(Tds)), zeros(n) .+ μ, zeros(n) .+ Sf, tol, max_iter,
+        Dn, Dss, Dds))
+    return Dn, Dss, Dds
+end
+
 # The LCP x ≥ 0, A x + b ≥ 0, x'(A x + b) = 0 (FischerNewton.fischer_newton(A, b)).
 function fischer_newton(A, b; tol::Real=1e-10, max_iter::Integer=100)
     n = length(b)

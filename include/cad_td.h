@@ -201,6 +201,22 @@ int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P
                                  const double* mu, const double* Sf, double tol, int max_iter, double* Dn,
                                  double* Dss, double* Dds);
 
+/* The two halves of cad_slip_calculator_friction, for many loads on one
+ * geometry (the reference prepares the LCP once, src/SlipCalculator3D.jl:90-175,
+ * and solves it per load, :177-238, as its fluid-volume search does).
+ * cad_friction_prepare assembles A and keeps C = inv(A Scl) in the context;
+ * cad_friction_solve solves the LCP for one set of element tractions and
+ * friction parameters with it (no early exit: the caller decides, as the
+ * reference's prepared overloads do).  The prepared system stays valid until
+ * the next cad_friction_prepare, cad_slip_calculator_friction or
+ * cad_fischer_newton call on the context; cad_friction_solve returns
+ * CAD_ERR_ARG when there is none of N elements. */
+int cad_friction_prepare(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                         double G, double lambda, const double* midpoints, const double* normals, int hs_flag);
+int cad_friction_solve(cad_ctx* ctx, int64_t N, const double* Tn, const double* Tss, const double* Tds,
+                       const double* mu, const double* Sf, double tol, int max_iter, double* Dn, double* Dss,
+                       double* Dds);
+
 /* Linear complementarity problem x >= 0, y = A x + b >= 0, x'y = 0 for a dense
  * A (n x n, column-major) and b (n): the call FischerNewton.fischer_newton(A, b)
  * makes at src/SlipCalculator3D.jl:196, solved by the same Fischer-Burmeister

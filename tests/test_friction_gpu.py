@@ -155,3 +155,31 @@ def test_fischer_newton_rank_deficient_complementarity(cad):
     s = np.abs(q).max()
     assert x.min() >= -1e-10 * s and y.min() >= -1e-10 * s
     assert np.abs(x * y).max() <= 1e-10 * s * max(1.0, np.abs(x).max())
+
+
+def test_prepared_friction_solver_many_loads(cad):
+    """One prepared system (C = inv(A Scl) kept on the GPU), three loads: each
+    equals the one-shot frictional solve of the same load (the same device
+    code path; 1e-12 norm-wise leaves room for a captured replay of the
+    factorisation picking other library kernels than its eager first run);
+    solving after the prepared system was replaced raises."""
+    c = burgmann_case(1)
+    args = (c["P1"], c["P2"], c["P3"], c["nu"], c["G"], c["lam"], c["mid"], c["nrm"], 0)
+    S = c["S"]
+    loads = []
+    for k, (syy, sxy, mu) in enumerate(((-0.05, 1.0, 0.0), (-0.1, 0.7, 0.2), (-0.2, -1.2, 0.4))):
+        sig = (0.0, syy * S, 0.0, sxy * S, 0.0, 0.0)
+        loads.append(cad.MixedBoundaryConditionsFriction(
+            cad.MixedBoundaryConditions(cad.Stresses(*sig), cad.Tractions(0.0, 0.0, 0.0)),
+            cad.FrictionParameters(mu, c["Sf"] * (1 + k))))
+    solver = cad.FrictionSolver(*args)
+    prepared = [solver.solve(bc) for bc in loads]
+    for bc, got in zip(loads, prepared):
+        ref = np.concatenate(cad.SlipCalculator3D(*args, bc, None))
+        assert np.linalg.norm(np.concatenate(got) - ref) <= 1e-12 * np.linalg.norm(ref)
+    assert np.abs(prepared[1][1]).max() > 0
+    M = np.asfortranarray(np.eye(4) + 0.1)
+    cad.fischer_newton(M, -np.ones(4))   # replaces the prepared system on this device
+    with pytest.raises(cad.CadError) as e:
+        solver.solve(loads[0])
+    assert e.value.code == cad._lib.CAD_ERR_ARG
