@@ -37,6 +37,7 @@ EXPORTS = [
     "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
     "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
     "cad_slip_calculator_friction", "cad_fischer_newton", "cad_friction_prepare", "cad_friction_solve",
+    "cad_assemble_columns_dev",
 ]
 
 
@@ -105,6 +106,7 @@ def load():
     L.cad_td_sum_eval_noalloc.argtypes = [P, P, P, P, I64, P, P, P, I64, P, P, P, D, INT, INT, INT, P, P]
     L.cad_slip_calculator_friction.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, D, INT, P, P, P]
     L.cad_fischer_newton.argtypes = [P, I64, P, P, D, INT, P]
+    L.cad_assemble_columns_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, I64, I64, P, I64]
     L.cad_friction_prepare.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT]
     L.cad_friction_solve.argtypes = [P, I64, P, P, P, P, P, D, INT, P, P, P]
     _lib = L

@@ -1202,6 +1202,41 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
     return assemble_device(ctx, normals, midpoints, P1, P2, P3, N, nu, G, lambda, hs_flag, OUT_AMAT, nullptr, A, lda);
 }
 
+int cad_assemble_columns_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                             const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                             int hs_flag, int64_t j0, int64_t j1, double* A_block, int64_t lda)
+{
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || bad_flag(hs_flag) || j0 < 0 || j1 < j0 || j1 > N || lda < 3 * N || (j1 > j0 && !A_block))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    const int64_t nb = j1 - j0;
+    void *obs, *dirs, *tri;
+    if (int r = ensure(ctx, S_OBS, (size_t)3 * N * sizeof(double), &obs)) return r;
+    if (int r = ensure(ctx, S_DIRS, (size_t)9 * N * sizeof(double), &dirs)) return r;
+    double* X = (double*)obs;
+    ++ctx->launches;
+    CK(launch_colloc(normals, midpoints, N, X, X + N, X + 2 * N, (double*)dirs, ctx->stream));
+    if (hs_flag == 1 && N > 0)
+        if (int r = hs_check(ctx, X + 2 * N, N, P1, P2, P3, N)) return r;
+    if (nb == 0) return CAD_OK;
+    // every triangle record (one thread each, cheap); the pair kernel reads the block's
+    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    ++ctx->launches;
+    CK(launch_td_setup(P1, P2, P3, N, nullptr, nullptr, nullptr, 1, nu, hs_flag == 1, (TriDev*)tri, ctx->stream));
+    PairArgs a{};
+    a.X = X; a.Y = X + N; a.Z = X + 2 * N; a.M = N;
+    a.tri = (const TriDev*)tri + j0; a.N = nb;
+    a.tri_chunk = pick_chunk(N, nb, false);
+    a.lambda = lambda; a.G = G; a.dirs = (const double*)dirs;
+    a.A = A_block; a.lda = lda;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    ++ctx->launches;
+    CK(launch_td_pairs(a, OUT_AMAT, hs_flag == 1, true, false, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->timed[0] = true;
+    return CAD_OK;
+}
+
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
 {
     if (int r = set_device(ctx)) return r;

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
                     } else {
 #pragma unroll
                         for (int r = 0; r < 3; ++r)
-                            a.A[(int64_t)(r * NS + io) + a.lda * (int64_t)(m * NS + jt)] = -tr[r];
+                            a.A[(int64_t)(r * MD + io) + a.lda * (int64_t)(m * NS + jt)] = -tr[r];
                     }
                 }
             }

@@ -27,7 +27,8 @@ struct PairArgs {
     double* disp;        // OUT_INF: 9 x M x N
     double* partial;     // OUT_SUM: nchunk x 9 x M
     double* trac;        // OUT_TRAC: 9 x M x N
-    double* A;           // OUT_AMAT: 3N x 3N column-major, leading dimension lda
+    double* A;           // OUT_AMAT: 3M x 3N column-major, leading dimension lda (row r*M + i,
+                         // column m*N + j; a column block of a system when N < M)
     int64_t lda;
     const double* dirs;  // OUT_TRAC / OUT_AMAT: 9 x M (normal, strike, dip of each observed element)
     // mixed-precision assembly (OUT_AMAT): FP32 records of the triangles, and

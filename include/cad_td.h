@@ -256,6 +256,15 @@ int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* m
                             int hs_flag, const int64_t* changed, int64_t k, double* A, int64_t lda);
 /* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
  * (n x nrhs, ldb) by the solution. */
+/* A column block of the system matrix of cad_assemble_dev: the columns of
+ * elements j0 .. j1-1 (all 3N rows), for sharding the assembly across GPUs
+ * with no exchange (the reference fills whole columns per thread,
+ * src/CalculateInfluenceMatrices3D.jl:84-112).  A_block (3N x 3(j1-j0), lda
+ * >= 3N) holds the Dn columns of the block, then its Dss columns, then its
+ * Dds columns, each as in A = -[Atn;Atss;Atds]. */
+int cad_assemble_columns_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
+                             const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
+                             int hs_flag, int64_t j0, int64_t j1, double* A_block, int64_t lda);
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
 
 /* ---------------------------------------------- learned preconditioner ---
