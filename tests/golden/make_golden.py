@@ -9,6 +9,8 @@ GPU machines); the resulting .npz files are what the tests read.
                    test/test_TDvsMogi.jl:6-20 builds it; also holds FixedEls
   blade500.npz     test/BladeFaultShort_500Tris_Vertical_NorthDip_0.5.ts (GoCadAsciiReader), as read;
                    test/test_TDvsBurgmannLinearFrictionCrack.jl flattens and scales it itself
+  valley1000.npz   test/ValleySurface_ProperEq_1000Faces.ts (GoCadAsciiReader), as read
+                   (test/test_TDvsSavageGravityValley.jl)
 
 Each file holds P1, P2, P3 (N x 3 float64), built as CreateP1P2P3 does
 (src/CreateP1P2P3.jl): vertex k of triangle i is the point whose index the
@@ -89,6 +91,10 @@ def main(ref):
     P1, P2, P3 = p1p2p3(pts, tris)
     np.savez_compressed(os.path.join(HERE, "blade500.npz"), P1=P1, P2=P2, P3=P3)
     print("wrote blade500.npz (%d tris)" % len(tris))
+    pts, tris = read_gocad_ts(os.path.join(test_dir, "ValleySurface_ProperEq_1000Faces.ts"))
+    P1, P2, P3 = p1p2p3(pts, tris)
+    np.savez_compressed(os.path.join(HERE, "valley1000.npz"), P1=P1, P2=P2, P3=P3)
+    print("wrote valley1000.npz (%d tris)" % len(tris))
 
 
 if __name__ == "__main__":

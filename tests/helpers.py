@@ -169,3 +169,47 @@ def random_lcp(rng, n, frac_active=0.5, frac_degenerate=0.0):
     y = np.where(act | deg, 0.0, rng.uniform(0.5, 2.0, n))
     q = y - M @ x
     return np.asfortranarray(M), q, x
+
+
+def savage_valley_case():
+    """test/test_TDvsSavageGravityValley.jl: the 1019-triangle valley surface
+    in full space under gravitational stress (density x g = 1, no tectonic
+    stress, nu = 0.25, G = 1), observed on the 50 x 46 grid of the Savage
+    (1984) solution mapped under the valley (a = 2, b = -1), shifted to the
+    valley centre x = 50."""
+    from oracle.geometry import elastic_constants, face_normal_and_midpoint
+    from oracle.savage84 import savage1984_gravity_valley_stress
+    P1, P2, P3 = load_mesh("valley1000")
+    nrm, mid = face_normal_and_midpoint(P1, P2, P3)
+    _, _, lam, nu, G = elastic_constants(1.0, 0.25)
+    rg = 1.0
+    sxx = (nu / (1 - nu)) * rg * mid[:, 2]
+    szz = rg * mid[:, 2]
+    syy = nu * (sxx + szz)
+    z = np.zeros(len(P1))
+    u, v = np.meshgrid(np.linspace(0, 4, 50), np.linspace(-0.3265, -4, 46))
+    Sxx, Syy, Sxy, Xo, Yo = savage1984_gravity_valley_stress(0.0, rg, nu, 2.0, -1.0, u, v)
+    X = Xo.ravel(order="F") + 50
+    Z = Yo.ravel(order="F")
+    return dict(P1=P1, P2=P2, P3=P3, nrm=nrm, mid=mid, lam=lam, nu=nu, G=G, rg=rg,
+                sig=(sxx, syy, szz, z, z, z), X=X, Y=np.zeros_like(X), Z=Z,
+                an=(Sxx.ravel(order="F"), Syy.ravel(order="F"), Sxy.ravel(order="F")))
+
+
+def savage_valley_check(case, strain6):
+    """The reference's acceptance: gravity added back to the TD stresses,
+    the signed mean residual of sxx, szz and sxz against Savage (NaNs
+    dropped) each at most 0.15.  Returns the three means."""
+    exx, eyy, ezz, exy, exz, eyz = strain6
+    lam, G, nu, rg, Z = case["lam"], case["G"], case["nu"], case["rg"], case["Z"]
+    tr = exx + eyy + ezz
+    sxx = (nu / (1 - nu)) * rg * Z + 2 * G * exx + lam * tr
+    szz = rg * Z + 2 * G * ezz + lam * tr
+    sxz = 2 * G * exz
+    Sxx, Syy, Sxy = case["an"]
+    means = []
+    for num, an in ((sxx, Sxx), (szz, Syy), (sxz, Sxy)):
+        r = num - an
+        means.append(float(np.mean(r[~np.isnan(r)])))
+    assert not any(p > 0.15 for p in means), means
+    return means

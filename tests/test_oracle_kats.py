@@ -4,6 +4,7 @@
   traction-free crack, 5 orientations      test/test_TractionFreeSurface.jl (<= 1e-8)
   Eshelby penny crack slip                 test/test_TDvsEshelbyPennyCrack.jl (<= 11 %)
   Mogi cavity with fixed elements          test/test_TDvsMogi.jl (spread <= 0.05, <= 20 %)
+  Savage (1984) gravitational valley       test/test_TDvsSavageGravityValley.jl (mean residual <= 0.15)
 plus self-consistency of the oracle (influence matrices + TD_sum == summing
 overload; strain == symmetric gradient of displacement at depth, FS and HS).
 """
@@ -12,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import GOLDEN, load_mesh, okada_case
+from helpers import GOLDEN, load_mesh, okada_case, savage_valley_case, savage_valley_check
 
 
 def test_okada_kat(oracle):
@@ -162,3 +163,17 @@ def test_mogi_kat(oracle):
             pct = 100.0 / a * u
             pct[np.isinf(pct)] = np.nan
             assert not np.any(np.abs(pct - 100) > 20)
+
+
+def test_savage_valley_kat(oracle):
+    c = savage_valley_case()
+    n = len(c["P1"])
+    assert n == 1019
+    Tn, Tds, Tss = oracle.normal_and_shear_tractions(*c["sig"], c["nrm"])
+    Dn, Dss, Dds, _, _ = oracle.slip_calculator(c["P1"], c["P2"], c["P3"], c["nu"], c["G"], c["lam"], c["mid"],
+                                                c["nrm"], 0, Tn, Tss, Tds)
+    S, _ = oracle.td_sum_eval(c["X"], c["Y"], c["Z"], c["P1"], c["P2"], c["P3"], Dss, Dds, Dn, c["nu"], c["G"], 1,
+                              1, 0)
+    means = savage_valley_check(c, S)
+    # the oracle's residuals (about -0.040, -0.028, 0.002) are well inside the bound on both sides
+    assert max(abs(m) for m in means) < 0.06

@@ -221,3 +221,23 @@ def test_repeated_solves_same_size(cad, n):
         Xo = np.linalg.solve(A, B)
         cond = np.linalg.cond(A)
         assert np.max(np.abs(X - Xo)) <= 1e-14 * cond * np.max(np.abs(Xo)), rep
+
+
+def test_savage_valley_kat_on_gpu(cad, oracle):
+    """test/test_TDvsSavageGravityValley.jl through the GPU: the plain solve of
+    the valley surface under gravity, the summed strain at the Savage grid,
+    the reference's residual bound, and agreement with the oracle's run."""
+    from helpers import savage_valley_case, savage_valley_check
+    c = savage_valley_case()
+    Dn, Dss, Dds, _, _ = cad.SlipCalculator3D(c["P1"], c["P2"], c["P3"], c["nu"], c["G"], c["lam"], c["mid"],
+                                              c["nrm"], 0, cad.Stresses(*c["sig"]), np.zeros(len(c["P1"])))
+    S, _ = cad.TD(c["X"], c["Y"], c["Z"], c["P1"], c["P2"], c["P3"], Dss, Dds, Dn, c["nu"], c["G"], 1, 1, 0,
+                  cad.Strains(), cad.Disps())
+    means = savage_valley_check(c, np.stack(list(S)))
+    Tn, Tds, Tss = oracle.normal_and_shear_tractions(*c["sig"], c["nrm"])
+    Dno, Dsso, Ddso, _, _ = oracle.slip_calculator(c["P1"], c["P2"], c["P3"], c["nu"], c["G"], c["lam"], c["mid"],
+                                                   c["nrm"], 0, Tn, Tss, Tds)
+    So, _ = oracle.td_sum_eval(c["X"], c["Y"], c["Z"], c["P1"], c["P2"], c["P3"], Dsso, Ddso, Dno, c["nu"], c["G"],
+                               1, 1, 0)
+    means_o = savage_valley_check(c, So)
+    assert np.allclose(means, means_o, rtol=0, atol=1e-8)
