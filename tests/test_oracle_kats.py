@@ -177,3 +177,26 @@ def test_savage_valley_kat(oracle):
     means = savage_valley_check(c, S)
     # the oracle's residuals (about -0.040, -0.028, 0.002) are well inside the bound on both sides
     assert max(abs(m) for m in means) < 0.06
+
+
+def test_oracle_independent_of_thread_count(oracle):
+    """Determinism of the oracle: influence matrices, the traction assembly and
+    the summing overload give the same bits on 1 and 4 threads."""
+    rng = np.random.default_rng(11)
+    from helpers import random_points, random_triangles
+    P1, P2, P3 = random_triangles(rng, 23)
+    pts = random_points(rng, 150)
+    sl = rng.uniform(-1, 1, (3, 23))
+    for hs in (0, 1):
+        a = oracle.td_inf(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, 1, 1, hs, nthreads=1)
+        b = oracle.td_inf(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, 1, 1, hs, nthreads=4)
+        assert all(np.array_equal(x, y, equal_nan=True) for x, y in zip(a, b))
+        a = oracle.td_sum_eval(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, 1, 1, hs, nthreads=1)
+        b = oracle.td_sum_eval(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, 1, 1, hs, nthreads=4)
+        assert all(np.array_equal(x, y, equal_nan=True) for x, y in zip(a, b))
+    from oracle import geometry as g
+    P1, P2, P3 = load_mesh("circle581")
+    nrm, mid = g.face_normal_and_midpoint(P1, P2, P3)
+    A1 = oracle.influence_traction(nrm, mid, P1, P2, P3, 0.25, 1.0, 1.0, 0, nthreads=1, want_A=True)
+    A4 = oracle.influence_traction(nrm, mid, P1, P2, P3, 0.25, 1.0, 1.0, 0, nthreads=4, want_A=True)
+    assert np.array_equal(A1, A4)

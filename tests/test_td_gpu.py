@@ -241,3 +241,26 @@ def test_savage_valley_kat_on_gpu(cad, oracle):
                                1, 1, 0)
     means_o = savage_valley_check(c, So)
     assert np.allclose(means, means_o, rtol=0, atol=1e-8)
+
+
+def test_results_are_reproducible(cad):
+    """Run-to-run determinism: the summing evaluation (fixed-order partial
+    sums, no floating-point atomics) gives the same bits on repeated calls,
+    and so does the assembly + FP64 solve once its factorisation replays."""
+    from cutanddisplacejulia_b200 import workloads
+    rng = np.random.default_rng(21)
+    P1, P2, P3 = random_triangles(rng, 40)
+    pts = random_points(rng, 3000)
+    sl = rng.uniform(-1, 1, (3, 40))
+    runs = [cad.TD(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, 1, 1, 1, cad.Strains(), cad.Disps()) for _ in range(2)]
+    for a, b in zip(runs[0], runs[1]):
+        assert all(np.array_equal(x, y, equal_nan=True) for x, y in zip(a, b))
+    P1, P2, P3 = workloads.penny(seed=0, spacing=0.1)
+    nrm, mid = cad.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
+    n = len(P1)
+    bc = cad.Tractions(np.full(n, -1e-3), np.full(n, 2e-4), np.zeros(n))
+    sols = [np.concatenate(cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 0, bc, np.zeros(n))[:3])
+            for _ in range(3)]
+    assert np.array_equal(sols[1], sols[2])
+    assert np.linalg.norm(sols[0] - sols[1]) <= 1e-13 * np.linalg.norm(sols[1])
