@@ -13,8 +13,9 @@ from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTrac
                        SlipCalculator3D_batched, fischer_newton, solve)
 from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint, HookesLaw3DStrain2Stress,  # noqa: F401
                        CreateP1P2P3, ElasticConstantsCheck)
-from .structs import (DispInf, Disps, FrictionParameters, MixedBoundaryConditions,  # noqa: F401
-                      MixedBoundaryConditionsFriction, StrainInf, Strains, Stresses, TractionInf, Tractions)
+from .structs import (BulkModulus, DispInf, Disps, FrictionParameters, LamesConstant,  # noqa: F401
+                      MixedBoundaryConditions, MixedBoundaryConditionsFriction, PoissonsRatio, ShearModulus,
+                      StrainInf, Strains, Stresses, TractionInf, Tractions, YoungsModulus)
 from .td import TD, TD_sum  # noqa: F401
 
 __version__ = "1.0.0"

@@ -68,12 +68,54 @@ def AreaOfTriangle3D(P1, P2, P3):
     return np.sqrt(s * (s - a) * (s - b) * (s - c)), s
 
 
-def ElasticConstantsCheck(G, nu):
-    """(K, E, lambda, nu, G) from the shear modulus and Poisson's ratio."""
-    K = (2 * G * (1 + nu)) / (3 * (1 - 2 * nu))
-    E = 2 * G * (1 + nu)
-    lam = (2 * G * nu) / (1 - 2 * nu)
+def _elastic_from(vals):
+    """(K, E, lambda, nu, G) of an isotropic material from any two of them
+    (dict with two of the keys K, E, lam, nu, G), by the standard conversions."""
+    from math import sqrt
+    k = set(vals)
+    K, E, lam, nu, G = (vals.get(x) for x in ("K", "E", "lam", "nu", "G"))
+    if k == {"G", "nu"}:
+        K, E, lam = 2 * G * (1 + nu) / (3 * (1 - 2 * nu)), 2 * G * (1 + nu), 2 * G * nu / (1 - 2 * nu)
+    elif k == {"K", "E"}:
+        lam, nu, G = 3 * K * (3 * K - E) / (9 * K - E), (3 * K - E) / (6 * K), 3 * K * E / (9 * K - E)
+    elif k == {"K", "lam"}:
+        E, nu, G = 9 * K * (K - lam) / (3 * K - lam), lam / (3 * K - lam), 1.5 * (K - lam)
+    elif k == {"K", "nu"}:
+        E, lam, G = 3 * K * (1 - 2 * nu), 3 * K * nu / (1 + nu), 3 * K * (1 - 2 * nu) / (2 * (1 + nu))
+    elif k == {"K", "G"}:
+        E, lam, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / 3, (3 * K - 2 * G) / (6 * K + 2 * G)
+    elif k == {"E", "lam"}:
+        R = sqrt(E * E + 9 * lam * lam + 2 * E * lam)
+        K, nu, G = (E + 3 * lam + R) / 6, 2 * lam / (E + lam + R), (E - 3 * lam + R) / 4
+    elif k == {"E", "nu"}:
+        K, lam, G = E / (3 * (1 - 2 * nu)), E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+    elif k == {"E", "G"}:
+        K, lam, nu = E * G / (3 * (3 * G - E)), G * (E - 2 * G) / (3 * G - E), (E - 2 * G) / (2 * G)
+    elif k == {"lam", "nu"}:
+        K, E, G = lam * (1 + nu) / (3 * nu), lam * (1 + nu) * (1 - 2 * nu) / nu, lam * (1 - 2 * nu) / (2 * nu)
+    elif k == {"lam", "G"}:
+        K, E, nu = (3 * lam + 2 * G) / 3, G * (3 * lam + 2 * G) / (lam + G), lam / (2 * (lam + G))
+    else:
+        raise TypeError("ElasticConstantsCheck needs two different elastic constants")
     return K, E, lam, nu, G
+
+
+def ElasticConstantsCheck(a, b):
+    """(K, E, lambda, nu, G) from any two elastic constants
+    (src/ElasticConstantsCheck.jl): typed values (ShearModulus, PoissonsRatio,
+    BulkModulus, YoungsModulus, LamesConstant) in either order, or plain
+    numbers taken as (G, nu)."""
+    from .structs import BulkModulus, LamesConstant, PoissonsRatio, ShearModulus, YoungsModulus
+    typed = {ShearModulus: "G", PoissonsRatio: "nu", BulkModulus: "K", YoungsModulus: "E", LamesConstant: "lam"}
+    if type(a) in typed and type(b) in typed:
+        vals = {}
+        for x in (a, b):
+            key = typed[type(x)]
+            vals[key] = float(getattr(x, key))
+        if len(vals) != 2:
+            raise TypeError("ElasticConstantsCheck needs two different elastic constants")
+        return _elastic_from(vals)
+    return _elastic_from({"G": a, "nu": b})
 
 
 def read_stl(path):

@@ -120,3 +120,30 @@ class TractionInf(_Record):
 
 def empty_like_record(cls):
     return cls(*([np.empty(0)] * len(fields(cls))))
+
+
+# Elastic constants as typed values (src/CutAndDisplaceJulia.jl:33-37), so that
+# ElasticConstantsCheck can tell which two of them it was given.
+@dataclass
+class PoissonsRatio:
+    nu: float
+
+
+@dataclass
+class ShearModulus:
+    G: float
+
+
+@dataclass
+class BulkModulus:
+    K: float
+
+
+@dataclass
+class YoungsModulus:
+    E: float
+
+
+@dataclass
+class LamesConstant:
+    lam: float
