@@ -9,7 +9,7 @@ orders and error messages); julia/CutAndDisplaceB200.jl is the Julia one.
 """
 from ._lib import CadError, context, load  # noqa: F401
 from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTractions3D,  # noqa: F401
-                       FrictionSolver, KnockOutFixedRows, SetupTractionVector, SlipCalculator3D,
+                       FrictionSolver, KnockOutFixedRows, RemoveFixedElements3D, SetupTractionVector, SlipCalculator3D,
                        SlipCalculator3D_batched, fischer_newton, solve)
 from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint, HookesLaw3DStrain2Stress,  # noqa: F401
                        CreateP1P2P3, ElasticConstantsCheck)

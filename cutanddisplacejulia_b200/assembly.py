@@ -72,6 +72,15 @@ def KnockOutFixedRows(FixedEls, Tn, Tds, Tss):
     return Tn, Tds, Tss
 
 
+def RemoveFixedElements3D(FixedEls, Triangles, FaceNormalVector, MidPoint, P1, P2, P3):
+    """Drop the rows of fixed elements (FixedEls != 0) from the element arrays
+    (src/RemoveFixedElements3D.jl); FixedEls itself is returned unchanged, as
+    the reference does.  Triangles may be None."""
+    keep = np.asarray(FixedEls).reshape(-1) == 0
+    pick = (lambda a: None if a is None else np.asarray(a)[keep])
+    return (FixedEls, pick(Triangles), pick(FaceNormalVector), pick(MidPoint), pick(P1), pick(P2), pick(P3))
+
+
 def CalculateInfluenceMatrices3D(FaceNormalVector, MidPoint, P1, P2, P3, nu, G, lam, FixedEls, HSFlag, n,
                                  device=0):
     """Traction influence matrices (TractionInf of nine n x n arrays; with

@@ -1,7 +1,8 @@
-"""CPU test of ElasticConstantsCheck (src/ElasticConstantsCheck.jl) as the
-reference's test/test_ElasticConstantsCheck.jl runs it: G = 50, nu = 0.01
-passed through every pair of constants in turn must come back unchanged;
-and every pair, in either order, agrees with the (G, nu) conversion."""
+"""CPU tests of host utilities: ElasticConstantsCheck (src/ElasticConstantsCheck.jl)
+as the reference's test/test_ElasticConstantsCheck.jl runs it (G = 50, nu = 0.01
+passed through every pair of constants in turn must come back unchanged; every
+pair, in either order, agrees with the (G, nu) conversion), and
+RemoveFixedElements3D (src/RemoveFixedElements3D.jl)."""
 import itertools
 
 import numpy as np
@@ -30,3 +31,21 @@ def test_every_pair_either_order():
             cad.ShearModulus(G)]
     for a, b in itertools.permutations(vals, 2):
         assert np.allclose(cad.ElasticConstantsCheck(a, b), ref, rtol=1e-12, atol=0)
+
+
+def test_remove_fixed_elements():
+    """RemoveFixedElements3D (src/RemoveFixedElements3D.jl) on the Mogi mesh
+    with its 6 fixed elements: the other 46 rows remain, in order."""
+    import os
+
+    import cutanddisplacejulia_b200 as cad
+    from helpers import GOLDEN
+    d = np.load(os.path.join(GOLDEN, "mogi.npz"))
+    P1, P2, P3, fixed = d["P1"], d["P2"], d["P3"], d["FixedEls"]
+    nrm, mid = cad.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    tris = np.arange(3 * len(P1)).reshape(-1, 3)
+    F, T, N, M, Q1, Q2, Q3 = cad.RemoveFixedElements3D(fixed, tris, nrm, mid, P1, P2, P3)
+    keep = fixed == 0
+    assert F is fixed and len(Q1) == 46
+    for a, b in ((T, tris), (N, nrm), (M, mid), (Q1, P1), (Q2, P2), (Q3, P3)):
+        assert np.array_equal(a, np.asarray(b)[keep])
