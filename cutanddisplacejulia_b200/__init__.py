@@ -11,8 +11,10 @@ from ._lib import CadError, context, load  # noqa: F401
 from .assembly import (CalculateInfluenceMatrices3D, CalculateNormalAndShearTractions3D,  # noqa: F401
                        FrictionSolver, KnockOutFixedRows, RemoveFixedElements3D, SetupTractionVector, SlipCalculator3D,
                        SlipCalculator3D_batched, fischer_newton, solve)
-from .geometry import (AreaOfTriangle3D, CalculateSSandDSDirs, CreateFaceNormalAndMidPoint, HookesLaw3DStrain2Stress,  # noqa: F401
-                       CreateP1P2P3, ElasticConstantsCheck)
+from .geometry import (AreaOfTriangle3D, CalculateNormalTraction3D, CalculateSSandDSDirs,  # noqa: F401
+                       CalculateTractionInChosenDirection3D, CreateFaceNormalAndMidPoint, CreateP1P2P3,
+                       ElasticConstantsCheck, HookesLaw3DStrain2Stress, TensorTransformation3D,
+                       TractionVectorCartesianComponents3D)
 from .structs import (BulkModulus, DispInf, Disps, FrictionParameters, LamesConstant,  # noqa: F401
                       MixedBoundaryConditions, MixedBoundaryConditionsFriction, PoissonsRatio, ShearModulus,
                       StrainInf, Strains, Stresses, TractionInf, Tractions, YoungsModulus)

@@ -118,6 +118,54 @@ def ElasticConstantsCheck(a, b):
     return _elastic_from({"G": a, "nu": b})
 
 
+def _rows(c, like):
+    """Per-element cosines broadcast along the rows of `like` (element i on row i)."""
+    c = np.asarray(c, dtype=np.float64).reshape(-1)
+    like = np.asarray(like)
+    return c.reshape((-1,) + (1,) * (like.ndim - 1)) if like.ndim > 1 else c
+
+
+def CalculateNormalTraction3D(Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, CosAx, CosAy, CosAz):
+    """Normal traction n.sigma.n of each row's stress on that row's element
+    (src/CalculateNormalTraction3D.jl); stresses are vectors or matrices whose
+    row i belongs to element i."""
+    cx, cy, cz = (_rows(c, Pxx) for c in (CosAx, CosAy, CosAz))
+    return (Pxx * (cx * cx) + Pyy * (cy * cy) + Pzz * (cz * cz) + 2 * Pxy * (cx * cy) + 2 * Pyz * (cy * cz)
+            + 2 * Pxz * (cz * cx))
+
+
+def TractionVectorCartesianComponents3D(Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, CosAx, CosAy, CosAz):
+    """Traction vector sigma.n (Tx, Ty, Tz) (src/TractionVectorCartesianComponents3D.jl)."""
+    cx, cy, cz = (_rows(c, Pxx) for c in (CosAx, CosAy, CosAz))
+    return (Pxx * cx + Pxy * cy + Pxz * cz, Pxy * cx + Pyy * cy + Pyz * cz, Pxz * cx + Pyz * cy + Pzz * cz)
+
+
+def CalculateTractionInChosenDirection3D(Tx, Ty, Tz, CosAx, CosAy, CosAz, ChosenDirectionCos):
+    """Shear traction (I - n n^T) t projected on a direction in the element
+    plane (src/CalculateTractionInChosenDirection3D.jl); ChosenDirectionCos is
+    N x 3, one direction per element."""
+    cx, cy, cz = (_rows(c, Tx) for c in (CosAx, CosAy, CosAz))
+    D = np.asarray(ChosenDirectionCos, dtype=np.float64).reshape(-1, 3)
+    d1, d2, d3 = (_rows(D[:, k], Tx) for k in range(3))
+    a = (Tx * (1 - cx * cx) - Ty * (cx * cy) - Tz * (cz * cx)) * d1
+    b = (Tx * -(cx * cy) + Ty * (1 - cy * cy) - Tz * (cy * cz)) * d2
+    c = (Tx * -(cz * cx) - Ty * (cy * cz) + Tz * (1 - cz * cz)) * d3
+    return a + b + c
+
+
+def TensorTransformation3D(Txx1, Tyy1, Tzz1, Txy1, Txz1, Tyz1, A):
+    """Symmetric tensor in the frame whose axes are the rows of the 3 x 3
+    direction-cosine matrix A: T2 = A T1 A^T (src/TensorTransformation3D.jl)."""
+    A = np.asarray(A, dtype=np.float64).reshape(3, 3)
+
+    def comp(p, q):
+        ap, aq = A[p, :], A[q, :]
+        return (ap[0] * aq[0] * Txx1 + ap[1] * aq[1] * Tyy1 + ap[2] * aq[2] * Tzz1
+                + (ap[0] * aq[1] + ap[1] * aq[0]) * Txy1 + (ap[0] * aq[2] + ap[2] * aq[0]) * Txz1
+                + (ap[1] * aq[2] + ap[2] * aq[1]) * Tyz1)
+    return comp(0, 0), comp(1, 1), comp(2, 2), comp(0, 1), comp(0, 2), comp(1, 2)
+
+
 def read_stl(path):
     """ASCII STL (src/STLReader.jl): Points (id, x, y, z), Triangles (1-based)."""
     pts = []
