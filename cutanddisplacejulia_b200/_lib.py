@@ -26,6 +26,9 @@ CAD_ERR_TOO_LARGE = 10
 CAD_SOLVER_LU64 = 0
 CAD_SOLVER_MIXED = 1
 CAD_SOLVER_GMRES_SPAI = 2
+CAD_SOLVER_GMRES_LEARNED = 3
+CAD_SOLVER_GMRES_BLOCK_JACOBI = 4
+CAD_SOLVER_GMRES = 5
 CAD_ASSEMBLY_FP64 = 0
 CAD_ASSEMBLY_MIXED = 1
 
@@ -37,7 +40,10 @@ EXPORTS = [
     "cad_solve_dev", "cad_set_preconditioner", "cad_block_jacobi_dev", "cad_lpc_param_count", "cad_lpc_step",
     "cad_slip_calculator_batched", "cad_slip_calculator_batched_dev", "cad_td_sum_eval_noalloc",
     "cad_slip_calculator_friction", "cad_fischer_newton", "cad_friction_prepare", "cad_friction_solve",
-    "cad_assemble_columns_dev",
+    "cad_assemble_columns_dev", "cad_gemm_sub_dev", "cad_lpc_features_dev", "cad_lpc_set_network",
+    "cad_lpc_get_network", "cad_lpc_dataset_add", "cad_lpc_dataset_rows", "cad_lpc_dataset_clear",
+    "cad_lpc_dataset_get", "cad_lpc_dataset_set", "cad_lpc_forward_backward", "cad_lpc_train", "cad_lpc_install_dev",
+    "cad_lpc_install", "cad_set_wait_limit", "cad_wait_timeout_probe",
 ]
 
 
@@ -107,6 +113,22 @@ def load():
     L.cad_slip_calculator_friction.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT, P, P, P, P, P, D, INT, P, P, P]
     L.cad_fischer_newton.argtypes = [P, I64, P, P, D, INT, P]
     L.cad_assemble_columns_dev.argtypes = [P, P, P, P, P, P, I64, D, D, D, INT, I64, I64, P, I64]
+    L.cad_gemm_sub_dev.argtypes = [P, INT, I64, I64, I64, P, I64, P, I64, P, I64]
+    L.cad_lpc_features_dev.argtypes = [P, P, P, P, I64, P, P, P]
+    L.cad_lpc_set_network.argtypes = [P, P]
+    L.cad_lpc_get_network.argtypes = [P, P]
+    L.cad_lpc_dataset_add.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT]
+    L.cad_lpc_dataset_rows.argtypes = [P]
+    L.cad_lpc_dataset_rows.restype = I64
+    L.cad_lpc_dataset_clear.argtypes = [P]
+    L.cad_lpc_dataset_get.argtypes = [P, I64, I64, P, P]
+    L.cad_lpc_dataset_set.argtypes = [P, P, P, I64]
+    L.cad_lpc_forward_backward.argtypes = [P, P, P, I64, P, P, P]
+    L.cad_lpc_train.argtypes = [P, I64, I64, ctypes.c_float, ctypes.c_uint64, P]
+    L.cad_lpc_install_dev.argtypes = [P, P, P, P, I64, D]
+    L.cad_lpc_install.argtypes = [P, P, P, P, I64, D]
+    L.cad_set_wait_limit.argtypes = [P, I64]
+    L.cad_wait_timeout_probe.argtypes = [P, I64]
     L.cad_friction_prepare.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT]
     L.cad_friction_solve.argtypes = [P, I64, P, P, P, P, P, D, INT, P, P, P]
     _lib = L
@@ -143,12 +165,18 @@ def ptr_array(arrays):
 class solver_mode:
     """Context manager selecting the dense solver of `ctx` for the calls inside it
     ("lu64": FP64 LU as the reference's A\\b; "mixed": FP32/TF32 LU preconditioning
-    FP64 GMRES to relative residual `tol`), restoring the FP64 LU afterwards."""
+    FP64 GMRES to relative residual `tol`; "gmres_spai": FP64 GMRES with the
+    installed block-sparse preconditioner; "gmres_learned": the same, the
+    network's preconditioner installed by cad_slip_calculator for its mesh;
+    "gmres_block_jacobi" / "gmres": element-block Jacobi / no preconditioner),
+    restoring the FP64 LU afterwards."""
 
     def __init__(self, ctx, solver="lu64", tol=1e-10, max_iter=200):
-        modes = {"lu64": CAD_SOLVER_LU64, "mixed": CAD_SOLVER_MIXED, "gmres_spai": CAD_SOLVER_GMRES_SPAI}
+        modes = {"lu64": CAD_SOLVER_LU64, "mixed": CAD_SOLVER_MIXED, "gmres_spai": CAD_SOLVER_GMRES_SPAI,
+                 "gmres_learned": CAD_SOLVER_GMRES_LEARNED, "gmres_block_jacobi": CAD_SOLVER_GMRES_BLOCK_JACOBI,
+                 "gmres": CAD_SOLVER_GMRES}
         if solver not in modes:
-            raise ValueError("solver must be 'lu64', 'mixed' or 'gmres_spai'")
+            raise ValueError("solver must be one of " + ", ".join(sorted(modes)))
         self.ctx, self.mode, self.tol, self.max_iter = ctx, modes[solver], float(tol), int(max_iter)
 
     def __enter__(self):

@@ -7,8 +7,10 @@
 // path directly on caller-provided device memory.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -16,7 +18,9 @@
 #include <vector>
 
 #include "../../include/cad_td.h"
+#include "gemm.h"
 #include "lcp.h"
+#include "lpc.h"
 #include "lu.h"
 #include "mixed.h"
 #include "mlp.h"
@@ -34,7 +38,8 @@ namespace {
 enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
-    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_COUNT
+    S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -93,6 +98,7 @@ struct cad_ctx {
     int64_t spai_N = 0;
     int spai_k = 0;
     double near_factor = 3.0;
+    long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     double tol = 1e-10;
     int max_iter = 200;
     bool fric_ready = false;      // cad_friction_prepare: C = inv(A Scl) of fric_N elements in S_LCPC
@@ -100,10 +106,27 @@ struct cad_ctx {
     double fric_scl = 0.0;
     int last_iters = 0;           // of the last mixed solve (all right-hand sides)
     double last_relres = 0.0;     // largest over its right-hand sides
+    // learned preconditioner: network weights, Adam moments and gradients in
+    // S_LPC_NET (4 x mlp_param_count floats), Adam step count, training set
+    bool lpc_net = false;
+    int64_t lpc_t = 0;
+    float* lpc_X = nullptr;       // lpc_rows x 112 network inputs
+    float* lpc_T = nullptr;       // lpc_rows x 144 exact-inverse targets
+    int64_t lpc_rows = 0, lpc_cap = 0;
     std::string err;
 };
 
 namespace {
+
+// One NVTX range per C-ABI call, named after the entry point: a profiler's
+// timeline shows which call each kernel belongs to (no cost without a tool).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define CAD_NVTX_RANGE() NvtxRange nvtx_range_(__func__)
 
 int fail(cad_ctx* c, int code, const std::string& msg)
 {
@@ -283,7 +306,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     if (int r = ensure(ctx, S_WORK, (size_t)n * sizeof(double), &work)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
-                        ctx->graphs};
+                        ctx->graphs, ctx->wait_limit};
     ctx->timed[1] = ctx->timed[2] = false;
     int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
@@ -315,6 +338,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     g.x32 = (float*)v32 + n;
     g.sync = (int*)sync;
     g.launches = &ctx->launches;
+    g.wait_limit = ctx->wait_limit;
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
     bool converged = true;
@@ -396,6 +420,7 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     g.hd = w + 3 * n;
     g.sync = (int*)sync;
     g.launches = &ctx->launches;
+    g.wait_limit = ctx->wait_limit;
     g.spai_nbr = ctx->spai_nbr;
     g.spai_blocks = ctx->spai_blocks;
     g.spai_k = ctx->spai_k;
@@ -424,9 +449,37 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
 int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
 {
     if (n == 0 || nrhs == 0) return CAD_OK;
-    if (ctx->solver == CAD_SOLVER_GMRES_SPAI) {
+    if (ctx->solver == CAD_SOLVER_GMRES_SPAI || ctx->solver == CAD_SOLVER_GMRES_LEARNED ||
+        ctx->solver == CAD_SOLVER_GMRES_BLOCK_JACOBI || ctx->solver == CAD_SOLVER_GMRES) {
         if (n > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX || nrhs > INT32_MAX)
             return fail(ctx, CAD_ERR_ARG, "matrix dimension exceeds 2^31-1");
+        if (ctx->solver == CAD_SOLVER_GMRES_BLOCK_JACOBI || ctx->solver == CAD_SOLVER_GMRES) {
+            // the element-diagonal preconditioner of this A (or identity blocks)
+            if (n % 3 != 0) return fail(ctx, CAD_ERR_ARG, "system size is not 3N");
+            const int64_t N = n / 3;
+            void *nbr, *blk;
+            if (int r = ensure(ctx, S_BJ_NBR, (size_t)N * sizeof(int), &nbr)) return r;
+            if (int r = ensure(ctx, S_BJ_BLK, (size_t)N * 9 * sizeof(float), &blk)) return r;
+            ++ctx->launches;
+            if (ctx->solver == CAD_SOLVER_GMRES_BLOCK_JACOBI)
+                CK(block_jacobi(ctx->stream, A, lda, N, (int*)nbr, (float*)blk));
+            else
+                CK(lpc_identity_blocks(ctx->stream, N, (int*)nbr, (float*)blk, nullptr));
+            const int* keep_nbr = ctx->spai_nbr;
+            const float* keep_blk = ctx->spai_blocks;
+            const int64_t keep_N = ctx->spai_N;
+            const int keep_k = ctx->spai_k;
+            ctx->spai_nbr = (const int*)nbr;
+            ctx->spai_blocks = (const float*)blk;
+            ctx->spai_N = N;
+            ctx->spai_k = 1;
+            const int r = solve_spai_device(ctx, n, A, lda, B, ldb, nrhs);
+            ctx->spai_nbr = keep_nbr;
+            ctx->spai_blocks = keep_blk;
+            ctx->spai_N = keep_N;
+            ctx->spai_k = keep_k;
+            return r;
+        }
         return solve_spai_device(ctx, n, A, lda, B, ldb, nrhs);
     }
     if (ctx->solver == CAD_SOLVER_MIXED) {
@@ -445,7 +498,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     ctx->timed[1] = ctx->timed[2] = false;
     const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
-                        ctx->graphs};
+                        ctx->graphs, ctx->wait_limit};
     if (nrhs == 1) {   // one right-hand side: factorise, then the two chain launches
         void* chain;
         if (int r = ensure(ctx, S_CHAIN, (size_t)n * sizeof(double) + lu_chain_sync_ints(n) * sizeof(int), &chain))
@@ -457,7 +510,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
         double* y = (double*)chain;
         CK(lu_solve_chain_f64(ctx->stream, A, lda, n, (const int*)perm, B, y, (double*)work, (int*)(y + n),
-                              (int*)info, &ctx->launches));
+                              (int*)info, &ctx->launches, ctx->wait_limit));
         CK(cudaMemcpyAsync(B, work, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         ctx->timed[1] = true;
@@ -607,7 +660,7 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         double* A = b.Aall + (*b.aoff)[c];
         CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
                             b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
-        const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr};
+        const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr, ctx->wait_limit};
         int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, nullptr, (int*)l.buf[L_PIV].p,
                                (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, false);
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "batched solve: FP32 LU failed");
@@ -827,6 +880,8 @@ int cad_destroy(cad_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& b : ctx->buf)
         if (b.p) cudaFree(b.p);
+    if (ctx->lpc_X) cudaFree(ctx->lpc_X);
+    if (ctx->lpc_T) cudaFree(ctx->lpc_T);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
@@ -868,12 +923,46 @@ int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor)
 int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
 {
     if (!ctx) return CAD_ERR_ARG;
-    if ((mode != CAD_SOLVER_LU64 && mode != CAD_SOLVER_MIXED && mode != CAD_SOLVER_GMRES_SPAI) || !(tol > 0.0) ||
-        max_iter < 1)
+    if (mode < CAD_SOLVER_LU64 || mode > CAD_SOLVER_GMRES || !(tol > 0.0) || max_iter < 1)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->solver = mode;
     ctx->tol = tol;
     ctx->max_iter = max_iter;
+    return CAD_OK;
+}
+
+int cad_set_wait_limit(cad_ctx* ctx, int64_t polls)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (polls < 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->wait_limit = (long)polls;
+    return CAD_OK;
+}
+
+int cad_wait_timeout_probe(cad_ctx* ctx, int64_t n)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (n < 128 || n > 8192) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    void *a, *vec, *perm, *chain, *info;
+    if (int r = ensure(ctx, S_WORK, (size_t)n * n * sizeof(double), &a)) return r;
+    if (int r = ensure(ctx, S_B, 3 * (size_t)n * sizeof(double), &vec)) return r;
+    if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
+    if (int r = ensure(ctx, S_CHAIN, lu_chain_sync_ints(n) * sizeof(int), &chain)) return r;
+    if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
+    CK(cudaMemsetAsync(a, 0, (size_t)n * n * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(vec, 0, 3 * (size_t)n * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(perm, 0, (size_t)n * sizeof(int), ctx->stream));
+    const int big = INT_MAX;
+    CK(cudaMemcpyAsync(info, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    double* v = (double*)vec;
+    CK(lu_chain_timeout_probe(ctx->stream, (const double*)a, n, n, (const int*)perm, v, v + n, v + 2 * n, (int*)chain,
+                              (int*)info, ctx->wait_limit));
+    ctx->launches += 2;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h < 0) return fail(ctx, CAD_ERR_TIMEOUT, "a device wait ran out (triangular-solve chain flag)");
     return CAD_OK;
 }
 
@@ -887,6 +976,7 @@ int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residu
 
 int cad_set_stream(cad_ctx* ctx, void* stream)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     ctx->stream = (cudaStream_t)stream;   // NULL is CUDA's default stream, as everywhere in CUDA
     if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS)
@@ -957,6 +1047,7 @@ int cad_td_inf(cad_ctx* ctx, const double* X, const double* Y, const double* Z, 
                const double* Dn, double nu, double G, int disp_flag, int strain_flag, int hs_flag,
                double* const* strain_out, double* const* disp_out)
 {
+    CAD_NVTX_RANGE();
     (void)G;
     return td_host(ctx, false, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag,
                    strain_out, disp_out);
@@ -967,6 +1058,7 @@ int cad_td_sum_eval(cad_ctx* ctx, const double* X, const double* Y, const double
                     const double* Dds, const double* Dn, double nu, double G, int disp_flag, int strain_flag,
                     int hs_flag, double* const* strain_out, double* const* disp_out)
 {
+    CAD_NVTX_RANGE();
     (void)G;
     return td_host(ctx, true, X, Y, Z, M, P1, P2, P3, N, Dss, Dds, Dn, nu, disp_flag, strain_flag, hs_flag,
                    strain_out, disp_out);
@@ -975,6 +1067,7 @@ int cad_td_sum_eval(cad_ctx* ctx, const double* X, const double* Y, const double
 int cad_td_sum(cad_ctx* ctx, int64_t M, int64_t N, const double* const* strain_in, const double* const* disp_in,
                double* const* strain_out, double* const* disp_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (M < 0 || N < 0) return fail(ctx, CAD_ERR_ARG, "invalid size");
     const int64_t MN = M * N;
@@ -1080,6 +1173,7 @@ int cad_influence_traction(cad_ctx* ctx, const double* normals, const double* mi
                            const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                            const double* fixed_els, int hs_flag, double* const* trac_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || !trac_out) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     double* g;
@@ -1109,6 +1203,7 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
                         const double* Tn, const double* Tss, const double* Tds, double* Dn, double* Dss,
                         double* Dds, double* A_out, double* b_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || !Tn || !Tss || !Tds || !Dn || !Dss || !Dds)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1127,6 +1222,8 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
     if (r) return r;
     if (A_out) CK(cudaMemcpyAsync(A_out, A, (size_t)n3 * n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (b_out) CK(cudaMemcpyAsync(b_out, bd, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (ctx->solver == CAD_SOLVER_GMRES_LEARNED && N > 0)
+        if ((r = cad_lpc_install_dev(ctx, g, g + 3 * N, g + 6 * N, N, G))) return r;
     if ((r = solve_device(ctx, n3, (double*)A, n3, bd, n3, 1))) return r;
     int info = 0;
     if (n3 > 0)
@@ -1141,6 +1238,7 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
 
 int cad_solve(cad_ctx* ctx, int64_t n, const double* A, const double* B, int64_t nrhs, double* X)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (n < 0 || nrhs < 0 || (n > 0 && (!A || !B || !X))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     void *Ad, *Bd;
@@ -1165,6 +1263,7 @@ int cad_td_inf_dev(cad_ctx* ctx, const double* X, const double* Y, const double*
                    const double* Dn, double nu, int disp_flag, int strain_flag, int hs_flag, double* strain_out,
                    double* disp_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (M < 0 || N < 0 || bad_flag(disp_flag) || bad_flag(strain_flag) || bad_flag(hs_flag))
         return fail(ctx, CAD_ERR_ARG, "invalid size or flag");
@@ -1177,6 +1276,7 @@ int cad_td_sum_eval_dev(cad_ctx* ctx, const double* X, const double* Y, const do
                         const double* Dds, const double* Dn, double nu, int disp_flag, int strain_flag,
                         int hs_flag, double* strain_out, double* disp_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (M < 0 || N < 0 || bad_flag(disp_flag) || bad_flag(strain_flag) || bad_flag(hs_flag))
         return fail(ctx, CAD_ERR_ARG, "invalid size or flag");
@@ -1197,6 +1297,7 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
                      const double* P2, const double* P3, int64_t N, double nu, double G, double lambda, int hs_flag,
                      double* A, int64_t lda)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || lda < 3 * N) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     return assemble_device(ctx, normals, midpoints, P1, P2, P3, N, nu, G, lambda, hs_flag, OUT_AMAT, nullptr, A, lda);
@@ -1206,6 +1307,7 @@ int cad_assemble_columns_dev(cad_ctx* ctx, const double* normals, const double* 
                              const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                              int hs_flag, int64_t j0, int64_t j1, double* A_block, int64_t lda)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || j0 < 0 || j1 < j0 || j1 > N || lda < 3 * N || (j1 > j0 && !A_block))
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1239,6 +1341,7 @@ int cad_assemble_columns_dev(cad_ctx* ctx, const double* normals, const double* 
 
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (n < 0 || nrhs < 0 || lda < n || ldb < n) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     if (int r = solve_device(ctx, n, A, lda, B, ldb, nrhs)) return r;
@@ -1249,11 +1352,38 @@ int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, in
     return CAD_OK;
 }
 
+int cad_gemm_sub_dev(cad_ctx* ctx, int precision, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda,
+                     const void* B, int64_t ldb, void* C, int64_t ldc)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (m < 0 || n < 0 || k < 0 || m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || lda < (m > 0 ? m : 1) ||
+        ldb < (k > 0 ? k : 1) || ldc < (m > 0 ? m : 1) || (precision != 0 && precision != 1))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (m == 0 || n == 0 || k == 0) return CAD_OK;
+    void* st;
+    if (int r = ensure(ctx, S_GEMM, sizeof(int), &st)) return r;
+    CK(cudaMemsetAsync(st, 0, sizeof(int), ctx->stream));
+    if (precision == 0)
+        CK(gemm_sub(ctx->stream, (int)m, (int)n, (int)k, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc,
+                    (int*)st));
+    else
+        CK(gemm_sub(ctx->stream, (int)m, (int)n, (int)k, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc,
+                    (int*)st));
+    ++ctx->launches;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h < 0) return fail(ctx, CAD_ERR_TIMEOUT, "GEMM: a pipeline wait ran out");
+    return CAD_OK;
+}
+
 int cad_slip_calculator_batched_dev(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const double* P1,
                                     const double* P2, const double* P3, const double* normals,
                                     const double* midpoints, double nu, double G, double lambda, int hs_flag,
                                     const double* T, double* D, double* rel_residual)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (nbatch < 0 || bad_flag(hs_flag) || (nbatch > 0 && !offsets)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     if (nbatch > 0 && offsets[0] != 0) return fail(ctx, CAD_ERR_ARG, "offsets[0] must be 0");
@@ -1270,6 +1400,7 @@ int cad_slip_calculator_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* off
                                 double nu, double G, double lambda, int hs_flag, const double* T, double* D,
                                 double* rel_residual)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (nbatch < 0 || (nbatch > 0 && !offsets)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     const int64_t ntot = nbatch > 0 ? offsets[nbatch] : 0;
@@ -1308,6 +1439,7 @@ int cad_set_preconditioner(cad_ctx* ctx, int64_t N, int k, const int* nbr, const
 
 int cad_block_jacobi_dev(cad_ctx* ctx, int64_t N, const double* A, int64_t lda, int* nbr, float* blocks)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || lda < 3 * N || (N > 0 && (!A || !nbr || !blocks))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ++ctx->launches;
@@ -1317,9 +1449,307 @@ int cad_block_jacobi_dev(cad_ctx* ctx, int64_t N, const double* A, int64_t lda, 
 
 int64_t cad_lpc_param_count(void) { return (int64_t)mlp_param_count(); }
 
+int cad_lpc_features_dev(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, float* X,
+                         int* nbr, double* h)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (N < 0 || (N > 0 && (!P1 || !P2 || !P3 || !X || !nbr))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (N > INT32_MAX) return fail(ctx, CAD_ERR_ARG, "too many elements");
+    if (N == 0) return CAD_OK;
+    void* geom;
+    if (int r = ensure(ctx, S_LPC_GEOM, lpc_geom_doubles(N) * sizeof(double), &geom)) return r;
+    CK(lpc_features(ctx->stream, P1, P2, P3, N, (double*)geom, nbr, X, &ctx->launches));
+    if (h)
+        CK(cudaMemcpyAsync(h, lpc_geom_h((const double*)geom, N), (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    return CAD_OK;
+}
+
+static float* lpc_net_ptr(cad_ctx* ctx) { return (float*)ctx->buf[S_LPC_NET].p; }
+
+int cad_lpc_set_network(cad_ctx* ctx, const float* params)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (!params) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    const size_t P = mlp_param_count();
+    void* net;
+    if (int r = ensure(ctx, S_LPC_NET, 4 * P * sizeof(float), &net)) return r;
+    CK(cudaMemcpyAsync(net, params, P * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync((float*)net + P, 0, 3 * P * sizeof(float), ctx->stream));   // Adam moments, gradients
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->lpc_net = true;
+    ctx->lpc_t = 0;
+    return CAD_OK;
+}
+
+int cad_lpc_get_network(cad_ctx* ctx, float* params)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (!params) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (!ctx->lpc_net) return fail(ctx, CAD_ERR_ARG, "no network set (cad_lpc_set_network)");
+    CK(cudaMemcpyAsync(params, lpc_net_ptr(ctx), mlp_param_count() * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_lpc_dataset_clear(cad_ctx* ctx)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    ctx->lpc_rows = 0;
+    return CAD_OK;
+}
+
+int64_t cad_lpc_dataset_rows(const cad_ctx* ctx) { return ctx ? ctx->lpc_rows : 0; }
+
+// room for `need` rows in the training set, keeping the rows already there
+static int lpc_grow(cad_ctx* ctx, int64_t need)
+{
+    if (need <= ctx->lpc_cap) return CAD_OK;
+    int64_t cap = ctx->lpc_cap * 2 > need ? ctx->lpc_cap * 2 : need;
+    if (cap < 4096) cap = 4096;
+    float *X = nullptr, *T = nullptr;
+    CK(cudaMalloc(&X, (size_t)cap * kLpcIn * sizeof(float)));
+    if (cudaMalloc(&T, (size_t)cap * kLpcOut * sizeof(float)) != cudaSuccess) {
+        cudaFree(X);
+        return fail(ctx, CAD_ERR_OOM, "training set: out of device memory");
+    }
+    if (ctx->lpc_rows > 0) {
+        CK(cudaMemcpyAsync(X, ctx->lpc_X, (size_t)ctx->lpc_rows * kLpcIn * sizeof(float), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+        CK(cudaMemcpyAsync(T, ctx->lpc_T, (size_t)ctx->lpc_rows * kLpcOut * sizeof(float), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->lpc_X) cudaFree(ctx->lpc_X);
+    if (ctx->lpc_T) cudaFree(ctx->lpc_T);
+    ctx->lpc_X = X;
+    ctx->lpc_T = T;
+    ctx->lpc_cap = cap;
+    return CAD_OK;
+}
+
+int cad_lpc_dataset_add(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                        double G, double lambda, const double* midpoints, const double* normals, int hs_flag)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (N < 1 || bad_flag(hs_flag) || !P1 || !P2 || !P3 || !midpoints || !normals)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (3 * N > 46000) return fail(ctx, CAD_ERR_ARG, "training meshes are limited to 15333 elements");
+    double* g;
+    if (int r = upload_geometry(ctx, normals, midpoints, P1, P2, P3, N, &g)) return r;
+    const int64_t n3 = 3 * N;
+    void *mat, *geom, *nbr;
+    if (int r = ensure(ctx, S_LPC_MAT, 2 * (size_t)n3 * n3 * sizeof(double), &mat)) return r;
+    if (int r = ensure(ctx, S_LPC_GEOM, lpc_geom_doubles(N) * sizeof(double), &geom)) return r;
+    if (int r = ensure(ctx, S_LPC_TNBR, (size_t)N * kLpcK * sizeof(int), &nbr)) return r;
+    if (int r = lpc_grow(ctx, ctx->lpc_rows + N)) return r;
+    double* A = (double*)mat;
+    double* Ainv = A + n3 * n3;
+    // the exact inverse the targets come from: FP64 assembly, FP64 LU
+    const int keep_asm = ctx->assembly, keep_solver = ctx->solver;
+    ctx->assembly = CAD_ASSEMBLY_FP64;
+    ctx->solver = CAD_SOLVER_LU64;
+    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
+                            nullptr, A, n3);
+    if (!r) {
+        const cudaError_t e = lpc_identity(ctx->stream, Ainv, n3, n3, &ctx->launches);
+        r = e != cudaSuccess ? cuda_fail(ctx, e, "identity") : solve_device(ctx, n3, A, n3, Ainv, n3, n3);
+    }
+    ctx->assembly = keep_asm;
+    ctx->solver = keep_solver;
+    if (r) return r;
+    int info = 0;
+    if (int rr = read_info(ctx, &info)) return rr;
+    if (info > 0) return fail(ctx, CAD_ERR_SINGULAR, "SingularException: the system matrix is singular");
+    CK(lpc_features(ctx->stream, g, g + 3 * N, g + 6 * N, N, (double*)geom, (int*)nbr,
+                    ctx->lpc_X + ctx->lpc_rows * kLpcIn, &ctx->launches));
+    CK(lpc_targets(ctx->stream, Ainv, n3, (const int*)nbr, lpc_geom_h((const double*)geom, N), G, N,
+                   ctx->lpc_T + ctx->lpc_rows * kLpcOut, &ctx->launches));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->lpc_rows += N;
+    return CAD_OK;
+}
+
+int cad_lpc_dataset_set(cad_ctx* ctx, const float* X, const float* T, int64_t rows)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (rows < 0 || (rows > 0 && (!X || !T))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->lpc_rows = 0;
+    if (rows == 0) return CAD_OK;
+    if (int r = lpc_grow(ctx, rows)) return r;
+    CK(cudaMemcpyAsync(ctx->lpc_X, X, (size_t)rows * kLpcIn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->lpc_T, T, (size_t)rows * kLpcOut * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->lpc_rows = rows;
+    return CAD_OK;
+}
+
+// One pass of the context's network over host rows: outputs (out) and, with
+// T set, the gradient of the mean squared error (grads) and the sum of
+// squared errors (loss); host arrays in and out.
+int cad_lpc_forward_backward(cad_ctx* ctx, const float* X, const float* T, int64_t rows, float* out, float* grads,
+                             float* loss)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (rows < 1 || !X || (T && !grads) || (!T && (grads || loss))) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (rows > INT32_MAX) return fail(ctx, CAD_ERR_ARG, "too many rows");
+    if (!ctx->lpc_net) return fail(ctx, CAD_ERR_ARG, "no network set (cad_lpc_set_network)");
+    const size_t P = mlp_param_count();
+    const size_t mlpws = (mlp_workspace_bytes(rows) + 255) / 256 * 256;
+    const size_t io = (size_t)rows * (kLpcIn + 2 * kLpcOut) + P + 1;
+    void* ws;
+    if (int r = ensure(ctx, S_LPC_WS, mlpws + io * sizeof(float), &ws)) return r;
+    float* xd = (float*)((char*)ws + mlpws);
+    float* td = xd + rows * kLpcIn;
+    float* od = td + rows * kLpcOut;
+    float* gd = od + rows * kLpcOut;
+    float* ld = gd + P;
+    CK(cudaMemcpyAsync(xd, X, (size_t)rows * kLpcIn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    if (T) CK(cudaMemcpyAsync(td, T, (size_t)rows * kLpcOut * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    MlpStep st{};
+    st.stream = ctx->stream;
+    st.params = lpc_net_ptr(ctx);
+    st.X = xd;
+    st.T = T ? td : nullptr;
+    st.rows = rows;
+    st.out = out ? od : nullptr;
+    st.grads = T ? gd : nullptr;
+    st.loss = T ? ld : nullptr;
+    st.workspace = ws;
+    st.launches = &ctx->launches;
+    const int e = mlp_step(st);
+    if (e != 0) return cuda_fail(ctx, (cudaError_t)e, "learned-preconditioner network");
+    if (out) CK(cudaMemcpyAsync(out, od, (size_t)rows * kLpcOut * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (grads) CK(cudaMemcpyAsync(grads, gd, P * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (loss) CK(cudaMemcpyAsync(loss, ld, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_lpc_dataset_get(cad_ctx* ctx, int64_t row0, int64_t rows, float* X, float* T)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (row0 < 0 || rows < 0 || row0 + rows > ctx->lpc_rows || (rows > 0 && (!X || !T)))
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (rows == 0) return CAD_OK;
+    CK(cudaMemcpyAsync(X, ctx->lpc_X + row0 * kLpcIn, (size_t)rows * kLpcIn * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(T, ctx->lpc_T + row0 * kLpcOut, (size_t)rows * kLpcOut * sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CAD_OK;
+}
+
+int cad_lpc_train(cad_ctx* ctx, int64_t steps, int64_t batch, float lr, uint64_t seed, float* loss_hist)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (steps < 0 || batch < 1 || !(lr > 0.f)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (!ctx->lpc_net) return fail(ctx, CAD_ERR_ARG, "no network set (cad_lpc_set_network)");
+    if (ctx->lpc_rows < 1) return fail(ctx, CAD_ERR_ARG, "empty training set (cad_lpc_dataset_add)");
+    const int64_t b = batch < ctx->lpc_rows ? batch : ctx->lpc_rows;
+    if (b > INT32_MAX) return fail(ctx, CAD_ERR_ARG, "batch too large");
+    const int64_t nhist = (steps + 99) / 100;
+    const size_t mlpws = (mlp_workspace_bytes(b) + 255) / 256 * 256;
+    const size_t xbytes = ((size_t)b * (kLpcIn + kLpcOut) * sizeof(float) + 255) / 256 * 256;
+    void* ws;
+    if (int r = ensure(ctx, S_LPC_WS, mlpws + xbytes + (size_t)(nhist + 1) * sizeof(float), &ws)) return r;
+    float* xb = (float*)((char*)ws + mlpws);
+    float* tb = xb + b * kLpcIn;
+    float* hist = (float*)((char*)ws + mlpws + xbytes);
+    const size_t P = mlp_param_count();
+    float* net = lpc_net_ptr(ctx);
+    for (int64_t s = 0; s < steps; ++s) {
+        CK(lpc_gather(ctx->stream, ctx->lpc_X, ctx->lpc_T, ctx->lpc_rows, b, seed, ctx->lpc_t, xb, tb,
+                      &ctx->launches));
+        ++ctx->lpc_t;
+        MlpStep st{};
+        st.stream = ctx->stream;
+        st.params = net;
+        st.X = xb;
+        st.T = tb;
+        st.rows = b;
+        st.grads = net + 3 * P;
+        st.loss = (s % 100 == 0) ? hist + s / 100 : nullptr;
+        st.adam_m = net + P;
+        st.adam_v = net + 2 * P;
+        // cosine step size over this call's steps
+        st.lr = (float)(lr * 0.5 * (1.0 + cos(M_PI * (double)s / (double)steps)));
+        st.bias_c1 = 1.f - powf(0.9f, (float)ctx->lpc_t);
+        st.bias_c2 = 1.f - powf(0.999f, (float)ctx->lpc_t);
+        st.workspace = ws;
+        st.launches = &ctx->launches;
+        const int e = mlp_step(st);
+        if (e != 0) return cuda_fail(ctx, (cudaError_t)e, "learned-preconditioner training step");
+    }
+    if (loss_hist && nhist > 0) {
+        CK(cudaMemcpyAsync(loss_hist, hist, (size_t)nhist * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int64_t k = 0; k < nhist; ++k) loss_hist[k] /= (float)(b * kLpcOut);
+    }
+    return CAD_OK;
+}
+
+int cad_lpc_install_dev(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double G)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (N < 1 || !P1 || !P2 || !P3) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    if (N > INT32_MAX) return fail(ctx, CAD_ERR_ARG, "too many elements");
+    if (!ctx->lpc_net) return fail(ctx, CAD_ERR_ARG, "no network set (cad_lpc_set_network)");
+    void *geom, *nbr, *feat, *out, *blk, *ws;
+    if (int r = ensure(ctx, S_LPC_GEOM, lpc_geom_doubles(N) * sizeof(double), &geom)) return r;
+    if (int r = ensure(ctx, S_LPC_NBR, (size_t)N * kLpcK * sizeof(int), &nbr)) return r;
+    if (int r = ensure(ctx, S_LPC_FEAT, (size_t)N * kLpcIn * sizeof(float), &feat)) return r;
+    if (int r = ensure(ctx, S_LPC_OUT, (size_t)N * kLpcOut * sizeof(float), &out)) return r;
+    if (int r = ensure(ctx, S_LPC_BLK, (size_t)N * kLpcOut * sizeof(float), &blk)) return r;
+    if (int r = ensure(ctx, S_MLP, mlp_workspace_bytes(N), &ws)) return r;
+    CK(lpc_features(ctx->stream, P1, P2, P3, N, (double*)geom, (int*)nbr, (float*)feat, &ctx->launches));
+    MlpStep st{};
+    st.stream = ctx->stream;
+    st.params = lpc_net_ptr(ctx);
+    st.X = (const float*)feat;
+    st.rows = N;
+    st.out = (float*)out;
+    st.workspace = ws;
+    st.launches = &ctx->launches;
+    const int e = mlp_step(st);
+    if (e != 0) return cuda_fail(ctx, (cudaError_t)e, "learned-preconditioner network");
+    CK(lpc_scale_blocks(ctx->stream, (const float*)out, lpc_geom_h((const double*)geom, N), G, N, (float*)blk,
+                        &ctx->launches));
+    ctx->spai_N = N;
+    ctx->spai_k = kLpcK;
+    ctx->spai_nbr = (const int*)nbr;
+    ctx->spai_blocks = (const float*)blk;
+    return CAD_OK;
+}
+
+int cad_lpc_install(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double G)
+{
+    CAD_NVTX_RANGE();
+    if (int r = set_device(ctx)) return r;
+    if (N < 1 || !P1 || !P2 || !P3) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    void* pg;
+    if (int r = ensure(ctx, S_LPC_PGEOM, (size_t)9 * N * sizeof(double), &pg)) return r;
+    double* g = (double*)pg;
+    if (int r = upload(ctx, g, P1, 3 * N)) return r;
+    if (int r = upload(ctx, g + 3 * N, P2, 3 * N)) return r;
+    if (int r = upload(ctx, g + 6 * N, P3, 3 * N)) return r;
+    return cad_lpc_install_dev(ctx, g, g + 3 * N, g + 6 * N, N, G);
+}
+
 int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, int64_t rows, float* out, float* grads,
                  float* loss, float* adam_m, float* adam_v, int64_t t, float lr)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (rows < 0 || !params || (rows > 0 && !X) || (grads && !T) || ((adam_m || adam_v) && (!adam_m || !adam_v ||
                                                                                              !grads || t < 1)))
@@ -1355,6 +1785,7 @@ int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, 
                               const double* fixed_els, double* Dn, double* Dss, double* Dds, double* A_out,
                               double* b_out)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || bad_flag(hs_flag) || !Tn || !Tss || !Tds || !Dn || !Dss || !Dds)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1411,6 +1842,7 @@ int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* m
                             const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                             int hs_flag, const int64_t* changed, int64_t k, double* A, int64_t lda)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || k < 0 || bad_flag(hs_flag) || lda < 3 * N || (k > 0 && !changed) || N > INT32_MAX)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1592,6 +2024,7 @@ int lcp_status(cad_ctx* ctx, int iters, double rel, double tol)
 int cad_fischer_newton(cad_ctx* ctx, int64_t n, const double* A, const double* b, double tol, int max_iter,
                        double* x)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (n < 0 || !(tol > 0.0) || max_iter < 0 || (n > 0 && (!A || !b || !x)) || n > INT32_MAX)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1733,6 +2166,7 @@ int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P
                                  const double* mu, const double* Sf, double tol, int max_iter, double* Dn,
                                  double* Dss, double* Dds)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (!friction_geometry_args_ok(N, hs_flag, G, P1, P2, P3, midpoints, normals) ||
         !friction_load_args_ok(N, tol, max_iter, Tn, Tss, Tds, mu, Sf, Dn, Dss, Dds))
@@ -1761,6 +2195,7 @@ int cad_slip_calculator_friction(cad_ctx* ctx, const double* P1, const double* P
 int cad_friction_prepare(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
                          double G, double lambda, const double* midpoints, const double* normals, int hs_flag)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (!friction_geometry_args_ok(N, hs_flag, G, P1, P2, P3, midpoints, normals))
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
@@ -1773,6 +2208,7 @@ int cad_friction_solve(cad_ctx* ctx, int64_t N, const double* Tn, const double* 
                        const double* mu, const double* Sf, double tol, int max_iter, double* Dn, double* Dss,
                        double* Dds)
 {
+    CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (N < 0 || !friction_load_args_ok(N, tol, max_iter, Tn, Tss, Tds, mu, Sf, Dn, Dss, Dds))
         return fail(ctx, CAD_ERR_ARG, "invalid argument");

@@ -9,13 +9,13 @@
 // |entry|, the cluster agrees on the pivot through DSMEM, the pivot row and the
 // displaced row are exchanged through DSMEM, and every CTA updates its own rows
 // -- two hardware cluster barriers per column, no global-memory spin.  Rank-nb
-// trailing updates and the intra-panel updates are plain cuBLAS GEMMs (DGEMM,
-// or SGEMM on TF32 tensor cores for the single-precision factorisation).
+// trailing updates and the intra-panel updates are the library's own tensor-
+// core GEMMs (csrc/gemm.cu: DMMA tiles in FP64; tcgen05 TF32 with TMA-staged
+// operands for the single-precision factorisation).
 //
 // Pivot choice is LAPACK's: the first row of largest magnitude; scaling by the
 // reciprocal pivot; ipiv[k] = absolute row swapped with row k.
 #include <cooperative_groups.h>
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "gemm.h"
 #include "lu.h"
 
 namespace cg = cooperative_groups;
@@ -121,9 +122,6 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned mbar, unsigned parity)
     return ok != 0u;
 }
 
-// try_wait rounds before a leaf gives up on a push and reports failure
-constexpr long kWaitLimit = 1L << 20;
-
 // Factorises the m x w panel at A (leading dimension lda, w <= W) in place.
 // CTA q of the cluster owns panel rows [q*R, (q+1)*R), R = 512 * RPT; thread t
 // keeps rows t + 512*k (k < RPT) in registers for the whole leaf and never
@@ -141,7 +139,8 @@ constexpr long kWaitLimit = 1L << 20;
 template <typename T, int W, int RPT>
 __global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict__ A, int64_t lda, int m, int w,
                                                                 int* __restrict__ piv, int piv_base,
-                                                                int* __restrict__ info, int col_base)
+                                                                int* __restrict__ info, int col_base,
+                                                                long wait_limit)
 {
     static_assert(W * RPT <= kLeafRegs && W <= 32, "leaf tile exceeds its register budget");
     cg::cluster_group cluster = cg::this_cluster();
@@ -237,7 +236,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict_
             const unsigned parity = (unsigned)((j >> 1) & 1);
             long spins = 0;
             while (!mbar_try_wait(bar, parity))
-                if (++spins > kWaitLimit) {
+                if (++spins > (wait_limit >> 2)) {   // a try_wait round may suspend briefly
                     s_fail = 1;
                     break;
                 }
@@ -489,36 +488,26 @@ __global__ void permute_rows_kernel(const T* __restrict__ X, int64_t ldx, const 
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
-// ------------------------------------------------------------ GEMM wrapper
-// C (m x n, ldc) -= A (m x k, lda) * B (k x n, ldb)
-cublasStatus_t gemm_sub(cublasHandle_t h, int m, int n, int k, const double* A, int64_t lda, const double* B,
-                        int64_t ldb, double* C, int64_t ldc)
-{
-    const double one = 1.0, mone = -1.0;
-    return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, (int)lda, B, (int)ldb, &one, C, (int)ldc);
-}
-cublasStatus_t gemm_sub(cublasHandle_t h, int m, int n, int k, const float* A, int64_t lda, const float* B,
-                        int64_t ldb, float* C, int64_t ldc)
-{
-    const float one = 1.0f, mone = -1.0f;
-    return cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, CUDA_R_32F, (int)lda, B, CUDA_R_32F, (int)ldb,
-                        &one, C, CUDA_R_32F, (int)ldc, CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
-}
-
 template <typename T>
 struct Lu {
-    cublasHandle_t h;   // the handle and stream the next launches go to
-    cudaStream_t st;
-    cublasHandle_t main_h, side_h;
+    cudaStream_t st;   // the stream the next launches go to
     cudaStream_t main_st, side_st;
     int* ipiv;    // absolute pivots, device
     int* info;
     int cluster;  // largest leaf cluster (16 where the device co-schedules it, else 8)
-    int64_t launches = 0;   // own kernels launched (cuBLAS calls not counted)
+    long wait_limit = kDefaultWaitLimit;   // try_wait rounds before a leaf gives up on a push
+    int64_t launches = 0;   // own kernels launched
     cudaError_t err = cudaSuccess;
-    cublasStatus_t berr = CUBLAS_STATUS_SUCCESS;
 
-    bool ok() const { return err == cudaSuccess && berr == CUBLAS_STATUS_SUCCESS; }
+    bool ok() const { return err == cudaSuccess; }
+
+    // C (m x n) -= A (m x k) * B (k x n) on the current stream
+    void gemm(int m, int n, int k, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc)
+    {
+        if (!ok() || m <= 0 || n <= 0 || k <= 0) return;
+        err = gemm_sub(st, m, n, k, A, lda, B, ldb, C, ldc, info);
+        ++launches;
+    }
 
     // rows per leaf thread for an m-row panel: the fewest that fit one cluster
     int leaf_rpt(int m) const
@@ -549,8 +538,7 @@ struct Lu {
             trsm_diag_kernel<T, false><<<(ncol + 31) / 32, 128, 0, st>>>(L + d + d * ldl, ldl, db, B + d, ldb, ncol);
             ++launches;
             err = cudaGetLastError();
-            if (d + db < b && ok())
-                berr = gemm_sub(h, b - d - db, ncol, db, L + (d + db) + d * ldl, ldl, B + d, ldb, B + d + db, ldb);
+            if (d + db < b) gemm(b - d - db, ncol, db, L + (d + db) + d * ldl, ldl, B + d, ldb, B + d + db, ldb);
         }
     }
 
@@ -570,7 +558,8 @@ struct Lu {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        err = cudaLaunchKernelEx(&cfg, leaf_lu_kernel<T, W, RPT>, A, lda, m, w, piv, piv_base, info, col_base);
+        err = cudaLaunchKernelEx(&cfg, leaf_lu_kernel<T, W, RPT>, A, lda, m, w, piv, piv_base, info, col_base,
+                                 wait_limit);
         ++launches;
     }
 
@@ -600,18 +589,13 @@ struct Lu {
         panel(A, lda, m, w1, piv, piv_base, col_base);
         laswp(piv, w1, piv_base, A + w1 * lda, w - w1, nullptr, 0, lda);
         trsm_lower(A, lda, w1, A + w1 * lda, lda, w - w1);
-        if (m > w1 && ok())
-            berr = gemm_sub(h, m - w1, w - w1, w1, A + w1, lda, A + w1 * lda, lda, A + w1 + w1 * lda, lda);
+        if (m > w1) gemm(m - w1, w - w1, w1, A + w1, lda, A + w1 * lda, lda, A + w1 + w1 * lda, lda);
         panel(A + w1 + w1 * lda, lda, m - w1, w - w1, piv + w1, piv_base + w1, col_base + w1);
         // the right half's pivots (rows w1.. of the panel) applied to the left half's columns
         laswp(piv + w1, w - w1, piv_base + w1, A + w1, w1, nullptr, 0, lda);
     }
 
-    void use(bool side)
-    {
-        st = side ? side_st : main_st;
-        h = side ? side_h : main_h;
-    }
+    void use(bool side) { st = side ? side_st : main_st; }
 
     // Right-looking blocked LU with a look-ahead of one block column.  Block
     // b's update is split: the main stream swaps, solves and updates block
@@ -654,9 +638,7 @@ struct Lu {
             laswp(ipiv + k, kb, (int)k, A + k, (int)k, A + k + k1 * lda, kb1, lda);
             if (kb1 > 0) {
                 trsm_lower(Akk, lda, kb, A + k + k1 * lda, lda, kb1);
-                if (ok())
-                    berr = gemm_sub(h, (int)(n - k1), kb1, kb, A + k1 + k * lda, lda, A + k + k1 * lda, lda,
-                                    A + k1 + k1 * lda, lda);
+                gemm((int)(n - k1), kb1, kb, A + k1 + k * lda, lda, A + k + k1 * lda, lda, A + k1 + k1 * lda, lda);
                 panel(A + k1 + k1 * lda, lda, (int)(n - k1), kb1, ipiv + k1, (int)k1, (int)k1);
                 if (ok()) err = cudaEventRecord(ev_panel[b + 1], main_st);
             }
@@ -666,9 +648,7 @@ struct Lu {
                 err = cudaStreamWaitEvent(side_st, ev_panel[b], 0);
                 laswp(ipiv + k, kb, (int)k, A + k + k2 * lda, nr2, nullptr, 0, lda);
                 trsm_lower(Akk, lda, kb, A + k + k2 * lda, lda, nr2);
-                if (ok())
-                    berr = gemm_sub(h, (int)(n - k1), nr2, kb, A + k1 + k * lda, lda, A + k + k2 * lda, lda,
-                                    A + k1 + k2 * lda, lda);
+                gemm((int)(n - k1), nr2, kb, A + k1 + k * lda, lda, A + k + k2 * lda, lda, A + k1 + k2 * lda, lda);
             }
             if (ok()) err = cudaEventRecord(ev_rest[b], side_st);
         }
@@ -697,8 +677,7 @@ struct Lu {
             trsm_diag_kernel<T, false><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
             ++launches;
             err = cudaGetLastError();
-            if (d + db < n && ok())
-                berr = gemm_sub(h, (int)(n - d - db), nrhs, db, A + (d + db) + d * lda, lda, X + d, ldx, X + d + db, ldx);
+            if (d + db < n) gemm((int)(n - d - db), nrhs, db, A + (d + db) + d * lda, lda, X + d, ldx, X + d + db, ldx);
         }
         // backward: U x = y, 64-row blocks from the bottom
         for (int64_t e = n; e > 0 && ok(); e -= 64) {
@@ -707,7 +686,7 @@ struct Lu {
             trsm_diag_kernel<T, true><<<(nrhs + 31) / 32, 128, 0, st>>>(A + d + d * lda, lda, db, X + d, ldx, nrhs);
             ++launches;
             err = cudaGetLastError();
-            if (d > 0 && ok()) berr = gemm_sub(h, (int)d, nrhs, db, A + d * lda, lda, X + d, ldx, X, ldx);
+            if (d > 0) gemm((int)d, nrhs, db, A + d * lda, lda, X + d, ldx, X, ldx);
         }
     }
 };
@@ -766,13 +745,13 @@ struct LuGraphKey {
     const int *ipiv, *perm, *info;
     bool factor, solve;
     cudaStream_t main, side;
-    cublasHandle_t main_blas, side_blas;
+    long wait_limit;
     bool same(const LuGraphKey& o) const
     {
         return type == o.type && A == o.A && B == o.B && X == o.X && n == o.n && lda == o.lda && ldb == o.ldb &&
                ldx == o.ldx && nrhs == o.nrhs && nb == o.nb && ipiv == o.ipiv && perm == o.perm && info == o.info &&
                factor == o.factor && solve == o.solve && main == o.main && side == o.side &&
-               main_blas == o.main_blas && side_blas == o.side_blas;
+               wait_limit == o.wait_limit;
     }
 };
 
@@ -885,26 +864,22 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
                     int64_t ldx, int* ipiv, int* perm, int* info, int nb, bool factor, bool solve)
 {
     Lu<T> lu;
-    lu.main_h = s.main_blas;
     lu.main_st = s.main;
     // without a side stream the look-ahead degenerates to one in-order stream
-    lu.side_h = s.side_blas ? s.side_blas : s.main_blas;
-    lu.side_st = s.side_blas ? s.side : s.main;
+    lu.side_st = s.side ? s.side : s.main;
     lu.use(false);
     lu.ipiv = ipiv;
     lu.info = info;
+    lu.wait_limit = s.wait_limit > 0 ? s.wait_limit : kDefaultWaitLimit;
     configure(lu);
     // nb bounds the pivots one row-swap launch applies; a leaf cluster holds
     // at most cluster * 512 * 8 rows
     if (nb < 1 || nb > kMaxSwaps || n > (int64_t)lu.cluster * kLeafThreads * 8 || n > INT32_MAX)
         return LU_TOO_LARGE;
-    if (cublasSetStream(lu.main_h, lu.main_st) != CUBLAS_STATUS_SUCCESS ||
-        cublasSetStream(lu.side_h, lu.side_st) != CUBLAS_STATUS_SUCCESS)
-        return LU_BLAS_ERROR;
     LuGraphEntry* entry = nullptr;
     if (s.graphs && n > 0) {
         const LuGraphKey key{(int)sizeof(T), A, B, X, n, lda, ldb, ldx, nrhs, nb, ipiv, perm, info, factor, solve,
-                             lu.main_st, lu.side_st, lu.main_h, lu.side_h};
+                             lu.main_st, lu.side_st, lu.wait_limit};
         entry = s.graphs->find(key);
         if (entry && entry->exec) {   // replay
             if (cudaGraphLaunch(entry->exec, lu.main_st) != cudaSuccess) return LU_CUDA_ERROR;
@@ -919,7 +894,6 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     if (entry) {                      // second sighting: capture, then launch
         cudaGraphExec_t exec = nullptr;
         lu_capture(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve, &exec);
-        if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;
         if (lu.err != cudaSuccess || !exec) return LU_CUDA_ERROR;
         entry->exec = exec;
         entry->launches = lu.launches;
@@ -930,7 +904,6 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     lu_body(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve);
     if (s.launches) *s.launches += lu.launches;
     if (lu.err != cudaSuccess) return LU_CUDA_ERROR;
-    if (lu.berr != CUBLAS_STATUS_SUCCESS) return LU_BLAS_ERROR;
     return LU_OK;
 }
 

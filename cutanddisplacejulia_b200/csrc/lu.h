@@ -31,7 +31,12 @@ struct LuStreams {
     cublasHandle_t side_blas;
     int64_t* launches;       // if set, incremented by the number of own kernel launches
     LuGraphCache* graphs;    // if set, repeated call signatures replay a captured graph
+    long wait_limit = 0;     // polls a device wait makes before it gives up (0: kDefaultWaitLimit)
 };
+
+// Polls of a device-side wait (a pivot exchange, a chain flag) before the
+// kernel gives up, records the failure in the info word and returns.
+constexpr long kDefaultWaitLimit = 1L << 22;
 
 // Factorise A (n x n, lda, column-major) in place (if factor) and / or solve
 // A X = B with the factors (if solve).  ipiv (n ints), perm (n ints) and info
@@ -48,7 +53,13 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
 // (csrc/trsv.cu).  y: n doubles of workspace; sync: lu_chain_sync_ints(n)
 // ints; a dependency wait that runs out sets *info to -1.
 cudaError_t lu_solve_chain_f64(cudaStream_t st, const double* A, int64_t lda, int64_t n, const int* perm,
-                               const double* b, double* y, double* x, int* sync, int* info, int64_t* launches);
+                               const double* b, double* y, double* x, int* sync, int* info, int64_t* launches,
+                               long wait_limit);
+// The lower chain launch with its ticket counter started at 1: every block
+// waits for block 0's flag, which no block publishes, so each wait runs out
+// after wait_limit polls and *info ends at -1 (exercises the timeout path).
+cudaError_t lu_chain_timeout_probe(cudaStream_t st, const double* A, int64_t lda, int64_t n, const int* perm,
+                                   const double* b, double* y, double* x, int* sync, int* info, long wait_limit);
 size_t lu_chain_sync_ints(int64_t n);
 
 // perm[i] = row of the original matrix that the factorisation's row i came

@@ -31,7 +31,6 @@ namespace {
 
 constexpr int kRB = 128;            // row block of the triangular solves
 constexpr int kChainThreads = 512;  // four threads per row: quarters of each 128-column block
-constexpr long kSpinLimit = 1L << 22;
 
 // B (n x n, leading dimension n) = (float) A (n x n, lda); columns strided over grid.y
 __global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64_t n, float* __restrict__ B)
@@ -119,7 +118,7 @@ template <bool UPPER>
 __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
     const float* __restrict__ A, int64_t lda, int n, int nblk, const float* __restrict__ Dinv,
     const double* __restrict__ v_in, const int* __restrict__ perm, const float* y_in, float* x32,
-    double* __restrict__ out, int* flags, int* ticket, int* fail)
+    double* __restrict__ out, int* flags, int* ticket, int* fail, long wait_limit)
 {
     constexpr int kQ = kChainThreads / kRB;   // column quarters
     constexpr int kC = kRB / kQ;              // columns per quarter
@@ -146,7 +145,7 @@ __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
         if (tid == 0) {
             long spins = 0;
             while (ld_acquire(flags + j) == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > wait_limit) {
                     atomicExch(fail, 1);
                     break;
                 }
@@ -244,6 +243,7 @@ struct Precond {
     const int* spai_nbr;
     const float* spai_blocks;
     int spai_k;
+    long wait_limit;
 
     // z = M^-1 v (FP64 in and out, FP32 inside)
     bool apply(const double* v, double* z) const
@@ -260,9 +260,9 @@ struct Precond {
         const float* DL = Dinv;
         const float* DU = Dinv + (int64_t)nblk * kRB * kRB;
         trsv_chain_kernel<false><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DL, v, perm, nullptr, y32, nullptr,
-                                                                 fl, tk, fail);
+                                                                 fl, tk, fail, wait_limit);
         trsv_chain_kernel<true><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DU, nullptr, nullptr, y32, x32, z, fu,
-                                                                tk + 1, fail);
+                                                                tk + 1, fail, wait_limit);
         if (launches) *launches += 2;
         return cudaGetLastError() == cudaSuccess;
     }
@@ -283,7 +283,7 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
     cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
     const int nblk = (int)((n + kRB - 1) / kRB);
     Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.y32, a.x32, a.sync, st, a.launches, a.spai_nbr, a.spai_blocks,
-              a.spai_k};
+              a.spai_k, a.wait_limit > 0 ? a.wait_limit : kDefaultWaitLimit};
     double* V = a.V;        // n x (m + 1)
     double* w = a.w;
     double* z = a.z;

@@ -52,6 +52,7 @@ struct GmresArgs {
     const int* spai_nbr = nullptr;
     const float* spai_blocks = nullptr;
     int spai_k = 0;
+    long wait_limit = 0;   // polls of a triangular-solve flag wait (0: kDefaultWaitLimit)
 };
 
 struct GmresResult {

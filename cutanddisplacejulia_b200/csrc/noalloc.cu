@@ -77,7 +77,9 @@ extern "C" int cad_td_sum_eval_noalloc(void* stream, const double* X, const doub
         return CAD_ERR_ARG;
     if ((strain_flag == 1 && !strain_out) || (disp_flag == 1 && !disp_out)) return CAD_ERR_ARG;
     if (M > kMaxObs || N > kMaxTri) return CAD_ERR_TOO_LARGE;
-    if (M == 0) return CAD_OK;
+    // with no points there is nothing to evaluate, but half-space triangles
+    // are still checked, as cad_td_sum_eval_dev and the reference do
+    if (M == 0 && (hs_flag == 0 || N == 0)) return CAD_OK;
     cudaStream_t st = (cudaStream_t)stream;
     void* base = nullptr;
     if (int r = scratch_address(&base)) return r;
@@ -95,6 +97,7 @@ extern "C" int cad_td_sum_eval_noalloc(void* stream, const double* X, const doub
             return CAD_ERR_CUDA;
         if (h) return CAD_ERR_HS_ABOVE_SURFACE;
     }
+    if (M == 0) return CAD_OK;
     if (N == 0) {
         if (strain_flag == 1 && cudaMemsetAsync(strain_out, 0, 6 * M * sizeof(double), st) != cudaSuccess)
             return CAD_ERR_CUDA;

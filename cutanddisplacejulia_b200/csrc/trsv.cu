@@ -24,7 +24,6 @@ constexpr int kB = 64;            // rows per block
 constexpr int kThreads = 256;     // four threads per row: quarters of each 64-column block
 constexpr int kQ = kThreads / kB;
 constexpr int kC = kB / kQ;       // 16 columns per quarter
-constexpr long kSpinLimit = 1L << 22;
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -43,7 +42,8 @@ template <bool UPPER>
 __global__ void __launch_bounds__(kThreads) trsv_chain_f64_kernel(const double* __restrict__ A, int64_t lda, int n,
                                                                   int nblk, const double* __restrict__ b,
                                                                   const int* __restrict__ perm, double* y, double* x,
-                                                                  int* flags, int* ticket, int* info)
+                                                                  int* flags, int* ticket, int* info,
+                                                                  long wait_limit)
 {
     __shared__ double s_d[kB][kB + 1];
     __shared__ double s_x[kB];
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kThreads) trsv_chain_f64_kernel(const double* 
         if (tid == 0) {
             long spins = 0;
             while (ld_acquire(flags + j) == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > wait_limit) {
                     atomicMin(info, -1);
                     break;
                 }
@@ -139,8 +139,10 @@ __global__ void __launch_bounds__(kThreads) trsv_chain_f64_kernel(const double* 
 size_t lu_chain_sync_ints(int64_t n) { return (size_t)2 * ((n + kB - 1) / kB) + 2; }
 
 cudaError_t lu_solve_chain_f64(cudaStream_t st, const double* A, int64_t lda, int64_t n, const int* perm,
-                               const double* b, double* y, double* x, int* sync, int* info, int64_t* launches)
+                               const double* b, double* y, double* x, int* sync, int* info, int64_t* launches,
+                               long wait_limit)
 {
+    if (wait_limit <= 0) wait_limit = kDefaultWaitLimit;
     if (n <= 0) return cudaSuccess;
     const int nblk = (int)((n + kB - 1) / kB);
     cudaError_t e = cudaMemsetAsync(sync, 0, lu_chain_sync_ints(n) * sizeof(int), st);
@@ -148,9 +150,28 @@ cudaError_t lu_solve_chain_f64(cudaStream_t st, const double* A, int64_t lda, in
     int* fl = sync;
     int* fu = sync + nblk;
     int* tk = sync + 2 * nblk;
-    trsv_chain_f64_kernel<false><<<nblk, kThreads, 0, st>>>(A, lda, (int)n, nblk, b, perm, y, x, fl, tk, info);
-    trsv_chain_f64_kernel<true><<<nblk, kThreads, 0, st>>>(A, lda, (int)n, nblk, b, perm, y, x, fu, tk + 1, info);
+    trsv_chain_f64_kernel<false><<<nblk, kThreads, 0, st>>>(A, lda, (int)n, nblk, b, perm, y, x, fl, tk, info,
+                                                            wait_limit);
+    trsv_chain_f64_kernel<true><<<nblk, kThreads, 0, st>>>(A, lda, (int)n, nblk, b, perm, y, x, fu, tk + 1, info,
+                                                           wait_limit);
     if (launches) *launches += 2;
+    return cudaGetLastError();
+}
+
+__global__ void set_ticket_kernel(int* ticket, int v) { *ticket = v; }
+
+cudaError_t lu_chain_timeout_probe(cudaStream_t st, const double* A, int64_t lda, int64_t n, const int* perm,
+                                   const double* b, double* y, double* x, int* sync, int* info, long wait_limit)
+{
+    const int nblk = (int)((n + kB - 1) / kB);
+    if (nblk < 2 || wait_limit <= 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(sync, 0, lu_chain_sync_ints(n) * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    int* tk = sync + 2 * nblk;
+    set_ticket_kernel<<<1, 1, 0, st>>>(tk, 1);
+    // tickets 1 .. nblk - 1: blocks 1 .. nblk - 1, none of which is block 0
+    trsv_chain_f64_kernel<false><<<nblk - 1, kThreads, 0, st>>>(A, lda, (int)n, nblk, b, perm, y, x, sync, tk, info,
+                                                                wait_limit);
     return cudaGetLastError();
 }
 

@@ -7,7 +7,8 @@
 # declared in include/cad_td.h.  Usage inside CutAndDisplaceJulia:
 #
 #     include("CutAndDisplaceB200.jl"); using .CutAndDisplaceB200
-#     # and route the calls (see INTEGRATION.md for the one-line changes)
+#     # then call TD / TD_sum / CalculateInfluenceMatrices3D / SlipCalculator3D
+#     # through this module in place of the reference's methods
 module CutAndDisplaceB200
 
 const libcad = get(ENV, "CAD_TD_LIB", joinpath(@__DIR__, "..", "libcad_td.so"))

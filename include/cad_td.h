@@ -6,8 +6,8 @@
  * (src/TD_sum.jl:1-41), the traction assembly of CalculateInfluenceMatrices3D
  * (src/CalculateInfluenceMatrices3D.jl:2-48, :73-114) and the dense solve
  * D = A\b of SlipCalculator3D (src/SlipCalculator3D.jl:1-33).  Julia binds
- * these with ccall; every argument is a plain pointer or
- * number, nothing here depends on any framework type.
+ * these with ccall; every argument is a plain pointer or number, nothing here
+ * depends on any framework type.
  *
  * Conventions (all follow the reference's Julia layout):
  *   - FP64 everywhere.
@@ -52,6 +52,10 @@ extern "C" {
 #define CAD_SOLVER_LU64 0  /* FP64 LU with partial pivoting: the reference's A\b (default) */
 #define CAD_SOLVER_MIXED 1 /* FP32 LU (TF32 tensor-core updates) preconditioning FP64 GMRES */
 #define CAD_SOLVER_GMRES_SPAI 2 /* FP64 GMRES, block-sparse preconditioner of cad_set_preconditioner */
+#define CAD_SOLVER_GMRES_LEARNED 3 /* as GMRES_SPAI; cad_slip_calculator first installs the context
+                                      network's preconditioner for its mesh (cad_lpc_install_dev) */
+#define CAD_SOLVER_GMRES_BLOCK_JACOBI 4 /* FP64 GMRES, inverses of A's 3 x 3 element self blocks */
+#define CAD_SOLVER_GMRES 5 /* FP64 GMRES with no preconditioner */
 
 /* Precision of the system-matrix assembly (cad_set_assembly). */
 #define CAD_ASSEMBLY_FP64 0  /* every pair in FP64, as the reference (default) */
@@ -109,6 +113,18 @@ int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor);
 /* GMRES iterations (summed over right-hand sides) and the largest final
  * relative residual of the last mixed solve. */
 int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual);
+/* Device waits (a leaf's pivot exchange, a triangular-solve chain flag) poll
+ * at most `polls` times (default 4194304, a few seconds at worst) before the
+ * kernel records the failure and returns; the call then reports
+ * CAD_ERR_TIMEOUT and the context stays usable.  No counterpart in the
+ * reference (its waits are CPU thread joins). */
+int cad_set_wait_limit(cad_ctx* ctx, int64_t polls);
+/* Exercises that timeout path on an n x n zero system (128 <= n <= 8192): the
+ * lower chain of the one-right-hand-side solve is launched with its order
+ * counter started past block 0, so every block waits for a flag that no block
+ * sets.  Returns CAD_ERR_TIMEOUT once the waits run out (the kernels end
+ * normally; nothing faults or hangs). */
+int cad_wait_timeout_probe(cad_ctx* ctx, int64_t n);
 /* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 flops
  * per FMA), the denominator of the TD kernels' roofline.  No counterpart in
  * the reference (a measurement utility). */
@@ -254,8 +270,6 @@ int cad_assemble_dev(cad_ctx* ctx, const double* normals, const double* midpoint
 int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
                             const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                             int hs_flag, const int64_t* changed, int64_t k, double* A, int64_t lda);
-/* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
- * (n x nrhs, ldb) by the solution. */
 /* A column block of the system matrix of cad_assemble_dev: the columns of
  * elements j0 .. j1-1 (all 3N rows), for sharding the assembly across GPUs
  * with no exchange (the reference fills whole columns per thread,
@@ -265,7 +279,18 @@ int cad_assemble_update_dev(cad_ctx* ctx, const double* normals, const double* m
 int cad_assemble_columns_dev(cad_ctx* ctx, const double* normals, const double* midpoints, const double* P1,
                              const double* P2, const double* P3, int64_t N, double nu, double G, double lambda,
                              int hs_flag, int64_t j0, int64_t j1, double* A_block, int64_t lda);
+/* In-place LU solve: A (n x n, lda) is overwritten by its LU factors, B
+ * (n x nrhs, ldb) by the solution. */
 int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int64_t ldb, int64_t nrhs);
+/* C (m x n, ldc) -= A (m x k, lda) * B (k x n, ldb), column-major device
+ * arrays, precision 0 = FP64 (DMMA tensor cores), 1 = FP32 (TF32 tensor cores
+ * through tcgen05 when A and B start on 16-byte boundaries and lda, ldb are
+ * multiples of 4; FP32 CUDA cores otherwise).  The trailing-update product of
+ * the dense LU that replaces the reference's A\b (src/SlipCalculator3D.jl:22),
+ * exposed on its own for testing and measurement; synchronises the context
+ * stream. */
+int cad_gemm_sub_dev(cad_ctx* ctx, int precision, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda,
+                     const void* B, int64_t ldb, void* C, int64_t ldc);
 
 /* ---------------------------------------------- learned preconditioner ---
  * No counterpart in the reference (its only solver is the dense A\b).  A
@@ -291,6 +316,48 @@ int cad_block_jacobi_dev(cad_ctx* ctx, int64_t N, const double* A, int64_t lda, 
 int64_t cad_lpc_param_count(void);
 int cad_lpc_step(cad_ctx* ctx, float* params, const float* X, const float* T, int64_t rows, float* out, float* grads,
                  float* loss, float* adam_m, float* adam_v, int64_t t, float lr);
+/* The learned path without any host-side numerics (no counterpart in the
+ * reference):
+ * - cad_lpc_features_dev: device vertex lists (N x 3 column-major) -> the
+ *   network inputs X (N x 112), the 16 nearest elements of each element by
+ *   centroid distance, itself first (nbr, N x 16), and h = sqrt(2 area)
+ *   (N, may be NULL); all device arrays.
+ * - cad_lpc_set_network / cad_lpc_get_network: the context's network weights
+ *   (host, cad_lpc_param_count floats); setting them resets the Adam state.
+ * - cad_lpc_dataset_add: appends one mesh to the context's training set
+ *   (host arrays as cad_slip_calculator): the library assembles its FP64
+ *   system, inverts it with the FP64 LU and keeps, per element, its features
+ *   and the 16 3 x 3 blocks of A^-1 toward its neighbours divided by h / G.
+ *   cad_lpc_dataset_rows / _clear: its size (elements) / empty it.
+ * - cad_lpc_train: `steps` Adam steps (cosine step size from lr) on
+ *   minibatches of `batch` rows drawn from the training set by a seeded hash;
+ *   loss_hist (host, ceil(steps / 100) floats, may be NULL) gets the mean
+ *   squared error of every 100th minibatch.
+ * - cad_lpc_install_dev / cad_lpc_install (host vertex lists): runs the
+ *   network on a mesh and installs the blocks (x h / G) as the context's
+ *   preconditioner for CAD_SOLVER_GMRES_SPAI / _LEARNED solves; the arrays
+ *   belong to the context. */
+int cad_lpc_features_dev(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, float* X,
+                         int* nbr, double* h);
+int cad_lpc_set_network(cad_ctx* ctx, const float* params);
+int cad_lpc_get_network(cad_ctx* ctx, float* params);
+int cad_lpc_dataset_add(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double nu,
+                        double G, double lambda, const double* midpoints, const double* normals, int hs_flag);
+int64_t cad_lpc_dataset_rows(const cad_ctx* ctx);
+int cad_lpc_dataset_clear(cad_ctx* ctx);
+/* Host-array forms: cad_lpc_dataset_set replaces the training set by `rows`
+ * host rows (X rows x 112, T rows x 144); cad_lpc_dataset_get copies rows
+ * row0 .. row0 + rows - 1 of it out; cad_lpc_forward_backward runs the
+ * context's network over host rows X and returns its outputs (out, rows x
+ * 144, may be NULL) and, with T set, the gradient of the mean squared error
+ * (grads, cad_lpc_param_count floats) and the sum of squared errors (loss). */
+int cad_lpc_dataset_set(cad_ctx* ctx, const float* X, const float* T, int64_t rows);
+int cad_lpc_dataset_get(cad_ctx* ctx, int64_t row0, int64_t rows, float* X, float* T);
+int cad_lpc_forward_backward(cad_ctx* ctx, const float* X, const float* T, int64_t rows, float* out, float* grads,
+                             float* loss);
+int cad_lpc_train(cad_ctx* ctx, int64_t steps, int64_t batch, float lr, uint64_t seed, float* loss_hist);
+int cad_lpc_install_dev(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double G);
+int cad_lpc_install(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, double G);
 
 /* Batched SlipCalculator3D over independent cracks (no counterpart in the
  * reference, which solves one crack per call; src/SlipCalculator3D.jl:1-33 per
@@ -333,8 +400,9 @@ int cad_slip_calculator_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* off
  * M <= 16384 points (CAD_ERR_TOO_LARGE beyond).  Calls share that array, so
  * calls that overlap on the GPU race; order them on one stream.  The first
  * call on a device looks up the array's address with that device current:
- * make it before any stream capture.  The half-space check synchronises the
- * stream once, as in the other entry points. */
+ * make it before any stream capture.  With hs_flag = 1 every call
+ * synchronises `stream`: the half-space check reads its flag back to the
+ * host before the evaluation starts, as in the other entry points. */
 int cad_td_sum_eval_noalloc(void* stream, const double* X, const double* Y, const double* Z, int64_t M,
                             const double* P1, const double* P2, const double* P3, int64_t N, const double* Dss,
                             const double* Dds, const double* Dn, double nu, int disp_flag, int strain_flag,

@@ -16,7 +16,7 @@ Each file holds P1, P2, P3 (N x 3 float64), built as CreateP1P2P3 does
 (src/CreateP1P2P3.jl): vertex k of triangle i is the point whose index the
 triangle row names.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py <path of the CutAndDisplaceJulia checkout>
 """
 import os
 import sys
@@ -98,4 +98,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of the CutAndDisplaceJulia checkout>")
+    main(sys.argv[1])

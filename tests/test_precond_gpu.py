@@ -1,9 +1,12 @@
 """GPU tests of the learned preconditioner (an addition to the reference):
 the library's BF16 training kernels against the CPU reference of the same
 network (oracle/mlp_ref.py: float64 with BF16 rounding at the kernels'
-rounding points), and the trained preconditioner against block Jacobi and
-no preconditioning on held-out meshes (GMRES iterations to relative residual
-1e-10, solution against the FP64 LU)."""
+rounding points); the device features, neighbour lists and training targets
+against their CPU reference (oracle/lpc_ref.py); and the trained
+preconditioner against block Jacobi and no preconditioning on held-out meshes
+(GMRES iterations to relative residual 1e-10, solution against the FP64 LU).
+The product path (cutanddisplacejulia_b200.precond) passes host arrays to the
+C ABI only."""
 import numpy as np
 import pytest
 
@@ -46,9 +49,10 @@ def test_training_reduces_loss(cad):
 def test_learned_preconditioner_beats_block_jacobi(cad):
     from cutanddisplacejulia_b200 import precond, workloads
     meshes = precond.training_meshes(seed=0, count=16, n_range=(250, 600))
-    X, T = precond.training_set(meshes)
+    ts = precond.training_set(meshes)
+    assert ts.rows == sum(len(P[0]) for P, _ in meshes)
     net = precond.Network(seed=0)
-    net.train(X, T, steps=1500, batch=4096, lr=1e-3)
+    net.train(ts, steps=1500, batch=4096, lr=1e-3)
     _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
     for (P1, P2, P3), hs in ((workloads.ellipse_crack(seed=101, a=1.3, b=0.8, ntri=700), 0),
                              (workloads.dipping_rect(seed=102, ntri=700, dip=45.0, top_depth=1.0), 1)):
@@ -65,3 +69,69 @@ def test_learned_preconditioner_beats_block_jacobi(cad):
         assert np.linalg.norm(x - D) <= 1e-8 * np.linalg.norm(D)
         print("GMRES iterations: learned %d, block Jacobi %d, none %d" % (it_lp, it_bj, it_none))
         assert it_lp < it_bj <= it_none + 2, (it_lp, it_bj, it_none)
+
+
+def test_device_features_match_cpu_reference(cad):
+    from cutanddisplacejulia_b200 import _lib, workloads
+    from oracle import lpc_ref
+    L = _lib.load()
+    ctx = _lib.context(0)
+    for P, n in ((workloads.dipping_rect(seed=11, ntri=900, dip=50.0, top_depth=1.0), 900),
+                 (workloads.ellipse_crack(seed=12, a=1.2, b=0.7, ntri=400), 400),
+                 (workloads.ellipse_crack(seed=13, a=1.0, b=1.0, ntri=12), 12)):
+        P1, P2, P3 = P
+        N = len(P1)
+        X0, nbr0, h0 = lpc_ref.features(P1, P2, P3)
+        cols = [np.ascontiguousarray(np.asfortranarray(p).ravel(order="F")) for p in (P1, P2, P3)]
+        X = np.empty((N, lpc_ref.N_IN), dtype=np.float32)
+        nbr = np.empty((N, lpc_ref.K), dtype=np.int32)
+        h = np.empty(N)
+        _gpu_features(L, ctx, cols, N, X, nbr, h)
+        assert np.array_equal(nbr, nbr0)
+        assert np.allclose(h, h0, rtol=1e-14, atol=0)
+        assert np.max(np.abs(X - X0)) <= 1e-5 * max(1.0, np.max(np.abs(X0)))
+
+
+def _gpu_features(L, ctx, cols, N, X, nbr, h):
+    """cad_lpc_features_dev on device copies of the vertex lists (torch
+    tensors as test plumbing)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    dP = [torch.tensor(c, device=dev) for c in cols]
+    dX = torch.empty(X.shape, dtype=torch.float32, device=dev)
+    dn = torch.empty(nbr.shape, dtype=torch.int32, device=dev)
+    dh = torch.empty(N, dtype=torch.float64, device=dev)
+    _lib_check(L, ctx, L.cad_lpc_features_dev(ctx, *[p.data_ptr() for p in dP], N, dX.data_ptr(), dn.data_ptr(),
+                                              dh.data_ptr()))
+    torch.cuda.synchronize()
+    X[:] = dX.cpu().numpy()
+    nbr[:] = dn.cpu().numpy()
+    h[:] = dh.cpu().numpy()
+
+
+def _lib_check(L, ctx, rc):
+    from cutanddisplacejulia_b200 import _lib
+    _lib.check(rc, ctx)
+
+
+def test_training_targets_match_exact_inverse(cad):
+    from cutanddisplacejulia_b200 import _lib, precond, workloads
+    from oracle import lpc_ref
+    L = _lib.load()
+    ctx = _lib.context(0)
+    _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
+    (P1, P2, P3) = workloads.dipping_rect(seed=21, ntri=300, dip=70.0, top_depth=0.8)
+    n = len(P1)
+    nrm, mid = cad.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    A = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1,
+                             cad.Tractions(np.ones(n), np.zeros(n), np.zeros(n)), np.zeros(n))[3]
+    X0, nbr0, h0 = lpc_ref.features(P1, P2, P3)
+    T0 = lpc_ref.inverse_blocks(np.linalg.inv(A), nbr0, h0, G)
+    ts = precond.TrainingSet()
+    ts.add(P1, P2, P3, 1)
+    assert ts.rows == n
+    X = np.empty((n, lpc_ref.N_IN), dtype=np.float32)
+    T = np.empty((n, lpc_ref.N_OUT), dtype=np.float32)
+    _lib.check(L.cad_lpc_dataset_get(ctx, 0, n, X.ctypes.data, T.ctypes.data), ctx)
+    assert np.max(np.abs(X - X0)) <= 1e-5 * np.max(np.abs(X0))
+    assert np.max(np.abs(T - T0)) <= 1e-5 * np.max(np.abs(T0))

@@ -109,3 +109,27 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                    tri.data_ptr(), tri.data_ptr(), 1025, tri.data_ptr(), tri.data_ptr(), tri.data_ptr(),
                                    0.25, 1, 1, 0, out.data_ptr(), out.data_ptr())
     assert rc == _lib.CAD_ERR_TOO_LARGE
+
+
+def test_noalloc_checks_half_space_triangles_without_points():
+    # no observation points but a triangle above z = 0: both entry points
+    # reject it in half space (src/TD.jl:606-619), and accept it in full space
+    torch = pytest.importorskip("torch")
+    from cutanddisplacejulia_b200 import _lib, build
+    build.build()
+    L = _lib.load()
+    ctx = _lib.context(0)
+    dev = torch.device("cuda", 0)
+    col = (lambda p: torch.tensor(np.asfortranarray(np.array([p], dtype=np.float64)).ravel(order="F"), device=dev))
+    P1, P2, P3 = col([0.0, 0.0, 0.5]), col([1.0, 0.0, -1.0]), col([0.0, 1.0, -1.0])
+    sl = torch.full((1,), 1e-3, dtype=torch.float64, device=dev)
+    pt = torch.zeros(1, dtype=torch.float64, device=dev)
+    out = torch.zeros(9, dtype=torch.float64, device=dev)
+    for hs, want in ((1, _lib.CAD_ERR_HS_ABOVE_SURFACE), (0, 0)):
+        rc = L.cad_td_sum_eval_noalloc(None, pt.data_ptr(), pt.data_ptr(), pt.data_ptr(), 0, P1.data_ptr(),
+                                       P2.data_ptr(), P3.data_ptr(), 1, sl.data_ptr(), sl.data_ptr(), sl.data_ptr(),
+                                       0.25, 1, 1, hs, out.data_ptr(), out.data_ptr())
+        rc_dev = L.cad_td_sum_eval_dev(ctx, pt.data_ptr(), pt.data_ptr(), pt.data_ptr(), 0, P1.data_ptr(),
+                                       P2.data_ptr(), P3.data_ptr(), 1, sl.data_ptr(), sl.data_ptr(), sl.data_ptr(),
+                                       0.25, 1, 1, hs, out.data_ptr(), out.data_ptr())
+        assert rc == want and rc_dev == want, (hs, rc, rc_dev)
