@@ -43,7 +43,7 @@ EXPORTS = [
     "cad_assemble_columns_dev", "cad_gemm_sub_dev", "cad_lpc_features_dev", "cad_lpc_set_network",
     "cad_lpc_get_network", "cad_lpc_dataset_add", "cad_lpc_dataset_rows", "cad_lpc_dataset_clear",
     "cad_lpc_dataset_get", "cad_lpc_dataset_set", "cad_lpc_forward_backward", "cad_lpc_train", "cad_lpc_install_dev",
-    "cad_lpc_install", "cad_set_wait_limit", "cad_wait_timeout_probe",
+    "cad_lpc_install", "cad_set_wait_limit", "cad_wait_timeout_probe", "cad_set_gmres_matvec",
 ]
 
 
@@ -128,6 +128,7 @@ def load():
     L.cad_lpc_install_dev.argtypes = [P, P, P, P, I64, D]
     L.cad_lpc_install.argtypes = [P, P, P, P, I64, D]
     L.cad_set_wait_limit.argtypes = [P, I64]
+    L.cad_set_gmres_matvec.argtypes = [P, INT]
     L.cad_wait_timeout_probe.argtypes = [P, I64]
     L.cad_friction_prepare.argtypes = [P, P, P, P, I64, D, D, D, P, P, INT]
     L.cad_friction_solve.argtypes = [P, I64, P, P, P, P, P, D, INT, P, P, P]

@@ -19,6 +19,7 @@
 
 #include "../../include/cad_td.h"
 #include "gemm.h"
+#include "krylov.h"
 #include "lcp.h"
 #include "lpc.h"
 #include "lu.h"
@@ -39,7 +40,7 @@ enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
-    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_COUNT
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -52,7 +53,7 @@ struct DevBuf {
 // One lane of the batched solve: its own streams, cuBLAS handles and
 // workspaces, so cracks on different lanes run concurrently.
 enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS, L_BLASWS,
-                L_COUNT };
+                L_KWORK, L_COUNT };
 struct Lane {
     cudaStream_t main = nullptr, side = nullptr;
     cublasHandle_t main_blas = nullptr, side_blas = nullptr;
@@ -99,6 +100,7 @@ struct cad_ctx {
     int spai_k = 0;
     double near_factor = 3.0;
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
+    int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
     double tol = 1e-10;
     int max_iter = 200;
     bool fric_ready = false;      // cad_friction_prepare: C = inv(A Scl) of fric_N elements in S_LCPC
@@ -339,6 +341,11 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     g.sync = (int*)sync;
     g.launches = &ctx->launches;
     g.wait_limit = ctx->wait_limit;
+    {
+        void* kw;
+        if (int r = ensure(ctx, S_KWORK, krylov_work_doubles(n) * sizeof(double), &kw)) return r;
+        g.kwork = (double*)kw;
+    }
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
     bool converged = true;
@@ -421,9 +428,24 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     g.sync = (int*)sync;
     g.launches = &ctx->launches;
     g.wait_limit = ctx->wait_limit;
+    {
+        void* kw;
+        if (int r = ensure(ctx, S_KWORK, krylov_work_doubles(n) * sizeof(double), &kw)) return r;
+        g.kwork = (double*)kw;
+    }
     g.spai_nbr = ctx->spai_nbr;
     g.spai_blocks = ctx->spai_blocks;
     g.spai_k = ctx->spai_k;
+    if (ctx->gmres_matvec32) {
+        // FP32 copy of A for the Arnoldi products (half the bytes per
+        // iteration); every restart's residual b - A x stays FP64
+        const int64_t ld32 = (n + 31) / 32 * 32;
+        void* a32;
+        if (int r = ensure(ctx, S_A32MV, (size_t)ld32 * n * sizeof(float), &a32)) return r;
+        CK(krylov_cast_f32(ctx->stream, A, lda, n, (float*)a32, ld32, &ctx->launches));
+        g.A32mv = (const float*)a32;
+        g.ld32 = ld32;
+    }
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
     bool converged = true;
@@ -667,7 +689,8 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         float* r32 = (float*)l.buf[L_IR32].p;
         IrArgs ia{ls, n3, A, n3, b.T + 3 * o, n3, 1, b.D + 3 * o, (float*)l.buf[L_A32].p, (int*)l.buf[L_PIV].p,
                   (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, ctx->tol, kBatchSweeps,
-                  (double*)l.buf[L_IR].p, r32, r32 + n3, (double*)l.buf[L_NORMS].p};
+                  (double*)l.buf[L_IR].p, r32, r32 + n3, (double*)l.buf[L_NORMS].p,
+                  (double*)l.buf[L_KWORK].p};
         if (ir_solve_fixed(ia, kBatchSweeps, b.rel + c) != GMRES_OK)
             return fail(ctx, CAD_ERR_CUDA, "batched solve: refinement launch failed");
     }
@@ -756,6 +779,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         if (int r = lane_ensure(ctx, l, L_IR, n3 * sizeof(double), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_IR32, 2 * n3 * sizeof(float), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_NORMS, 2 * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_KWORK, krylov_work_doubles(n3) * sizeof(double), &p)) return r;
     }
     BatchArgs b{nbatch, offsets, P1, P2, P3, normals, midpoints, T, D, nu, G, lambda, hs, (double*)Aall, &aoff,
                 &lane_of, &order, (double*)rel};
@@ -928,6 +952,14 @@ int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
     ctx->solver = mode;
     ctx->tol = tol;
     ctx->max_iter = max_iter;
+    return CAD_OK;
+}
+
+int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (fp32 != 0 && fp32 != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->gmres_matvec32 = fp32;
     return CAD_OK;
 }
 

@@ -12,7 +12,6 @@
 // its off-diagonal blocks against the solved pieces as they are published
 // (flag per block, release/acquire), and finishes with a GEMV against the
 // explicitly inverted diagonal block.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -23,6 +22,8 @@
 
 #include "lu.h"
 #include "mixed.h"
+#include "gemm.h"
+#include "krylov.h"
 #include "mlp.h"
 
 namespace cad {
@@ -274,43 +275,45 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
 {
     const int64_t n = a.n;
     const int m = a.restart;
-    cublasHandle_t h = a.blas;
     cudaStream_t st = a.stream;
     res->iterations = 0;
     res->rel_residual = 0.0;
     res->status = GMRES_OK;
-    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
-    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
+    if (m < 1 || m + 1 > kMaxBasis || n > INT32_MAX || !a.kwork) return GMRES_CUDA_ERROR;
+    const int nn = (int)n;
     const int nblk = (int)((n + kRB - 1) / kRB);
     Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.y32, a.x32, a.sync, st, a.launches, a.spai_nbr, a.spai_blocks,
               a.spai_k, a.wait_limit > 0 ? a.wait_limit : kDefaultWaitLimit};
+    const KrylovWork kw = krylov_carve(a.kwork, n);
     double* V = a.V;        // n x (m + 1)
     double* w = a.w;
     double* z = a.z;
     double* r = a.r;
-    double* hd = a.hd;      // 2 (m + 1) device scratch
+    double* hd = a.hd;      // 2 (m + 1) device scratch: the Hessenberg column, then y
     double* x = a.x;
-    const double one = 1.0, zero = 0.0, mone = -1.0;
-    bool ok = true;
-    auto B = [&](cublasStatus_t s) { ok = ok && s == CUBLAS_STATUS_SUCCESS; };
+    int64_t* L = a.launches;
+#define GM_CK(e)                                  \
+    do {                                          \
+        if ((e) != cudaSuccess) return GMRES_CUDA_ERROR; \
+    } while (0)
 
-    if (cudaMemsetAsync(a.sync + 2 * nblk + 2, 0, sizeof(int), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+    GM_CK(cudaMemsetAsync(a.sync + 2 * nblk + 2, 0, sizeof(int), st));
     double bnorm = 0.0;
-    B(cublasDnrm2(h, (int)n, a.b, 1, &bnorm));
-    if (!ok) return GMRES_BLAS_ERROR;
-    if (cudaMemsetAsync(x, 0, n * sizeof(double), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+    GM_CK(krylov_norm(st, a.b, nn, kw.scalar, kw, L));
+    GM_CK(cudaMemcpyAsync(&bnorm, kw.scalar, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GM_CK(cudaMemsetAsync(x, 0, n * sizeof(double), st));
+    GM_CK(cudaStreamSynchronize(st));
     if (bnorm == 0.0) return GMRES_OK;
 
-    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hcol(2 * (m + 1)), y(m);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hcol(m + 2), y(m);
     int total = 0;
     while (true) {
-        // true residual r = b - A x
-        if (cudaMemcpyAsync(r, a.b, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
-        B(cublasDgemv(h, CUBLAS_OP_N, (int)n, (int)n, &mone, a.A, (int)a.lda, x, 1, &one, r, 1));
+        // true residual r = b - A x, in FP64
+        GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, x, -1.0, a.b, r, kw, nullptr, 0, 0, L));
+        GM_CK(krylov_norm(st, r, nn, kw.scalar + 1, kw, L));
         double beta = 0.0;
-        B(cublasDnrm2(h, (int)n, r, 1, &beta));
-        if (!ok) return GMRES_BLAS_ERROR;
+        GM_CK(cudaMemcpyAsync(&beta, kw.scalar + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        GM_CK(cudaStreamSynchronize(st));
         res->rel_residual = beta / bnorm;
         res->iterations = total;
         if (res->rel_residual <= a.tol) return GMRES_OK;
@@ -318,39 +321,26 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
             res->status = GMRES_NOT_CONVERGED;
             return GMRES_NOT_CONVERGED;
         }
-        const double ib = 1.0 / beta;
-        if (cudaMemcpyAsync(V, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
-        B(cublasDscal(h, (int)n, &ib, V, 1));
+        GM_CK(krylov_scale(st, r, nn, kw.scalar + 1, V, L));
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int kend = 0;
         for (int k = 0; k < m; ++k) {
             double* vk = V + (int64_t)k * n;
             if (!M.apply(vk, z)) return GMRES_CUDA_ERROR;
-            B(cublasDgemv(h, CUBLAS_OP_N, (int)n, (int)n, &one, a.A, (int)a.lda, z, 1, &zero, w, 1));
-            // classical Gram-Schmidt, twice
-            for (int pass = 0; pass < 2; ++pass) {
-                B(cublasDgemv(h, CUBLAS_OP_T, (int)n, k + 1, &one, V, (int)n, w, 1, &zero, hd + pass * (m + 1), 1));
-                B(cublasDgemv(h, CUBLAS_OP_N, (int)n, k + 1, &mone, V, (int)n, hd + pass * (m + 1), 1, &one, w, 1));
-            }
-            double hn = 0.0;
-            B(cublasDnrm2(h, (int)n, w, 1, &hn));
-            if (!ok) return GMRES_BLAS_ERROR;
-            if (cudaMemcpyAsync(hcol.data(), hd, 2 * (m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st) !=
-                    cudaSuccess ||
-                cudaStreamSynchronize(st) != cudaSuccess)
-                return GMRES_CUDA_ERROR;
+            // w = A z (the FP32 copy of A when one is given: the Arnoldi
+            // matrix only needs to be accurate to the restart's reduction),
+            // with the first Gram-Schmidt pass's dot products
+            if (a.A32mv)
+                GM_CK(krylov_gemv<float>(st, a.A32mv, a.ld32, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L));
+            else
+                GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L));
+            GM_CK(krylov_orthogonalise(st, V, n, nn, k + 1, w, hd, V + (int64_t)(k + 1) * n, kw, L));
+            GM_CK(cudaMemcpyAsync(hcol.data(), hd, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            GM_CK(cudaStreamSynchronize(st));
             double* Hk = H.data() + (size_t)k * (m + 1);
-            for (int q = 0; q <= k; ++q) Hk[q] = hcol[q] + hcol[(m + 1) + q];
-            Hk[k + 1] = hn;
-            if (hn > 0.0 && k + 1 < m + 1) {
-                const double ih = 1.0 / hn;
-                double* vn = V + (int64_t)(k + 1) * n;
-                if (cudaMemcpyAsync(vn, w, n * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-                    return GMRES_CUDA_ERROR;
-                B(cublasDscal(h, (int)n, &ih, vn, 1));
-            }
+            for (int q = 0; q <= k + 1; ++q) Hk[q] = hcol[q];
+            const double hn = hcol[k + 1];
             // previous rotations, then a new one zeroing H[k+1][k]
             for (int q = 0; q < k; ++q) {
                 const double t0 = cs[q] * Hk[q] + sn[q] * Hk[q + 1];
@@ -376,18 +366,16 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
             for (int c = q + 1; c < kend; ++c) s -= H[(size_t)c * (m + 1) + q] * y[c];
             y[q] = s / H[(size_t)q * (m + 1) + q];
         }
-        if (cudaMemcpyAsync(hd, y.data(), kend * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
-        B(cublasDgemv(h, CUBLAS_OP_N, (int)n, kend, &one, V, (int)n, hd, 1, &zero, w, 1));
+        GM_CK(cudaMemcpyAsync(hd, y.data(), kend * sizeof(double), cudaMemcpyHostToDevice, st));
+        GM_CK(krylov_combine(st, V, n, nn, kend, hd, w, L));
         if (!M.apply(w, z)) return GMRES_CUDA_ERROR;
-        B(cublasDaxpy(h, (int)n, &one, z, 1, x, 1));
-        if (!ok) return GMRES_BLAS_ERROR;
+        GM_CK(krylov_axpy(st, 1.0, z, nn, x, L));
         int fail = 0;
-        if (cudaMemcpyAsync(&fail, a.sync + 2 * nblk + 2, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
+        GM_CK(cudaMemcpyAsync(&fail, a.sync + 2 * nblk + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GM_CK(cudaStreamSynchronize(st));
         if (fail) return GMRES_TIMEOUT;
     }
+#undef GM_CK
 }
 
 
@@ -433,19 +421,35 @@ __global__ void __launch_bounds__(256) col_norms_kernel(const double* __restrict
 
 }  // namespace
 
+namespace {
+
+// R = B - A X (n x nrhs): one column as a matrix-vector product, several as
+// the library's FP64 tensor-core GEMM
+cudaError_t ir_residual(const IrArgs& a, cudaStream_t st)
+{
+    const int64_t n = a.n;
+    if (a.nrhs == 1 && a.kwork)
+        return krylov_gemv<double>(st, a.A, a.lda, (int)n, a.X, -1.0, a.B, a.R, krylov_carve(a.kwork, n), nullptr,
+                                   0, 0, a.ls.launches);
+    cudaError_t e = cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double),
+                                      a.nrhs, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    if (a.ls.launches) ++*a.ls.launches;
+    return gemm_sub(st, (int)n, a.nrhs, (int)n, a.A, a.lda, a.X, n, a.R, n, nullptr);
+}
+
+}  // namespace
+
 int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converged)
 {
     const int64_t n = a.n;
     const int nrhs = a.nrhs;
     cudaStream_t st = a.ls.main;
-    cublasHandle_t h = a.ls.main_blas;
     res->status = GMRES_OK;
     res->iterations = 0;
     res->max_rel_residual = 0.0;
     converged.assign(nrhs, 0);
     if (n == 0 || nrhs == 0) return GMRES_OK;
-    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
-    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
     int64_t* launches = a.ls.launches;
     const dim3 g((unsigned)((n + 255) / 256), (unsigned)nrhs);
     std::vector<double> hn(2 * (size_t)nrhs);
@@ -456,7 +460,6 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
         return GMRES_CUDA_ERROR;
     if (launches) ++*launches;
     double prev = INFINITY;
-    const double one = 1.0, mone = -1.0;
     for (int it = 1; it <= a.max_iter; ++it) {
         d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
         if (launches) ++*launches;
@@ -466,12 +469,7 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
         if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
         add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
         if (launches) ++*launches;
-        if (cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
-                              cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
-        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nrhs, (int)n, &mone, a.A, (int)a.lda, a.X, (int)n, &one,
-                        a.R, (int)n) != CUBLAS_STATUS_SUCCESS)
-            return GMRES_BLAS_ERROR;
+        if (ir_residual(a, st) != cudaSuccess) return GMRES_CUDA_ERROR;
         col_norms_kernel<<<nrhs, 256, 0, st>>>(a.R, n, n, a.norms + nrhs);
         if (launches) ++*launches;
         if (cudaMemcpyAsync(hn.data(), a.norms, 2 * (size_t)nrhs * sizeof(double), cudaMemcpyDeviceToHost, st) !=
@@ -513,10 +511,7 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
     const int64_t n = a.n;
     const int nrhs = a.nrhs;
     cudaStream_t st = a.ls.main;
-    cublasHandle_t h = a.ls.main_blas;
     if (n == 0 || nrhs == 0) return GMRES_OK;
-    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return GMRES_BLAS_ERROR;
-    cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
     int64_t* launches = a.ls.launches;
     const dim3 g((unsigned)((n + 255) / 256), (unsigned)nrhs);
     col_norms_kernel<<<nrhs, 256, 0, st>>>(a.B, a.ldb, n, a.norms);
@@ -525,7 +520,6 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
         cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
                           cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return GMRES_CUDA_ERROR;
-    const double one = 1.0, mone = -1.0;
     for (int it = 0; it < iters; ++it) {
         d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
         if (launches) ++*launches;
@@ -535,12 +529,7 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
         if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
         add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
         if (launches) ++*launches;
-        if (cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
-                              cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            return GMRES_CUDA_ERROR;
-        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nrhs, (int)n, &mone, a.A, (int)a.lda, a.X, (int)n, &one,
-                        a.R, (int)n) != CUBLAS_STATUS_SUCCESS)
-            return GMRES_BLAS_ERROR;
+        if (ir_residual(a, st) != cudaSuccess) return GMRES_CUDA_ERROR;
     }
     col_norms_kernel<<<nrhs, 256, 0, st>>>(a.R, n, n, a.norms + nrhs);
     relres_kernel<<<1, 1, 0, st>>>(a.norms, nrhs, rel_out);

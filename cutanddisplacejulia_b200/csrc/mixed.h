@@ -24,10 +24,10 @@ size_t mixed_sync_ints(int64_t n);   // flags, tickets and the failure word of o
 enum { GMRES_OK = 0, GMRES_NOT_CONVERGED = 1, GMRES_CUDA_ERROR = 2, GMRES_BLAS_ERROR = 3, GMRES_TIMEOUT = 4 };
 
 struct GmresArgs {
-    cublasHandle_t blas;
+    cublasHandle_t blas;   // unused by gmres_ir_solve (own kernels)
     cudaStream_t stream;
     int64_t n;
-    const double* A;   // FP64 system matrix (n x n, lda)
+    const double* A;   // FP64 system matrix (n x n, lda): the true residual of every restart
     int64_t lda;
     const double* b;   // right-hand side (n)
     double* x;         // solution (n)
@@ -53,6 +53,9 @@ struct GmresArgs {
     const float* spai_blocks = nullptr;
     int spai_k = 0;
     long wait_limit = 0;   // polls of a triangular-solve flag wait (0: kDefaultWaitLimit)
+    double* kwork = nullptr;       // krylov_work_doubles(n) doubles of device scratch
+    const float* A32mv = nullptr;  // if set, an FP32 copy of A (ld32) for the Arnoldi products
+    int64_t ld32 = 0;
 };
 
 struct GmresResult {
@@ -90,6 +93,7 @@ struct IrArgs {
     float* R32;         // n x nrhs
     float* X32;         // n x nrhs
     double* norms;      // 2 nrhs
+    double* kwork = nullptr;   // krylov_work_doubles(n): one-column residuals as a GEMV (else a GEMM)
 };
 
 struct IrResult {

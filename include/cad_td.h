@@ -113,6 +113,12 @@ int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor);
 /* GMRES iterations (summed over right-hand sides) and the largest final
  * relative residual of the last mixed solve. */
 int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual);
+/* Arnoldi products of the preconditioned-GMRES solvers (CAD_SOLVER_GMRES_*):
+ * fp32 = 1 (default) multiplies with an FP32 copy of A (half the bytes per
+ * iteration; the solve keeps an extra n x n FP32 array), every restart still
+ * forming the residual b - A x in FP64, so the tolerance is met in FP64;
+ * fp32 = 0 multiplies with the FP64 A.  No counterpart in the reference. */
+int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
 /* Device waits (a leaf's pivot exchange, a triangular-solve chain flag) poll
  * at most `polls` times (default 4194304, a few seconds at worst) before the
  * kernel records the failure and returns; the call then reports
