@@ -699,6 +699,17 @@ def run_learned(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+TUNE_CACHE = os.path.join(ROOT, "cutanddisplacejulia_b200", "autotune_b200.txt")
+
+
+def _autotune_summary(L, ctx, args):
+    if args.no_autotune:
+        return None
+    tuned = ctypes.c_int64(0)
+    entries = L.cad_autotune_entries(ctx, ctypes.byref(tuned))
+    return {"cache": os.path.relpath(TUNE_CACHE, ROOT), "entries": int(entries), "timed_in_this_run": tuned.value}
+
+
 def train_network(args, device):
     """The learned preconditioner's network, trained on this GPU by the
     library's kernels on exact inverse blocks of seeded meshes (outside every
@@ -749,6 +760,10 @@ def run_c3(args, rank, world, local_rank):
     _lib.check(L.cad_fp64_fma_probe(ctx, 20000, ctypes.byref(peak)), ctx)
     fp64_peak = peak.value
     pairs = float(n) * n
+    # launch shapes from the autotune cache (keys missing from it are timed
+    # during the warm-up steps and added)
+    if not args.no_autotune:
+        _lib.check(L.cad_set_autotune(ctx, 1, TUNE_CACHE.encode()), ctx)
 
     def assemble():
         _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
@@ -917,6 +932,7 @@ def run_c3(args, rank, world, local_rank):
         "mixed": mixed,
         "batch_rhs": batch,
         "training": training,
+        "autotune": _autotune_summary(L, ctx, args),
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -1223,6 +1239,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the same system")
+    ap.add_argument("--no-autotune", action="store_true", help="fixed launch shapes instead of the autotune cache")
     ap.add_argument("--batch-rhs", type=int, default=0,
                     help="also time K seeded remote-stress right-hand sides on the same system (FP64 LU and mixed)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dipping",

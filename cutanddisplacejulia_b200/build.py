@@ -10,8 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcad_td.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu", "noalloc.cu", "lu.cu", "mixed.cu", "mlp.cu", "trsv.cu", "lcp.cu", "gemm.cu", "lpc.cu", "krylov.cu"]
-HEADERS = ["td_device.cuh", "tde_closed_form.cuh", "td_kernels.h", "lu.h", "mixed.h", "mlp.h", "lcp.h", "gemm.h", "sm100.cuh", "lpc.h", "krylov.h",
+SOURCES = ["capi.cu", "td_kernels.cu", "probe.cu", "noalloc.cu", "lu.cu", "mixed.cu", "mlp.cu", "trsv.cu", "lcp.cu", "gemm.cu", "lpc.cu", "krylov.cu", "tune.cu"]
+HEADERS = ["td_device.cuh", "tde_closed_form.cuh", "td_kernels.h", "lu.h", "mixed.h", "mlp.h", "lcp.h", "gemm.h", "sm100.cuh", "lpc.h", "krylov.h", "tune.h",
            os.path.join("..", "..", "include", "cad_td.h")]
 
 NVCC_FLAGS = [

@@ -22,6 +22,7 @@
 #include "krylov.h"
 #include "lcp.h"
 #include "lpc.h"
+#include "tune.h"
 #include "lu.h"
 #include "mixed.h"
 #include "mlp.h"
@@ -40,7 +41,7 @@ enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
-    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_COUNT
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -101,6 +102,7 @@ struct cad_ctx {
     double near_factor = 3.0;
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
+    Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
     int max_iter = 200;
     bool fric_ready = false;      // cad_friction_prepare: C = inv(A Scl) of fric_N elements in S_LCPC
@@ -276,6 +278,18 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         ctx->timed[0] = true;
         return CAD_OK;
     }
+    if (out_kind == OUT_AMAT && ctx->tuner.mode != TUNE_OFF) {
+        // triangles per block of the pair kernel (each block stages one
+        // triangle record at a time into shared memory)
+        char key[96];
+        std::snprintf(key, sizeof key, "pair_amat_f64_hs%d_N%lld", hs, (long long)tune_class(N));
+        PairArgs t = a;
+        a.tri_chunk = tune_choice(ctx->tuner, key, ctx->stream, {2, 4, 8, 16, 32}, (int)a.tri_chunk, [&](int c) {
+            t.tri_chunk = c;
+            ++ctx->launches;
+            return launch_td_pairs(t, out_kind, hs == 1, true, false, ctx->stream);
+        });
+    }
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     ++ctx->launches;
     CK(launch_td_pairs(a, out_kind, hs == 1, true, false, ctx->stream));
@@ -446,6 +460,18 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
         g.A32mv = (const float*)a32;
         g.ld32 = ld32;
     }
+    if (ctx->tuner.mode != TUNE_OFF && n > 0 && n <= INT32_MAX) {
+        // column chunks of the Arnoldi product (y = A b into the work vector)
+        char key[64];
+        std::snprintf(key, sizeof key, "gemv_%s_n%lld", g.A32mv ? "f32" : "f64", (long long)tune_class(n));
+        const KrylovWork kw = krylov_carve(g.kwork, n);
+        g.gemv_chunks = tune_choice(ctx->tuner, key, ctx->stream, {4, 8, 16}, kGemvChunks, [&](int c) {
+            return g.A32mv ? krylov_gemv<float>(ctx->stream, g.A32mv, g.ld32, (int)n, B, 1.0, nullptr, g.w, kw,
+                                                nullptr, 0, 0, &ctx->launches, c)
+                           : krylov_gemv<double>(ctx->stream, A, lda, (int)n, B, 1.0, nullptr, g.w, kw, nullptr, 0,
+                                                 0, &ctx->launches, c);
+        });
+    }
     ctx->last_iters = 0;
     ctx->last_relres = 0.0;
     bool converged = true;
@@ -519,8 +545,31 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     ctx->timed[1] = ctx->timed[2] = false;
-    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
-                        ctx->graphs, ctx->wait_limit};
+    LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
+                 ctx->graphs, ctx->wait_limit};
+    if (ctx->tuner.mode != TUNE_OFF) {
+        // leaf width of the panel factorisation (rows per leaf thread), timed
+        // on a scratch copy of A for systems up to 12288 unknowns
+        char key[64];
+        std::snprintf(key, sizeof key, "lu_leaf_f64_n%lld", (long long)tune_class(n));
+        if (ctx->tuner.find(key) >= 0 || (ctx->tuner.mode == TUNE_ON && n <= 12288)) {
+            void* scratch = nullptr;
+            if (ctx->tuner.find(key) < 0)
+                if (int r = ensure(ctx, S_TUNE, (size_t)n * n * sizeof(double), &scratch)) return r;
+            LuStreams lt = ls;
+            lt.graphs = nullptr;
+            ls.min_leaf_rpt = tune_choice(ctx->tuner, key, ctx->stream, {1, 2, 4}, 1, [&](int c) {
+                cudaError_t e = cudaMemcpy2DAsync(scratch, n * sizeof(double), A, lda * sizeof(double),
+                                                  n * sizeof(double), n, cudaMemcpyDeviceToDevice, ctx->stream);
+                if (e != cudaSuccess) return e;
+                lt.min_leaf_rpt = c;
+                return lu_factor_solve<double>(lt, (double*)scratch, n, n, nullptr, 0, 0, nullptr, 0, (int*)piv,
+                                               (int*)perm, (int*)info, kLuBlock, true, false) == LU_OK
+                           ? cudaSuccess
+                           : cudaErrorUnknown;
+            });
+        }
+    }
     if (nrhs == 1) {   // one right-hand side: factorise, then the two chain launches
         void* chain;
         if (int r = ensure(ctx, S_CHAIN, (size_t)n * sizeof(double) + lu_chain_sync_ints(n) * sizeof(int), &chain))
@@ -953,6 +1002,22 @@ int cad_set_solver(cad_ctx* ctx, int mode, double tol, int max_iter)
     ctx->tol = tol;
     ctx->max_iter = max_iter;
     return CAD_OK;
+}
+
+int cad_set_autotune(cad_ctx* ctx, int mode, const char* cache_path)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (mode < TUNE_OFF || mode > TUNE_CACHED) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->tuner.mode = mode;
+    ctx->tuner.load(cache_path ? std::string(cache_path) : std::string());
+    return CAD_OK;
+}
+
+int64_t cad_autotune_entries(const cad_ctx* ctx, int64_t* tuned_here)
+{
+    if (!ctx) return 0;
+    if (tuned_here) *tuned_here = ctx->tuner.tuned;
+    return (int64_t)ctx->tuner.table.size();
 }
 
 int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)

@@ -214,9 +214,9 @@ int krylov_blocks(int64_t n) { return (int)((n + kRows - 1) / kRows); }
 
 size_t krylov_work_doubles(int64_t n)
 {
-    // gemv partials (kGemvChunks x n), two dot buffers, norms, two h vectors
+    // gemv partials (kMaxGemvChunks x n), two dot buffers, norms, two h vectors
     const size_t nblk = (size_t)krylov_blocks(n);
-    return (size_t)kGemvChunks * (size_t)n + 2 * nblk * kMaxBasis + nblk + 2 * kMaxBasis + 64;
+    return (size_t)kMaxGemvChunks * (size_t)n + 2 * nblk * kMaxBasis + nblk + 2 * kMaxBasis + 64;
 }
 
 KrylovWork krylov_carve(double* base, int64_t n)
@@ -224,7 +224,7 @@ KrylovWork krylov_carve(double* base, int64_t n)
     const size_t nblk = (size_t)krylov_blocks(n);
     KrylovWork k;
     k.part = base;
-    k.dots1 = k.part + (size_t)kGemvChunks * (size_t)n;
+    k.dots1 = k.part + (size_t)kMaxGemvChunks * (size_t)n;
     k.dots2 = k.dots1 + nblk * kMaxBasis;
     k.norms = k.dots2 + nblk * kMaxBasis;
     k.h1 = k.norms + nblk;
@@ -236,10 +236,11 @@ KrylovWork krylov_carve(double* base, int64_t n)
 template <typename TA>
 cudaError_t krylov_gemv(cudaStream_t st, const TA* A, int64_t lda, int n, const double* x, double alpha,
                         const double* b, double* y, const KrylovWork& k, const double* V, int64_t ldv, int nv,
-                        int64_t* launches)
+                        int64_t* launches, int nchunks)
 {
     if (n <= 0) return cudaSuccess;
-    const int chunk = (n + kGemvChunks - 1) / kGemvChunks;
+    if (nchunks < 1 || nchunks > kMaxGemvChunks) nchunks = kGemvChunks;
+    const int chunk = (n + nchunks - 1) / nchunks;
     const int nchunk = (n + chunk - 1) / chunk;
     gemv_part_kernel<TA><<<dim3(nb(n), (unsigned)nchunk), kRows, 0, st>>>(A, lda, n, x, chunk, k.part);
     gemv_reduce_kernel<<<nb(n), kRows, 0, st>>>(k.part, nchunk, n, alpha, b, y, V, ldv, V ? nv : 0, k.dots1);
@@ -248,9 +249,9 @@ cudaError_t krylov_gemv(cudaStream_t st, const TA* A, int64_t lda, int n, const 
 }
 template cudaError_t krylov_gemv<double>(cudaStream_t, const double*, int64_t, int, const double*, double,
                                          const double*, double*, const KrylovWork&, const double*, int64_t, int,
-                                         int64_t*);
+                                         int64_t*, int);
 template cudaError_t krylov_gemv<float>(cudaStream_t, const float*, int64_t, int, const double*, double, const double*,
-                                        double*, const KrylovWork&, const double*, int64_t, int, int64_t*);
+                                        double*, const KrylovWork&, const double*, int64_t, int, int64_t*, int);
 
 cudaError_t krylov_orthogonalise(cudaStream_t st, const double* V, int64_t ldv, int n, int nv, double* w,
                                  double* hcol, double* vnext, const KrylovWork& k, int64_t* launches)

@@ -8,11 +8,12 @@
 namespace cad {
 
 constexpr int kMaxBasis = 64;     // Krylov basis vectors one orthogonalisation handles
-constexpr int kGemvChunks = 8;    // column chunks of the matrix-vector product
+constexpr int kGemvChunks = 8;     // default column chunks of the matrix-vector product
+constexpr int kMaxGemvChunks = 16;
 
 // Device scratch of the kernels below (krylov_work_doubles(n) doubles).
 struct KrylovWork {
-    double* part;    // kGemvChunks x n partial products
+    double* part;    // kMaxGemvChunks x n partial products
     double* dots1;   // blocks x kMaxBasis
     double* dots2;
     double* norms;   // blocks
@@ -31,7 +32,7 @@ int krylov_blocks(int64_t n);
 template <typename TA>
 cudaError_t krylov_gemv(cudaStream_t st, const TA* A, int64_t lda, int n, const double* x, double alpha,
                         const double* b, double* y, const KrylovWork& k, const double* V, int64_t ldv, int nv,
-                        int64_t* launches);
+                        int64_t* launches, int nchunks = kGemvChunks);
 // w := w - V h twice (classical Gram-Schmidt with re-orthogonalisation, the
 // first pass's dots from krylov_gemv); hcol[0..nv) = h, hcol[nv] = ||w||;
 // vnext = w / ||w||.  All on the device.

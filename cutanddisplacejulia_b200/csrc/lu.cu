@@ -496,6 +496,7 @@ struct Lu {
     int* info;
     int cluster;  // largest leaf cluster (16 where the device co-schedules it, else 8)
     long wait_limit = kDefaultWaitLimit;   // try_wait rounds before a leaf gives up on a push
+    int min_rpt = 1;        // fewest rows per leaf thread (wider leaves with fewer rows each)
     int64_t launches = 0;   // own kernels launched
     cudaError_t err = cudaSuccess;
 
@@ -512,7 +513,7 @@ struct Lu {
     // rows per leaf thread for an m-row panel: the fewest that fit one cluster
     int leaf_rpt(int m) const
     {
-        int rpt = 1;
+        int rpt = min_rpt;
         while (rpt < 8 && (int64_t)cluster * kLeafThreads * rpt < m) rpt *= 2;
         return rpt;
     }
@@ -746,12 +747,13 @@ struct LuGraphKey {
     bool factor, solve;
     cudaStream_t main, side;
     long wait_limit;
+    int min_rpt;
     bool same(const LuGraphKey& o) const
     {
         return type == o.type && A == o.A && B == o.B && X == o.X && n == o.n && lda == o.lda && ldb == o.ldb &&
                ldx == o.ldx && nrhs == o.nrhs && nb == o.nb && ipiv == o.ipiv && perm == o.perm && info == o.info &&
                factor == o.factor && solve == o.solve && main == o.main && side == o.side &&
-               wait_limit == o.wait_limit;
+               wait_limit == o.wait_limit && min_rpt == o.min_rpt;
     }
 };
 
@@ -871,6 +873,7 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     lu.ipiv = ipiv;
     lu.info = info;
     lu.wait_limit = s.wait_limit > 0 ? s.wait_limit : kDefaultWaitLimit;
+    lu.min_rpt = (s.min_leaf_rpt == 2 || s.min_leaf_rpt == 4) ? s.min_leaf_rpt : 1;
     configure(lu);
     // nb bounds the pivots one row-swap launch applies; a leaf cluster holds
     // at most cluster * 512 * 8 rows
@@ -879,7 +882,7 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     LuGraphEntry* entry = nullptr;
     if (s.graphs && n > 0) {
         const LuGraphKey key{(int)sizeof(T), A, B, X, n, lda, ldb, ldx, nrhs, nb, ipiv, perm, info, factor, solve,
-                             lu.main_st, lu.side_st, lu.wait_limit};
+                             lu.main_st, lu.side_st, lu.wait_limit, lu.min_rpt};
         entry = s.graphs->find(key);
         if (entry && entry->exec) {   // replay
             if (cudaGraphLaunch(entry->exec, lu.main_st) != cudaSuccess) return LU_CUDA_ERROR;

@@ -32,6 +32,7 @@ struct LuStreams {
     int64_t* launches;       // if set, incremented by the number of own kernel launches
     LuGraphCache* graphs;    // if set, repeated call signatures replay a captured graph
     long wait_limit = 0;     // polls a device wait makes before it gives up (0: kDefaultWaitLimit)
+    int min_leaf_rpt = 1;    // fewest rows per leaf thread (1, 2, 4): leaves of 32 / rpt columns
 };
 
 // Polls of a device-side wait (a pivot exchange, a chain flag) before the

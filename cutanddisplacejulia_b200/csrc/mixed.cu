@@ -331,10 +331,11 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
             // w = A z (the FP32 copy of A when one is given: the Arnoldi
             // matrix only needs to be accurate to the restart's reduction),
             // with the first Gram-Schmidt pass's dot products
+            const int gc = a.gemv_chunks > 0 ? a.gemv_chunks : kGemvChunks;
             if (a.A32mv)
-                GM_CK(krylov_gemv<float>(st, a.A32mv, a.ld32, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L));
+                GM_CK(krylov_gemv<float>(st, a.A32mv, a.ld32, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc));
             else
-                GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L));
+                GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc));
             GM_CK(krylov_orthogonalise(st, V, n, nn, k + 1, w, hd, V + (int64_t)(k + 1) * n, kw, L));
             GM_CK(cudaMemcpyAsync(hcol.data(), hd, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
             GM_CK(cudaStreamSynchronize(st));

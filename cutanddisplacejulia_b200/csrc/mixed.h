@@ -56,6 +56,7 @@ struct GmresArgs {
     double* kwork = nullptr;       // krylov_work_doubles(n) doubles of device scratch
     const float* A32mv = nullptr;  // if set, an FP32 copy of A (ld32) for the Arnoldi products
     int64_t ld32 = 0;
+    int gemv_chunks = 0;           // column chunks of the Arnoldi product (0: the default)
 };
 
 struct GmresResult {

@@ -113,6 +113,19 @@ int cad_set_assembly(cad_ctx* ctx, int mode, double near_factor);
 /* GMRES iterations (summed over right-hand sides) and the largest final
  * relative residual of the last mixed solve. */
 int cad_last_solve_stats(const cad_ctx* ctx, int* iterations, double* rel_residual);
+/* Autotuning of launch shapes (no counterpart in the reference): mode 0
+ * (default) uses fixed shapes; 1 uses the shapes stored in cache_path (a text
+ * file of "key value" lines, may be NULL) and times the candidates of any key
+ * not there on its first use, adding the winner to the file; 2 uses stored
+ * shapes only.  Keys are (kernel, size class = the power of two at or above
+ * the size, precision): the pair kernel's triangles per block for the FP64
+ * system matrix, the Arnoldi product's column chunks, and the FP64 LU's leaf
+ * width (timed on a scratch copy of A, systems up to 12288 unknowns).  A call
+ * that meets a new key in mode 1 runs each candidate twice first.
+ * cad_autotune_entries: the number of stored keys (and, in tuned_here, how many
+ * this process timed). */
+int cad_set_autotune(cad_ctx* ctx, int mode, const char* cache_path);
+int64_t cad_autotune_entries(const cad_ctx* ctx, int64_t* tuned_here);
 /* Arnoldi products of the preconditioned-GMRES solvers (CAD_SOLVER_GMRES_*):
  * fp32 = 1 (default) multiplies with an FP32 copy of A (half the bytes per
  * iteration; the solve keeps an extra n x n FP32 array), every restart still
