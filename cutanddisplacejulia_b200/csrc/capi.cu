@@ -54,7 +54,7 @@ struct DevBuf {
 // One lane of the batched solve: its own streams, cuBLAS handles and
 // workspaces, so cracks on different lanes run concurrently.
 enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS, L_BLASWS,
-                L_KWORK, L_COUNT };
+                L_KWORK, L_DINV, L_SYNC, L_Z, L_COUNT };
 struct Lane {
     cudaStream_t main = nullptr, side = nullptr;
     cublasHandle_t main_blas = nullptr, side_blas = nullptr;
@@ -732,14 +732,15 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
                             b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
         const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr, ctx->wait_limit};
-        int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, nullptr, (int*)l.buf[L_PIV].p,
-                               (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, false);
+        int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, (float*)l.buf[L_DINV].p,
+                               (int*)l.buf[L_PIV].p, (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, true);
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "batched solve: FP32 LU failed");
         float* r32 = (float*)l.buf[L_IR32].p;
         IrArgs ia{ls, n3, A, n3, b.T + 3 * o, n3, 1, b.D + 3 * o, (float*)l.buf[L_A32].p, (int*)l.buf[L_PIV].p,
                   (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, ctx->tol, kBatchSweeps,
                   (double*)l.buf[L_IR].p, r32, r32 + n3, (double*)l.buf[L_NORMS].p,
-                  (double*)l.buf[L_KWORK].p};
+                  (double*)l.buf[L_KWORK].p, (const float*)l.buf[L_DINV].p, (int*)l.buf[L_SYNC].p,
+                  (double*)l.buf[L_Z].p, ctx->wait_limit};
         if (ir_solve_fixed(ia, kBatchSweeps, b.rel + c) != GMRES_OK)
             return fail(ctx, CAD_ERR_CUDA, "batched solve: refinement launch failed");
     }
@@ -829,6 +830,9 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         if (int r = lane_ensure(ctx, l, L_IR32, 2 * n3 * sizeof(float), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_NORMS, 2 * sizeof(double), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_KWORK, krylov_work_doubles(n3) * sizeof(double), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_DINV, mixed_dinv_floats(n3) * sizeof(float), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_SYNC, mixed_sync_ints(n3) * sizeof(int), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_Z, n3 * sizeof(double), &p)) return r;
     }
     BatchArgs b{nbatch, offsets, P1, P2, P3, normals, midpoints, T, D, nu, G, lambda, hs, (double*)Aall, &aoff,
                 &lane_of, &order, (double*)rel};

@@ -521,15 +521,25 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
         cudaMemcpy2DAsync(a.R, n * sizeof(double), a.B, a.ldb * sizeof(double), n * sizeof(double), nrhs,
                           cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return GMRES_CUDA_ERROR;
+    const bool chain = nrhs == 1 && a.Dinv && a.sync && a.Z;
+    const int nblk = (int)((n + kRB - 1) / kRB);
+    Precond M{a.A32, a.Dinv, a.perm, (int)n, nblk, a.R32, a.X32, a.sync, st, launches, nullptr, nullptr, 0,
+              a.wait_limit > 0 ? a.wait_limit : kDefaultWaitLimit};
     for (int it = 0; it < iters; ++it) {
-        d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
-        if (launches) ++*launches;
-        if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
-        const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
-                                              a.nb, false, true);
-        if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
-        add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
-        if (launches) ++*launches;
+        if (chain) {
+            // X += LU32 \ R: two chain launches, FP64 in and out
+            if (!M.apply(a.R, a.Z)) return GMRES_CUDA_ERROR;
+            if (krylov_axpy(st, 1.0, a.Z, (int)n, a.X, launches) != cudaSuccess) return GMRES_CUDA_ERROR;
+        } else {
+            d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
+            if (launches) ++*launches;
+            if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
+            const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
+                                                  a.nb, false, true);
+            if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
+            add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
+            if (launches) ++*launches;
+        }
         if (ir_residual(a, st) != cudaSuccess) return GMRES_CUDA_ERROR;
     }
     col_norms_kernel<<<nrhs, 256, 0, st>>>(a.R, n, n, a.norms + nrhs);

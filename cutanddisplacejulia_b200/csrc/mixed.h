@@ -95,6 +95,13 @@ struct IrArgs {
     float* X32;         // n x nrhs
     double* norms;      // 2 nrhs
     double* kwork = nullptr;   // krylov_work_doubles(n): one-column residuals as a GEMV (else a GEMM)
+    // one column with these set: each correction LU32 \ R is two ticket-
+    // ordered chain launches on the factors (explicit inverses of the
+    // diagonal blocks from mixed_prepare) instead of a blocked triangular solve
+    const float* Dinv = nullptr;   // mixed_dinv_floats(n)
+    int* sync = nullptr;           // mixed_sync_ints(n)
+    double* Z = nullptr;           // n doubles
+    long wait_limit = 0;
 };
 
 struct IrResult {

@@ -5,17 +5,24 @@
 //
 // The network is 112 -> 256 -> 256 -> 144 (ReLU), BF16 weights and
 // activations with FP32 accumulation and FP32 master weights (Adam).  All of
-// it -- forward, backward, loss, optimiser -- is this file's kernels: a tiled
-// BF16 GEMM on the tensor cores (mma.sync m16n8k16, FP32 accumulate; the
-// network is small, so one general kernel serves the six GEMM shapes of a
-// training step), bias + ReLU forward / backward, column sums, MSE, Adam.
+// it -- forward, backward, loss, optimiser -- is this file's kernels: a BF16
+// GEMM on the 5th-generation tensor cores (tcgen05.mma kind::f16 with
+// TMA-staged 128-byte-swizzled operand tiles and the FP32 accumulator in
+// tensor memory; K-major or MN-major operands, so one kernel serves the six
+// GEMM shapes of a training step without transposing anything), bias + ReLU
+// forward / backward, column sums, MSE, Adam.  A tiled mma.sync kernel takes
+// operands whose strides TMA cannot describe.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "mlp.h"
+#include "sm100.cuh"
 
 namespace cad {
 
@@ -105,6 +112,176 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_kernel(const __nv_bflo
                 }
             }
 }
+
+// ------------------------------------------------------ tcgen05 BF16 GEMM
+// C (M x N, row-major FP32) (+)= op(A) op(B) with BF16 operands.  One CTA per
+// 128 x BN tile of C; k-steps of 64 (128 bytes of BF16 = one swizzle row)
+// through a 4-stage TMA ring; warp 0 issues the loads, warp 1 the MMAs (K = 16
+// each) into tensor memory, warps 2-5 read the accumulator back and write C.
+// A K-major operand (K contiguous) is one box {64 k, rows} per stage; an
+// MN-major one (M or N contiguous) is boxes {64 mn, 64 k}, 8 KB apart.
+constexpr int GBM = 128, GBK = 64, GSTAGES = 4, GTHREADS = 192, GBN_MAX = 256;
+constexpr uint32_t GSTAGE_A = GBM * GBK * 2;
+constexpr uint32_t GSTAGE_B = GBN_MAX * GBK * 2;
+constexpr uint32_t GSTAGE = GSTAGE_A + GSTAGE_B;
+constexpr size_t GSMEM = (size_t)GSTAGES * GSTAGE + 1024 + 256;
+constexpr long kGemmWaitLimit = 1L << 24;
+
+template <bool A_MN, bool B_MN>
+__global__ void __launch_bounds__(GTHREADS, 1) gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA,
+                                                                   const __grid_constant__ CUtensorMap mapB, int M,
+                                                                   int N, int K, int BN, float* __restrict__ C,
+                                                                   int64_t ldc, int accumulate, int* __restrict__ status)
+{
+    extern __shared__ uint8_t gsm_raw[];
+    uint8_t* gsm = (uint8_t*)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(gsm + GSTAGES * GSTAGE);
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * GSTAGES + 1);
+    __shared__ int s_fail;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * BN;
+    const int nk = (K + GBK - 1) / GBK;
+    const int nbox_b = (BN + 63) / 64;
+    const uint32_t bytes = GSTAGE_A + (B_MN ? (uint32_t)nbox_b * 8192u : (uint32_t)BN * 128u);
+    const uint32_t idesc = sm100::instr_desc(GBM, BN, 1, 1, A_MN ? 1u : 0u, B_MN ? 1u : 0u);
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int q = 0; q < 2 * GSTAGES + 1; ++q) sm100::mbar_init(sm100::smem_addr(&bars[q]), 1);
+        sm100::fence_barrier_init();
+        sm100::prefetch_tensormap(&mapA);
+        sm100::prefetch_tensormap(&mapB);
+    }
+    if (warp == 1) {
+        sm100::tmem_alloc(sm100::smem_addr(tmem_slot), GBN_MAX);
+        sm100::tmem_relinquish();
+    }
+    sm100::tc_fence_before();
+    __syncthreads();
+    sm100::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        int issued = 0;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int q = kt % GSTAGES;
+            const uint32_t ph = (uint32_t)((kt / GSTAGES) & 1);
+            if (!sm100::mbar_wait(sm100::smem_addr(&bars[GSTAGES + q]), ph ^ 1u, kGemmWaitLimit)) {
+                s_fail = 1;
+                break;
+            }
+            const uint32_t full = sm100::smem_addr(&bars[q]);
+            sm100::mbar_arrive_expect_tx(full, bytes);
+            const uint32_t sa = sm100::smem_addr(gsm + q * GSTAGE);
+            const uint32_t sb = sa + GSTAGE_A;
+            if (A_MN) {
+                sm100::tma_load_2d(sa, &mapA, m0, kt * GBK, full);
+                sm100::tma_load_2d(sa + 8192, &mapA, m0 + 64, kt * GBK, full);
+            } else {
+                sm100::tma_load_2d(sa, &mapA, kt * GBK, m0, full);
+            }
+            if (B_MN) {
+                for (int j = 0; j < nbox_b; ++j) sm100::tma_load_2d(sb + j * 8192, &mapB, n0 + 64 * j, kt * GBK, full);
+            } else {
+                sm100::tma_load_2d(sb, &mapB, kt * GBK, n0, full);
+            }
+            issued = kt + 1;
+        }
+        for (int kt = issued > GSTAGES ? issued - GSTAGES : 0; kt < issued; ++kt)
+            if (!sm100::mbar_wait(sm100::smem_addr(&bars[kt % GSTAGES]), (uint32_t)((kt / GSTAGES) & 1), kGemmWaitLimit))
+                s_fail = 1;
+    } else if (warp == 1 && lane == 0) {
+        bool ok = true;
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int q = kt % GSTAGES;
+            const uint32_t ph = (uint32_t)((kt / GSTAGES) & 1);
+            if (!sm100::mbar_wait(sm100::smem_addr(&bars[q]), ph, kGemmWaitLimit)) {
+                s_fail = 1;
+                ok = false;
+                break;
+            }
+            sm100::tc_fence_after();
+            const uint32_t sa = sm100::smem_addr(gsm + q * GSTAGE);
+            const uint32_t sb = sa + GSTAGE_A;
+#pragma unroll
+            for (int kk = 0; kk < GBK / 16; ++kk) {
+                // K-major: +32 bytes per K = 16 inside the 128-byte row, 8-row atoms 1 KB apart.
+                // MN-major: one 128-byte row per k, K = 16 = two 8-row atoms (1 KB apart),
+                // 64-element MN groups in boxes 8 KB apart.
+                const uint64_t da = A_MN ? sm100::smem_desc_sw128(sa + kk * 2048, 8192, 1024)
+                                         : sm100::smem_desc_sw128(sa + kk * 32, 16, 1024);
+                const uint64_t db = B_MN ? sm100::smem_desc_sw128(sb + kk * 2048, 8192, 1024)
+                                         : sm100::smem_desc_sw128(sb + kk * 32, 16, 1024);
+                sm100::mma_f16(tmem, da, db, idesc, kt > 0 || kk > 0);
+            }
+            sm100::mma_commit(sm100::smem_addr(&bars[GSTAGES + q]));
+        }
+        sm100::mma_commit(sm100::smem_addr(&bars[2 * GSTAGES]));
+        if (!sm100::mbar_wait(sm100::smem_addr(&bars[2 * GSTAGES]), 0, kGemmWaitLimit)) s_fail = 1;
+    } else if (warp >= 2) {
+        const int qd = warp & 3;
+        const int row = m0 + 32 * qd + lane;
+        const bool got = sm100::mbar_wait(sm100::smem_addr(&bars[2 * GSTAGES]), 0, kGemmWaitLimit);
+        sm100::tc_fence_after();
+        if (!got) {
+            s_fail = 1;
+        } else if (nk > 0) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                if (n0 + c0 >= N) break;
+                uint32_t v[32];
+                sm100::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)c0, v);
+                sm100::tmem_wait_ld();
+                if (row < M) {
+                    float* cr = C + (int64_t)row * ldc + n0 + c0;
+                    const int ncol = N - (n0 + c0) < 32 ? N - (n0 + c0) : 32;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c)
+                        if (c < ncol) cr[c] = (accumulate ? cr[c] : 0.f) + __uint_as_float(v[c]);
+                }
+            }
+        }
+    }
+    sm100::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        sm100::tc_fence_after();
+        sm100::tmem_dealloc(tmem, GBN_MAX);
+    }
+    if (threadIdx.x == 0 && s_fail) atomicExch(status, 1);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// Row-major BF16 matrix (rows x cols, ld elements) as a 2-D tensor map:
+// dimension 0 = cols (contiguous), box {box_c, box_r}, 128-byte swizzle.
+bool encode_bf16(CUtensorMap* map, const __nv_bfloat16* base, int rows, int cols, int64_t ld, int box_c, int box_r)
+{
+    auto fn = encode_tiled();
+    if (!fn || ((uintptr_t)base & 15u) || (ld * 2) % 16 != 0) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)box_c, (cuuint32_t)box_r};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The device word the tcgen05 GEMMs raise when a pipeline wait runs out.
+__device__ int g_mlp_gemm_status;
 
 // pre = C + bias (kept, FP32), act = relu(pre) (BF16) -- or, for the output
 // layer (relu false), out = C + bias.
@@ -255,10 +432,42 @@ cudaError_t block_jacobi(cudaStream_t st, const double* A, int64_t lda, int64_t 
     return cudaGetLastError();
 }
 
+template <bool A_MN, bool B_MN>
+cudaError_t launch_gemm_tc(cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, int BN,
+                           float* C, int64_t ldc, bool accumulate)
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(gemm_bf16_tc_kernel<A_MN, B_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GSMEM);
+    });
+    int* status = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&status, g_mlp_gemm_status);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((unsigned)((M + GBM - 1) / GBM), (unsigned)((N + BN - 1) / BN));
+    gemm_bf16_tc_kernel<A_MN, B_MN><<<grid, GTHREADS, GSMEM, st>>>(ma, mb, M, N, K, BN, C, ldc, accumulate ? 1 : 0,
+                                                                   status);
+    return cudaGetLastError();
+}
+
 cudaError_t mlp_gemm(cudaStream_t st, bool ta, bool tb, const __nv_bfloat16* A, int64_t lda, const __nv_bfloat16* B,
                      int64_t ldb, float* C, int64_t ldc, int M, int N, int K, bool accumulate)
 {
     if (M <= 0 || N <= 0) return cudaSuccess;
+    if (K > 0) {
+        // tensor-core path: N tile of 256, or 144 / 128 columns when N is one of those
+        const int BN = N <= 128 ? 128 : (N <= 144 ? 144 : 256);
+        CUtensorMap ma, mb;
+        // op(A) = A (M x K, row-major: K-major) or A^T (A stored K x M: M-major);
+        // op(B) = B (K x N row-major: N-major) or B^T (B stored N x K: K-major)
+        const bool okA = ta ? encode_bf16(&ma, A, K, M, lda, 64, 64) : encode_bf16(&ma, A, M, K, lda, 64, GBM);
+        const bool okB = tb ? encode_bf16(&mb, B, N, K, ldb, 64, BN) : encode_bf16(&mb, B, K, N, ldb, 64, 64);
+        if (okA && okB) {
+            if (!ta && !tb) return launch_gemm_tc<false, true>(st, ma, mb, M, N, K, BN, C, ldc, accumulate);
+            if (ta && !tb) return launch_gemm_tc<true, true>(st, ma, mb, M, N, K, BN, C, ldc, accumulate);
+            if (!ta && tb) return launch_gemm_tc<false, false>(st, ma, mb, M, N, K, BN, C, ldc, accumulate);
+            return launch_gemm_tc<true, false>(st, ma, mb, M, N, K, BN, C, ldc, accumulate);
+        }
+    }
     dim3 grid((unsigned)((N + kTile - 1) / kTile), (unsigned)((M + kTile - 1) / kTile));
     if (!ta && !tb) gemm_bf16_kernel<false, false><<<grid, kGemmThreads, 0, st>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate);
     else if (ta && !tb) gemm_bf16_kernel<true, false><<<grid, kGemmThreads, 0, st>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate);
