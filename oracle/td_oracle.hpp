@@ -3,7 +3,10 @@
 // TEST INFRASTRUCTURE ONLY.  A scalar FP64 restatement of the reference's
 // algorithm (src/TD.jl of CutAndDisplaceJulia), used as the checker by tests/,
 // by the smoke check and as the benchmark's CPU baseline.  The CUDA product
-// never includes or links this file.
+// never includes or links this file.  Parity unpinned: the reference (Julia)
+// cannot run here and stores no golden vectors, so this restatement is pinned
+// only by the reference's analytic known-answer tests (Okada, Mogi, Eshelby,
+// traction-free surface, Savage, Burgmann).
 //
 // The reference evaluates one triangle at a time and makes several passes over
 // all observation points (src/TD.jl:146-214, :735-867, :1499-1620).  Every pass
