@@ -309,7 +309,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
                        int* info_out)
 {
     void *a32, *dinv, *piv, *perm, *info, *kry, *v32, *sync, *work;
-    if (int r = ensure(ctx, S_A32, (size_t)n * n * sizeof(float), &a32)) return r;
+    if (int r = ensure(ctx, S_A32, (size_t)mixed_ld(n) * n * sizeof(float), &a32)) return r;
     if (int r = ensure(ctx, S_DINV, mixed_dinv_floats(n) * sizeof(float), &dinv)) return r;
     if (int r = ensure(ctx, S_PIV, (size_t)n * sizeof(int), &piv)) return r;
     if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
@@ -822,7 +822,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         if (int r = lane_ensure(ctx, l, L_TRI, N * tri_record_bytes(), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_TRI32, N * tri_record_bytes_f32(), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_NEAR, (3 * N + 1) * sizeof(double), &p)) return r;
-        if (int r = lane_ensure(ctx, l, L_A32, n3 * n3 * sizeof(float), &p)) return r;
+        if (int r = lane_ensure(ctx, l, L_A32, mixed_ld(n3) * n3 * sizeof(float), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_PIV, n3 * sizeof(int), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_PERM, n3 * sizeof(int), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_INFO, sizeof(int), &p)) return r;

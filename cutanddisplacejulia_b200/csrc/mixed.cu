@@ -33,12 +33,13 @@ namespace {
 constexpr int kRB = 128;            // row block of the triangular solves
 constexpr int kChainThreads = 512;  // four threads per row: quarters of each 128-column block
 
-// B (n x n, leading dimension n) = (float) A (n x n, lda); columns strided over grid.y
-__global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64_t n, float* __restrict__ B)
+// B (n x n, leading dimension ldb) = (float) A (n x n, lda); columns strided over grid.y
+__global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64_t n, float* __restrict__ B,
+                                int64_t ldb)
 {
     for (int64_t c = blockIdx.y; c < n; c += gridDim.y)
         for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-            B[r + c * n] = (float)A[r + c * lda];
+            B[r + c * ldb] = (float)A[r + c * lda];
 }
 
 // Inverse of diagonal block i (kRB x kRB, zero-padded to the identity past n)
@@ -204,11 +205,12 @@ int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, 
 {
     if (n <= 0) return LU_OK;
     const int64_t rb = (n + 255) / 256;
+    const int64_t ld = mixed_ld(n);
     cast_f32_kernel<<<dim3((unsigned)(rb < 8 ? rb : 8), (unsigned)(n < 4096 ? n : 4096)), 256, 0, ls.main>>>(A, lda, n,
-                                                                                                     A32);
+                                                                                                     A32, ld);
     if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
     if (ls.launches) ++*ls.launches;
-    int rc = lu_factor_solve<float>(ls, A32, n, n, nullptr, 0, 0, nullptr, 0, ipiv, perm, info, nb, true, false);
+    int rc = lu_factor_solve<float>(ls, A32, n, ld, nullptr, 0, 0, nullptr, 0, ipiv, perm, info, nb, true, false);
     if (rc != LU_OK) return rc;
     rc = lu_pivots_to_perm(ls, ipiv, n, perm);
     if (rc != LU_OK || !inverses) return rc;
@@ -219,12 +221,14 @@ int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, 
         cudaFuncSetAttribute(invert_diag_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
         return LU_CUDA_ERROR;
-    invert_diag_kernel<false><<<nblk, kRB, smem, ls.main>>>(A32, n, (int)n, Dinv);
-    invert_diag_kernel<true><<<nblk, kRB, smem, ls.main>>>(A32, n, (int)n, Dinv + (int64_t)nblk * kRB * kRB);
+    invert_diag_kernel<false><<<nblk, kRB, smem, ls.main>>>(A32, ld, (int)n, Dinv);
+    invert_diag_kernel<true><<<nblk, kRB, smem, ls.main>>>(A32, ld, (int)n, Dinv + (int64_t)nblk * kRB * kRB);
     if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
     if (ls.launches) *ls.launches += 2;
     return LU_OK;
 }
+
+int64_t mixed_ld(int64_t n) { return (n + 3) / 4 * 4; }
 
 size_t mixed_dinv_floats(int64_t n) { return (size_t)2 * ((n + kRB - 1) / kRB) * kRB * kRB; }
 size_t mixed_sync_ints(int64_t n) { return (size_t)2 * ((n + kRB - 1) / kRB) + 4; }
@@ -260,9 +264,9 @@ struct Precond {
         int* fail = sync + 2 * nblk + 2;
         const float* DL = Dinv;
         const float* DU = Dinv + (int64_t)nblk * kRB * kRB;
-        trsv_chain_kernel<false><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DL, v, perm, nullptr, y32, nullptr,
+        trsv_chain_kernel<false><<<nblk, kChainThreads, 0, st>>>(A32, mixed_ld(n), n, nblk, DL, v, perm, nullptr, y32, nullptr,
                                                                  fl, tk, fail, wait_limit);
-        trsv_chain_kernel<true><<<nblk, kChainThreads, 0, st>>>(A32, n, n, nblk, DU, nullptr, nullptr, y32, x32, z, fu,
+        trsv_chain_kernel<true><<<nblk, kChainThreads, 0, st>>>(A32, mixed_ld(n), n, nblk, DU, nullptr, nullptr, y32, x32, z, fu,
                                                                 tk + 1, fail, wait_limit);
         if (launches) *launches += 2;
         return cudaGetLastError() == cudaSuccess;
@@ -465,7 +469,7 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
         d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
         if (launches) ++*launches;
         if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
-        const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
+        const int rc = lu_factor_solve<float>(a.ls, a.A32, n, mixed_ld(n), a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
                                               a.nb, false, true);
         if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
         add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
@@ -534,7 +538,7 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
             d2f_kernel<<<g, 256, 0, st>>>(a.R, n, n, a.R32, n);
             if (launches) ++*launches;
             if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
-            const int rc = lu_factor_solve<float>(a.ls, a.A32, n, n, a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
+            const int rc = lu_factor_solve<float>(a.ls, a.A32, n, mixed_ld(n), a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
                                                   a.nb, false, true);
             if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
             add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);

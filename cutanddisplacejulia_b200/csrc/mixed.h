@@ -11,7 +11,7 @@
 
 namespace cad {
 
-// Casts A (FP64, n x n, lda) to A32 (n x n, leading dimension n), factorises
+// Casts A (FP64, n x n, lda) to A32 (n x n, leading dimension mixed_ld(n)), factorises
 // A32 in place (partial pivoting; TF32 tensor-core trailing updates), forms
 // the row permutation and inverts the 128-row diagonal blocks of both
 // triangles into Dinv (mixed_dinv_floats(n) floats).  Returns an LU_* code;
@@ -19,6 +19,9 @@ namespace cad {
 int mixed_prepare(const LuStreams& ls, const double* A, int64_t lda, int64_t n, float* A32, float* Dinv, int* ipiv,
                   int* perm, int* info, int nb, bool inverses = true);
 size_t mixed_dinv_floats(int64_t n);
+// Leading dimension of the FP32 factors: n rounded up to a multiple of 4
+// floats, so the TF32 trailing updates can stage them with TMA.
+int64_t mixed_ld(int64_t n);
 size_t mixed_sync_ints(int64_t n);   // flags, tickets and the failure word of one preconditioner apply
 
 enum { GMRES_OK = 0, GMRES_NOT_CONVERGED = 1, GMRES_CUDA_ERROR = 2, GMRES_BLAS_ERROR = 3, GMRES_TIMEOUT = 4 };
