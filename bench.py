@@ -57,6 +57,8 @@ MIXED_TOL = 1e-10       # relative residual the mixed-precision solve iterates t
 NEAR_FACTOR = 3.0       # near field of the mixed assembly, in mean edge lengths
 
 UNIT = "pair-evals/s"
+# the headline metric as the benchmark's definition names it
+BASELINE_METRIC = "TD pair-evals/s vs FP64 peak; solve time at rel-residual 1e-10, mixed vs FP64"
 WORKLOADS = {
     "penny": ("TD pair-evals/s (FS penny crack: influence assembly + FP64 LU solve)",
               "penny crack, full space, %d triangles, 3N=%d unknowns, FP64 assembly + LU"),
@@ -72,8 +74,6 @@ WORKLOADS = {
               "200-2000 triangles each (log-uniform), %d triangles in all"),
 }
 METRIC = WORKLOADS["penny"][0]
-# the headline metric as the benchmark's definition names it
-BASELINE_METRIC = "TD pair-evals/s vs FP64 peak; solve time at rel-residual 1e-10, mixed vs FP64"
 
 
 def _hbm_peak():

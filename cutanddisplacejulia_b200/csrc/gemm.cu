@@ -2,13 +2,14 @@
 // written for sm_100a:
 //
 // * FP64 (the plain FP64 solve, A\b of src/SlipCalculator3D.jl:22): DMMA
-//   tensor-core tiles (mma.sync m8n8k4 f64).  A 128 x 128 block of C per CTA,
-//   8 warps of 64 x 32, k-steps of 16 staged through a 4-deep cp.async ring
+//   tensor-core tiles (mma.sync m8n8k4 f64).  A 128 x 64 block of C per CTA,
+//   4 warps of 64 x 32, two CTAs per SM, k-steps of 16 through a 4-deep cp.async ring
 //   (8-byte copies: any leading dimension and any row offset).  Shared-memory
 //   rows are padded so that every fragment load is free of bank conflicts.
 // * FP32 with TF32 tensor cores (the mixed solve's FP32 factorisation):
 //   tcgen05.mma kind::tf32 with operands staged by TMA in 128-byte-swizzled
-//   tiles and the 128 x 128 FP32 accumulator in tensor memory.  One warp
+//   tiles (the MN-major A in 32-byte swizzle atoms, the only layout MN-major
+//   32-bit operands take) and the 128 x 128 FP32 accumulator in tensor memory.  One warp
 //   issues the TMA loads, one the MMAs, four run the epilogue (tensor memory
 //   -> registers, C -= product with coalesced column accesses); a 3-stage
 //   ring of 32 KB stages, two CTAs per SM so that one CTA's epilogue overlaps
@@ -30,7 +31,10 @@ namespace cad {
 namespace {
 
 // ------------------------------------------------------------------ FP64 DMMA
-constexpr int DBM = 128, DBN = 128, DBK = 16, DSTAGES = 4, DTHREADS = 256;
+// CTA tile 128 x 64, 4 warps of 64 x 32 (8 x 4 DMMA tiles of 8 x 8 each), two
+// CTAs per SM so that one CTA's prologue and epilogue overlap the other's
+// main loop.
+constexpr int DBM = 128, DBN = 64, DBK = 16, DSTAGES = 4, DTHREADS = 128;
 constexpr int DLDA = DBM + 4;   // shared row (one k) of the A tile, doubles: 132 = 4 mod 16
 constexpr int DLDB = DBK + 4;   // shared row (one n) of the B tile, doubles: 20 = 4 mod 16
 constexpr int DSTAGE_A = DBK * DLDA;
@@ -54,7 +58,7 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 }
 
 // Stage s of the ring <- k-step kt: the A tile (128 rows x 16 columns, stored
-// k-major: row k holds 128 consecutive m) and the B tile (16 rows x 128
+// k-major: row k holds 128 consecutive m) and the B tile (16 rows x 64
 // columns, stored n-major: row n holds 16 consecutive k).
 __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const double* __restrict__ A, int64_t lda,
                                                  const double* __restrict__ B, int64_t ldb, int m, int n, int k,
@@ -80,7 +84,7 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
     }
 }
 
-__global__ void __launch_bounds__(DTHREADS, 1) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
+__global__ void __launch_bounds__(DTHREADS, 2) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
                                                                 int64_t lda, const double* __restrict__ B, int64_t ldb,
                                                                 double* __restrict__ C, int64_t ldc)
 {
@@ -89,7 +93,7 @@ __global__ void __launch_bounds__(DTHREADS, 1) dgemm_sub_kernel(int m, int n, in
     double* sB = dsm + DSTAGES * DSTAGE_A;
     const int m0 = blockIdx.x * DBM, n0 = blockIdx.y * DBN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;   // 2 x 4 warps of 64 x 32
+    const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;   // 2 x 2 warps of 64 x 32
     const int g = lane >> 2, t = lane & 3;
     double acc[8][4][2];
 #pragma unroll
@@ -153,8 +157,9 @@ constexpr size_t TSMEM = (size_t)TSTAGES * TSTAGE + 1024 /* alignment slack */ +
 constexpr uint32_t TIDESC = sm100::instr_desc(TBM, TBN, 2, 2, 1 /* A MN-major */, 0 /* B K-major */);
 constexpr long kTcWaitLimit = 1L << 24;
 
-// A: dims {m, k}, box {32, 32}; B: dims {k, n}, box {32, 128}; both FP32,
-// 128-byte swizzle, out-of-range elements read as zero.
+// A: dims {m, k}, box {32, 32}, 128-byte rows swizzled in 32-byte chunks;
+// B: dims {k, n}, box {32, 128}, 128-byte swizzle; both FP32, out-of-range
+// elements read as zero.
 __global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap mapA,
                                                                      const __grid_constant__ CUtensorMap mapB, int m,
                                                                      int n, int k, float* __restrict__ C, int64_t ldc,
@@ -226,11 +231,12 @@ __global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __gri
             const uint32_t sb = sa + TSTAGE_A;
 #pragma unroll
             for (int kk = 0; kk < TBK / 8; ++kk) {
-                // A (MN-major): k-rows of 128 bytes, 8 per swizzle atom -> +1 KB per
-                // K = 8; the four 32-row m boxes 4 KB apart (leading byte offset).
-                // B (K-major): rows of 32 k -> +32 bytes per K = 8; 8-row atoms
-                // 1 KB apart (stride byte offset).
-                const uint64_t da = sm100::smem_desc_sw128(sa + kk * 1024, 4096, 1024);
+                // A (MN-major, 32-bit): k-rows of 128 bytes swizzled in 32-byte
+                // chunks, 4 rows per atom (512 bytes apart: stride byte offset),
+                // +1 KB per K = 8; the four 32-row m boxes 4 KB apart (leading
+                // byte offset).  B (K-major): rows of 32 k -> +32 bytes per K =
+                // 8; 8-row atoms 1 KB apart (stride byte offset).
+                const uint64_t da = sm100::smem_desc(sa + kk * 1024, 4096, 512, sm100::kLayoutSW128Atom32);
                 const uint64_t db = sm100::smem_desc_sw128(sb + kk * 32, 16, 1024);
                 sm100::mma_tf32(tmem, da, db, TIDESC, kt > 0 || kk > 0);
             }
@@ -337,7 +343,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 // Column-major FP32 matrix (rows x cols, ld) as a 2-D tensor map with
 // box {box_rows, box_cols} and 128-byte swizzle.
-bool encode_f32(CUtensorMap* map, const float* base, int rows, int cols, int64_t ld, int box_rows, int box_cols)
+bool encode_f32(CUtensorMap* map, const float* base, int rows, int cols, int64_t ld, int box_rows, int box_cols,
+                CUtensorMapSwizzle swizzle)
 {
     auto fn = encode_fn();
     if (!fn) return false;
@@ -346,7 +353,7 @@ bool encode_f32(CUtensorMap* map, const float* base, int rows, int cols, int64_t
     const cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
     const cuuint32_t estr[2] = {1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -365,6 +372,7 @@ cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const double* A, int6
     static std::once_flag once;
     std::call_once(once, [] {
         cudaFuncSetAttribute(dgemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DSMEM);
+        cudaFuncSetAttribute(dgemm_sub_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
     const dim3 grid((unsigned)((m + DBM - 1) / DBM), (unsigned)((n + DBN - 1) / DBN));
     dgemm_sub_kernel<<<grid, DTHREADS, DSMEM, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
@@ -376,8 +384,11 @@ cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const float* A, int64
 {
     if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
     CUtensorMap ma, mb;
-    if (status && tma_ok(A, lda) && tma_ok(B, ldb) && encode_f32(&ma, A, m, k, lda, 32, 32) &&
-        encode_f32(&mb, B, k, n, ldb, 32, TBN)) {
+    // A column-major (m contiguous: MN-major, 32-byte swizzle atoms); B
+    // column-major (k contiguous: K-major, 16-byte atoms)
+    if (status && tma_ok(A, lda) && tma_ok(B, ldb) &&
+        encode_f32(&ma, A, m, k, lda, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B) &&
+        encode_f32(&mb, B, k, n, ldb, 32, TBN, CU_TENSOR_MAP_SWIZZLE_128B)) {
         static std::once_flag once;
         std::call_once(once, [] {
             cudaFuncSetAttribute(sgemm_tf32_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TSMEM);

@@ -76,18 +76,25 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor of a 128-byte-swizzled operand tile:
-// start address, leading and stride byte offsets (16-byte units), the
-// sm_100 descriptor version (1) and the swizzle mode (2 = 128 B).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+// Shared-memory matrix descriptor of a swizzled operand tile: start
+// address, leading and stride byte offsets (16-byte units), the sm_100
+// descriptor version (1) and the layout: 2 = 128-byte swizzle of 16-byte
+// chunks (8-row atoms), 1 = 128-byte swizzle of 32-byte chunks (4-row atoms,
+// the layout MN-major 32-bit operands take).
+constexpr uint32_t kLayoutSW128 = 2, kLayoutSW128Atom32 = 1;
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes, uint32_t layout)
 {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);
     d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1u << 46;
-    d |= (uint64_t)2u << 61;
+    d |= (uint64_t)layout << 61;
     return d;
+}
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    return smem_desc(addr, lbo_bytes, sbo_bytes, kLayoutSW128);
 }
 
 // D[tmem] (+)= A[smem] * B[smem], kind::tf32 or kind::f16 (FP32 accumulate);
