@@ -132,9 +132,21 @@ __global__ void __launch_bounds__(DTHREADS, 2) dgemm_sub_kernel(int m, int n, in
         }
     }
     cp_async_wait<0>();
-    // C -= acc: thread holds rows wm + 8i + g, columns wn + 8j + 2t + {0, 1}
+    // C -= acc: thread holds rows wm + 8i + g, columns wn + 8j + 2t + {0, 1}.
+    // Per column pair, all 16 loads are issued before any store (the compiler
+    // cannot reorder a load of C past a store to C), so their latencies overlap.
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < 4; ++j) {
+        double c[2][8];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int col = n0 + wn + 8 * j + 2 * t + h;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int row = m0 + wm + 8 * i + g;
+                c[h][i] = (col < n && row < m) ? C[(int64_t)col * ldc + row] : 0.0;
+            }
+        }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int col = n0 + wn + 8 * j + 2 * t + h;
@@ -143,9 +155,10 @@ __global__ void __launch_bounds__(DTHREADS, 2) dgemm_sub_kernel(int m, int n, in
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int row = m0 + wm + 8 * i + g;
-                if (row < m) cc[row] -= acc[i][j][h];
+                if (row < m) cc[row] = c[h][i] - acc[i][j][h];
             }
         }
+    }
 }
 
 // ------------------------------------------------------- FP32: tcgen05 + TMA
