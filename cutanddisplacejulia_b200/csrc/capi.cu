@@ -289,6 +289,16 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
             ++ctx->launches;
             return launch_td_pairs(t, out_kind, hs == 1, true, false, ctx->stream);
         });
+        if (hs == 1) {
+            // then the half-space kernel's occupancy variant at that chunk
+            std::snprintf(key, sizeof key, "pair_amat_f64_hs1_minblocks_N%lld", (long long)tune_class(N));
+            t = a;
+            a.min_blocks = tune_choice(ctx->tuner, key, ctx->stream, {1, 3, 4}, 1, [&](int c) {
+                t.min_blocks = c;
+                ++ctx->launches;
+                return launch_td_pairs(t, out_kind, true, true, false, ctx->stream);
+            });
+        }
     }
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     ++ctx->launches;

@@ -3,9 +3,10 @@
 //
 // * FP64 (the plain FP64 solve, A\b of src/SlipCalculator3D.jl:22): DMMA
 //   tensor-core tiles (mma.sync m8n8k4 f64).  A 128 x 64 block of C per CTA,
-//   4 warps of 64 x 32, two CTAs per SM, k-steps of 16 through a 4-deep cp.async ring
-//   (8-byte copies: any leading dimension and any row offset).  Shared-memory
-//   rows are padded so that every fragment load is free of bank conflicts.
+//   4 warps of 64 x 32, three CTAs per SM, k-steps of 16 through a 3-deep
+//   cp.async ring (8-byte copies: any leading dimension and any row offset).
+//   Shared-memory words are XOR-swizzled by row so that every fragment load is
+//   free of bank conflicts.
 // * FP32 with TF32 tensor cores (the mixed solve's FP32 factorisation):
 //   tcgen05.mma kind::tf32 with operands staged by TMA in 128-byte-swizzled
 //   tiles (the MN-major A in 32-byte swizzle atoms, the only layout MN-major
@@ -31,14 +32,20 @@ namespace cad {
 namespace {
 
 // ------------------------------------------------------------------ FP64 DMMA
-// CTA tile 128 x 64, 4 warps of 64 x 32 (8 x 4 DMMA tiles of 8 x 8 each), two
-// CTAs per SM so that one CTA's prologue and epilogue overlap the other's
-// main loop.
-constexpr int DBM = 128, DBN = 64, DBK = 16, DSTAGES = 4, DTHREADS = 128;
-constexpr int DLDA = DBM + 4;   // shared row (one k) of the A tile, doubles: 132 = 4 mod 16
-constexpr int DLDB = DBK + 4;   // shared row (one n) of the B tile, doubles: 20 = 4 mod 16
+// CTA tile 128 x 64, 4 warps of 64 x 32 (8 x 4 DMMA tiles of 8 x 8 each),
+// three CTAs per SM (72 KB of shared memory each: 3 stages of unpadded,
+// swizzled tiles) so that the DMMA latency is hidden by 12 warps and one
+// CTA's prologue and epilogue overlap the others' main loops.
+constexpr int DBM = 128, DBN = 64, DBK = 16, DSTAGES = 3, DTHREADS = 128, DMINB = 3;
+constexpr int DLDA = DBM;       // shared row (one k) of the A tile, doubles
+constexpr int DLDB = DBK;       // shared row (one n) of the B tile, doubles
 constexpr int DSTAGE_A = DBK * DLDA;
 constexpr int DSTAGE_B = DBN * DLDB;
+// Unpadded rows with the 8-byte words XOR-swizzled by the row index: a
+// fragment load (4 rows x 4 (A) or 4 x 4 (B) words per half warp) then hits 16
+// distinct banks pairs.  Element (row, col) of a tile with rows of `ld` words
+// sits at row * ld + (col ^ (4 * (row & 3))).
+__device__ __forceinline__ int swz(int row, int col, int ld) { return row * ld + (col ^ ((row & 3) << 2)); }
 constexpr size_t DSMEM = (size_t)DSTAGES * (DSTAGE_A + DSTAGE_B) * sizeof(double);
 
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, bool pred)
@@ -72,7 +79,7 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
         const int kk = e / DBM, mm = e % DBM;
         const bool ok = (m0 + mm < m) && (k0 + kk < k);
         const double* src = ok ? A + (int64_t)(m0 + mm) + (int64_t)(k0 + kk) * lda : A;
-        cp_async8(sm100::smem_addr(sA + kk * DLDA + mm), src, ok);
+        cp_async8(sm100::smem_addr(sA + swz(kk, mm, DLDA)), src, ok);
     }
 #pragma unroll
     for (int i = 0; i < (DBN * DBK) / DTHREADS; ++i) {
@@ -80,11 +87,11 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
         const int nn = e / DBK, kk = e % DBK;
         const bool ok = (n0 + nn < n) && (k0 + kk < k);
         const double* src = ok ? B + (int64_t)(k0 + kk) + (int64_t)(n0 + nn) * ldb : B;
-        cp_async8(sm100::smem_addr(sB + nn * DLDB + kk), src, ok);
+        cp_async8(sm100::smem_addr(sB + swz(nn, kk, DLDB)), src, ok);
     }
 }
 
-__global__ void __launch_bounds__(DTHREADS, 2) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
+__global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
                                                                 int64_t lda, const double* __restrict__ B, int64_t ldb,
                                                                 double* __restrict__ C, int64_t ldc)
 {
@@ -122,9 +129,9 @@ __global__ void __launch_bounds__(DTHREADS, 2) dgemm_sub_kernel(int m, int n, in
         for (int kk = 0; kk < DBK; kk += 4) {
             double af[8], bf[4];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) af[i] = a_s[(kk + t) * DLDA + wm + 8 * i + g];
+            for (int i = 0; i < 8; ++i) af[i] = a_s[swz(kk + t, wm + 8 * i + g, DLDA)];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = b_s[(wn + 8 * j + g) * DLDB + kk + t];
+            for (int j = 0; j < 4; ++j) bf[j] = b_s[swz(wn + 8 * j + g, kk + t, DLDB)];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll

@@ -119,8 +119,11 @@ __device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, co
 // radius of some point of the block (the FP64 pass of the mixed assembly).
 // LIST (OUT_AMAT only): incremental re-assembly through a.tri_list /
 // a.obs_list into a system of a.Ntot elements.
-template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false>
-__global__ void __launch_bounds__(kPairThreads) td_pair_kernel(PairArgs a)
+// MINB > 1: compiled for MINB resident blocks per SM (fewer registers per
+// thread, more warps to hide the FP64 latency, some spilling) -- a launch
+// shape the autotuner may pick for the half-space system matrix.
+template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false, int MINB = 1>
+__global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 {
     extern __shared__ double smem[];
     constexpr int words = HS ? kTriWordsHS : kTriWordsFS;
@@ -397,11 +400,11 @@ __global__ void __launch_bounds__(kPairThreads) td_pair_f32_kernel(PairArgs a)
 }
 
 // ------------------------------------------------------------ launchers
-template <bool HS, bool STRAIN, bool DISP, int OUT>
+template <bool HS, bool STRAIN, bool DISP, int OUT, int MINB = 1>
 static cudaError_t launch_pair(const PairArgs& a, cudaStream_t st)
 {
     const size_t smem = (HS ? kTriWordsHS : kTriWordsFS) * sizeof(double);
-    auto kern = td_pair_kernel<HS, STRAIN, DISP, OUT>;
+    auto kern = td_pair_kernel<HS, STRAIN, DISP, OUT, false, false, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t ntile = (a.M + kPairThreads - 1) / kPairThreads;
@@ -433,7 +436,11 @@ cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bo
             if (hs) return launch_pair<true, true, false, OUT_TRAC>(a, st);
             return launch_pair<false, true, false, OUT_TRAC>(a, st);
         case OUT_AMAT:
-            if (hs) return launch_pair<true, true, false, OUT_AMAT>(a, st);
+            if (hs) {
+                if (a.min_blocks == 3) return launch_pair<true, true, false, OUT_AMAT, 3>(a, st);
+                if (a.min_blocks == 4) return launch_pair<true, true, false, OUT_AMAT, 4>(a, st);
+                return launch_pair<true, true, false, OUT_AMAT>(a, st);
+            }
             return launch_pair<false, true, false, OUT_AMAT>(a, st);
     }
     return cudaErrorInvalidValue;

@@ -41,6 +41,9 @@ struct PairArgs {
     const int* tri_list;
     const int* obs_list;
     int64_t Ntot;
+    // half-space system matrix: the kernel variant compiled for this many
+    // resident blocks per SM (1: the full register file; 3 or 4)
+    int min_blocks = 1;
 };
 
 // Mixed-precision system matrix: every pair in FP32 (far field), then the
