@@ -475,7 +475,7 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
         char key[64];
         std::snprintf(key, sizeof key, "gemv_%s_n%lld", g.A32mv ? "f32" : "f64", (long long)tune_class(n));
         const KrylovWork kw = krylov_carve(g.kwork, n);
-        g.gemv_chunks = tune_choice(ctx->tuner, key, ctx->stream, {4, 8, 16}, kGemvChunks, [&](int c) {
+        g.gemv_chunks = tune_choice(ctx->tuner, key, ctx->stream, {8, 16, 32}, kGemvChunks, [&](int c) {
             return g.A32mv ? krylov_gemv<float>(ctx->stream, g.A32mv, g.ld32, (int)n, B, 1.0, nullptr, g.w, kw,
                                                 nullptr, 0, 0, &ctx->launches, c)
                            : krylov_gemv<double>(ctx->stream, A, lda, (int)n, B, 1.0, nullptr, g.w, kw, nullptr, 0,

@@ -8,8 +8,8 @@
 namespace cad {
 
 constexpr int kMaxBasis = 64;     // Krylov basis vectors one orthogonalisation handles
-constexpr int kGemvChunks = 8;     // default column chunks of the matrix-vector product
-constexpr int kMaxGemvChunks = 16;
+constexpr int kGemvChunks = 16;    // default column chunks of the matrix-vector product
+constexpr int kMaxGemvChunks = 32;
 
 // Device scratch of the kernels below (krylov_work_doubles(n) doubles).
 struct KrylovWork {
