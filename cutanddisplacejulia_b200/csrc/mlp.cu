@@ -320,14 +320,25 @@ __global__ void relu_back_kernel(const float* __restrict__ dact, const float* __
     dfp[i] = g;
 }
 
-// out[c] = sum over rows of X[r][c] (fixed order); one thread per column
-__global__ void colsum_kernel(const float* __restrict__ X, int64_t rows, int cols, float* __restrict__ out)
+// out[c] = sum over rows of X[r][c] in a fixed order: a block of 32 x 32
+// threads takes 32 columns; thread (x, y) sums rows y, y + 32, ... of column
+// x (coalesced rows), then the 32 partial sums are added in order of y.
+__global__ void __launch_bounds__(1024) colsum_kernel(const float* __restrict__ X, int64_t rows, int cols,
+                                                      float* __restrict__ out)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+    __shared__ float part[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + tx;
     float s = 0.f;
-    for (int64_t r = 0; r < rows; ++r) s += X[r * cols + c];
-    out[c] = s;
+    if (c < cols)
+        for (int64_t r = ty; r < rows; r += 32) s += X[r * cols + c];
+    part[ty][tx] = s;
+    __syncthreads();
+    if (ty == 0 && c < cols) {
+        float t = 0.f;
+        for (int y = 0; y < 32; ++y) t += part[y][tx];
+        out[c] = t;
+    }
 }
 
 // sum of x, one block, fixed order
@@ -567,18 +578,18 @@ int mlp_step(const MlpStep& s)
                                                              dOf, sq);
     if (s.loss) sum_kernel<<<1, 1024, 0, st>>>(sq, R * kMlpOut, s.loss);
     MLP_CK(mlp_gemm(st, true, false, A2, kMlpHidden, dOb, kMlpOut, Gd.W3, kMlpOut, kMlpHidden, kMlpOut, (int)R, false));
-    colsum_kernel<<<(kMlpOut + 127) / 128, 128, 0, st>>>(dOf, R, kMlpOut, Gd.b3);
+    colsum_kernel<<<(kMlpOut + 31) / 32, 1024, 0, st>>>(dOf, R, kMlpOut, Gd.b3);
     MLP_CK(mlp_gemm(st, false, true, dOb, kMlpOut, W3b, kMlpOut, dAf, kMlpHidden, (int)R, kMlpHidden, kMlpOut, false));
     relu_back_kernel<<<blocks_for(R * kMlpHidden), 256, 0, st>>>(dAf, pre2, R * kMlpHidden, dH2b, dHf);
     MLP_CK(mlp_gemm(st, true, false, A1, kMlpHidden, dH2b, kMlpHidden, Gd.W2, kMlpHidden, kMlpHidden, kMlpHidden, (int)R,
                     false));
-    colsum_kernel<<<(kMlpHidden + 127) / 128, 128, 0, st>>>(dHf, R, kMlpHidden, Gd.b2);
+    colsum_kernel<<<(kMlpHidden + 31) / 32, 1024, 0, st>>>(dHf, R, kMlpHidden, Gd.b2);
     MLP_CK(mlp_gemm(st, false, true, dH2b, kMlpHidden, W2b, kMlpHidden, dAf, kMlpHidden, (int)R, kMlpHidden,
                     kMlpHidden, false));
     relu_back_kernel<<<blocks_for(R * kMlpHidden), 256, 0, st>>>(dAf, pre1, R * kMlpHidden, dH1b, dHf);
     MLP_CK(mlp_gemm(st, true, false, Xb, kMlpIn, dH1b, kMlpHidden, Gd.W1, kMlpHidden, kMlpIn, kMlpHidden, (int)R,
                     false));
-    colsum_kernel<<<(kMlpHidden + 127) / 128, 128, 0, st>>>(dHf, R, kMlpHidden, Gd.b1);
+    colsum_kernel<<<(kMlpHidden + 31) / 32, 1024, 0, st>>>(dHf, R, kMlpHidden, Gd.b1);
     nl += 13 + (s.loss ? 1 : 0);
     if (s.adam_m) {
         const int64_t n = (int64_t)mlp_param_count();
