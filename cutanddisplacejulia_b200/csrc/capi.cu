@@ -71,7 +71,7 @@ struct BatchGraph {
     std::vector<int64_t> offsets;
     const void* ptrs[8] = {};
     double params[5] = {};
-    int flags[2] = {};
+    int flags[3] = {};
     int64_t launches = 0;
 };
 
@@ -102,6 +102,7 @@ struct cad_ctx {
     double near_factor = 3.0;
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
+    int batch_chain = 0;                   // cad_set_batch_solve: chained triangular solves in the batch sweeps
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
     int max_iter = 200;
@@ -742,15 +743,16 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
                             b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
         const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr, ctx->wait_limit};
+        const bool chain = ctx->batch_chain != 0;
         int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, (float*)l.buf[L_DINV].p,
-                               (int*)l.buf[L_PIV].p, (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, true);
+                               (int*)l.buf[L_PIV].p, (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, chain);
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "batched solve: FP32 LU failed");
         float* r32 = (float*)l.buf[L_IR32].p;
         IrArgs ia{ls, n3, A, n3, b.T + 3 * o, n3, 1, b.D + 3 * o, (float*)l.buf[L_A32].p, (int*)l.buf[L_PIV].p,
                   (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, ctx->tol, kBatchSweeps,
                   (double*)l.buf[L_IR].p, r32, r32 + n3, (double*)l.buf[L_NORMS].p,
-                  (double*)l.buf[L_KWORK].p, (const float*)l.buf[L_DINV].p, (int*)l.buf[L_SYNC].p,
-                  (double*)l.buf[L_Z].p, ctx->wait_limit};
+                  (double*)l.buf[L_KWORK].p, chain ? (const float*)l.buf[L_DINV].p : nullptr,
+                  chain ? (int*)l.buf[L_SYNC].p : nullptr, chain ? (double*)l.buf[L_Z].p : nullptr, ctx->wait_limit};
         if (ir_solve_fixed(ia, kBatchSweeps, b.rel + c) != GMRES_OK)
             return fail(ctx, CAD_ERR_CUDA, "batched solve: refinement launch failed");
     }
@@ -850,11 +852,11 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
     BatchGraph& g = ctx->batch;
     const void* ptrs[8] = {P1, P2, P3, normals, midpoints, T, D, Aall};
     const double params[5] = {nu, G, lambda, ctx->tol, ctx->near_factor};
-    const int flags[2] = {hs, ctx->assembly};
+    const int flags[3] = {hs, ctx->assembly, ctx->batch_chain};
     const bool same = g.exec && g.offsets.size() == (size_t)nbatch + 1 &&
                       std::equal(g.offsets.begin(), g.offsets.end(), offsets) &&
                       std::equal(ptrs, ptrs + 8, g.ptrs) && std::equal(params, params + 5, g.params) &&
-                      std::equal(flags, flags + 2, g.flags);
+                      std::equal(flags, flags + 3, g.flags);
     cudaEvent_t fork = nullptr;
     CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     int rc = CAD_OK;
@@ -887,7 +889,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
             g.offsets.assign(offsets, offsets + nbatch + 1);
             std::copy(ptrs, ptrs + 8, g.ptrs);
             std::copy(params, params + 5, g.params);
-            std::copy(flags, flags + 2, g.flags);
+            std::copy(flags, flags + 3, g.flags);
             g.launches = ctx->launches - l0;
             e = cudaGraphLaunch(g.exec, ctx->stream);
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: graph launch");
@@ -1039,6 +1041,14 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)
     if (!ctx) return CAD_ERR_ARG;
     if (fp32 != 0 && fp32 != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->gmres_matvec32 = fp32;
+    return CAD_OK;
+}
+
+int cad_set_batch_solve(cad_ctx* ctx, int chain)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (chain != 0 && chain != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->batch_chain = chain;
     return CAD_OK;
 }
 
@@ -1469,16 +1479,17 @@ int cad_gemm_sub_dev(cad_ctx* ctx, int precision, int64_t m, int64_t n, int64_t 
     CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     if (m < 0 || n < 0 || k < 0 || m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || lda < (m > 0 ? m : 1) ||
-        ldb < (k > 0 ? k : 1) || ldc < (m > 0 ? m : 1) || (precision != 0 && precision != 1))
+        ldb < (k > 0 ? k : 1) || ldc < (m > 0 ? m : 1) || precision < 0 || precision > 4)
         return fail(ctx, CAD_ERR_ARG, "invalid argument");
     if (m == 0 || n == 0 || k == 0) return CAD_OK;
     void* st;
     if (int r = ensure(ctx, S_GEMM, sizeof(int), &st)) return r;
     CK(cudaMemsetAsync(st, 0, sizeof(int), ctx->stream));
-    if (precision == 0)
+    if (precision != 1) {
+        static const int dmma_k[5] = {0, 0, 4, 8, 16};
         CK(gemm_sub(ctx->stream, (int)m, (int)n, (int)k, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc,
-                    (int*)st));
-    else
+                    (int*)st, dmma_k[precision]));
+    } else
         CK(gemm_sub(ctx->stream, (int)m, (int)n, (int)k, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc,
                     (int*)st));
     ++ctx->launches;

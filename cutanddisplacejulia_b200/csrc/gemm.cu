@@ -64,6 +64,33 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
+// 16 x 8 x MK DMMA (MK = 8 or 16).  Thread (g = lane / 4, t = lane % 4) holds
+// A elements (row g + 8 (r & 1), k t + 4 (r >> 1)) for r < MK / 2, B elements
+// (k t + 4 r, column g) for r < MK / 4, and C elements (row g, columns 2t,
+// 2t + 1) in c0, c1 and (row g + 8, the same columns) in c2, c3.
+template <int MK>
+__device__ __forceinline__ void dmma16(double& c0, double& c1, double& c2, double& c3, const double* a,
+                                       const double* b);
+template <>
+__device__ __forceinline__ void dmma16<8>(double& c0, double& c1, double& c2, double& c3, const double* a,
+                                          const double* b)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+template <>
+__device__ __forceinline__ void dmma16<16>(double& c0, double& c1, double& c2, double& c3, const double* a,
+                                           const double* b)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+                 "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+                 : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+                   "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // Stage s of the ring <- k-step kt: the A tile (128 rows x 16 columns, stored
 // k-major: row k holds 128 consecutive m) and the B tile (16 rows x 64
 // columns, stored n-major: row n holds 16 consecutive k).
@@ -91,6 +118,8 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
     }
 }
 
+// MK: k-extent of one DMMA (4: m8n8k4 tiles; 8 or 16: m16n8k8 / m16n8k16)
+template <int MK>
 __global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
                                                                 int64_t lda, const double* __restrict__ B, int64_t ldb,
                                                                 double* __restrict__ C, int64_t ldc)
@@ -125,17 +154,41 @@ __global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n
         cp_async_commit();
         const double* a_s = sA + (kt % DSTAGES) * DSTAGE_A;
         const double* b_s = sB + (kt % DSTAGES) * DSTAGE_B;
+        if constexpr (MK == 4) {
 #pragma unroll
-        for (int kk = 0; kk < DBK; kk += 4) {
-            double af[8], bf[4];
+            for (int kk = 0; kk < DBK; kk += 4) {
+                double af[8], bf[4];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) af[i] = a_s[swz(kk + t, wm + 8 * i + g, DLDA)];
+                for (int i = 0; i < 8; ++i) af[i] = a_s[swz(kk + t, wm + 8 * i + g, DLDA)];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = b_s[swz(wn + 8 * j + g, kk + t, DLDB)];
+                for (int j = 0; j < 4; ++j) bf[j] = b_s[swz(wn + 8 * j + g, kk + t, DLDB)];
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+                for (int i = 0; i < 8; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+            }
+        } else {
+            // 16-row blocks: acc[2I] holds rows wm + 16I + g, acc[2I + 1]
+            // rows wm + 16I + 8 + g (the 8-row layout of the m8n8k4 path)
+#pragma unroll
+            for (int kk = 0; kk < DBK; kk += MK) {
+                double af[4][MK / 2], bf[4][MK / 4];
+#pragma unroll
+                for (int I = 0; I < 4; ++I)
+#pragma unroll
+                    for (int r = 0; r < MK / 2; ++r)
+                        af[I][r] = a_s[swz(kk + t + 4 * (r >> 1), wm + 16 * I + 8 * (r & 1) + g, DLDA)];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int r = 0; r < MK / 4; ++r) bf[j][r] = b_s[swz(wn + 8 * j + g, kk + t + 4 * r, DLDB)];
+#pragma unroll
+                for (int I = 0; I < 4; ++I)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        dmma16<MK>(acc[2 * I][j][0], acc[2 * I][j][1], acc[2 * I + 1][j][0], acc[2 * I + 1][j][1],
+                                   af[I], bf[j]);
+            }
         }
     }
     cp_async_wait<0>();
@@ -384,19 +437,33 @@ bool tma_ok(const float* p, int64_t ld)
 
 }  // namespace
 
+namespace {
+template <int MK>
+cudaError_t launch_dgemm(cudaStream_t st, int m, int n, int k, const double* A, int64_t lda, const double* B,
+                         int64_t ldb, double* C, int64_t ldc)
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(dgemm_sub_kernel<MK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DSMEM);
+        cudaFuncSetAttribute(dgemm_sub_kernel<MK>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    });
+    const dim3 grid((unsigned)((m + DBM - 1) / DBM), (unsigned)((n + DBN - 1) / DBN));
+    dgemm_sub_kernel<MK><<<grid, DTHREADS, DSMEM, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const double* A, int64_t lda, const double* B, int64_t ldb,
-                     double* C, int64_t ldc, int* status)
+                     double* C, int64_t ldc, int* status, int dmma_k)
 {
     (void)status;   // the FP64 kernel has no waits
     if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(dgemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DSMEM);
-        cudaFuncSetAttribute(dgemm_sub_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    });
-    const dim3 grid((unsigned)((m + DBM - 1) / DBM), (unsigned)((n + DBN - 1) / DBN));
-    dgemm_sub_kernel<<<grid, DTHREADS, DSMEM, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
-    return cudaGetLastError();
+    switch (dmma_k > 0 ? dmma_k : kDefaultDmmaK) {
+    case 4: return launch_dgemm<4>(st, m, n, k, A, lda, B, ldb, C, ldc);
+    case 8: return launch_dgemm<8>(st, m, n, k, A, lda, B, ldb, C, ldc);
+    case 16: return launch_dgemm<16>(st, m, n, k, A, lda, B, ldb, C, ldc);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const float* A, int64_t lda, const float* B, int64_t ldb,

@@ -132,6 +132,13 @@ int64_t cad_autotune_entries(const cad_ctx* ctx, int64_t* tuned_here);
  * forming the residual b - A x in FP64, so the tolerance is met in FP64;
  * fp32 = 0 multiplies with the FP64 A.  No counterpart in the reference. */
 int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
+/* Triangular solves of the many-crack batch's refinement sweeps
+ * (cad_slip_calculator_batched*): chain = 0 (default) uses the blocked
+ * solves (64-row diagonal blocks and GEMM updates); chain = 1 the two
+ * ticket-ordered chain launches per sweep with precomputed inverses of the
+ * diagonal blocks.  Both give the same slips to the refinement tolerance.  No
+ * counterpart in the reference. */
+int cad_set_batch_solve(cad_ctx* ctx, int chain);
 /* Device waits (a leaf's pivot exchange, a triangular-solve chain flag) poll
  * at most `polls` times (default 4194304, a few seconds at worst) before the
  * kernel records the failure and returns; the call then reports
@@ -304,7 +311,9 @@ int cad_solve_dev(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, in
 /* C (m x n, ldc) -= A (m x k, lda) * B (k x n, ldb), column-major device
  * arrays, precision 0 = FP64 (DMMA tensor cores), 1 = FP32 (TF32 tensor cores
  * through tcgen05 when A and B start on 16-byte boundaries and lda, ldb are
- * multiples of 4; FP32 CUDA cores otherwise).  The trailing-update product of
+ * multiples of 4; FP32 CUDA cores otherwise); 2, 3, 4 = FP64 with the DMMA
+ * shape m8n8k4, m16n8k8 or m16n8k16 (precision 0 takes the library's
+ * default shape).  The trailing-update product of
  * the dense LU that replaces the reference's A\b (src/SlipCalculator3D.jl:22),
  * exposed on its own for testing and measurement; synchronises the context
  * stream. */

@@ -7,7 +7,9 @@ Integer-valued operands are exact in TF32 and in FP64, and their products
 sum exactly in FP32 below 2^24: those cases must match bit for bit, which
 pins the tensor-memory and shared-memory descriptor layouts entry by entry.
 Random operands check the rounding: FP64 to 1e-13 of the product's scale,
-TF32 norm-wise to 2e-3 (10-bit mantissa inputs, FP32 accumulation)."""
+TF32 norm-wise to 2e-3 (10-bit mantissa inputs, FP32 accumulation).
+Precision codes 2, 3, 4 are FP64 with the DMMA shapes m8n8k4, m16n8k8 and
+m16n8k16, whose fragment layouts the integer cases pin element by element."""
 import numpy as np
 import pytest
 
@@ -20,7 +22,7 @@ def _run(cad, prec, m, n, k, lda, ldb, ldc, a_off=0, b_off=0, integer=False, see
     import torch
 
     from cutanddisplacejulia_b200 import _lib
-    dt = torch.float64 if prec == 0 else torch.float32
+    dt = torch.float32 if prec == 1 else torch.float64
     dev = torch.device("cuda", 0)
     g = torch.Generator(device="cpu").manual_seed(seed)
 
@@ -53,7 +55,7 @@ def _run(cad, prec, m, n, k, lda, ldb, ldc, a_off=0, b_off=0, integer=False, see
     return Cd, ref, (Ad @ Bd)
 
 
-@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("prec", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("m,n,k", SHAPES)
 def test_gemm_integer_exact(cad, prec, m, n, k):
     ld = lambda r: (r + 3) // 4 * 4 + 4   # multiples of 4: the tcgen05 + TMA path for FP32
@@ -61,17 +63,17 @@ def test_gemm_integer_exact(cad, prec, m, n, k):
     assert float((got - ref).abs().max()) == 0.0
 
 
-@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("prec", [0, 1, 3, 4])
 @pytest.mark.parametrize("m,n,k", SHAPES)
 def test_gemm_random(cad, prec, m, n, k):
     got, ref, prod = _run(cad, prec, m, n, k, m + 8, k + 12, m + 3, seed=1)
-    if prec == 0:
+    if prec != 1:
         assert float((got - ref).abs().max()) <= 1e-13 * k
     else:
         assert float((got - ref).norm() / prod.norm()) <= 2e-3
 
 
-@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("prec", [0, 1, 3, 4])
 def test_gemm_offsets_and_odd_leading_dimensions(cad, prec):
     # sub-matrices at row offsets of the LU's trailing updates (multiples of
     # 4) and odd leading dimensions (FP64: any; FP32: the CUDA-core kernel)
@@ -87,4 +89,5 @@ def test_gemm_empty_and_bad_arguments(cad):
     assert L.cad_gemm_sub_dev(ctx, 0, 0, 5, 5, None, 1, None, 5, None, 1) == 0
     assert L.cad_gemm_sub_dev(ctx, 1, 10, 5, 0, None, 10, None, 1, None, 10) == 0
     assert L.cad_gemm_sub_dev(ctx, 0, 10, 5, 5, None, 9, None, 5, None, 10) == _lib.CAD_ERR_ARG
-    assert L.cad_gemm_sub_dev(ctx, 2, 10, 5, 5, None, 10, None, 5, None, 10) == _lib.CAD_ERR_ARG
+    assert L.cad_gemm_sub_dev(ctx, 5, 10, 5, 5, None, 10, None, 5, None, 10) == _lib.CAD_ERR_ARG
+    assert L.cad_gemm_sub_dev(ctx, -1, 10, 5, 5, None, 10, None, 5, None, 10) == _lib.CAD_ERR_ARG
