@@ -73,6 +73,8 @@ WORKLOADS = {
               "%d full-space penny/elliptical cracks, semi-axis U[0.5,2], aspect U[0.3,1], random orientation, "
               "200-2000 triangles each (log-uniform), %d triangles in all"),
 }
+WORKLOADS["gemm"] = ("LU trailing-update GEMM TFLOP/s (C -= A B, column-major)",
+                     "%d x %d x %d, FP64 DMMA (each instruction shape) and TF32 tcgen05")
 METRIC = WORKLOADS["penny"][0]
 
 
@@ -1176,6 +1178,57 @@ def friction_call(L, ctx, c, out):
                                           out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data)
 
 
+def run_gemm(args, rank, world, local_rank):
+    """The dense LU's own trailing-update product on its own: C (m x m) -= A
+    (m x k) B (k x m) with k = 256 (the LU's block width), FP64 on DMMA tensor
+    cores (library default and each instruction shape) and FP32 on TF32
+    tcgen05 tensor cores; per-launch time from CUDA events on the library's
+    stream, inputs larger than L2 (C alone is m^2 x 8 bytes)."""
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
+    torch.cuda.set_stream(stream)
+    m, k = args.gemm_m, 256
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.cad_fp64_fma_probe(ctx, 20000, ctypes.byref(peak)), ctx)
+    res = {}
+    for name, prec, dt in (("fp64", 0, torch.float64), ("fp64_m8n8k4", 2, torch.float64),
+                           ("fp64_m16n8k8", 3, torch.float64), ("fp64_m16n8k16", 4, torch.float64),
+                           ("tf32", 1, torch.float32)):
+        g = torch.Generator(device=dev).manual_seed(0)
+        A = torch.rand(m * k, dtype=dt, device=dev, generator=g)
+        B = torch.rand(k * m, dtype=dt, device=dev, generator=g)
+        C = torch.rand(m * m, dtype=dt, device=dev, generator=g)
+
+        def call():
+            _lib.check(L.cad_gemm_sub_dev(ctx, prec, m, m, k, A.data_ptr(), m, B.data_ptr(), k, C.data_ptr(), m),
+                       ctx)
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = cdist.max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+        res[name] = {"ms": ms, "tflops": 2.0 * m * m * k / (ms * 1e-3) / 1e12}
+        del A, B, C
+    line = {"metric": WORKLOADS["gemm"][0], "value": res["fp64"]["tflops"], "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["fp64"]["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS["gemm"][1] % (m, m, k), "l2": "inputs larger than L2"},
+            "fp64_fma_peak_tflops": peak.value, "frac_fp64": res["fp64"]["tflops"] / peak.value, "variants": res}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_friction(args, rank, world, local_rank):
     """Frictional slip (src/SlipCalculator3D.jl:36-238) through the C ABI with
     host buffers: one step = assembly of A, C = inv(A Scl) by the FP64 LU,
@@ -1269,6 +1322,7 @@ def main():
     ap.add_argument("--friction-spacing", type=float, nargs="+", default=list(FRICTION_SPACINGS),
                     help="lattice spacings of the friction workload's penny cracks (0.12: 496 triangles)")
     ap.add_argument("--cracks", type=int, default=512, help="cracks of the batch workload")
+    ap.add_argument("--gemm-m", type=int, default=16384, help="rows and columns of the gemm workload's C")
     ap.add_argument("--train-meshes", type=int, default=32, help="training meshes of the learned preconditioner")
     ap.add_argument("--train-min", type=int, default=500, help="smallest training mesh (triangles)")
     ap.add_argument("--train-max", type=int, default=2000, help="largest training mesh (triangles)")
@@ -1296,6 +1350,8 @@ def main():
             run_learned(args, rank, world, local_rank)
         elif args.workload == "friction":
             run_friction(args, rank, world, local_rank)
+        elif args.workload == "gemm":
+            run_gemm(args, rank, world, local_rank)
         elif args.workload == "dipping":
             run_c3(args, rank, world, local_rank)
         else:

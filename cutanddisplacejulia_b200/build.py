@@ -19,7 +19,7 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC",
 ]
-LIBS = ["-lcublas"]
+LIBS: list = []
 
 
 def _nvcc():

@@ -5,7 +5,6 @@
 // (no allocation in steady state).  Host-pointer entry points copy inputs in,
 // run the device path and copy results out; *_dev entry points run the device
 // path directly on caller-provided device memory.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
@@ -41,7 +40,7 @@ enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
-    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_COUNT
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -53,17 +52,15 @@ struct DevBuf {
 
 // One lane of the batched solve: its own streams, cuBLAS handles and
 // workspaces, so cracks on different lanes run concurrently.
-enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS, L_BLASWS,
+enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS,
                 L_KWORK, L_DINV, L_SYNC, L_Z, L_COUNT };
 struct Lane {
     cudaStream_t main = nullptr, side = nullptr;
-    cublasHandle_t main_blas = nullptr, side_blas = nullptr;
     cudaEvent_t done = nullptr;
     DevBuf buf[L_COUNT];
 };
 constexpr int kLanes = 32;           // cracks of a batch in flight at once
 constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
-constexpr size_t kBlasWorkspace = 32u << 20;
 
 // The captured graph of the last batched call and what it was captured for.
 struct BatchGraph {
@@ -81,9 +78,7 @@ struct cad_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    cublasHandle_t blas = nullptr;
     cudaStream_t side_stream = nullptr;   // the LU's look-ahead trailing updates
-    cublasHandle_t side_blas = nullptr;
     LuGraphCache* graphs = nullptr;       // captured LU factorisations, replayed for repeated calls
     std::vector<Lane> lanes;              // batched solve (created on first use)
     BatchGraph batch;
@@ -332,7 +327,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     if (int r = ensure(ctx, S_SYNC, mixed_sync_ints(n) * sizeof(int), &sync)) return r;
     if (int r = ensure(ctx, S_WORK, (size_t)n * sizeof(double), &work)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    const LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
+    const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches,
                         ctx->graphs, ctx->wait_limit};
     ctx->timed[1] = ctx->timed[2] = false;
     int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
@@ -345,7 +340,6 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     double* V = (double*)kry;
     double* w = V + (size_t)n * (kRestart + 1);
     GmresArgs g{};
-    g.blas = ctx->blas;
     g.stream = ctx->stream;
     g.n = n;
     g.A = A;
@@ -437,7 +431,6 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     double* V = (double*)kry;
     double* w = V + (size_t)n * (kRestart + 1);
     GmresArgs g{};
-    g.blas = ctx->blas;
     g.stream = ctx->stream;
     g.n = n;
     g.A = A;
@@ -556,7 +549,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     ctx->timed[1] = ctx->timed[2] = false;
-    LuStreams ls{ctx->stream, ctx->blas, ctx->side_stream, ctx->side_blas, &ctx->launches,
+    LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches,
                  ctx->graphs, ctx->wait_limit};
     if (ctx->tuner.mode != TUNE_OFF) {
         // leaf width of the panel factorisation (rows per leaf thread), timed
@@ -673,17 +666,6 @@ int make_lanes(cad_ctx* ctx)
         CK(cudaStreamCreateWithPriority(&l.main, cudaStreamNonBlocking, prio_high));
         CK(cudaStreamCreateWithPriority(&l.side, cudaStreamNonBlocking, prio_low));
         CK(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming));
-        if (cublasCreate(&l.main_blas) != CUBLAS_STATUS_SUCCESS || cublasCreate(&l.side_blas) != CUBLAS_STATUS_SUCCESS)
-            return fail(ctx, CAD_ERR_CUDA, "cuBLAS handle creation failed");
-        // fixed workspaces: nothing is allocated while the batch is captured
-        void *w0, *w1;
-        if (int r = lane_ensure(ctx, l, L_BLASWS, 2 * kBlasWorkspace, &w0)) return r;
-        w1 = (char*)w0 + kBlasWorkspace;
-        if (cublasSetStream(l.main_blas, l.main) != CUBLAS_STATUS_SUCCESS ||
-            cublasSetStream(l.side_blas, l.side) != CUBLAS_STATUS_SUCCESS ||
-            cublasSetWorkspace(l.main_blas, w0, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS ||
-            cublasSetWorkspace(l.side_blas, w1, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS)
-            return fail(ctx, CAD_ERR_CUDA, "cuBLAS lane set-up failed");
     }
     return CAD_OK;
 }
@@ -742,7 +724,7 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         double* A = b.Aall + (*b.aoff)[c];
         CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
                             b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
-        const LuStreams ls{l.main, l.main_blas, l.side, l.side_blas, &ctx->launches, nullptr, ctx->wait_limit};
+        const LuStreams ls{l.main, l.side, &ctx->launches, nullptr, ctx->wait_limit};
         const bool chain = ctx->batch_chain != 0;
         int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, (float*)l.buf[L_DINV].p,
                                (int*)l.buf[L_PIV].p, (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, chain);
@@ -949,11 +931,7 @@ int cad_init(int device, cad_ctx** out)
             cad_destroy(ctx);
             return CAD_ERR_CUDA;
         }
-    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS ||
-        cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
-        cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
-        cublasCreate(&ctx->side_blas) != CUBLAS_STATUS_SUCCESS ||
-        cublasSetStream(ctx->side_blas, ctx->side_stream) != CUBLAS_STATUS_SUCCESS) {
+    if (cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, prio_low) != cudaSuccess) {
         cad_destroy(ctx);
         return CAD_ERR_CUDA;
     }
@@ -981,14 +959,10 @@ int cad_destroy(cad_ctx* ctx)
         if (l.side) cudaStreamSynchronize(l.side);
         for (auto& b : l.buf)
             if (b.p) cudaFree(b.p);
-        if (l.main_blas) cublasDestroy(l.main_blas);
-        if (l.side_blas) cublasDestroy(l.side_blas);
         if (l.main) cudaStreamDestroy(l.main);
         if (l.side) cudaStreamDestroy(l.side);
         if (l.done) cudaEventDestroy(l.done);
     }
-    if (ctx->blas) cublasDestroy(ctx->blas);
-    if (ctx->side_blas) cublasDestroy(ctx->side_blas);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -1100,8 +1074,6 @@ int cad_set_stream(cad_ctx* ctx, void* stream)
     CAD_NVTX_RANGE();
     if (int r = set_device(ctx)) return r;
     ctx->stream = (cudaStream_t)stream;   // NULL is CUDA's default stream, as everywhere in CUDA
-    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "cublasSetStream failed");
     return CAD_OK;
 }
 
@@ -1938,13 +1910,16 @@ int cad_slip_calculator_fixed(cad_ctx* ctx, const double* P1, const double* P2, 
     // matrix): normal equations A^T A D = A^T b, solved by the FP64 LU
     double* AtA = (double*)ata;
     double* Atb = AtA + (size_t)m3 * m3;
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)m3, (int)m3, (int)n3, &one, (const double*)A, (int)n3,
-                    (const double*)A, (int)n3, &zero, AtA, (int)m3) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemv(ctx->blas, CUBLAS_OP_T, (int)n3, (int)m3, &one, (const double*)A, (int)n3, (const double*)b, 1,
-                    &zero, Atb, 1) != CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "normal equations: cuBLAS error");
+    // A^T A = 0 - (-A^T) A through the library's DMMA product; A^T b by a
+    // column-wise reduction
+    void* atv;
+    if (int r = ensure(ctx, S_AT, (size_t)m3 * n3 * sizeof(double) + 16, &atv)) return r;
+    CK(krylov_transpose_neg(ctx->stream, (const double*)A, n3, n3, m3, (double*)atv, m3, &ctx->launches));
+    CK(cudaMemsetAsync(AtA, 0, (size_t)m3 * m3 * sizeof(double), ctx->stream));
+    CK(gemm_sub(ctx->stream, (int)m3, (int)m3, (int)n3, (const double*)atv, m3, (const double*)A, n3, AtA, m3,
+                nullptr));
+    ++ctx->launches;
+    CK(krylov_gemv_t(ctx->stream, (const double*)A, n3, n3, m3, (const double*)b, Atb, &ctx->launches));
     const int solver = ctx->solver;
     ctx->solver = CAD_SOLVER_LU64;
     int r = solve_device(ctx, m3, AtA, m3, Atb, m3, 1);
@@ -2032,6 +2007,9 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
     double *coef = V + 8 * n, *u0 = coef + 16 * op.m, *cu0 = u0 + 3 * op.m, *rhs = cu0 + 3 * op.m;
     double* stats = part + (size_t)kRedBlocks * (kLsSteps + 1);
     double* psi_dev = stats + 8;
+    void* kwv;
+    if (int r = ensure(ctx, S_KWORK, krylov_work_doubles(n) * sizeof(double), &kwv)) return r;
+    const KrylovWork kw = krylov_carve((double*)kwv, n);
     cudaStream_t st = ctx->stream;
     CK(cudaMemsetAsync(x, 0, n * sizeof(double), st));
     CK(cudaMemsetAsync(w, 0, n * sizeof(double), st));
@@ -2051,7 +2029,7 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
     bool stalled = false;
     double rel = 0.0;
     for (;;) {
-        if (lcp_matvec(op, ctx->blas, st, x, q, y, u, &ctx->launches))
+        if (lcp_matvec(op, kw, st, x, q, y, u, &ctx->launches))
             return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
         CK(lcp_fb_eval(x, y, n, phi, z, part, stats, st, &ctx->launches));
         CK(cudaMemcpyAsync(hs, stats, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -2060,17 +2038,15 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
         const double psi = 0.5 * hs[1];
         if (!(rel > tol) || it >= max_iter || stalled) break;
         if (hs[2] > 0.0)   // rows with x_i = y_i = 0: w = M z
-            if (lcp_matvec(op, ctx->blas, st, z, nullptr, w, u, &ctx->launches))
+            if (lcp_matvec(op, kw, st, z, nullptr, w, u, &ctx->launches))
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
         CK(lcp_fb_diag(x, y, z, w, phi, n, Da, Db, d, st, &ctx->launches));
         int info = 0;
         if (op.friction) {   // J d = -phi through the 3m x 3m reduced system
             const int64_t m = op.m, m3 = 3 * m;
-            const double one = 1.0, zero = 0.0;
             CK(friction_reduce_prep(Da, Db, d, op.mu, m, coef, u0, st, &ctx->launches));
-            if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS ||
-                cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)m3, (int)m3, &one, op.C, (int)op.ldc, u0, 1, &zero, cu0,
-                            1) != CUBLAS_STATUS_SUCCESS)
+            if (krylov_gemv<double>(st, op.C, op.ldc, (int)m3, u0, 1.0, nullptr, cu0, kw, nullptr, 0, 0,
+                                    &ctx->launches) != cudaSuccess)
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
             CK(friction_reduced_rhs(d, Da, Db, cu0, coef, m, rhs, st, &ctx->launches));
             CK(friction_reduced_jacobian(op.C, op.ldc, op.mu, Da, Db, coef, m, J, m3, st));
@@ -2087,7 +2063,7 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
         double slope = -2.0 * psi;
         bool newton = info == 0;
         if (newton) {
-            if (lcp_matvec(op, ctx->blas, st, d, nullptr, Md, u, &ctx->launches))
+            if (lcp_matvec(op, kw, st, d, nullptr, Md, u, &ctx->launches))
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
             CK(lcp_line_search(x, d, y, Md, n, part, psi_dev, st, &ctx->launches));
             CK(cudaMemcpyAsync(hs, psi_dev, (kLsSteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -2096,13 +2072,13 @@ int lcp_newton_device(cad_ctx* ctx, const LcpOperator& op, const double* q, doub
         }
         if (!newton) {   // steepest descent: d = -(Da phi + M^T (Db phi))
             CK(lcp_scale(Db, phi, n, Md, st, &ctx->launches));
-            if (lcp_matvec_t(op, ctx->blas, st, Md, d, u, &ctx->launches))
+            if (lcp_matvec_t(op, st, Md, d, u, &ctx->launches))
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
             CK(lcp_grad_dir(Da, phi, n, d, part, stats, st, &ctx->launches));
             CK(cudaMemcpyAsync(hs, stats + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             slope = -hs[0];
-            if (lcp_matvec(op, ctx->blas, st, d, nullptr, Md, u, &ctx->launches))
+            if (lcp_matvec(op, kw, st, d, nullptr, Md, u, &ctx->launches))
                 return fail(ctx, CAD_ERR_CUDA, "LCP: matrix-vector product failed");
             CK(lcp_line_search(x, d, y, Md, n, part, psi_dev, st, &ctx->launches));
             CK(cudaMemcpyAsync(hs, psi_dev, (kLsSteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -2241,11 +2217,12 @@ int friction_solve_device(cad_ctx* ctx, const double* Tn, const double* Tss, con
     if (int r = upload(ctx, b + 2 * N, Tds, N)) return r;
     // q = [C (b - [0; Sf; Sf]); 2 Sf; 2 Sf] (src/SlipCalculator3D.jl:158-163, :190-193)
     CK(friction_rhs(b, dsf, N, rr, q, ctx->stream, &ctx->launches));
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemv(ctx->blas, CUBLAS_OP_N, (int)n3, (int)n3, &one, C, (int)n3, rr, 1, &zero, q, 1) !=
-            CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, CAD_ERR_CUDA, "friction right-hand side: cuBLAS error");
+    {
+        void* kwv;
+        if (int r = ensure(ctx, S_KWORK, krylov_work_doubles(n3) * sizeof(double), &kwv)) return r;
+        CK(krylov_gemv<double>(ctx->stream, C, n3, (int)n3, rr, 1.0, nullptr, q, krylov_carve((double*)kwv, n3),
+                               nullptr, 0, 0, &ctx->launches));
+    }
     LcpOperator op;
     op.friction = true;
     op.n = n5;

@@ -263,6 +263,37 @@ __global__ void cast_to_f32_kernel(const double* __restrict__ A, int64_t lda, in
             B[r + c * ldb] = (float)A[r + c * lda];
 }
 
+// y[j] = sum_i A[i + j lda] x[i] (j < cols, i < rows): one warp per column,
+// lane-strided partial sums combined by a fixed shuffle tree
+__global__ void gemv_t_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int64_t cols,
+                              const double* __restrict__ x, double* __restrict__ y)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t j = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); j < cols; j += warps) {
+        const double* a = A + j * lda;
+        double s = 0.0;
+        for (int64_t i = lane; i < rows; i += 32) s = fma(a[i], x[i], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) y[j] = s;
+    }
+}
+
+// At[j + i ldt] = -A[i + j lda] through 32 x 32 shared-memory tiles
+__global__ void transpose_neg_kernel(const double* __restrict__ A, int64_t lda, int64_t rows, int64_t cols,
+                                     double* __restrict__ At, int64_t ldt)
+{
+    __shared__ double t[32][33];
+    const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+    for (int r = ty; r < 32; r += 8)
+        if (i0 + tx < rows && j0 + r < cols) t[r][tx] = A[(i0 + tx) + (j0 + r) * lda];
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8)
+        if (j0 + tx < cols && i0 + r < rows) At[(j0 + tx) + (i0 + r) * ldt] = -t[tx][r];
+}
+
 inline unsigned nb(int n) { return (unsigned)((n + kRows - 1) / kRows); }
 
 }  // namespace
@@ -368,6 +399,28 @@ cudaError_t krylov_cast_f32(cudaStream_t st, const double* A, int64_t lda, int64
     const int64_t rb = (n + 255) / 256;
     cast_to_f32_kernel<<<dim3((unsigned)(rb < 8 ? rb : 8), (unsigned)(n < 8192 ? n : 8192)), 256, 0, st>>>(A, lda, n,
                                                                                                       B, ldb);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t krylov_gemv_t(cudaStream_t st, const double* A, int64_t lda, int64_t rows, int64_t cols, const double* x,
+                          double* y, int64_t* launches)
+{
+    if (cols <= 0) return cudaSuccess;
+    if (rows <= 0) return cudaMemsetAsync(y, 0, (size_t)cols * sizeof(double), st);
+    const int64_t blocks = (cols + 7) / 8;
+    gemv_t_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(A, lda, rows, cols, x, y);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t krylov_transpose_neg(cudaStream_t st, const double* A, int64_t lda, int64_t rows, int64_t cols, double* At,
+                                 int64_t ldt, int64_t* launches)
+{
+    if (rows <= 0 || cols <= 0) return cudaSuccess;
+    if ((rows + 31) / 32 > INT32_MAX || (cols + 31) / 32 > 65535) return cudaErrorInvalidValue;
+    transpose_neg_kernel<<<dim3((unsigned)((rows + 31) / 32), (unsigned)((cols + 31) / 32)), 256, 0, st>>>(
+        A, lda, rows, cols, At, ldt);
     if (launches) ++*launches;
     return cudaGetLastError();
 }

@@ -51,4 +51,11 @@ cudaError_t krylov_axpy(cudaStream_t st, double a, const double* x, int n, doubl
 cudaError_t krylov_cast_f32(cudaStream_t st, const double* A, int64_t lda, int64_t n, float* B, int64_t ldb,
                             int64_t* launches);
 
+// y = A^T x (A column-major rows x cols, lda; FP64), cols outputs
+cudaError_t krylov_gemv_t(cudaStream_t st, const double* A, int64_t lda, int64_t rows, int64_t cols, const double* x,
+                          double* y, int64_t* launches);
+// At (cols x rows, ldt) = -A^T (A rows x cols, lda)
+cudaError_t krylov_transpose_neg(cudaStream_t st, const double* A, int64_t lda, int64_t rows, int64_t cols, double* At,
+                                 int64_t ldt, int64_t* launches);
+
 }  // namespace cad

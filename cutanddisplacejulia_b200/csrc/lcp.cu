@@ -13,7 +13,6 @@
 // values, Jacobian diagonals, trial points, the Newton matrix entries), the
 // same operations are written with round-to-nearest intrinsics so that no
 // multiply-add is contracted.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -132,12 +131,6 @@ __global__ void friction_post_t_kernel(const double* __restrict__ v, const doubl
         out[3 * m + r] = v[m + r];
         out[4 * m + r] = v[2 * m + r];
     }
-}
-
-__global__ void add_kernel(double* __restrict__ out, const double* __restrict__ q, int64_t n)
-{
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = __dadd_rn(out[i], q[i]);
 }
 
 // Per-block partials of (max |phi|, sum phi^2, degenerate count) at part[3 b + k]
@@ -461,45 +454,31 @@ unsigned cols_grid(int64_t n) { return (unsigned)(n < 32768 ? (n < 1 ? 1 : n) : 
 
 size_t lcp_partial_doubles() { return (size_t)kStat + 64; }
 
-int lcp_matvec(const LcpOperator& op, cublasHandle_t blas, cudaStream_t st, const double* v, const double* q,
+int lcp_matvec(const LcpOperator& op, const KrylovWork& kw, cudaStream_t st, const double* v, const double* q,
                double* out, double* u, int64_t* launches)
 {
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(blas, st) != CUBLAS_STATUS_SUCCESS) return 1;
     if (!op.friction) {
-        if (cublasDgemv(blas, CUBLAS_OP_N, (int)op.n, (int)op.n, &one, op.M, (int)op.ldm, v, 1, &zero, out, 1) !=
-            CUBLAS_STATUS_SUCCESS)
+        if (krylov_gemv<double>(st, op.M, op.ldm, (int)op.n, v, 1.0, q, out, kw, nullptr, 0, 0, launches) !=
+            cudaSuccess)
             return 1;
-        if (q) {
-            add_kernel<<<grid_for(op.n), kThreads, 0, st>>>(out, q, op.n);
-            if (launches) ++*launches;
-        }
-        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+        return 0;
     }
     const int64_t m = op.m;
     friction_pre_kernel<<<grid_for(m), kThreads, 0, st>>>(v, op.mu, m, u);
-    if (cublasDgemv(blas, CUBLAS_OP_N, (int)(3 * m), (int)(3 * m), &one, op.C, (int)op.ldc, u, 1, &zero, out, 1) !=
-        CUBLAS_STATUS_SUCCESS)
+    if (launches) ++*launches;
+    if (krylov_gemv<double>(st, op.C, op.ldc, (int)(3 * m), u, 1.0, nullptr, out, kw, nullptr, 0, 0, launches) !=
+        cudaSuccess)
         return 1;
     friction_post_kernel<<<grid_for(m), kThreads, 0, st>>>(v, op.mu, q, m, out);
-    if (launches) *launches += 2;
+    if (launches) ++*launches;
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
-int lcp_matvec_t(const LcpOperator& op, cublasHandle_t blas, cudaStream_t st, const double* v, double* out,
-                 double* u, int64_t* launches)
+int lcp_matvec_t(const LcpOperator& op, cudaStream_t st, const double* v, double* out, double* u, int64_t* launches)
 {
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(blas, st) != CUBLAS_STATUS_SUCCESS) return 1;
-    if (!op.friction)
-        return cublasDgemv(blas, CUBLAS_OP_T, (int)op.n, (int)op.n, &one, op.M, (int)op.ldm, v, 1, &zero, out, 1) ==
-                       CUBLAS_STATUS_SUCCESS
-                   ? 0
-                   : 1;
+    if (!op.friction) return krylov_gemv_t(st, op.M, op.ldm, op.n, op.n, v, out, launches) == cudaSuccess ? 0 : 1;
     const int64_t m = op.m;
-    if (cublasDgemv(blas, CUBLAS_OP_T, (int)(3 * m), (int)(3 * m), &one, op.C, (int)op.ldc, v, 1, &zero, u, 1) !=
-        CUBLAS_STATUS_SUCCESS)
-        return 1;
+    if (krylov_gemv_t(st, op.C, op.ldc, 3 * m, 3 * m, v, u, launches) != cudaSuccess) return 1;
     friction_post_t_kernel<<<grid_for(m), kThreads, 0, st>>>(v, op.mu, u, m, out);
     if (launches) ++*launches;
     return cudaGetLastError() == cudaSuccess ? 0 : 2;

@@ -2,10 +2,11 @@
 // of the frictional slip problem (src/SlipCalculator3D.jl:90-175) or a dense
 // matrix, and the element-wise pieces of a Fischer-Burmeister Newton method.
 #pragma once
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+
+#include "krylov.h"
 
 namespace cad {
 
@@ -35,11 +36,12 @@ constexpr int kLsSteps = 40;
 size_t lcp_partial_doubles();   // device workspace of the reductions
 
 // out = M v (+ q when q is set).  u: 3m doubles of workspace (friction).
-int lcp_matvec(const LcpOperator& op, cublasHandle_t blas, cudaStream_t st, const double* v, const double* q,
+// (krylov work: krylov_work_doubles(n) of device scratch, n = the operator's
+// size: 3m for friction)
+int lcp_matvec(const LcpOperator& op, const KrylovWork& kw, cudaStream_t st, const double* v, const double* q,
                double* out, double* u, int64_t* launches);
 // out = M^T v.  u: 3m doubles of workspace (friction).
-int lcp_matvec_t(const LcpOperator& op, cublasHandle_t blas, cudaStream_t st, const double* v, double* out,
-                 double* u, int64_t* launches);
+int lcp_matvec_t(const LcpOperator& op, cudaStream_t st, const double* v, double* out, double* u, int64_t* launches);
 
 // J (n x n, ldj) = diag(Da) + diag(Db) M.
 cudaError_t lcp_build_jacobian(const LcpOperator& op, const double* Da, const double* Db, double* J, int64_t ldj,

@@ -1,6 +1,5 @@
 // Dense LU with partial pivoting + solve (csrc/lu.cu).
 #pragma once
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -10,7 +9,7 @@ namespace cad {
 enum { LU_OK = 0, LU_CUDA_ERROR = 1, LU_BLAS_ERROR = 2, LU_TOO_LARGE = 3 };
 
 // Executable CUDA graphs of lu_factor_solve calls, one per call signature
-// (precision, sizes, every pointer, streams and handles).  The factorisation
+// (precision, sizes, every pointer and the streams).  The factorisation
 // is thousands of dependent launches -- leaves, row swaps, triangular blocks,
 // GEMMs -- whose launch gaps dominate at moderate n; a signature seen a second
 // time is captured once and replayed from then on as a single graph launch.
@@ -20,15 +19,12 @@ struct LuGraphCache;
 LuGraphCache* lu_graph_cache_create();
 void lu_graph_cache_destroy(LuGraphCache* c);
 
-// Where the factorisation runs: the caller's stream (and a cuBLAS handle for
-// it), plus an optional side stream with its own handle for the look-ahead's
-// trailing updates (side_blas null: everything on the main stream).  The
-// result is ordered on the main stream.
+// Where the factorisation runs: the caller's stream, plus an optional side
+// stream for the look-ahead's trailing updates (side null: everything on the
+// main stream).  The result is ordered on the main stream.
 struct LuStreams {
     cudaStream_t main;
-    cublasHandle_t main_blas;
     cudaStream_t side;
-    cublasHandle_t side_blas;
     int64_t* launches;       // if set, incremented by the number of own kernel launches
     LuGraphCache* graphs;    // if set, repeated call signatures replay a captured graph
     long wait_limit = 0;     // polls a device wait makes before it gives up (0: kDefaultWaitLimit)

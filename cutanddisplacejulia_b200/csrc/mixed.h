@@ -1,6 +1,5 @@
 // Mixed-precision solve: FP32/TF32 LU preconditioner + FP64 GMRES (csrc/mixed.cu).
 #pragma once
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -27,7 +26,6 @@ size_t mixed_sync_ints(int64_t n);   // flags, tickets and the failure word of o
 enum { GMRES_OK = 0, GMRES_NOT_CONVERGED = 1, GMRES_CUDA_ERROR = 2, GMRES_BLAS_ERROR = 3, GMRES_TIMEOUT = 4 };
 
 struct GmresArgs {
-    cublasHandle_t blas;   // unused by gmres_ir_solve (own kernels)
     cudaStream_t stream;
     int64_t n;
     const double* A;   // FP64 system matrix (n x n, lda): the true residual of every restart
