@@ -262,14 +262,19 @@ def solve(A, B, device=0, solver="lu64", tol=1e-10, max_iter=200):
     return X[:, 0] if vec else X
 
 
+BATCH_MODES = {"grouped": 0, "lanes": 1, "lanes_chain": 2}
+
+
 def SlipCalculator3D_batched(cracks, nu, G, lam, HSFlag, BoundaryConditions, device=0, tol=1e-10,
-                             assembly="mixed", near_factor=3.0):
+                             assembly="mixed", near_factor=3.0, mode="grouped"):
     """SlipCalculator3D (src/SlipCalculator3D.jl:1-33) over many independent
     cracks in one batched GPU call.  cracks: list of (P1, P2, P3); one
     boundary condition per crack (or one for all).  Each crack is assembled
     (assembly="mixed": FP32 far field, FP64 near field; "fp64": all FP64) and
-    solved by FP32 LU with FP64 refinement to relative residual tol.  Returns
-    a list of (Dn, Dss, Dds) and the final relative residuals."""
+    solved by FP32 LU with FP64 refinement to relative residual tol (mode:
+    "grouped" -- every crack in each launch; "lanes" / "lanes_chain" -- every
+    crack on its own stream lane).  Returns a list of (Dn, Dss, Dds) and the
+    final relative residuals."""
     from .geometry import CreateFaceNormalAndMidPoint
     bcs = BoundaryConditions if isinstance(BoundaryConditions, (list, tuple)) else [BoundaryConditions] * len(cracks)
     if len(bcs) != len(cracks):
@@ -290,13 +295,16 @@ def SlipCalculator3D_batched(cracks, nu, G, lam, HSFlag, BoundaryConditions, dev
     D = np.zeros(3 * offs[-1])
     rel = np.zeros(len(cracks))
     ctx = _lib.context(device)
+    L = _lib.load()
+    _lib.check(L.cad_set_batch_solve(ctx, BATCH_MODES[mode]), ctx)
     with _lib.solver_mode(ctx, "mixed", tol, 400), _lib.assembly_mode(ctx, assembly, near_factor):
-        rc = _lib.load().cad_slip_calculator_batched(ctx, len(cracks), offsets.ctypes.data, cat["P1"].ctypes.data,
+        rc = L.cad_slip_calculator_batched(ctx, len(cracks), offsets.ctypes.data, cat["P1"].ctypes.data,
                                                      cat["P2"].ctypes.data, cat["P3"].ctypes.data,
                                                      cat["nrm"].ctypes.data, cat["mid"].ctypes.data, float(nu),
                                                      float(G), float(lam), int(HSFlag), cat["T"].ctypes.data,
                                                      D.ctypes.data, rel.ctypes.data)
-        _lib.check(rc, ctx)
+    L.cad_set_batch_solve(ctx, 0)
+    _lib.check(rc, ctx)
     out = []
     for c in range(len(cracks)):
         o, N = offs[c], offs[c + 1] - offs[c]

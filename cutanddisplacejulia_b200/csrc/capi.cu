@@ -40,7 +40,7 @@ enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
-    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_COUNT
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS, S_COUNT
 };
 
 constexpr int kLuBlock = 256;   // outer block width of the LU
@@ -61,12 +61,13 @@ struct Lane {
 };
 constexpr int kLanes = 32;           // cracks of a batch in flight at once
 constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
+constexpr int kGroupBlock = 128;     // block width of the grouped FP32 factorisation (systems padded to it)
 
 // The captured graph of the last batched call and what it was captured for.
 struct BatchGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<int64_t> offsets;
-    const void* ptrs[8] = {};
+    const void* ptrs[9] = {};
     double params[5] = {};
     int flags[3] = {};
     int64_t launches = 0;
@@ -97,7 +98,8 @@ struct cad_ctx {
     double near_factor = 3.0;
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
-    int batch_chain = 0;                   // cad_set_batch_solve: chained triangular solves in the batch sweeps
+    int batch_mode = CAD_BATCH_GROUPED;    // cad_set_batch_solve
+    std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
     int max_iter = 200;
@@ -705,10 +707,21 @@ struct BatchArgs {
     const std::vector<int>* lane_of;
     const std::vector<int64_t>* order;   // issue order
     double* rel;                    // device, nbatch
+    // grouped solve (when set): every crack's records, FP32 systems, tensor
+    // maps, info words and the GEMM status word, sync words
+    const std::vector<CrackRec>* crecs = nullptr;
+    const std::vector<GroupSystem>* gsys = nullptr;
+    const CUtensorMap* maps = nullptr;
+    int* ginfo = nullptr;
+    int* gstatus = nullptr;
+    int* gsync = nullptr;
+    size_t gsync_ints = 0;
 };
 
-// Issues the whole batch: fork the lanes off the context stream, every crack
-// (assembly, FP32 LU, fixed refinement sweeps) on its lane, join.
+// Issues the whole batch: fork the lanes off the context stream, every
+// crack's assembly on its lane -- with the lanes path also its FP32 LU and
+// fixed refinement sweeps -- join; with the grouped path then every crack's
+// cast, FP32 LU and sweeps in grouped launches on the context stream.
 int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
 {
     CK(cudaEventRecord(fork, ctx->stream));
@@ -724,8 +737,9 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
         double* A = b.Aall + (*b.aoff)[c];
         CK(assemble_on_lane(l, &ctx->launches, b.normals + 3 * o, b.midpoints + 3 * o, b.P1 + 3 * o, b.P2 + 3 * o,
                             b.P3 + 3 * o, N, b.nu, b.G, b.lambda, b.hs, mixed, ctx->near_factor, A, n3));
+        if (b.crecs) continue;
         const LuStreams ls{l.main, l.side, &ctx->launches, nullptr, ctx->wait_limit};
-        const bool chain = ctx->batch_chain != 0;
+        const bool chain = ctx->batch_mode == CAD_BATCH_LANES_CHAIN;
         int rc = mixed_prepare(ls, A, n3, n3, (float*)l.buf[L_A32].p, (float*)l.buf[L_DINV].p,
                                (int*)l.buf[L_PIV].p, (int*)l.buf[L_PERM].p, (int*)l.buf[L_INFO].p, kLuBlock, chain);
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "batched solve: FP32 LU failed");
@@ -741,6 +755,13 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
     for (auto& l : ctx->lanes) {
         CK(cudaEventRecord(l.done, l.main));
         CK(cudaStreamWaitEvent(ctx->stream, l.done, 0));
+    }
+    if (b.crecs) {
+        CK(cudaMemsetAsync(b.gstatus, 0, sizeof(int), ctx->stream));
+        const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches, nullptr, ctx->wait_limit};
+        if (mixed_group_solve(ls, *b.crecs, *b.gsys, b.maps, b.ginfo, b.gstatus, b.gsync, b.gsync_ints, kBatchSweeps,
+                              kGroupBlock) != GMRES_OK)
+            return fail(ctx, CAD_ERR_CUDA, "batched solve: grouped launch failed");
     }
     return CAD_OK;
 }
@@ -803,6 +824,9 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
             }
         if (!any) break;
     }
+    // the grouped path takes every crack when the largest fits one leaf cluster
+    const int64_t pad_max = (3 * maxN + kGroupBlock - 1) / kGroupBlock * kGroupBlock;
+    const bool group = ctx->batch_mode == CAD_BATCH_GROUPED && pad_max <= lu_group_max_rows();
     // workspaces sized before anything is captured
     void *Aall, *rel, *p;
     if (int r = ensure(ctx, S_A, (size_t)aoff[nbatch] * sizeof(double), &Aall)) return r;
@@ -816,6 +840,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         if (int r = lane_ensure(ctx, l, L_TRI, N * tri_record_bytes(), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_TRI32, N * tri_record_bytes_f32(), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_NEAR, (3 * N + 1) * sizeof(double), &p)) return r;
+        if (group) continue;   // the lanes only assemble
         if (int r = lane_ensure(ctx, l, L_A32, mixed_ld(n3) * n3 * sizeof(float), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_PIV, n3 * sizeof(int), &p)) return r;
         if (int r = lane_ensure(ctx, l, L_PERM, n3 * sizeof(int), &p)) return r;
@@ -830,14 +855,74 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
     }
     BatchArgs b{nbatch, offsets, P1, P2, P3, normals, midpoints, T, D, nu, G, lambda, hs, (double*)Aall, &aoff,
                 &lane_of, &order, (double*)rel};
+    std::vector<CrackRec> crecs;
+    std::vector<GroupSystem> gsys;
+    void* ga32 = nullptr;
+    if (group) {
+        // group buffers: FP32 systems back to back; ints = [every crack's sync
+        // words][info per crack][GEMM status][pivots and permutation per
+        // crack]; floats = diagonal-block inverses, y32, x32 per crack;
+        // doubles = r, z per crack
+        std::vector<size_t> oa((size_t)nbatch), oi((size_t)nbatch), os((size_t)nbatch), of((size_t)nbatch),
+            od((size_t)nbatch);
+        size_t na = 0, ns = 0, ni = 0, nf = 0, nd = 0;
+        for (int64_t c = 0; c < nbatch; ++c) {
+            const size_t np = (size_t)((3 * (offsets[c + 1] - offsets[c]) + kGroupBlock - 1) / kGroupBlock) *
+                              kGroupBlock;
+            oa[c] = na;
+            na += np * np;
+            os[c] = ns;
+            ns += mixed_sync_ints((int64_t)np);
+            oi[c] = ni;
+            ni += 2 * np;
+            of[c] = nf;
+            nf += mixed_dinv_floats((int64_t)np) + 2 * np;
+            od[c] = nd;
+            nd += 2 * np;
+        }
+        void *gint, *gf32, *gf64, *gmaps;
+        if (int r = ensure(ctx, S_G_A32, na * sizeof(float) + 16, &ga32)) return r;
+        if (int r = ensure(ctx, S_G_INT, (ns + (size_t)nbatch + 1 + ni) * sizeof(int), &gint)) return r;
+        if (int r = ensure(ctx, S_G_F32, nf * sizeof(float) + 16, &gf32)) return r;
+        if (int r = ensure(ctx, S_G_F64, nd * sizeof(double) + 16, &gf64)) return r;
+        if (int r = ensure(ctx, S_G_MAPS, (size_t)nbatch * 2 * sizeof(CUtensorMap), &gmaps)) return r;
+        int* sync_all = (int*)gint;
+        int* infos = sync_all + ns;
+        int* status = infos + nbatch;
+        int* piv_all = status + 1;
+        ctx->gmaps_host.assign((size_t)nbatch * 2, CUtensorMap{});
+        for (int64_t c = 0; c < nbatch; ++c) {
+            const int64_t o = offsets[c], n3 = 3 * (offsets[c + 1] - o);
+            const int np = (int)((n3 + kGroupBlock - 1) / kGroupBlock * kGroupBlock);
+            float* A32 = (float*)ga32 + oa[c];
+            float* f = (float*)gf32 + of[c];
+            double* d = (double*)gf64 + od[c];
+            int* ip = piv_all + oi[c];
+            if (!gemm_group_maps(&ctx->gmaps_host[2 * c], A32, np, np, np))
+                return fail(ctx, CAD_ERR_CUDA, "batched solve: tensor map encoding failed");
+            gsys.push_back(GroupSystem{A32, np, np, ip, infos + c, (int)c});
+            crecs.push_back(CrackRec{(double*)Aall + aoff[c], T + 3 * o, D + 3 * o, A32, f, ip + np, sync_all + os[c],
+                                     d, d + np, f + mixed_dinv_floats(np), f + mixed_dinv_floats(np) + np,
+                                     (double*)rel + c, (int)n3, (int)n3, np, 0});
+        }
+        CK(cudaMemcpyAsync(gmaps, ctx->gmaps_host.data(), ctx->gmaps_host.size() * sizeof(CUtensorMap),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        b.crecs = &crecs;
+        b.gsys = &gsys;
+        b.maps = (const CUtensorMap*)gmaps;
+        b.ginfo = infos;
+        b.gstatus = status;
+        b.gsync = sync_all;
+        b.gsync_ints = ns;
+    }
     // the captured graph of an identical earlier call is replayed
     BatchGraph& g = ctx->batch;
-    const void* ptrs[8] = {P1, P2, P3, normals, midpoints, T, D, Aall};
+    const void* ptrs[9] = {P1, P2, P3, normals, midpoints, T, D, Aall, ga32};
     const double params[5] = {nu, G, lambda, ctx->tol, ctx->near_factor};
-    const int flags[3] = {hs, ctx->assembly, ctx->batch_chain};
+    const int flags[3] = {hs, ctx->assembly, ctx->batch_mode};
     const bool same = g.exec && g.offsets.size() == (size_t)nbatch + 1 &&
                       std::equal(g.offsets.begin(), g.offsets.end(), offsets) &&
-                      std::equal(ptrs, ptrs + 8, g.ptrs) && std::equal(params, params + 5, g.params) &&
+                      std::equal(ptrs, ptrs + 9, g.ptrs) && std::equal(params, params + 5, g.params) &&
                       std::equal(flags, flags + 3, g.flags);
     cudaEvent_t fork = nullptr;
     CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -869,7 +954,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         if (graph) cudaGraphDestroy(graph);
         if (rc == CAD_OK) {
             g.offsets.assign(offsets, offsets + nbatch + 1);
-            std::copy(ptrs, ptrs + 8, g.ptrs);
+            std::copy(ptrs, ptrs + 9, g.ptrs);
             std::copy(params, params + 5, g.params);
             std::copy(flags, flags + 3, g.flags);
             g.launches = ctx->launches - l0;
@@ -885,8 +970,13 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
     // every crack's residual; GMRES (on the context stream) for any crack the
     // refinement sweeps left above the tolerance
     std::vector<double> hrel((size_t)nbatch);
+    std::vector<int> hinfo(group ? (size_t)nbatch + 1 : 0);
     CK(cudaMemcpyAsync(hrel.data(), rel, (size_t)nbatch * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (group)
+        CK(cudaMemcpyAsync(hinfo.data(), b.ginfo, hinfo.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (int v : hinfo)   // a leaf, chain or tensor-core pipeline wait that ran out
+        if (v < 0) return fail(ctx, CAD_ERR_TIMEOUT, "batched solve: a device wait ran out");
     bool converged = true;
     for (int64_t c = 0; c < nbatch; ++c) {
         if (hrel[c] <= ctx->tol) continue;
@@ -1018,11 +1108,12 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)
     return CAD_OK;
 }
 
-int cad_set_batch_solve(cad_ctx* ctx, int chain)
+int cad_set_batch_solve(cad_ctx* ctx, int mode)
 {
     if (!ctx) return CAD_ERR_ARG;
-    if (chain != 0 && chain != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
-    ctx->batch_chain = chain;
+    if (mode != CAD_BATCH_GROUPED && mode != CAD_BATCH_LANES && mode != CAD_BATCH_LANES_CHAIN)
+        return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->batch_mode = mode;
     return CAD_OK;
 }
 

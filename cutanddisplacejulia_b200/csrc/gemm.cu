@@ -230,13 +230,24 @@ constexpr size_t TSMEM = (size_t)TSTAGES * TSTAGE + 1024 /* alignment slack */ +
 constexpr uint32_t TIDESC = sm100::instr_desc(TBM, TBN, 2, 2, 1 /* A MN-major */, 0 /* B K-major */);
 constexpr long kTcWaitLimit = 1L << 24;
 
+struct GemmGroup {
+    int count, pad;
+    const CUtensorMap* maps;
+    int* status;
+    GemmGroupRec rec[kGemmGroupMax];
+};
+static_assert(sizeof(GemmGroup) <= 32000, "grouped GEMM records exceed the kernel parameter space");
+
 // A: dims {m, k}, box {32, 32}, 128-byte rows swizzled in 32-byte chunks;
 // B: dims {k, n}, box {32, 128}, 128-byte swizzle; both FP32, out-of-range
 // elements read as zero.
-__global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap mapA,
-                                                                     const __grid_constant__ CUtensorMap mapB, int m,
-                                                                     int n, int k, float* __restrict__ C, int64_t ldc,
-                                                                     int* __restrict__ status)
+// One 128 x 128 tile (m0, n0) of C -= A B: A is rows [ax, ax + m), columns
+// [ay, ay + k) of the tensor behind mapA, B rows [bx, bx + k), columns [by, by
+// + n) of mapB's.  Rows and columns of the boxes past m, n are computed and
+// dropped; k must be a multiple of TBK where the tensors continue past it.
+__device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtensorMap* mapB, int ax, int ay, int bx,
+                                          int by, int m, int n, int k, float* __restrict__ C, int64_t ldc, int m0,
+                                          int n0, int* __restrict__ status)
 {
     extern __shared__ uint8_t tsm_raw[];
     uint8_t* tsm = (uint8_t*)(((uintptr_t)tsm_raw + 1023) & ~(uintptr_t)1023);   // swizzle atoms: 1024-byte aligned
@@ -246,15 +257,14 @@ __global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __gri
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * TSTAGES + 1);
     __shared__ int s_fail;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * TBM, n0 = blockIdx.y * TBN;
     const int nk = (k + TBK - 1) / TBK;
 
     if (threadIdx.x == 0) {
         s_fail = 0;
         for (int s = 0; s < 2 * TSTAGES + 1; ++s) sm100::mbar_init(sm100::smem_addr(&bars[s]), 1);
         sm100::fence_barrier_init();
-        sm100::prefetch_tensormap(&mapA);
-        sm100::prefetch_tensormap(&mapB);
+        sm100::prefetch_tensormap(mapA);
+        sm100::prefetch_tensormap(mapB);
     }
     if (warp == 1) {
         sm100::tmem_alloc(sm100::smem_addr(tmem_slot), TBN);
@@ -279,8 +289,9 @@ __global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __gri
             sm100::mbar_arrive_expect_tx(full, TSTAGE);
             const uint32_t sa = sm100::smem_addr(tsm + s * TSTAGE);
 #pragma unroll
-            for (int mb = 0; mb < TBM / 32; ++mb) sm100::tma_load_2d(sa + mb * 4096, &mapA, m0 + 32 * mb, kt * TBK, full);
-            sm100::tma_load_2d(sa + TSTAGE_A, &mapB, kt * TBK, n0, full);
+            for (int mb = 0; mb < TBM / 32; ++mb)
+                sm100::tma_load_2d(sa + mb * 4096, mapA, ax + m0 + 32 * mb, ay + kt * TBK, full);
+            sm100::tma_load_2d(sa + TSTAGE_A, mapB, bx + kt * TBK, by + n0, full);
             issued = kt + 1;
         }
         // no copy may still be landing when the CTA exits (a no-op unless a wait
@@ -351,6 +362,32 @@ __global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __gri
         sm100::tmem_dealloc(tmem, TBN);
     }
     if (threadIdx.x == 0 && s_fail) atomicMin(status, -1);
+}
+
+__global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap mapA,
+                                                                     const __grid_constant__ CUtensorMap mapB, int m,
+                                                                     int n, int k, float* __restrict__ C, int64_t ldc,
+                                                                     int* __restrict__ status)
+{
+    tf32_tile(&mapA, &mapB, 0, 0, 0, 0, m, n, k, C, ldc, blockIdx.x * TBM, blockIdx.y * TBN, status);
+}
+
+// Many products in one launch: CTA x takes tile x of the flattened tile list
+// (records in order, each record's tiles m-fastest).
+__global__ void __launch_bounds__(TTHREADS, 2) sgemm_tf32_group_kernel(const __grid_constant__ GemmGroup g)
+{
+    const int t = blockIdx.x;
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {   // last record whose first tile is at or before t
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.rec[mid].tile0 <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const GemmGroupRec& r = g.rec[lo];
+    const int mt = (r.m + TBM - 1) / TBM;
+    const int local = t - r.tile0;
+    tf32_tile(g.maps + 2 * r.map, g.maps + 2 * r.map + 1, r.ax, r.ay, r.bx, r.by, r.m, r.n, r.k, r.C, r.ldc,
+              (local % mt) * TBM, (local / mt) * TBN, g.status);
 }
 
 // ------------------------------------------- FP32 on CUDA cores (any layout)
@@ -464,6 +501,44 @@ cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const double* A, int6
     case 16: return launch_dgemm<16>(st, m, n, k, A, lda, B, ldb, C, ldc);
     default: return cudaErrorInvalidValue;
     }
+}
+
+bool gemm_group_maps(CUtensorMap* out, const float* base, int rows, int cols, int64_t ld)
+{
+    return tma_ok(base, ld) && encode_f32(&out[0], base, rows, cols, ld, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B) &&
+           encode_f32(&out[1], base, rows, cols, ld, 32, TBN, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+cudaError_t gemm_sub_group(cudaStream_t st, const CUtensorMap* dev_maps, std::vector<GemmGroupRec>& recs,
+                           int* status, int64_t* launches)
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(sgemm_tf32_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TSMEM);
+    });
+    GemmGroup g{};
+    g.maps = dev_maps;
+    g.status = status;
+    int64_t tiles = 0;
+    auto flush = [&]() -> cudaError_t {
+        if (g.count == 0) return cudaSuccess;
+        sgemm_tf32_group_kernel<<<(unsigned)tiles, TTHREADS, TSMEM, st>>>(g);
+        if (launches) ++*launches;
+        g.count = 0;
+        tiles = 0;
+        return cudaGetLastError();
+    };
+    for (auto& r : recs) {
+        if (r.m <= 0 || r.n <= 0 || r.k <= 0) continue;
+        if (r.k % TBK || r.ax % 4 || r.bx % 4) return cudaErrorInvalidValue;
+        if (g.count == kGemmGroupMax) {
+            if (cudaError_t e = flush()) return e;
+        }
+        r.tile0 = (int)tiles;
+        g.rec[g.count++] = r;
+        tiles += (int64_t)((r.m + TBM - 1) / TBM) * ((r.n + TBN - 1) / TBN);
+    }
+    return flush();
 }
 
 cudaError_t gemm_sub(cudaStream_t st, int m, int n, int k, const float* A, int64_t lda, const float* B, int64_t ldb,

@@ -20,6 +20,7 @@
 
 #include <atomic>
 #include <climits>
+#include <mutex>
 #include <cstdint>
 #include <vector>
 
@@ -38,6 +39,43 @@ constexpr int kMaxCluster = 16;
 constexpr int kLeafRegs = 32;   // row values one leaf thread keeps in registers (RPT * W)
 constexpr int kMaxSwaps = 256;
 constexpr int kMaxDevices = 64;  // devices whose leaf cluster size is remembered  // pivots one row-swap launch applies (outer block width bound)
+
+// ---------------------------------------------- records of grouped launches
+// One launch of a grouped factorisation (many independent FP32 systems) takes
+// its per-system arguments by value as a kernel parameter (up to 32 KB), one
+// record per system; grid dimension y selects the record.
+constexpr int kGroupMax = 512;   // records per grouped launch
+struct LeafRec {
+    float* A;     // panel top
+    int* piv;     // pivots of the panel's columns
+    int* info;
+    int lda, m, piv_base, col_base;
+};
+struct LeafGroup {
+    int count, w;
+    long wait_limit;
+    LeafRec rec[kGroupMax];
+};
+struct LaswpRec {
+    float *A1, *A2;
+    const int* piv;
+    int lda, ncol1, ncol2, row_base;
+};
+struct LaswpGroup {
+    int count, npiv;
+    LaswpRec rec[kGroupMax];
+};
+struct TrsmRec {
+    const float* L;
+    float* B;
+    int ldl, ldb, ncol, pad;
+};
+struct TrsmGroup {
+    int count, b;
+    TrsmRec rec[kGroupMax];
+};
+static_assert(sizeof(LeafGroup) <= 32000 && sizeof(LaswpGroup) <= 32000 && sizeof(TrsmGroup) <= 32000,
+              "grouped launch records exceed the kernel parameter space");
 
 // A pivot candidate as integers: |value| orders like the bit pattern of the
 // non-negative double, so hi = 1 + its high word (0: no candidate), lo = its
@@ -137,10 +175,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned mbar, unsigned parity)
 // position swapped with c (LAPACK order); info: smallest zero-pivot column
 // (1-based, + col_base), or -1 if a wait ran out.
 template <typename T, int W, int RPT>
-__global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict__ A, int64_t lda, int m, int w,
-                                                                int* __restrict__ piv, int piv_base,
-                                                                int* __restrict__ info, int col_base,
-                                                                long wait_limit)
+__device__ __forceinline__ void leaf_body(T* __restrict__ A, int64_t lda, int m, int w, int* __restrict__ piv,
+                                          int piv_base, int* __restrict__ info, int col_base, long wait_limit)
 {
     static_assert(W * RPT <= kLeafRegs && W <= 32, "leaf tile exceeds its register budget");
     cg::cluster_group cluster = cg::this_cluster();
@@ -282,6 +318,25 @@ __global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict_
     if (tid == 0 && s_fail) atomicMin(info, -1);
 }
 
+template <typename T, int W, int RPT>
+__global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict__ A, int64_t lda, int m, int w,
+                                                                int* __restrict__ piv, int piv_base,
+                                                                int* __restrict__ info, int col_base,
+                                                                long wait_limit)
+{
+    leaf_body<T, W, RPT>(A, lda, m, w, piv, piv_base, info, col_base, wait_limit);
+}
+
+// The leaves of many systems in one launch: cluster y of the grid factorises
+// the panel of record y (every cluster of the launch has the same size, so the
+// records of one launch need the same number of CTAs).
+template <int W, int RPT>
+__global__ void __launch_bounds__(kLeafThreads, 1) leaf_group_kernel(const __grid_constant__ LeafGroup g)
+{
+    const LeafRec& r = g.rec[blockIdx.y];
+    leaf_body<float, W, RPT>(r.A, r.lda, r.m, g.w, r.piv, r.piv_base, r.info, r.col_base, g.wait_limit);
+}
+
 // ------------------------------------------------------------ row swaps
 // Applies the swaps row k <-> row piv[k] - row_base (k = 0..npiv-1, in order,
 // rows relative to the block top) to columns [0, ncol1) of A1 and [0, ncol2)
@@ -289,8 +344,8 @@ __global__ void __launch_bounds__(kLeafThreads, 1) leaf_lu_kernel(T* __restrict_
 // its content through the swap sequence, giving at most 2 * npiv (dst, src)
 // pairs; then one warp per column gathers the sources and stores them.
 template <typename T>
-__global__ void __launch_bounds__(256) laswp_kernel(T* __restrict__ A1, int ncol1, T* __restrict__ A2, int ncol2,
-                                                    int64_t lda, const int* __restrict__ piv, int npiv, int row_base)
+__device__ __forceinline__ void laswp_body(T* __restrict__ A1, int ncol1, T* __restrict__ A2, int ncol2, int64_t lda,
+                                           const int* __restrict__ piv, int npiv, int row_base, int cta, int ncta)
 {
     constexpr int kPer = 2 * kMaxSwaps / 32;
     __shared__ int s_piv[kMaxSwaps];
@@ -331,8 +386,8 @@ __global__ void __launch_bounds__(256) laswp_kernel(T* __restrict__ A1, int ncol
         dst[t] = e < count ? s_dst[e] : -1;
         src[t] = e < count ? s_src[e] : 0;
     }
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int wid = (cta * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (ncta * blockDim.x) >> 5;
     for (int col = wid; col < ncol1 + ncol2; col += nw) {
         T* a = col < ncol1 ? A1 + (int64_t)col * lda : A2 + (int64_t)(col - ncol1) * lda;
         T v[kPer];
@@ -346,19 +401,33 @@ __global__ void __launch_bounds__(256) laswp_kernel(T* __restrict__ A1, int ncol
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) laswp_kernel(T* __restrict__ A1, int ncol1, T* __restrict__ A2, int ncol2,
+                                                    int64_t lda, const int* __restrict__ piv, int npiv, int row_base)
+{
+    laswp_body<T>(A1, ncol1, A2, ncol2, lda, piv, npiv, row_base, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) laswp_group_kernel(const __grid_constant__ LaswpGroup g)
+{
+    const LaswpRec& r = g.rec[blockIdx.y];
+    laswp_body<float>(r.A1, r.ncol1, r.A2, r.ncol2, r.lda, r.piv, g.npiv, r.row_base, blockIdx.x, gridDim.x);
+}
+
 // ------------------------------------------------- triangular diagonal blocks
 // B (b x ncol, ldb) := L^-1 B with L the b x b unit lower triangle at L (ldl),
 // or U^-1 B with U upper, non-unit; b <= 64.  A CTA of 4 warps takes 32
 // columns (8 per warp); lane l holds rows l and l + 32; the solved row c is
 // broadcast from its lane by shuffles.
 template <typename T, bool UPPER>
-__global__ void __launch_bounds__(128) trsm_diag_kernel(const T* __restrict__ L, int64_t ldl, int b, T* __restrict__ B,
-                                                        int64_t ldb, int ncol)
+__device__ __forceinline__ void trsm_diag_body(const T* __restrict__ L, int64_t ldl, int b, T* __restrict__ B,
+                                               int64_t ldb, int ncol, int cta)
 {
     __shared__ T s_L[64 * 64];
     __shared__ T s_inv[64];   // UPPER: reciprocal diagonal
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int col0 = blockIdx.x * 32 + warp * 8;
+    const int col0 = cta * 32 + warp * 8;
+    if (cta * 32 >= ncol) return;   // CTA-uniform: a grouped launch sizes x for its widest record
     {
         // every load of the block and of the right-hand sides in flight at once
         T t[32];
@@ -423,6 +492,19 @@ __global__ void __launch_bounds__(128) trsm_diag_kernel(const T* __restrict__ L,
             const int r = lane + 32 * h, col = col0 + k;
             if (r < b && col < ncol) B[r + (int64_t)col * ldb] = x[h][k];
         }
+}
+
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(128) trsm_diag_kernel(const T* __restrict__ L, int64_t ldl, int b, T* __restrict__ B,
+                                                        int64_t ldb, int ncol)
+{
+    trsm_diag_body<T, UPPER>(L, ldl, b, B, ldb, ncol, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(128) trsm_group_kernel(const __grid_constant__ TrsmGroup g)
+{
+    const TrsmRec& r = g.rec[blockIdx.y];
+    trsm_diag_body<float, false>(r.L, r.ldl, g.b, r.B, r.ldb, r.ncol, blockIdx.x);
 }
 
 // perm[i] = source row of row i after all n pivots (ipiv applied in order),
@@ -907,6 +989,333 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     lu_body(lu, A, n, lda, B, ldb, nrhs, X, ldx, perm, nb, factor, solve);
     if (s.launches) *s.launches += lu.launches;
     if (lu.err != cudaSuccess) return LU_CUDA_ERROR;
+    return LU_OK;
+}
+
+// ------------------------------------------------- grouped factorisation
+namespace {
+
+__global__ void set_ints_kernel(int* p, int n, int v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// perm of every system from its pivots: one CTA per system, in shared memory
+struct PermRec {
+    const int* ipiv;
+    int* perm;
+    int n, pad;
+};
+struct PermGroup {
+    int count, pad;
+    PermRec rec[kGroupMax];
+};
+__global__ void __launch_bounds__(1024) perm_group_kernel(const __grid_constant__ PermGroup g)
+{
+    extern __shared__ int s_perm[];
+    const PermRec& r = g.rec[blockIdx.x];
+    for (int i = threadIdx.x; i < r.n; i += blockDim.x) s_perm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < r.n; ++k) {
+            const int q = r.ipiv[k];
+            const int t = s_perm[k];
+            s_perm[k] = s_perm[q];
+            s_perm[q] = t;
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < r.n; i += blockDim.x) r.perm[i] = s_perm[i];
+}
+
+// The blocked right-looking LU of csrc/lu.cu's Lu::factor over many systems
+// at once: every launch covers the systems still active at its step (a system
+// of n_pad rows takes part in block steps k < n_pad).  Panels of nb columns
+// split recursively down to 32-column cluster leaves; trailing updates are
+// grouped TF32 tcgen05 products.  Look-ahead of one block column on a side
+// stream, as in the single-system factorisation.
+struct GroupLu {
+    cudaStream_t st, main_st, side_st;
+    const std::vector<GroupSystem>* sys;
+    const CUtensorMap* maps;
+    int* status;
+    int cluster = 8;
+    long wait_limit = kDefaultWaitLimit;
+    int64_t launches = 0;
+    cudaError_t err = cudaSuccess;
+    bool ok() const { return err == cudaSuccess; }
+    const GroupSystem& S(int p) const { return (*sys)[p]; }
+    static float* at(const GroupSystem& g, int r, int c) { return g.A + r + (int64_t)c * g.lda; }
+
+    // systems with n_pad > rows
+    std::vector<int> active(const std::vector<int>& from, int rows) const
+    {
+        std::vector<int> a;
+        for (int p : from)
+            if (S(p).n_pad > rows) a.push_back(p);
+        return a;
+    }
+
+    void gemm(std::vector<GemmGroupRec>& recs)
+    {
+        if (!ok() || recs.empty()) return;
+        err = gemm_sub_group(st, maps, recs, status, &launches);
+    }
+
+    // rows [o, o + npiv) swapped with ipiv[o ..] in the column ranges given by f
+    template <class F>
+    void laswp(const std::vector<int>& act, int npiv, F f)
+    {
+        if (!ok() || act.empty()) return;
+        LaswpGroup g{};
+        g.npiv = npiv;
+        int widest = 0;
+        auto flush = [&]() {
+            if (g.count == 0 || !ok()) return;
+            const int blocks = (widest + 7) / 8 < 64 ? (widest + 7) / 8 : 64;
+            laswp_group_kernel<<<dim3((unsigned)(blocks > 0 ? blocks : 1), (unsigned)g.count), 256, 0, st>>>(g);
+            ++launches;
+            err = cudaGetLastError();
+            g.count = 0;
+            widest = 0;
+        };
+        for (int p : act) {
+            LaswpRec r{};
+            f(S(p), r);
+            if (r.ncol1 + r.ncol2 <= 0) continue;
+            if (g.count == kGroupMax) flush();
+            widest = r.ncol1 + r.ncol2 > widest ? r.ncol1 + r.ncol2 : widest;
+            g.rec[g.count++] = r;
+        }
+        flush();
+    }
+
+    // B (b x ncol) := L^-1 B, L unit lower at diagonal position o, B columns
+    // [c1, c1 + ncol(p)): 64-row blocks and grouped products
+    template <class NC>
+    void trsm_lower(const std::vector<int>& act, int o, int b, int c1, NC ncol)
+    {
+        for (int d = 0; d < b && ok(); d += 64) {
+            const int db = b - d < 64 ? b - d : 64;
+            TrsmGroup g{};
+            g.b = db;
+            int widest = 0;
+            auto flush = [&]() {
+                if (g.count == 0 || !ok()) return;
+                trsm_group_kernel<<<dim3((unsigned)((widest + 31) / 32), (unsigned)g.count), 128, 0, st>>>(g);
+                ++launches;
+                err = cudaGetLastError();
+                g.count = 0;
+                widest = 0;
+            };
+            std::vector<GemmGroupRec> recs;
+            for (int p : act) {
+                const GroupSystem& y = S(p);
+                const int nc = ncol(y);
+                if (nc <= 0) continue;
+                if (g.count == kGroupMax) flush();
+                g.rec[g.count++] = TrsmRec{at(y, o + d, o + d), at(y, o + d, c1), y.lda, y.lda, nc, 0};
+                widest = nc > widest ? nc : widest;
+                if (d + db < b)
+                    recs.push_back(GemmGroupRec{at(y, o + d + db, c1), y.lda, b - d - db, nc, db, o + d + db, o + d,
+                                                o + d, c1, y.map, 0});
+            }
+            flush();
+            gemm(recs);
+        }
+    }
+
+    // 32-column leaves of the panel at diagonal position o, one launch per
+    // cluster size (CTAs of 512 rows)
+    void leaf(const std::vector<int>& act, int o, int w)
+    {
+        if (!ok()) return;
+        for (int C = 1; C <= cluster && ok(); ++C) {
+            LeafGroup g{};
+            g.w = w;
+            g.wait_limit = wait_limit;
+            auto flush = [&]() {
+                if (g.count == 0 || !ok()) return;
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)C, (unsigned)g.count);
+                cfg.blockDim = dim3(kLeafThreads);
+                cfg.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = (unsigned)C;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                err = cudaLaunchKernelEx(&cfg, leaf_group_kernel<32, 1>, g);
+                ++launches;
+                g.count = 0;
+            };
+            for (int p : act) {
+                const GroupSystem& y = S(p);
+                const int m = y.n_pad - o;
+                if (m <= 0 || (m + kLeafThreads - 1) / kLeafThreads != C) continue;
+                if (g.count == kGroupMax) flush();
+                g.rec[g.count++] = LeafRec{at(y, o, o), y.ipiv + o, y.info, y.lda, m, o, o};
+            }
+            flush();
+        }
+    }
+
+    void panel(const std::vector<int>& act, int o, int w)
+    {
+        if (!ok() || act.empty()) return;
+        if (w <= 32) {
+            leaf(act, o, w);
+            return;
+        }
+        int w1 = w / 2;
+        w1 = (w1 + 31) / 32 * 32;
+        if (w1 >= w) w1 = w - 32;
+        panel(act, o, w1);
+        laswp(act, w1, [&](const GroupSystem& y, LaswpRec& r) {
+            r = LaswpRec{at(y, o, o + w1), nullptr, y.ipiv + o, y.lda, w - w1, 0, o};
+        });
+        trsm_lower(act, o, w1, o + w1, [&](const GroupSystem&) { return w - w1; });
+        std::vector<GemmGroupRec> recs;
+        for (int p : act) {
+            const GroupSystem& y = S(p);
+            if (y.n_pad - o > w1)
+                recs.push_back(GemmGroupRec{at(y, o + w1, o + w1), y.lda, y.n_pad - o - w1, w - w1, w1, o + w1, o, o,
+                                            o + w1, y.map, 0});
+        }
+        gemm(recs);
+        panel(active(act, o + w1), o + w1, w - w1);
+        laswp(act, w - w1, [&](const GroupSystem& y, LaswpRec& r) {
+            r = LaswpRec{at(y, o + w1, o), nullptr, y.ipiv + o + w1, y.lda, w1, 0, o + w1};
+        });
+    }
+
+    void use(bool side) { st = side ? side_st : main_st; }
+
+    void factor(int nb)
+    {
+        use(false);
+        int nmax = 0;
+        std::vector<int> all;
+        for (int p = 0; p < (int)sys->size(); ++p) {
+            all.push_back(p);
+            nmax = S(p).n_pad > nmax ? S(p).n_pad : nmax;
+        }
+        const int nblk = (nmax + nb - 1) / nb;
+        if (nblk == 0) return;
+        std::vector<cudaEvent_t> ev_panel(nblk, nullptr), ev_rest(nblk, nullptr);
+        for (int b = 0; b < nblk && ok(); ++b) {
+            err = cudaEventCreateWithFlags(&ev_panel[b], cudaEventDisableTiming);
+            if (ok()) err = cudaEventCreateWithFlags(&ev_rest[b], cudaEventDisableTiming);
+        }
+        if (ok()) {
+            panel(all, 0, nb);
+            if (ok()) err = cudaEventRecord(ev_panel[0], main_st);
+        }
+        for (int b = 0; b < nblk && ok(); ++b) {
+            const int k = b * nb, k1 = k + nb, k2 = k1 + nb;
+            const std::vector<int> act = active(all, k), act1 = active(all, k1), act2 = active(all, k2);
+            use(false);
+            if (b > 0) err = cudaStreamWaitEvent(main_st, ev_rest[b - 1], 0);
+            laswp(act, nb, [&](const GroupSystem& y, LaswpRec& r) {
+                r = LaswpRec{at(y, k, 0), at(y, k, k1), y.ipiv + k, y.lda, k, y.n_pad > k1 ? nb : 0, k};
+            });
+            if (!act1.empty()) {
+                trsm_lower(act1, k, nb, k1, [&](const GroupSystem&) { return nb; });
+                std::vector<GemmGroupRec> recs;
+                for (int p : act1) {
+                    const GroupSystem& y = S(p);
+                    recs.push_back(GemmGroupRec{at(y, k1, k1), y.lda, y.n_pad - k1, nb, nb, k1, k, k, k1, y.map, 0});
+                }
+                gemm(recs);
+                panel(act1, k1, nb);
+                if (ok()) err = cudaEventRecord(ev_panel[b + 1], main_st);
+            }
+            use(true);
+            if (!act2.empty() && ok()) {
+                err = cudaStreamWaitEvent(side_st, ev_panel[b], 0);
+                laswp(act2, nb, [&](const GroupSystem& y, LaswpRec& r) {
+                    r = LaswpRec{at(y, k, k2), nullptr, y.ipiv + k, y.lda, y.n_pad - k2, 0, k};
+                });
+                trsm_lower(act2, k, nb, k2, [&](const GroupSystem& y) { return y.n_pad - k2; });
+                std::vector<GemmGroupRec> recs;
+                for (int p : act2) {
+                    const GroupSystem& y = S(p);
+                    recs.push_back(
+                        GemmGroupRec{at(y, k1, k2), y.lda, y.n_pad - k1, y.n_pad - k2, nb, k1, k, k, k2, y.map, 0});
+                }
+                gemm(recs);
+            }
+            if (ok()) err = cudaEventRecord(ev_rest[b], side_st);
+        }
+        use(false);
+        if (ok()) err = cudaStreamWaitEvent(main_st, ev_rest[nblk - 1], 0);
+        for (int b = 0; b < nblk; ++b) {
+            if (ev_panel[b]) cudaEventDestroy(ev_panel[b]);
+            if (ev_rest[b]) cudaEventDestroy(ev_rest[b]);
+        }
+    }
+};
+
+}  // namespace
+
+int lu_factor_group(const LuStreams& s, const std::vector<GroupSystem>& sys, const CUtensorMap* dev_maps,
+                    int* infos, int* status, int nb)
+{
+    if (sys.empty()) return LU_OK;
+    GroupLu g;
+    g.main_st = s.main;
+    g.side_st = s.side ? s.side : s.main;
+    g.use(false);
+    g.sys = &sys;
+    g.maps = dev_maps;
+    g.status = status;
+    g.wait_limit = s.wait_limit > 0 ? s.wait_limit : kDefaultWaitLimit;
+    {
+        Lu<float> probe;
+        configure(probe);
+        g.cluster = probe.cluster;
+        static std::once_flag once;
+        std::call_once(once, [] {
+            cudaFuncSetAttribute(leaf_group_kernel<32, 1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        });
+    }
+    if (nb < 32 || nb > kMaxSwaps || nb % 32) return LU_TOO_LARGE;
+    for (const auto& y : sys)
+        if (y.n_pad % nb || y.n_pad > g.cluster * kLeafThreads || y.lda < y.n_pad) return LU_TOO_LARGE;
+    set_ints_kernel<<<(unsigned)((sys.size() + 255) / 256), 256, 0, s.main>>>(infos, (int)sys.size(), INT_MAX);
+    ++g.launches;
+    g.err = cudaGetLastError();
+    if (g.ok()) g.factor(nb);
+    if (s.launches) *s.launches += g.launches;
+    return g.ok() ? LU_OK : LU_CUDA_ERROR;
+}
+
+int lu_group_max_rows()
+{
+    Lu<float> probe;
+    configure(probe);
+    return probe.cluster * kLeafThreads;
+}
+
+int lu_pivots_to_perm_group(cudaStream_t st, const std::vector<GroupSystem>& sys, const std::vector<int*>& perms,
+                            int64_t* launches)
+{
+    int nmax = 0;
+    for (const auto& y : sys) nmax = y.n_pad > nmax ? y.n_pad : nmax;
+    const size_t smem = (size_t)nmax * sizeof(int);
+    if (cudaFuncSetAttribute(perm_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return LU_CUDA_ERROR;
+    PermGroup g{};
+    for (size_t p = 0; p <= sys.size(); ++p) {
+        if (g.count == kGroupMax || (p == sys.size() && g.count > 0)) {
+            perm_group_kernel<<<(unsigned)g.count, 1024, smem, st>>>(g);
+            if (launches) ++*launches;
+            if (cudaGetLastError() != cudaSuccess) return LU_CUDA_ERROR;
+            g.count = 0;
+        }
+        if (p < sys.size()) g.rec[g.count++] = PermRec{sys[p].ipiv, perms[p], sys[p].n_pad, 0};
+    }
     return LU_OK;
 }
 

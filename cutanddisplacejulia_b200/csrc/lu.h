@@ -1,8 +1,10 @@
 // Dense LU with partial pivoting + solve (csrc/lu.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 namespace cad {
 
@@ -62,5 +64,29 @@ size_t lu_chain_sync_ints(int64_t n);
 // perm[i] = row of the original matrix that the factorisation's row i came
 // from (the pivots applied in order); perm: n ints, device.
 int lu_pivots_to_perm(const LuStreams& s, const int* ipiv, int64_t n, int* perm);
+
+// One FP32 system of a grouped factorisation: A (n_pad x n_pad, lda), n_pad a
+// multiple of the block width (the caller pads a system with the identity),
+// tensor maps 2 map, 2 map + 1 of gemm_group_maps for A in the device array
+// the factorisation is given; ipiv (n_pad ints); info points into the infos
+// array (one int per system: INT_MAX, the first zero-pivot column or -1).
+struct GroupSystem {
+    float* A;
+    int n_pad, lda;
+    int* ipiv;
+    int* info;
+    int map;
+};
+// Factorises every system in place with grouped launches (one launch per
+// step and kind covers every system still active; leaves grouped by cluster
+// size).  n_pad may not exceed 512 x the largest leaf cluster.  status:
+// device int, lowered to -1 when a tensor-core pipeline wait ran out.
+int lu_factor_group(const LuStreams& s, const std::vector<GroupSystem>& sys, const CUtensorMap* dev_maps,
+                    int* infos, int* status, int nb);
+// the largest n_pad lu_factor_group takes on this device
+int lu_group_max_rows();
+// perms[p] (n_pad ints) from system p's pivots, one launch per 512 systems
+int lu_pivots_to_perm_group(cudaStream_t st, const std::vector<GroupSystem>& sys, const std::vector<int*>& perms,
+                            int64_t* launches);
 
 }  // namespace cad

@@ -48,13 +48,13 @@ __global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64
 // the inverse by substitution; the block and the inverse sit in shared memory
 // (the inverse row-major with a pad, so the threads' columns are conflict-free).
 template <bool UPPER>
-__global__ void __launch_bounds__(kRB) invert_diag_kernel(const float* __restrict__ A, int64_t lda, int n,
-                                                         float* __restrict__ D)
+__device__ __forceinline__ void invert_diag_body(const float* __restrict__ A, int64_t lda, int n,
+                                                 float* __restrict__ D, int i)
 {
     extern __shared__ float sm[];
     float* s_a = sm;                  // [kRB][kRB] column-major
     float* s_x = sm + kRB * kRB;      // [kRB][kRB + 1] row-major: s_x[r * (kRB + 1) + j]
-    const int i = blockIdx.x, j = threadIdx.x;
+    const int j = threadIdx.x;
     const int r0 = i * kRB;
     const int b = n - r0 < kRB ? n - r0 : kRB;
     for (int e = j; e < kRB * kRB; e += kRB) {
@@ -97,6 +97,13 @@ __global__ void __launch_bounds__(kRB) invert_diag_kernel(const float* __restric
     }
 }
 
+template <bool UPPER>
+__global__ void __launch_bounds__(kRB) invert_diag_kernel(const float* __restrict__ A, int64_t lda, int n,
+                                                         float* __restrict__ D)
+{
+    invert_diag_body<UPPER>(A, lda, n, D, blockIdx.x);
+}
+
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
     int v;
@@ -117,10 +124,11 @@ __device__ __forceinline__ void st_release(int* p, int v)
 // 128-column block.  The quarter's 32 values of the next block are loaded
 // before its flag is awaited, so the memory latency overlaps the wait.
 template <bool UPPER>
-__global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
-    const float* __restrict__ A, int64_t lda, int n, int nblk, const float* __restrict__ Dinv,
-    const double* __restrict__ v_in, const int* __restrict__ perm, const float* y_in, float* x32,
-    double* __restrict__ out, int* flags, int* ticket, int* fail, long wait_limit)
+__device__ __forceinline__ void trsv_chain_body(const float* __restrict__ A, int64_t lda, int n, int nblk,
+                                                const float* __restrict__ Dinv, const double* __restrict__ v_in,
+                                                const int* __restrict__ perm, const float* y_in, float* x32,
+                                                double* __restrict__ out, int* flags, int* ticket, int* fail,
+                                                long wait_limit)
 {
     constexpr int kQ = kChainThreads / kRB;   // column quarters
     constexpr int kC = kRB / kQ;              // columns per quarter
@@ -196,6 +204,15 @@ __global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
         __threadfence();
         st_release(flags + i, 1);
     }
+}
+
+template <bool UPPER>
+__global__ void __launch_bounds__(kChainThreads) trsv_chain_kernel(
+    const float* __restrict__ A, int64_t lda, int n, int nblk, const float* __restrict__ Dinv,
+    const double* __restrict__ v_in, const int* __restrict__ perm, const float* y_in, float* x32,
+    double* __restrict__ out, int* flags, int* ticket, int* fail, long wait_limit)
+{
+    trsv_chain_body<UPPER>(A, lda, n, nblk, Dinv, v_in, perm, y_in, x32, out, flags, ticket, fail, wait_limit);
 }
 
 }  // namespace
@@ -552,4 +569,189 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
     return cudaGetLastError() == cudaSuccess ? GMRES_OK : GMRES_CUDA_ERROR;
 }
 
+// ------------------------------------------------ grouped many-crack solve
+namespace {
+
+constexpr int kCrackGroupMax = 256;   // cracks per grouped launch
+struct CrackGroup {
+    int count, pad;
+    CrackRec rec[kCrackGroupMax];
+};
+static_assert(sizeof(CrackGroup) <= 32000, "grouped solve records exceed the kernel parameter space");
+
+// A32 (n_pad x n_pad, leading dimension n_pad) = (float) A, the identity past n
+__global__ void __launch_bounds__(256) cast_pad_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    const CrackRec& r = g.rec[blockIdx.y];
+    for (int c = blockIdx.x; c < r.n_pad; c += gridDim.x) {
+        float* dst = r.A32 + (int64_t)c * r.n_pad;
+        const double* src = r.A + (int64_t)c * r.lda;
+        for (int i = threadIdx.x; i < r.n_pad; i += blockDim.x)
+            dst[i] = (i < r.n && c < r.n) ? (float)src[i] : (i == c ? 1.f : 0.f);
+    }
+}
+
+// inverses of the diagonal blocks: z = 0 unit lower, z = 1 upper
+__global__ void __launch_bounds__(kRB) invert_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    const CrackRec& r = g.rec[blockIdx.y];
+    const int nblk = r.n_pad / kRB;
+    if ((int)blockIdx.x >= nblk) return;
+    if (blockIdx.z == 0)
+        invert_diag_body<false>(r.A32, r.n_pad, r.n_pad, r.Dinv, blockIdx.x);
+    else
+        invert_diag_body<true>(r.A32, r.n_pad, r.n_pad, r.Dinv + (int64_t)nblk * kRB * kRB, blockIdx.x);
+}
+
+// one triangle of z = (LU)^-1 P r for every crack (per-crack tickets and
+// flags in its sync words: [nblk lower flags][nblk upper flags][2 tickets][fail])
+template <bool UPPER>
+__global__ void __launch_bounds__(kChainThreads) chain_group_kernel(const __grid_constant__ CrackGroup g,
+                                                                    long wait_limit)
+{
+    const CrackRec& r = g.rec[blockIdx.y];
+    const int nblk = r.n_pad / kRB;
+    if ((int)blockIdx.x >= nblk) return;   // before any ticket is taken
+    int* sync = r.sync;
+    if (!UPPER)
+        trsv_chain_body<false>(r.A32, r.n_pad, r.n_pad, nblk, r.Dinv, r.r, r.perm, nullptr, r.y32, nullptr, sync,
+                               sync + 2 * nblk, sync + 2 * nblk + 2, wait_limit);
+    else
+        trsv_chain_body<true>(r.A32, r.n_pad, r.n_pad, nblk, r.Dinv + (int64_t)nblk * kRB * kRB, nullptr, nullptr,
+                              r.y32, r.x32, r.z, sync + nblk, sync + 2 * nblk + 1, sync + 2 * nblk + 2, wait_limit);
+}
+
+// x = 0, r = b (zero past n)
+__global__ void __launch_bounds__(256) init_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    const CrackRec& r = g.rec[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n_pad; i += gridDim.x * blockDim.x) {
+        if (i < r.n) r.x[i] = 0.0;
+        r.r[i] = i < r.n ? r.b[i] : 0.0;
+    }
+}
+
+// x += z
+__global__ void __launch_bounds__(256) axpy_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    const CrackRec& r = g.rec[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) r.x[i] += r.z[i];
+}
+
+// r = b - A x in FP64: thread per row, columns in order (x staged through
+// shared memory), rows past n zero
+__global__ void __launch_bounds__(128) residual_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    __shared__ double s_x[1024];
+    const CrackRec& r = g.rec[blockIdx.y];
+    const int i = blockIdx.x * 128 + threadIdx.x;
+    if ((int)blockIdx.x * 128 >= r.n_pad) return;
+    double acc = 0.0;
+    for (int c0 = 0; c0 < r.n; c0 += 1024) {
+        const int cn = r.n - c0 < 1024 ? r.n - c0 : 1024;
+        __syncthreads();
+        for (int c = threadIdx.x; c < cn; c += 128) s_x[c] = r.x[c0 + c];
+        __syncthreads();
+        if (i < r.n) {
+            const double* a = r.A + i + (int64_t)c0 * r.lda;
+#pragma unroll 8
+            for (int c = 0; c < cn; ++c) acc = fma(a[(int64_t)c * r.lda], s_x[c], acc);
+        }
+    }
+    if (i < r.n_pad) r.r[i] = i < r.n ? r.b[i] - acc : 0.0;
+}
+
+// rel = ||r|| / ||b|| per crack (fixed-order block reduction)
+__global__ void __launch_bounds__(256) relres_group_kernel(const __grid_constant__ CrackGroup g)
+{
+    __shared__ double s_b[256], s_r[256];
+    const CrackRec& r = g.rec[blockIdx.x];
+    double bb = 0.0, rr = 0.0;
+    for (int i = threadIdx.x; i < r.n; i += 256) {
+        bb = fma(r.b[i], r.b[i], bb);
+        rr = fma(r.r[i], r.r[i], rr);
+    }
+    s_b[threadIdx.x] = bb;
+    s_r[threadIdx.x] = rr;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            s_b[threadIdx.x] += s_b[threadIdx.x + h];
+            s_r[threadIdx.x] += s_r[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *r.rel = s_b[0] > 0.0 ? sqrt(s_r[0]) / sqrt(s_b[0]) : 0.0;
+}
+
+}  // namespace
+
+int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, const std::vector<GroupSystem>& sys,
+                      const CUtensorMap* dev_maps, int* infos, int* status, int* sync_all, size_t sync_ints,
+                      int sweeps, int nb)
+{
+    if (cracks.empty()) return GMRES_OK;
+    if (cracks.size() != sys.size()) return GMRES_CUDA_ERROR;
+    cudaStream_t st = ls.main;
+    int64_t* L = ls.launches;
+    for (const auto& c : cracks)
+        if (c.n_pad % kRB || c.n_pad < c.n) return GMRES_CUDA_ERROR;
+    // every grouped launch, kCrackGroupMax cracks at a time
+    auto each = [&](auto&& launch) -> bool {
+        CrackGroup g{};
+        int nmax = 0;
+        for (size_t p = 0; p <= cracks.size(); ++p) {
+            if (g.count == kCrackGroupMax || (p == cracks.size() && g.count > 0)) {
+                launch(g, nmax);
+                if (L) ++*L;
+                if (cudaGetLastError() != cudaSuccess) return false;
+                g.count = 0;
+                nmax = 0;
+            }
+            if (p < cracks.size()) {
+                g.rec[g.count++] = cracks[p];
+                nmax = cracks[p].n_pad > nmax ? cracks[p].n_pad : nmax;
+            }
+        }
+        return true;
+    };
+    if (!each([&](const CrackGroup& g, int) { cast_pad_group_kernel<<<dim3(32, g.count), 256, 0, st>>>(g); }))
+        return GMRES_CUDA_ERROR;
+    if (lu_factor_group(ls, sys, dev_maps, infos, status, nb) != LU_OK) return GMRES_CUDA_ERROR;
+    std::vector<int*> perms;
+    for (const auto& c : cracks) perms.push_back(c.perm);
+    if (lu_pivots_to_perm_group(st, sys, perms, L) != LU_OK) return GMRES_CUDA_ERROR;
+    const size_t ismem = (size_t)(kRB * kRB + kRB * (kRB + 1)) * sizeof(float);
+    if (cudaFuncSetAttribute(invert_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem) !=
+        cudaSuccess)
+        return GMRES_CUDA_ERROR;
+    if (!each([&](const CrackGroup& g, int nmax) {
+            invert_group_kernel<<<dim3((unsigned)(nmax / kRB), g.count, 2), kRB, ismem, st>>>(g);
+        }))
+        return GMRES_CUDA_ERROR;
+    if (!each([&](const CrackGroup& g, int nmax) {
+            init_group_kernel<<<dim3((unsigned)((nmax + 255) / 256), g.count), 256, 0, st>>>(g);
+        }))
+        return GMRES_CUDA_ERROR;
+    const long wl = ls.wait_limit > 0 ? ls.wait_limit : kDefaultWaitLimit;
+    for (int it = 0; it < sweeps; ++it) {
+        if (cudaMemsetAsync(sync_all, 0, sync_ints * sizeof(int), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+        if (!each([&](const CrackGroup& g, int nmax) {
+                chain_group_kernel<false><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
+            }) ||
+            !each([&](const CrackGroup& g, int nmax) {
+                chain_group_kernel<true><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
+            }) ||
+            !each([&](const CrackGroup& g, int nmax) {
+                axpy_group_kernel<<<dim3((unsigned)((nmax + 255) / 256), g.count), 256, 0, st>>>(g);
+            }) ||
+            !each([&](const CrackGroup& g, int nmax) {
+                residual_group_kernel<<<dim3((unsigned)((nmax + 127) / 128), g.count), 128, 0, st>>>(g);
+            }))
+            return GMRES_CUDA_ERROR;
+    }
+    if (!each([&](const CrackGroup& g, int) { relres_group_kernel<<<g.count, 256, 0, st>>>(g); }))
+        return GMRES_CUDA_ERROR;
+    return GMRES_OK;
+}
 }  // namespace cad

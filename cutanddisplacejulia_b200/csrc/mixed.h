@@ -118,4 +118,35 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
 // ||b - A x|| / ||b||.  Returns a GMRES_* status (launch errors only).
 int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out);
 
+// One crack of a grouped many-crack solve (device pointers): the FP64 system
+// A (n x n, lda), right-hand side b and solution x (n); its FP32 factors A32
+// (n_pad x n_pad, leading dimension n_pad, n_pad a multiple of 128, the
+// identity past n), Dinv (mixed_dinv_floats(n_pad)), perm (n_pad), sync
+// (mixed_sync_ints(n_pad), inside the caller's contiguous sync array), r, z
+// (n_pad doubles), y32, x32 (n_pad floats) and where its relative residual
+// goes.
+struct CrackRec {
+    const double* A;
+    const double* b;
+    double* x;
+    float* A32;
+    float* Dinv;
+    int* perm;
+    int* sync;
+    double* r;
+    double* z;
+    float* y32;
+    float* x32;
+    double* rel;
+    int lda, n, n_pad, pad;
+};
+// Every crack: A32 = (float) A padded, grouped FP32 LU (sys[p] describes
+// cracks[p]'s A32, see lu_factor_group), then `sweeps` refinement sweeps x +=
+// (LU)^-1 (b - A x) with FP64 residuals, all cracks in each launch; *rel of
+// every crack at the end.  sync_all (sync_ints ints) holds every crack's sync
+// words and is cleared before each sweep.  Returns a GMRES_* code.
+int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, const std::vector<GroupSystem>& sys,
+                      const CUtensorMap* dev_maps, int* infos, int* status, int* sync_all, size_t sync_ints,
+                      int sweeps, int nb);
+
 }  // namespace cad

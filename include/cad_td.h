@@ -132,13 +132,22 @@ int64_t cad_autotune_entries(const cad_ctx* ctx, int64_t* tuned_here);
  * forming the residual b - A x in FP64, so the tolerance is met in FP64;
  * fp32 = 0 multiplies with the FP64 A.  No counterpart in the reference. */
 int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
-/* Triangular solves of the many-crack batch's refinement sweeps
- * (cad_slip_calculator_batched*): chain = 0 (default) uses the blocked
- * solves (64-row diagonal blocks and GEMM updates); chain = 1 the two
- * ticket-ordered chain launches per sweep with precomputed inverses of the
- * diagonal blocks.  Both give the same slips to the refinement tolerance.  No
- * counterpart in the reference. */
-int cad_set_batch_solve(cad_ctx* ctx, int chain);
+/* How cad_slip_calculator_batched* factorises and refines its cracks (every
+ * mode gives the same slips to the refinement tolerance; no counterpart in
+ * the reference, whose cracks are solved one SlipCalculator3D call at a
+ * time):
+ *   CAD_BATCH_GROUPED (default): after each crack's assembly, one launch per
+ *     step and kind covers every crack -- the FP32 blocked LU (cluster leaves,
+ *     row swaps, triangular blocks, TF32 tcgen05 products) and the FP64
+ *     refinement sweeps (ticket-ordered triangular chains, FP64 residuals);
+ *     cracks above 3N = 512 x the largest leaf cluster take the lanes path;
+ *   CAD_BATCH_LANES: every crack's own factorisation and sweeps on 32 stream
+ *     lanes, triangular solves in 64-row blocks;
+ *   CAD_BATCH_LANES_CHAIN: the lanes with ticket-ordered chain solves. */
+#define CAD_BATCH_GROUPED 0
+#define CAD_BATCH_LANES 1
+#define CAD_BATCH_LANES_CHAIN 2
+int cad_set_batch_solve(cad_ctx* ctx, int mode);
 /* Device waits (a leaf's pivot exchange, a triangular-solve chain flag) poll
  * at most `polls` times (default 4194304, a few seconds at worst) before the
  * kernel records the failure and returns; the call then reports

@@ -26,18 +26,35 @@ def _reference(cad, cracks, bcs, nu, G, lam):
     return out
 
 
+@pytest.mark.parametrize("mode", ["grouped", "lanes", "lanes_chain"])
 @pytest.mark.parametrize("assembly,tol", [("fp64", 1e-8), ("mixed", 1e-4)])
-def test_batched_matches_per_crack(cad, assembly, tol):
+def test_batched_matches_per_crack(cad, assembly, tol, mode):
     cracks, stresses = _cracks(14)
     _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
     bcs = [cad.Stresses(*s) for s in stresses]
     ref = _reference(cad, cracks, bcs, nu, G, lam)
     for rep in range(2):   # the second call replays the captured graph
-        out, rel = cad.SlipCalculator3D_batched(cracks, nu, G, lam, 0, bcs, tol=RESID_TOL, assembly=assembly)
+        out, rel = cad.SlipCalculator3D_batched(cracks, nu, G, lam, 0, bcs, tol=RESID_TOL, assembly=assembly,
+                                                mode=mode)
         assert np.all(rel <= RESID_TOL)
         for c in range(len(cracks)):
             D = np.concatenate(out[c])
             assert np.linalg.norm(D - ref[c]) <= tol * np.linalg.norm(ref[c]), (rep, c)
+
+
+@pytest.mark.parametrize("mode", ["grouped", "lanes"])
+def test_batched_sweeps_converge_without_fallback(cad, mode):
+    # tol = 1 leaves every crack to the fixed refinement sweeps (no GMRES
+    # finish): the sweeps alone reach the residual the batch promises
+    cracks, stresses = _cracks(20, seed=7)
+    _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
+    bcs = [cad.Stresses(*s) for s in stresses]
+    out, rel = cad.SlipCalculator3D_batched(cracks, nu, G, lam, 0, bcs, tol=1.0, assembly="fp64", mode=mode)
+    assert np.all(rel <= RESID_TOL), rel.max()
+    ref = _reference(cad, cracks, bcs, nu, G, lam)
+    for c in range(len(cracks)):
+        D = np.concatenate(out[c])
+        assert np.linalg.norm(D - ref[c]) <= 1e-8 * np.linalg.norm(ref[c]), c
 
 
 def test_batched_empty_and_single(cad):
