@@ -99,6 +99,7 @@ struct cad_ctx {
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
     int batch_mode = CAD_BATCH_GROUPED;    // cad_set_batch_solve
+    int lu_block = kLuBlock;               // cad_set_lu_block: outer block width of single-system LUs
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
@@ -332,7 +333,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches,
                         ctx->graphs, ctx->wait_limit};
     ctx->timed[1] = ctx->timed[2] = false;
-    int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, kLuBlock);
+    int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, ctx->lu_block);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
     CK(cudaEventRecord(ctx->ev[4], ctx->stream));
@@ -381,7 +382,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
         if (int r = ensure(ctx, S_IR32, 2 * (size_t)n * nrhs * sizeof(float), &ir32)) return r;
         if (int r = ensure(ctx, S_NORMS, 2 * (size_t)nrhs * sizeof(double), &norms)) return r;
         X = (double*)ir;
-        IrArgs ia{ls, n, A, lda, B, ldb, (int)nrhs, X, (float*)a32, (int*)piv, (int*)perm, (int*)info, kLuBlock,
+        IrArgs ia{ls, n, A, lda, B, ldb, (int)nrhs, X, (float*)a32, (int*)piv, (int*)perm, (int*)info, ctx->lu_block,
                   ctx->tol, kIrMaxIter, X + (size_t)n * nrhs, (float*)ir32, (float*)ir32 + (size_t)n * nrhs,
                   (double*)norms};
         IrResult res{};
@@ -570,7 +571,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
                 if (e != cudaSuccess) return e;
                 lt.min_leaf_rpt = c;
                 return lu_factor_solve<double>(lt, (double*)scratch, n, n, nullptr, 0, 0, nullptr, 0, (int*)piv,
-                                               (int*)perm, (int*)info, kLuBlock, true, false) == LU_OK
+                                               (int*)perm, (int*)info, ctx->lu_block, true, false) == LU_OK
                            ? cudaSuccess
                            : cudaErrorUnknown;
             });
@@ -581,7 +582,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
         if (int r = ensure(ctx, S_CHAIN, (size_t)n * sizeof(double) + lu_chain_sync_ints(n) * sizeof(int), &chain))
             return r;
         int rc = lu_factor_solve<double>(ls, A, n, lda, nullptr, 0, 0, nullptr, 0, (int*)piv, (int*)perm, (int*)info,
-                                         kLuBlock, true, false);
+                                         ctx->lu_block, true, false);
         if (rc == LU_OK) rc = lu_pivots_to_perm(ls, (const int*)piv, n, (int*)perm);
         if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
@@ -594,7 +595,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
         return CAD_OK;
     }
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
-                                           (int*)info, kLuBlock, true, true);
+                                           (int*)info, ctx->lu_block, true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
     CK(cudaMemcpy2DAsync(B, ldb * sizeof(double), work, n * sizeof(double), n * sizeof(double), nrhs,
@@ -1105,6 +1106,14 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)
     if (!ctx) return CAD_ERR_ARG;
     if (fp32 != 0 && fp32 != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->gmres_matvec32 = fp32;
+    return CAD_OK;
+}
+
+int cad_set_lu_block(cad_ctx* ctx, int nb)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (nb != 0 && (nb < 32 || nb > 1024)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->lu_block = nb == 0 ? kLuBlock : nb;
     return CAD_OK;
 }
 

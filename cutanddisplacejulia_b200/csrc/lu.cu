@@ -37,8 +37,9 @@ constexpr int kLeafThreads = 512;
 constexpr int kLeafWarps = kLeafThreads / 32;
 constexpr int kMaxCluster = 16;
 constexpr int kLeafRegs = 32;   // row values one leaf thread keeps in registers (RPT * W)
-constexpr int kMaxSwaps = 256;
-constexpr int kMaxDevices = 64;  // devices whose leaf cluster size is remembered  // pivots one row-swap launch applies (outer block width bound)
+constexpr int kMaxSwaps = 256;   // pivots one row-swap launch applies
+constexpr int kMaxBlock = 1024;  // widest outer block of lu_factor_solve
+constexpr int kMaxDevices = 64;  // devices whose leaf cluster size is remembered
 
 // ---------------------------------------------- records of grouped launches
 // One launch of a grouped factorisation (many independent FP32 systems) takes
@@ -606,6 +607,12 @@ struct Lu {
     void laswp(const int* piv, int npiv, int row_base, T* A1, int ncol1, T* A2, int ncol2, int64_t lda)
     {
         if (npiv <= 0 || ncol1 + ncol2 <= 0 || !ok()) return;
+        if (npiv > kMaxSwaps) {   // in order, kMaxSwaps swaps per launch (block tops moved down)
+            for (int c0 = 0; c0 < npiv; c0 += kMaxSwaps)
+                laswp(piv + c0, npiv - c0 < kMaxSwaps ? npiv - c0 : kMaxSwaps, row_base + c0, A1 ? A1 + c0 : nullptr,
+                      ncol1, A2 ? A2 + c0 : nullptr, ncol2, lda);
+            return;
+        }
         const int ncol = ncol1 + ncol2;
         const int blocks = (ncol + 7) / 8 < 148 * 2 ? (ncol + 7) / 8 : 148 * 2;
         laswp_kernel<T><<<blocks, 256, 0, st>>>(A1, ncol1, A2, ncol2, lda, piv, npiv, row_base);
@@ -957,9 +964,8 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     lu.wait_limit = s.wait_limit > 0 ? s.wait_limit : kDefaultWaitLimit;
     lu.min_rpt = (s.min_leaf_rpt == 2 || s.min_leaf_rpt == 4) ? s.min_leaf_rpt : 1;
     configure(lu);
-    // nb bounds the pivots one row-swap launch applies; a leaf cluster holds
-    // at most cluster * 512 * 8 rows
-    if (nb < 1 || nb > kMaxSwaps || n > (int64_t)lu.cluster * kLeafThreads * 8 || n > INT32_MAX)
+    // a leaf cluster holds at most cluster * 512 * 8 rows
+    if (nb < 1 || nb > kMaxBlock || n > (int64_t)lu.cluster * kLeafThreads * 8 || n > INT32_MAX)
         return LU_TOO_LARGE;
     LuGraphEntry* entry = nullptr;
     if (s.graphs && n > 0) {

@@ -41,7 +41,7 @@ constexpr long kDefaultWaitLimit = 1L << 22;
 // A X = B with the factors (if solve).  ipiv (n ints), perm (n ints) and info
 // (1 int) are device memory; info ends as INT_MAX when every pivot is
 // non-zero, else the 1-based column of the first zero pivot.  nb: outer block
-// width (1..256).
+// width (1..1024).
 // The single-precision variant runs its GEMMs on TF32 tensor cores.
 template <typename T>
 int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B, int64_t ldb, int nrhs, T* X,

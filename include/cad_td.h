@@ -144,6 +144,12 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
  *   CAD_BATCH_LANES: every crack's own factorisation and sweeps on 32 stream
  *     lanes, triangular solves in 64-row blocks;
  *   CAD_BATCH_LANES_CHAIN: the lanes with ticket-ordered chain solves. */
+/* Outer block width of the dense LU of a single system (the FP64 solve, the
+ * mixed solve's FP32 factorisation): 32..1024 columns, 0 = the library's
+ * default (256).  Wider blocks give the trailing-update products a longer
+ * inner dimension and the panels more work.  Same factors and pivots up to
+ * the order of the products' sums.  No counterpart in the reference. */
+int cad_set_lu_block(cad_ctx* ctx, int nb);
 #define CAD_BATCH_GROUPED 0
 #define CAD_BATCH_LANES 1
 #define CAD_BATCH_LANES_CHAIN 2
