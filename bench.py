@@ -1110,7 +1110,8 @@ def run_ours(args, rank, world, local_rank):
         # LU panel leaf, is latency-bound: one cluster-wide pivot exchange per
         # column); the TD pair kernel is the assembly's
         "roofline": {"kernel": "dense FP64 solve: blocked LU with look-ahead (cluster leaf_lu_kernel, own row-swap "
-                               "and triangular kernels, cuBLAS DGEMM trailing updates) + chained triangular solves",
+                               "and triangular kernels, own DMMA trailing-update products) + chained triangular "
+                               "solves",
                      "bound": "fp64", "achieved": solve_tflops, "peak": fp64_peak_tflops, "unit": "TFLOP/s",
                      "frac": solve_tflops / fp64_peak_tflops,
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",

@@ -1210,9 +1210,17 @@ struct GroupLu {
         const int nblk = (nmax + nb - 1) / nb;
         if (nblk == 0) return;
         std::vector<cudaEvent_t> ev_panel(nblk, nullptr), ev_rest(nblk, nullptr);
+        cudaEvent_t fork = nullptr;
+        err = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
         for (int b = 0; b < nblk && ok(); ++b) {
             err = cudaEventCreateWithFlags(&ev_panel[b], cudaEventDisableTiming);
             if (ok()) err = cudaEventCreateWithFlags(&ev_rest[b], cudaEventDisableTiming);
+        }
+        // the side stream follows the main stream from here on (and joins a
+        // stream capture of it) even where it gets no work
+        if (ok() && side_st != main_st) {
+            err = cudaEventRecord(fork, main_st);
+            if (ok()) err = cudaStreamWaitEvent(side_st, fork, 0);
         }
         if (ok()) {
             panel(all, 0, nb);
@@ -1260,6 +1268,7 @@ struct GroupLu {
             if (ev_panel[b]) cudaEventDestroy(ev_panel[b]);
             if (ev_rest[b]) cudaEventDestroy(ev_rest[b]);
         }
+        if (fork) cudaEventDestroy(fork);
     }
 };
 
