@@ -43,7 +43,8 @@ enum Slot {
     S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS, S_COUNT
 };
 
-constexpr int kLuBlock = 256;   // outer block width of the LU
+constexpr int kLuBlock = 256;     // outer block width of the FP64 LU
+constexpr int kLuBlock32 = 512;   // of the FP32 factorisation (its TF32 products gain more from a long k)
 
 struct DevBuf {
     void* p = nullptr;
@@ -62,6 +63,7 @@ struct Lane {
 constexpr int kLanes = 32;           // cracks of a batch in flight at once
 constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
 constexpr int kGroupBlock = 128;     // block width of the grouped FP32 factorisation (systems padded to it)
+constexpr int kGroupExtraRounds = 3; // rounds of two more grouped sweeps for cracks still above the tolerance
 
 // The captured graph of the last batched call and what it was captured for.
 struct BatchGraph {
@@ -99,7 +101,7 @@ struct cad_ctx {
     long wait_limit = kDefaultWaitLimit;   // cad_set_wait_limit
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
     int batch_mode = CAD_BATCH_GROUPED;    // cad_set_batch_solve
-    int lu_block = kLuBlock;               // cad_set_lu_block: outer block width of single-system LUs
+    int lu_block = 0;                      // cad_set_lu_block: outer block width of single-system LUs (0: default)
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
@@ -130,6 +132,9 @@ struct NvtxRange {
     NvtxRange& operator=(const NvtxRange&) = delete;
 };
 #define CAD_NVTX_RANGE() NvtxRange nvtx_range_(__func__)
+
+// outer block width of a single-system factorisation
+int lu_nb(const cad_ctx* c, bool fp32) { return c->lu_block > 0 ? c->lu_block : (fp32 ? kLuBlock32 : kLuBlock); }
 
 int fail(cad_ctx* c, int code, const std::string& msg)
 {
@@ -333,7 +338,8 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches,
                         ctx->graphs, ctx->wait_limit};
     ctx->timed[1] = ctx->timed[2] = false;
-    int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info, ctx->lu_block);
+    int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info,
+                           lu_nb(ctx, true));
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
     CK(cudaEventRecord(ctx->ev[4], ctx->stream));
@@ -382,7 +388,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
         if (int r = ensure(ctx, S_IR32, 2 * (size_t)n * nrhs * sizeof(float), &ir32)) return r;
         if (int r = ensure(ctx, S_NORMS, 2 * (size_t)nrhs * sizeof(double), &norms)) return r;
         X = (double*)ir;
-        IrArgs ia{ls, n, A, lda, B, ldb, (int)nrhs, X, (float*)a32, (int*)piv, (int*)perm, (int*)info, ctx->lu_block,
+        IrArgs ia{ls, n, A, lda, B, ldb, (int)nrhs, X, (float*)a32, (int*)piv, (int*)perm, (int*)info, lu_nb(ctx, true),
                   ctx->tol, kIrMaxIter, X + (size_t)n * nrhs, (float*)ir32, (float*)ir32 + (size_t)n * nrhs,
                   (double*)norms};
         IrResult res{};
@@ -571,7 +577,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
                 if (e != cudaSuccess) return e;
                 lt.min_leaf_rpt = c;
                 return lu_factor_solve<double>(lt, (double*)scratch, n, n, nullptr, 0, 0, nullptr, 0, (int*)piv,
-                                               (int*)perm, (int*)info, ctx->lu_block, true, false) == LU_OK
+                                               (int*)perm, (int*)info, lu_nb(ctx, false), true, false) == LU_OK
                            ? cudaSuccess
                            : cudaErrorUnknown;
             });
@@ -582,7 +588,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
         if (int r = ensure(ctx, S_CHAIN, (size_t)n * sizeof(double) + lu_chain_sync_ints(n) * sizeof(int), &chain))
             return r;
         int rc = lu_factor_solve<double>(ls, A, n, lda, nullptr, 0, 0, nullptr, 0, (int*)piv, (int*)perm, (int*)info,
-                                         ctx->lu_block, true, false);
+                                         lu_nb(ctx, false), true, false);
         if (rc == LU_OK) rc = lu_pivots_to_perm(ls, (const int*)piv, n, (int*)perm);
         if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
         if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
@@ -595,7 +601,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
         return CAD_OK;
     }
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
-                                           (int*)info, ctx->lu_block, true, true);
+                                           (int*)info, lu_nb(ctx, false), true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
     if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
     CK(cudaMemcpy2DAsync(B, ldb * sizeof(double), work, n * sizeof(double), n * sizeof(double), nrhs,
@@ -978,6 +984,22 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
     CK(cudaStreamSynchronize(ctx->stream));
     for (int v : hinfo)   // a leaf, chain or tensor-core pipeline wait that ran out
         if (v < 0) return fail(ctx, CAD_ERR_TIMEOUT, "batched solve: a device wait ran out");
+    if (group) {
+        // cracks the graph's sweeps left above the tolerance: more grouped
+        // sweeps on their factors, two at a time
+        for (int round = 0; round < kGroupExtraRounds; ++round) {
+            std::vector<CrackRec> left;
+            for (int64_t c = 0; c < nbatch; ++c)
+                if (!(hrel[c] <= ctx->tol) && std::isfinite(hrel[c])) left.push_back(crecs[c]);
+            if (left.empty()) break;
+            const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches, nullptr, ctx->wait_limit};
+            if (mixed_group_sweeps(ls, left, b.gsync, b.gsync_ints, 2) != GMRES_OK)
+                return fail(ctx, CAD_ERR_CUDA, "batched solve: grouped launch failed");
+            CK(cudaMemcpyAsync(hrel.data(), rel, (size_t)nbatch * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+    }
     bool converged = true;
     for (int64_t c = 0; c < nbatch; ++c) {
         if (hrel[c] <= ctx->tol) continue;
@@ -1113,7 +1135,7 @@ int cad_set_lu_block(cad_ctx* ctx, int nb)
 {
     if (!ctx) return CAD_ERR_ARG;
     if (nb != 0 && (nb < 32 || nb > 1024)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
-    ctx->lu_block = nb == 0 ? kLuBlock : nb;
+    ctx->lu_block = nb;
     return CAD_OK;
 }
 

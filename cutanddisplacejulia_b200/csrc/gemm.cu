@@ -32,21 +32,28 @@ namespace cad {
 namespace {
 
 // ------------------------------------------------------------------ FP64 DMMA
-// CTA tile 128 x 64, 4 warps of 64 x 32 (8 x 4 DMMA tiles of 8 x 8 each),
-// three CTAs per SM (72 KB of shared memory each: 3 stages of unpadded,
-// swizzled tiles) so that the DMMA latency is hidden by 12 warps and one
-// CTA's prologue and epilogue overlap the others' main loops.
-constexpr int DBM = 128, DBN = 64, DBK = 16, DSTAGES = 3, DTHREADS = 128, DMINB = 3;
-constexpr int DLDA = DBM;       // shared row (one k) of the A tile, doubles
+// CTA tile BM x BN (128 x 64 for large products, 64 x 32 where the large
+// tiles would not fill the GPU), 4 warps of BM/2 x BN/2 as DMMA tiles of
+// 8 x 8; k-steps of 16; several CTAs per SM (the large tile: three, 72 KB of
+// shared memory each -- 3 stages of unpadded, swizzled tiles) so that the
+// DMMA latency is hidden and one CTA's prologue and epilogue overlap the
+// others' main loops.
+constexpr int DBK = 16, DSTAGES = 3, DTHREADS = 128;
 constexpr int DLDB = DBK;       // shared row (one n) of the B tile, doubles
-constexpr int DSTAGE_A = DBK * DLDA;
-constexpr int DSTAGE_B = DBN * DLDB;
+template <int BM, int BN>
+struct DTile {
+    static constexpr int LDA = BM;             // shared row (one k) of the A tile, doubles
+    static constexpr int STAGE_A = DBK * BM;
+    static constexpr int STAGE_B = BN * DLDB;
+    static constexpr int MT = BM / 16;         // 8-row DMMA tiles per warp
+    static constexpr int NT = BN / 16;         // 8-column DMMA tiles per warp
+    static constexpr size_t SMEM = (size_t)DSTAGES * (STAGE_A + STAGE_B) * sizeof(double);
+};
 // Unpadded rows with the 8-byte words XOR-swizzled by the row index: a
 // fragment load (4 rows x 4 (A) or 4 x 4 (B) words per half warp) then hits 16
 // distinct banks pairs.  Element (row, col) of a tile with rows of `ld` words
 // sits at row * ld + (col ^ (4 * (row & 3))).
 __device__ __forceinline__ int swz(int row, int col, int ld) { return row * ld + (col ^ ((row & 3) << 2)); }
-constexpr size_t DSMEM = (size_t)DSTAGES * (DSTAGE_A + DSTAGE_B) * sizeof(double);
 
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, bool pred)
 {
@@ -91,9 +98,10 @@ __device__ __forceinline__ void dmma16<16>(double& c0, double& c1, double& c2, d
                    "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-// Stage s of the ring <- k-step kt: the A tile (128 rows x 16 columns, stored
-// k-major: row k holds 128 consecutive m) and the B tile (16 rows x 64
+// Stage s of the ring <- k-step kt: the A tile (BM rows x 16 columns, stored
+// k-major: row k holds BM consecutive m) and the B tile (16 rows x BN
 // columns, stored n-major: row n holds 16 consecutive k).
+template <int BM, int BN>
 __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const double* __restrict__ A, int64_t lda,
                                                  const double* __restrict__ B, int64_t ldb, int m, int n, int k,
                                                  int m0, int n0, int kt)
@@ -101,15 +109,15 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
     const int tid = threadIdx.x;
     const int k0 = kt * DBK;
 #pragma unroll
-    for (int i = 0; i < (DBM * DBK) / DTHREADS; ++i) {
+    for (int i = 0; i < (BM * DBK) / DTHREADS; ++i) {
         const int e = tid + DTHREADS * i;
-        const int kk = e / DBM, mm = e % DBM;
+        const int kk = e / BM, mm = e % BM;
         const bool ok = (m0 + mm < m) && (k0 + kk < k);
         const double* src = ok ? A + (int64_t)(m0 + mm) + (int64_t)(k0 + kk) * lda : A;
-        cp_async8(sm100::smem_addr(sA + swz(kk, mm, DLDA)), src, ok);
+        cp_async8(sm100::smem_addr(sA + swz(kk, mm, BM)), src, ok);
     }
 #pragma unroll
-    for (int i = 0; i < (DBN * DBK) / DTHREADS; ++i) {
+    for (int i = 0; i < (BN * DBK) / DTHREADS; ++i) {
         const int e = tid + DTHREADS * i;
         const int nn = e / DBK, kk = e % DBK;
         const bool ok = (n0 + nn < n) && (k0 + kk < k);
@@ -119,28 +127,31 @@ __device__ __forceinline__ void dgemm_load_stage(double* sA, double* sB, const d
 }
 
 // MK: k-extent of one DMMA (4: m8n8k4 tiles; 8 or 16: m16n8k8 / m16n8k16)
-template <int MK>
-__global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
-                                                                int64_t lda, const double* __restrict__ B, int64_t ldb,
-                                                                double* __restrict__ C, int64_t ldc)
+template <int MK, int BM, int BN, int MINB>
+__global__ void __launch_bounds__(DTHREADS, MINB) dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A,
+                                                               int64_t lda, const double* __restrict__ B, int64_t ldb,
+                                                               double* __restrict__ C, int64_t ldc)
 {
+    using TL = DTile<BM, BN>;
+    constexpr int MT = TL::MT, NT = TL::NT;
     extern __shared__ __align__(16) double dsm[];
     double* sA = dsm;
-    double* sB = dsm + DSTAGES * DSTAGE_A;
-    const int m0 = blockIdx.x * DBM, n0 = blockIdx.y * DBN;
+    double* sB = dsm + DSTAGES * TL::STAGE_A;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;   // 2 x 2 warps of 64 x 32
+    const int wm = (warp & 1) * (BM / 2), wn = (warp >> 1) * (BN / 2);   // 2 x 2 warps
     const int g = lane >> 2, t = lane & 3;
-    double acc[8][4][2];
+    double acc[MT][NT][2];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     const int nk = (k + DBK - 1) / DBK;
 #pragma unroll
     for (int s = 0; s < DSTAGES - 1; ++s) {
-        if (s < nk) dgemm_load_stage(sA + s * DSTAGE_A, sB + s * DSTAGE_B, A, lda, B, ldb, m, n, k, m0, n0, s);
+        if (s < nk)
+            dgemm_load_stage<BM, BN>(sA + s * TL::STAGE_A, sB + s * TL::STAGE_B, A, lda, B, ldb, m, n, k, m0, n0, s);
         cp_async_commit();
     }
     for (int kt = 0; kt < nk; ++kt) {
@@ -149,43 +160,43 @@ __global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n
         // refill the stage consumed one step ago (every warp is past it)
         const int kn = kt + DSTAGES - 1;
         if (kn < nk)
-            dgemm_load_stage(sA + (kn % DSTAGES) * DSTAGE_A, sB + (kn % DSTAGES) * DSTAGE_B, A, lda, B, ldb, m, n, k,
-                             m0, n0, kn);
+            dgemm_load_stage<BM, BN>(sA + (kn % DSTAGES) * TL::STAGE_A, sB + (kn % DSTAGES) * TL::STAGE_B, A, lda, B,
+                                     ldb, m, n, k, m0, n0, kn);
         cp_async_commit();
-        const double* a_s = sA + (kt % DSTAGES) * DSTAGE_A;
-        const double* b_s = sB + (kt % DSTAGES) * DSTAGE_B;
+        const double* a_s = sA + (kt % DSTAGES) * TL::STAGE_A;
+        const double* b_s = sB + (kt % DSTAGES) * TL::STAGE_B;
         if constexpr (MK == 4) {
 #pragma unroll
             for (int kk = 0; kk < DBK; kk += 4) {
-                double af[8], bf[4];
+                double af[MT], bf[NT];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) af[i] = a_s[swz(kk + t, wm + 8 * i + g, DLDA)];
+                for (int i = 0; i < MT; ++i) af[i] = a_s[swz(kk + t, wm + 8 * i + g, BM)];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) bf[j] = b_s[swz(wn + 8 * j + g, kk + t, DLDB)];
+                for (int j = 0; j < NT; ++j) bf[j] = b_s[swz(wn + 8 * j + g, kk + t, DLDB)];
 #pragma unroll
-                for (int i = 0; i < 8; ++i)
+                for (int i = 0; i < MT; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                    for (int j = 0; j < NT; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
             }
         } else {
             // 16-row blocks: acc[2I] holds rows wm + 16I + g, acc[2I + 1]
             // rows wm + 16I + 8 + g (the 8-row layout of the m8n8k4 path)
 #pragma unroll
             for (int kk = 0; kk < DBK; kk += MK) {
-                double af[4][MK / 2], bf[4][MK / 4];
+                double af[MT / 2][MK / 2], bf[NT][MK / 4];
 #pragma unroll
-                for (int I = 0; I < 4; ++I)
+                for (int I = 0; I < MT / 2; ++I)
 #pragma unroll
                     for (int r = 0; r < MK / 2; ++r)
-                        af[I][r] = a_s[swz(kk + t + 4 * (r >> 1), wm + 16 * I + 8 * (r & 1) + g, DLDA)];
+                        af[I][r] = a_s[swz(kk + t + 4 * (r >> 1), wm + 16 * I + 8 * (r & 1) + g, BM)];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
+                for (int j = 0; j < NT; ++j)
 #pragma unroll
                     for (int r = 0; r < MK / 4; ++r) bf[j][r] = b_s[swz(wn + 8 * j + g, kk + t + 4 * r, DLDB)];
 #pragma unroll
-                for (int I = 0; I < 4; ++I)
+                for (int I = 0; I < MT / 2; ++I)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j)
+                    for (int j = 0; j < NT; ++j)
                         dmma16<MK>(acc[2 * I][j][0], acc[2 * I][j][1], acc[2 * I + 1][j][0], acc[2 * I + 1][j][1],
                                    af[I], bf[j]);
             }
@@ -193,16 +204,16 @@ __global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n
     }
     cp_async_wait<0>();
     // C -= acc: thread holds rows wm + 8i + g, columns wn + 8j + 2t + {0, 1}.
-    // Per column pair, all 16 loads are issued before any store (the compiler
+    // Per column pair, all loads are issued before any store (the compiler
     // cannot reorder a load of C past a store to C), so their latencies overlap.
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        double c[2][8];
+    for (int j = 0; j < NT; ++j) {
+        double c[2][MT];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int col = n0 + wn + 8 * j + 2 * t + h;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < MT; ++i) {
                 const int row = m0 + wm + 8 * i + g;
                 c[h][i] = (col < n && row < m) ? C[(int64_t)col * ldc + row] : 0.0;
             }
@@ -213,7 +224,7 @@ __global__ void __launch_bounds__(DTHREADS, DMINB) dgemm_sub_kernel(int m, int n
             if (col >= n) continue;
             double* cc = C + (int64_t)col * ldc;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < MT; ++i) {
                 const int row = m0 + wm + 8 * i + g;
                 if (row < m) cc[row] = c[h][i] - acc[i][j][h];
             }
@@ -475,18 +486,30 @@ bool tma_ok(const float* p, int64_t ld)
 }  // namespace
 
 namespace {
+template <int MK, int BM, int BN, int MINB>
+cudaError_t launch_dgemm_tile(cudaStream_t st, int m, int n, int k, const double* A, int64_t lda, const double* B,
+                              int64_t ldb, double* C, int64_t ldc)
+{
+    constexpr size_t smem = DTile<BM, BN>::SMEM;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(dgemm_sub_kernel<MK, BM, BN, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(dgemm_sub_kernel<MK, BM, BN, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    });
+    const dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));
+    dgemm_sub_kernel<MK, BM, BN, MINB><<<grid, DTHREADS, smem, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+    return cudaGetLastError();
+}
+
+// the large tile where it gives at least two CTAs per SM, else the small one
 template <int MK>
 cudaError_t launch_dgemm(cudaStream_t st, int m, int n, int k, const double* A, int64_t lda, const double* B,
                          int64_t ldb, double* C, int64_t ldc)
 {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(dgemm_sub_kernel<MK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DSMEM);
-        cudaFuncSetAttribute(dgemm_sub_kernel<MK>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    });
-    const dim3 grid((unsigned)((m + DBM - 1) / DBM), (unsigned)((n + DBN - 1) / DBN));
-    dgemm_sub_kernel<MK><<<grid, DTHREADS, DSMEM, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
-    return cudaGetLastError();
+    const int64_t big = (int64_t)((m + 127) / 128) * ((n + 63) / 64);
+    if (big >= 2 * 148) return launch_dgemm_tile<MK, 128, 64, 3>(st, m, n, k, A, lda, B, ldb, C, ldc);
+    return launch_dgemm_tile<MK, 64, 32, 6>(st, m, n, k, A, lda, B, ldb, C, ldc);
 }
 }  // namespace
 

@@ -686,6 +686,60 @@ __global__ void __launch_bounds__(256) relres_group_kernel(const __grid_constant
 
 }  // namespace
 
+namespace {
+
+// every grouped launch over the cracks, kCrackGroupMax at a time
+template <class F>
+bool each_group(const std::vector<CrackRec>& cracks, int64_t* launches, F&& launch)
+{
+    CrackGroup g{};
+    int nmax = 0;
+    for (size_t p = 0; p <= cracks.size(); ++p) {
+        if (g.count == kCrackGroupMax || (p == cracks.size() && g.count > 0)) {
+            launch(g, nmax);
+            if (launches) ++*launches;
+            if (cudaGetLastError() != cudaSuccess) return false;
+            g.count = 0;
+            nmax = 0;
+        }
+        if (p < cracks.size()) {
+            g.rec[g.count++] = cracks[p];
+            nmax = cracks[p].n_pad > nmax ? cracks[p].n_pad : nmax;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+int mixed_group_sweeps(const LuStreams& ls, const std::vector<CrackRec>& cracks, int* sync_all, size_t sync_ints,
+                       int sweeps)
+{
+    if (cracks.empty()) return GMRES_OK;
+    cudaStream_t st = ls.main;
+    int64_t* L = ls.launches;
+    const long wl = ls.wait_limit > 0 ? ls.wait_limit : kDefaultWaitLimit;
+    for (int it = 0; it < sweeps; ++it) {
+        if (cudaMemsetAsync(sync_all, 0, sync_ints * sizeof(int), st) != cudaSuccess) return GMRES_CUDA_ERROR;
+        if (!each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
+                chain_group_kernel<false><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
+            }) ||
+            !each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
+                chain_group_kernel<true><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
+            }) ||
+            !each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
+                axpy_group_kernel<<<dim3((unsigned)((nmax + 255) / 256), g.count), 256, 0, st>>>(g);
+            }) ||
+            !each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
+                residual_group_kernel<<<dim3((unsigned)((nmax + 127) / 128), g.count), 128, 0, st>>>(g);
+            }))
+            return GMRES_CUDA_ERROR;
+    }
+    if (!each_group(cracks, L, [&](const CrackGroup& g, int) { relres_group_kernel<<<g.count, 256, 0, st>>>(g); }))
+        return GMRES_CUDA_ERROR;
+    return GMRES_OK;
+}
+
 int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, const std::vector<GroupSystem>& sys,
                       const CUtensorMap* dev_maps, int* infos, int* status, int* sync_all, size_t sync_ints,
                       int sweeps, int nb)
@@ -696,26 +750,8 @@ int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, 
     int64_t* L = ls.launches;
     for (const auto& c : cracks)
         if (c.n_pad % kRB || c.n_pad < c.n) return GMRES_CUDA_ERROR;
-    // every grouped launch, kCrackGroupMax cracks at a time
-    auto each = [&](auto&& launch) -> bool {
-        CrackGroup g{};
-        int nmax = 0;
-        for (size_t p = 0; p <= cracks.size(); ++p) {
-            if (g.count == kCrackGroupMax || (p == cracks.size() && g.count > 0)) {
-                launch(g, nmax);
-                if (L) ++*L;
-                if (cudaGetLastError() != cudaSuccess) return false;
-                g.count = 0;
-                nmax = 0;
-            }
-            if (p < cracks.size()) {
-                g.rec[g.count++] = cracks[p];
-                nmax = cracks[p].n_pad > nmax ? cracks[p].n_pad : nmax;
-            }
-        }
-        return true;
-    };
-    if (!each([&](const CrackGroup& g, int) { cast_pad_group_kernel<<<dim3(32, g.count), 256, 0, st>>>(g); }))
+    if (!each_group(cracks, L,
+                    [&](const CrackGroup& g, int) { cast_pad_group_kernel<<<dim3(32, g.count), 256, 0, st>>>(g); }))
         return GMRES_CUDA_ERROR;
     if (lu_factor_group(ls, sys, dev_maps, infos, status, nb) != LU_OK) return GMRES_CUDA_ERROR;
     std::vector<int*> perms;
@@ -725,33 +761,15 @@ int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, 
     if (cudaFuncSetAttribute(invert_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem) !=
         cudaSuccess)
         return GMRES_CUDA_ERROR;
-    if (!each([&](const CrackGroup& g, int nmax) {
+    if (!each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
             invert_group_kernel<<<dim3((unsigned)(nmax / kRB), g.count, 2), kRB, ismem, st>>>(g);
         }))
         return GMRES_CUDA_ERROR;
-    if (!each([&](const CrackGroup& g, int nmax) {
+    if (!each_group(cracks, L, [&](const CrackGroup& g, int nmax) {
             init_group_kernel<<<dim3((unsigned)((nmax + 255) / 256), g.count), 256, 0, st>>>(g);
         }))
         return GMRES_CUDA_ERROR;
-    const long wl = ls.wait_limit > 0 ? ls.wait_limit : kDefaultWaitLimit;
-    for (int it = 0; it < sweeps; ++it) {
-        if (cudaMemsetAsync(sync_all, 0, sync_ints * sizeof(int), st) != cudaSuccess) return GMRES_CUDA_ERROR;
-        if (!each([&](const CrackGroup& g, int nmax) {
-                chain_group_kernel<false><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
-            }) ||
-            !each([&](const CrackGroup& g, int nmax) {
-                chain_group_kernel<true><<<dim3((unsigned)(nmax / kRB), g.count), kChainThreads, 0, st>>>(g, wl);
-            }) ||
-            !each([&](const CrackGroup& g, int nmax) {
-                axpy_group_kernel<<<dim3((unsigned)((nmax + 255) / 256), g.count), 256, 0, st>>>(g);
-            }) ||
-            !each([&](const CrackGroup& g, int nmax) {
-                residual_group_kernel<<<dim3((unsigned)((nmax + 127) / 128), g.count), 128, 0, st>>>(g);
-            }))
-            return GMRES_CUDA_ERROR;
-    }
-    if (!each([&](const CrackGroup& g, int) { relres_group_kernel<<<g.count, 256, 0, st>>>(g); }))
-        return GMRES_CUDA_ERROR;
-    return GMRES_OK;
+    return mixed_group_sweeps(ls, cracks, sync_all, sync_ints, sweeps);
 }
+
 }  // namespace cad

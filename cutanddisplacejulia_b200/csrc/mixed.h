@@ -148,5 +148,9 @@ struct CrackRec {
 int mixed_group_solve(const LuStreams& ls, const std::vector<CrackRec>& cracks, const std::vector<GroupSystem>& sys,
                       const CUtensorMap* dev_maps, int* infos, int* status, int* sync_all, size_t sync_ints,
                       int sweeps, int nb);
+// `sweeps` more refinement sweeps of the given cracks (factors, x and r from
+// an earlier mixed_group_solve), then their *rel.
+int mixed_group_sweeps(const LuStreams& ls, const std::vector<CrackRec>& cracks, int* sync_all, size_t sync_ints,
+                       int sweeps);
 
 }  // namespace cad

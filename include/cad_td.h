@@ -146,8 +146,8 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
  *   CAD_BATCH_LANES_CHAIN: the lanes with ticket-ordered chain solves. */
 /* Outer block width of the dense LU of a single system (the FP64 solve, the
  * mixed solve's FP32 factorisation): 32..1024 columns, 0 = the library's
- * default (256).  Wider blocks give the trailing-update products a longer
- * inner dimension and the panels more work.  Same factors and pivots up to
+ * defaults (256 for FP64, 512 for FP32).  Wider blocks give the trailing-
+ * update products a longer inner dimension and the panels more work.  Same factors and pivots up to
  * the order of the products' sums.  No counterpart in the reference. */
 int cad_set_lu_block(cad_ctx* ctx, int nb);
 #define CAD_BATCH_GROUPED 0

@@ -15,7 +15,9 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(128, 128, 32), (300, 200, 100), (1000, 700, 256), (4100, 130, 64), (37, 900, 300), (256, 256, 8)]
+# the last two take the FP64 kernel's large tiles (at least two CTAs per SM), the others its small ones
+SHAPES = [(128, 128, 32), (300, 200, 100), (1000, 700, 256), (4100, 130, 64), (37, 900, 300), (256, 256, 8),
+          (2500, 1100, 96), (2600, 1200, 33)]
 
 
 def _run(cad, prec, m, n, k, lda, ldb, ldc, a_off=0, b_off=0, integer=False, seed=0):
