@@ -359,6 +359,42 @@ def surface_grid(hs, n=100, extent=4.0):
     return X.ravel(), Y.ravel(), np.full(X.size, 0.0 if hs else 0.5)
 
 
+def near_field_study(ctx, L, stream, step_asm_args, A, b0, x64, factors):
+    """Mixed assembly with the FP64 near field widened: per near-field radius
+    (in mean edge lengths), the assembly time, the mixed solve's slip error
+    against the FP64 LU and the system matrix's largest entry error (A is
+    overwritten)."""
+    import torch
+
+    from cutanddisplacejulia_b200 import _lib
+    dN, dM, dP1, dP2, dP3, n, lam, hs = step_asm_args
+    n3 = 3 * n
+    A64 = torch.empty_like(A)
+    _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(),
+                                  n, NU, G, lam, hs, A64.data_ptr(), n3), ctx)
+    scale = float(A64.abs().max())
+    out = []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for f in factors:
+        with _lib.solver_mode(ctx, "mixed", tol=MIXED_TOL, max_iter=200), _lib.assembly_mode(ctx, "mixed", f):
+            for rep in range(2):   # the second assembly is timed
+                torch.cuda.synchronize()
+                ev[0].record(stream)
+                _lib.check(L.cad_assemble_dev(ctx, dN.data_ptr(), dM.data_ptr(), dP1.data_ptr(), dP2.data_ptr(),
+                                              dP3.data_ptr(), n, NU, G, lam, hs, A.data_ptr(), n3), ctx)
+                ev[1].record(stream)
+                torch.cuda.synchronize()
+            asm_ms = ev[0].elapsed_time(ev[1])
+            mat_err = float((A - A64).abs().max()) / scale
+            x = b0.clone()
+            _lib.check(L.cad_solve_dev(ctx, n3, A.data_ptr(), n3, x.data_ptr(), n3, 1), ctx)
+            torch.cuda.synchronize()
+        out.append({"near_factor": f, "assembly_ms": asm_ms, "matrix_max_rel_err": mat_err,
+                    "slip_rel_err_vs_fp64_lu": float(torch.linalg.vector_norm(x - x64) / torch.linalg.vector_norm(x64))})
+    del A64
+    return out
+
+
 def mixed_solve_timing(args, ctx, L, stream, step_asm_args, A, b0, x64, ms_fp64, world, dev):
     """The mixed-precision step on the same workload: far-field pairs assembled
     in FP32 (near field -- within 3 mean edge lengths -- in FP64), then FP32 LU
@@ -865,6 +901,8 @@ def run_c3(args, rank, world, local_rank):
                                                           A=A, b0=b0, x64=x64, ms_fp64=ms64, world=world, dev=dev)
     batch = None if args.batch_rhs <= 0 else batch_rhs_timing(args, ctx, L, stream, (dN, dM, dP1, dP2, dP3, n, lam,
                                                                                       hs), nrm, A, dev)
+    near = None if not args.near_study else near_field_study(ctx, L, stream, (dN, dM, dP1, dP2, dP3, n, lam, hs), A,
+                                                             b0, x64, [3.0, 6.0, 12.0, 24.0, 48.0])
 
     # end to end through the host C ABI: cad_slip_calculator in the learned
     # mode (assembly, preconditioner and GMRES inside the call), pinned host
@@ -953,6 +991,7 @@ def run_c3(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "mixed": mixed,
         "batch_rhs": batch,
+        "near_field_study": near,
         "training": training,
         "autotune": _autotune_summary(L, ctx, args),
     }
@@ -1314,6 +1353,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision solve of the same system")
     ap.add_argument("--no-autotune", action="store_true", help="fixed launch shapes instead of the autotune cache")
+    ap.add_argument("--near-study", action="store_true",
+                    help="dipping: mixed assembly with the FP64 near field at 3-48 mean edge lengths (slip errors)")
     ap.add_argument("--batch-rhs", type=int, default=0,
                     help="also time K seeded remote-stress right-hand sides on the same system (FP64 LU and mixed)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dipping",
