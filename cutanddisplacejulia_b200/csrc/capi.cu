@@ -64,6 +64,7 @@ constexpr int kLanes = 32;           // cracks of a batch in flight at once
 constexpr int kBatchSweeps = 4;      // refinement sweeps per crack inside the batch graph
 constexpr int kGroupBlock = 128;     // block width of the grouped FP32 factorisation (systems padded to it)
 constexpr int kGroupExtraRounds = 3; // rounds of two more grouped sweeps for cracks still above the tolerance
+constexpr int kLeafAux = 4;          // streams for the grouped leaves of different cluster sizes
 
 // The captured graph of the last batched call and what it was captured for.
 struct BatchGraph {
@@ -103,6 +104,7 @@ struct cad_ctx {
     int batch_mode = CAD_BATCH_GROUPED;    // cad_set_batch_solve
     int lu_block = 0;                      // cad_set_lu_block: outer block width of single-system LUs (0: default)
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
+    cudaStream_t leaf_aux[kLeafAux] = {};  // grouped leaves of different cluster sizes, side by side
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
     int max_iter = 200;
@@ -765,7 +767,9 @@ int batch_body(cad_ctx* ctx, const BatchArgs& b, cudaEvent_t fork)
     }
     if (b.crecs) {
         CK(cudaMemsetAsync(b.gstatus, 0, sizeof(int), ctx->stream));
-        const LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches, nullptr, ctx->wait_limit};
+        LuStreams ls{ctx->stream, ctx->side_stream, &ctx->launches, nullptr, ctx->wait_limit};
+        ls.aux = ctx->leaf_aux;
+        ls.naux = kLeafAux;
         if (mixed_group_solve(ls, *b.crecs, *b.gsys, b.maps, b.ginfo, b.gstatus, b.gsync, b.gsync_ints, kBatchSweeps,
                               kGroupBlock) != GMRES_OK)
             return fail(ctx, CAD_ERR_CUDA, "batched solve: grouped launch failed");
@@ -955,7 +959,7 @@ int slip_batched(cad_ctx* ctx, int64_t nbatch, const int64_t* offsets, const dou
         e = cudaStreamEndCapture(ctx->stream, &graph);
         if (rc == CAD_OK && e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: stream capture");
         if (rc == CAD_OK) {
-            e = cudaGraphInstantiate(&g.exec, graph, 0);
+            e = cudaGraphInstantiate(&g.exec, graph, cudaGraphInstantiateFlagUseNodePriority);
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batched solve: graph instantiation");
         }
         if (graph) cudaGraphDestroy(graph);
@@ -1048,6 +1052,11 @@ int cad_init(int device, cad_ctx** out)
         cad_destroy(ctx);
         return CAD_ERR_CUDA;
     }
+    for (auto& a : ctx->leaf_aux)
+        if (cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
+            cad_destroy(ctx);
+            return CAD_ERR_CUDA;
+        }
     ctx->graphs = lu_graph_cache_create();
     *out = ctx;
     return CAD_OK;
@@ -1077,6 +1086,8 @@ int cad_destroy(cad_ctx* ctx)
         if (l.done) cudaEventDestroy(l.done);
     }
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    for (auto a : ctx->leaf_aux)
+        if (a) cudaStreamDestroy(a);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return CAD_OK;

@@ -18,6 +18,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <climits>
 #include <mutex>
@@ -935,7 +936,10 @@ cudaError_t lu_capture(Lu<T>& lu, T* A, int64_t n, int64_t lda, const T* B, int6
         cudaGraph_t graph = nullptr;
         const cudaError_t ee = cudaStreamEndCapture(lu.main_st, &graph);
         if (lu.err == cudaSuccess) lu.err = ee;
-        if (lu.ok() && graph) lu.err = cudaGraphInstantiate(exec, graph, 0);
+        // the nodes keep the priorities of the streams they were captured on
+        // (panel chain high, side-stream updates low); by default a graph
+        // would run every node at the priority of the stream it is launched on
+        if (lu.ok() && graph) lu.err = cudaGraphInstantiate(exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         if (graph) cudaGraphDestroy(graph);
         e = lu.err;
         if (!lu.ok() && *exec) {
@@ -1041,6 +1045,10 @@ __global__ void __launch_bounds__(1024) perm_group_kernel(const __grid_constant_
 // stream, as in the single-system factorisation.
 struct GroupLu {
     cudaStream_t st, main_st, side_st;
+    cudaStream_t* aux = nullptr;   // leaf streams
+    int naux = 0;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_join;
     const std::vector<GroupSystem>* sys;
     const CUtensorMap* maps;
     int* status;
@@ -1131,11 +1139,27 @@ struct GroupLu {
     }
 
     // 32-column leaves of the panel at diagonal position o, one launch per
-    // cluster size (CTAs of 512 rows)
+    // cluster size (CTAs of 512 rows); the launches of different sizes run
+    // side by side on the auxiliary streams when there are any
     void leaf(const std::vector<int>& act, int o, int w)
     {
         if (!ok()) return;
+        std::vector<int> sizes;
+        for (int p : act) {
+            const int m = S(p).n_pad - o;
+            const int C = (m + kLeafThreads - 1) / kLeafThreads;
+            if (m > 0 && std::find(sizes.begin(), sizes.end(), C) == sizes.end()) sizes.push_back(C);
+        }
+        const bool fan = naux > 0 && sizes.size() > 1;
+        cudaStream_t home = st;
+        if (fan) {
+            err = cudaEventRecord(ev_fork, home);
+            for (int q = 0; q < naux && ok(); ++q) err = cudaStreamWaitEvent(aux[q], ev_fork, 0);
+        }
+        int used = 0;
         for (int C = 1; C <= cluster && ok(); ++C) {
+            if (std::find(sizes.begin(), sizes.end(), C) == sizes.end()) continue;
+            if (fan) st = aux[used++ % naux];
             LeafGroup g{};
             g.w = w;
             g.wait_limit = wait_limit;
@@ -1165,6 +1189,12 @@ struct GroupLu {
             }
             flush();
         }
+        st = home;
+        if (fan)   // the home stream continues once every size's leaves are done
+            for (int q = 0; q < (used < naux ? used : naux) && ok(); ++q) {
+                err = cudaEventRecord(ev_join[q], aux[q]);
+                if (ok()) err = cudaStreamWaitEvent(home, ev_join[q], 0);
+            }
     }
 
     void panel(const std::vector<int>& act, int o, int w)
@@ -1286,6 +1316,24 @@ int lu_factor_group(const LuStreams& s, const std::vector<GroupSystem>& sys, con
     g.maps = dev_maps;
     g.status = status;
     g.wait_limit = s.wait_limit > 0 ? s.wait_limit : kDefaultWaitLimit;
+    g.aux = s.aux;
+    g.naux = s.aux ? s.naux : 0;
+    if (g.naux > 0) {
+        g.err = cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming);
+        g.ev_join.assign((size_t)g.naux, nullptr);
+        for (auto& e : g.ev_join)
+            if (g.ok()) g.err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+    struct Cleanup {   // the events of the leaf fan-out
+        GroupLu& g;
+        ~Cleanup()
+        {
+            if (g.ev_fork) cudaEventDestroy(g.ev_fork);
+            for (auto e : g.ev_join)
+                if (e) cudaEventDestroy(e);
+        }
+    } cleanup{g};
+    if (!g.ok()) return LU_CUDA_ERROR;
     {
         Lu<float> probe;
         configure(probe);

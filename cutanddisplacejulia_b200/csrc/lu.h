@@ -31,6 +31,10 @@ struct LuStreams {
     LuGraphCache* graphs;    // if set, repeated call signatures replay a captured graph
     long wait_limit = 0;     // polls a device wait makes before it gives up (0: kDefaultWaitLimit)
     int min_leaf_rpt = 1;    // fewest rows per leaf thread (1, 2, 4): leaves of 32 / rpt columns
+    // grouped factorisations: streams on which the leaf launches of different
+    // cluster sizes run side by side (none: one after the other on main)
+    cudaStream_t* aux = nullptr;
+    int naux = 0;
 };
 
 // Polls of a device-side wait (a pivot exchange, a chain flag) before the

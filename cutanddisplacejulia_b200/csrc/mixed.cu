@@ -638,15 +638,17 @@ __global__ void __launch_bounds__(256) axpy_group_kernel(const __grid_constant__
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) r.x[i] += r.z[i];
 }
 
-// r = b - A x in FP64: thread per row, columns in order (x staged through
-// shared memory), rows past n zero
+// r = b - A x in FP64: thread per row (coalesced down each column), x staged
+// through shared memory, eight column loads in flight per thread into four
+// accumulators (column c to accumulator c % 4, combined in a fixed order);
+// rows past n zero
 __global__ void __launch_bounds__(128) residual_group_kernel(const __grid_constant__ CrackGroup g)
 {
     __shared__ double s_x[1024];
     const CrackRec& r = g.rec[blockIdx.y];
     const int i = blockIdx.x * 128 + threadIdx.x;
     if ((int)blockIdx.x * 128 >= r.n_pad) return;
-    double acc = 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int c0 = 0; c0 < r.n; c0 += 1024) {
         const int cn = r.n - c0 < 1024 ? r.n - c0 : 1024;
         __syncthreads();
@@ -654,11 +656,18 @@ __global__ void __launch_bounds__(128) residual_group_kernel(const __grid_consta
         __syncthreads();
         if (i < r.n) {
             const double* a = r.A + i + (int64_t)c0 * r.lda;
-#pragma unroll 8
-            for (int c = 0; c < cn; ++c) acc = fma(a[(int64_t)c * r.lda], s_x[c], acc);
+            int c = 0;
+            for (; c + 8 <= cn; c += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = a[(int64_t)(c + u) * r.lda];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[u & 3] = fma(v[u], s_x[c + u], acc[u & 3]);
+            }
+            for (; c < cn; ++c) acc[c & 3] = fma(a[(int64_t)c * r.lda], s_x[c], acc[c & 3]);
         }
     }
-    if (i < r.n_pad) r.r[i] = i < r.n ? r.b[i] - acc : 0.0;
+    if (i < r.n_pad) r.r[i] = i < r.n ? r.b[i] - ((acc[0] + acc[1]) + (acc[2] + acc[3])) : 0.0;
 }
 
 // rel = ||r|| / ||b|| per crack (fixed-order block reduction)
