@@ -213,3 +213,22 @@ def savage_valley_check(case, strain6):
         means.append(float(np.mean(r[~np.isnan(r)])))
     assert not any(p > 0.15 for p in means), means
     return means
+
+
+def oracle_system_columns(oracle, sample, P1, P2, P3, nrm, mid, nu, G, lam, hs):
+    """Columns [sample; N + sample; 2N + sample] of the system matrix
+    A = -[Atn; Atss; Atds] from the oracle's strain influences and traction
+    conversion (src/CalculateInfluenceMatrices3D.jl:73-114)."""
+    n = len(P1)
+    obs = mid - 1e-12 * nrm
+    k = len(sample)
+    ones = np.ones(k)
+    S, _ = oracle.td_inf(obs[:, 0], obs[:, 1], obs[:, 2], P1[sample], P2[sample], P3[sample], ones, ones, ones, nu,
+                         G, 0, 1, hs)
+    T = oracle.strain_to_traction(S, nrm, lam, G)
+    ref = np.empty((3 * n, 3 * k))
+    for m in range(3):
+        for r in range(3):
+            ref[r * n:(r + 1) * n, m * k:(m + 1) * k] = -T[3 * m + r]
+    return ref
+

@@ -2,15 +2,18 @@
 system matrix sharded by element columns as dist.column_block splits it for
 3 ranks (run one after another on this GPU; the blocks need no exchange)
 must reproduce the columns of the full assembly (cad_assemble_dev) exactly,
-in full space and half space."""
+in full space and half space, and seeded columns of each block must match the
+oracle's restatement of the assembly."""
 import numpy as np
 import pytest
+
+from helpers import assert_parity, oracle_system_columns
 
 pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("hs", [0, 1])
-def test_column_blocks_equal_full_assembly(cad, hs):
+def test_column_blocks_equal_full_assembly(cad, oracle, hs):
     import torch
 
     from cutanddisplacejulia_b200 import _lib, dist, workloads
@@ -40,6 +43,11 @@ def test_column_blocks_equal_full_assembly(cad, hs):
         block = B.view(3 * nb, n3).cpu().numpy().T
         cols = np.concatenate([m * n + np.arange(j0, j1) for m in range(3)])
         assert np.array_equal(block, full[:, cols])
+        # four seeded element columns of the block against the oracle
+        pick = np.sort(np.random.default_rng(rank).choice(nb, 4, replace=False))
+        ref = oracle_system_columns(oracle, j0 + pick, P1, P2, P3, nrm, mid, nu, G, lam, hs)
+        got = block[:, np.concatenate([m * nb + pick for m in range(3)])]
+        assert_parity(got[None], ref[None])
 
 
 def test_column_block_argument_checks(cad):

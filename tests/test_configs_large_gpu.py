@@ -18,30 +18,13 @@ oracle (the CPU restatement of the reference) or on LAPACK through it:
 import numpy as np
 import pytest
 
-from helpers import assert_parity
+from helpers import assert_parity, oracle_system_columns
 
 pytestmark = pytest.mark.gpu
 
 
 def _col(torch, dev, a):
     return torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device=dev)
-
-
-def _oracle_columns(oracle, sample, P1, P2, P3, nrm, mid, nu, G, lam, hs):
-    """Columns [sample; N + sample; 2N + sample] of A = -[Atn; Atss; Atds]
-    from the oracle's strain influences and traction conversion."""
-    n = len(P1)
-    obs = mid - 1e-12 * nrm
-    k = len(sample)
-    ones = np.ones(k)
-    S, _ = oracle.td_inf(obs[:, 0], obs[:, 1], obs[:, 2], P1[sample], P2[sample], P3[sample], ones, ones, ones, nu,
-                         G, 0, 1, hs)
-    T = oracle.strain_to_traction(S, nrm, lam, G)
-    ref = np.empty((3 * n, 3 * k))
-    for m in range(3):
-        for r in range(3):
-            ref[r * n:(r + 1) * n, m * k:(m + 1) * k] = -T[3 * m + r]
-    return ref
 
 
 def test_c5_sampled_columns_and_learned_gmres(cad, oracle):
@@ -65,7 +48,7 @@ def test_c5_sampled_columns_and_learned_gmres(cad, oracle):
     sample = np.sort(np.random.default_rng(7).choice(n, 16, replace=False))
     cols = np.concatenate([sample, n + sample, 2 * n + sample])
     got = At[torch.tensor(cols, device=dev)].cpu().numpy().T
-    ref = _oracle_columns(oracle, sample, P1, P2, P3, nrm, mid, nu, G, lam, 1)
+    ref = oracle_system_columns(oracle, sample, P1, P2, P3, nrm, mid, nu, G, lam, 1)
     assert_parity(got[None], ref[None])
     # learned preconditioner (trained here on seeded 500-2000-triangle meshes)
     net = precond.Network(seed=0)

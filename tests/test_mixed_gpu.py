@@ -67,6 +67,23 @@ def test_mixed_slip_calculator_halfspace_dipping_matches_fp64(cad):
     assert _rel(Dm, D) <= SLIP_TOL
 
 
+@pytest.mark.parametrize("solver", ["mixed", "gmres_block_jacobi"])
+def test_mixed_and_gmres_slip_against_lapack_on_oracle_matrix(cad, oracle, solver):
+    # anchored on the oracle, not on the GPU's own FP64 path: numpy LAPACK on
+    # the oracle's system matrix of a half-space crack
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=8, ntri=300)
+    nrm, mid, lam, nu, G = _geom(P1, P2, P3)
+    n = len(P1)
+    s = workloads.remote_stress(seed=8)
+    bc = cad.Stresses(*[np.full(n, v) for v in s])
+    got = cad.SlipCalculator3D(P1, P2, P3, nu, G, lam, mid, nrm, 1, bc, np.zeros(n), solver=solver, tol=RESID_TOL)
+    Ao = oracle.influence_traction(nrm, mid, P1, P2, P3, nu, G, lam, 1, want_A=True)
+    Tn, Tds, Tss = cad.CalculateNormalAndShearTractions3D(*s, nrm)
+    Do = np.linalg.solve(Ao, np.concatenate([Tn, Tss, Tds]))
+    assert np.linalg.norm(np.concatenate(got[:3]) - Do) <= SLIP_TOL * np.linalg.norm(Do)
+
+
 def test_mixed_solve_dev_leaves_matrix_unchanged(cad):
     torch = pytest.importorskip("torch")
     from cutanddisplacejulia_b200 import _lib
