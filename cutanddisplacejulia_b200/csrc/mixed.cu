@@ -47,6 +47,23 @@ __global__ void cast_f32_kernel(const double* __restrict__ A, int64_t lda, int64
 // factors, column-major into D + i * kRB * kRB.  Thread j computes column j of
 // the inverse by substitution; the block and the inverse sit in shared memory
 // (the inverse row-major with a pad, so the threads' columns are conflict-free).
+// sum over k in [k0, k1) of a[k kRB] x[k (kRB + 1)]: four accumulators over
+// consecutive k (added in a fixed order), the last k1 - k0 mod 4 terms into
+// the first
+__device__ __forceinline__ float dot_range(const float* a, const float* x, int k0, int k1)
+{
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+        s0 = fmaf(a[k * kRB], x[k * (kRB + 1)], s0);
+        s1 = fmaf(a[(k + 1) * kRB], x[(k + 1) * (kRB + 1)], s1);
+        s2 = fmaf(a[(k + 2) * kRB], x[(k + 2) * (kRB + 1)], s2);
+        s3 = fmaf(a[(k + 3) * kRB], x[(k + 3) * (kRB + 1)], s3);
+    }
+    for (; k < k1; ++k) s0 = fmaf(a[k * kRB], x[k * (kRB + 1)], s0);
+    return (s0 + s1) + (s2 + s3);
+}
+
 template <bool UPPER>
 __device__ __forceinline__ void invert_diag_body(const float* __restrict__ A, int64_t lda, int n,
                                                  float* __restrict__ D, int i)
@@ -64,28 +81,27 @@ __device__ __forceinline__ void invert_diag_body(const float* __restrict__ A, in
         s_a[e] = v;
     }
     __syncthreads();
+    // The k loops run over the warp's common range (the column's own entries
+    // outside [j, r) are the zeros written above), so every read of the
+    // triangle is a broadcast; four accumulators (k mod 4, added in a fixed
+    // order) keep four multiply-adds in flight.
+    const int jw0 = j & ~31, jw1 = j | 31;
     if (!UPPER) {
         for (int r = 0; r < kRB; ++r) {
             float v;
+            const float sum = dot_range(s_a + r, s_x + j, jw0, r);
             if (r < j) v = 0.f;
             else if (r == j) v = 1.f;
-            else {
-                float s = 0.f;
-                for (int k = j; k < r; ++k) s = fmaf(s_a[r + k * kRB], s_x[k * (kRB + 1) + j], s);
-                v = -s;
-            }
+            else v = -sum;
             s_x[r * (kRB + 1) + j] = v;
         }
     } else {
         for (int r = kRB - 1; r >= 0; --r) {
             float v;
+            const float sum = dot_range(s_a + r, s_x + j, r + 1, jw1 + 1);
             if (r > j) v = 0.f;
             else if (r == j) v = 1.f / s_a[r + r * kRB];
-            else {
-                float s = 0.f;
-                for (int k = r + 1; k <= j; ++k) s = fmaf(s_a[r + k * kRB], s_x[k * (kRB + 1) + j], s);
-                v = -s / s_a[r + r * kRB];
-            }
+            else v = -sum / s_a[r + r * kRB];
             s_x[r * (kRB + 1) + j] = v;
         }
     }
