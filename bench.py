@@ -568,7 +568,11 @@ def run_batch(args, rank, world, local_rank):
     rel = np.zeros(len(cracks))
     L = _lib.load()
     ctx = _lib.context(local_rank)
-    stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
+    if args.eager:   # CUDA's default stream: the batch is issued directly, not captured
+        _lib.check(L.cad_set_stream(ctx, None), ctx)
+        stream = torch.cuda.default_stream(dev)
+    else:
+        stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
     torch.cuda.set_stream(stream)
 
     def batched():
@@ -1365,6 +1369,8 @@ def main():
                     help="lattice spacings of the friction workload's penny cracks (0.12: 496 triangles)")
     ap.add_argument("--cracks", type=int, default=512, help="cracks of the batch workload")
     ap.add_argument("--gemm-m", type=int, default=16384, help="rows and columns of the gemm workload's C")
+    ap.add_argument("--eager", action="store_true",
+                    help="batch: issue every launch directly instead of replaying the captured graph (for profilers)")
     ap.add_argument("--train-meshes", type=int, default=32, help="training meshes of the learned preconditioner")
     ap.add_argument("--train-min", type=int, default=500, help="smallest training mesh (triangles)")
     ap.add_argument("--train-max", type=int, default=2000, help="largest training mesh (triangles)")
