@@ -44,12 +44,11 @@ FALG_ASSEMBLY_FS = 2960.0 + 288.0
 # collocation pairs) plus the same traction epilogue.
 FALG_ASSEMBLY_HS = 43867.0 + 288.0
 # DRAM bytes (read + write) of one assembly launch from the committed ncu captures
-# (profiles/td_pair_kernel_*.md): (triangles captured, bytes; the half-space one
-# as dram__bytes.sum.per_second x duration).  Output scales as N^2.
-PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 144.824e9 * 5.114e-3)}
+# (profiles/td_pair_kernel_*.md): (triangles captured, bytes).  Output scales as N^2.
+PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (3968, 75.39e6 + 3.003e9)}
 # share of the step's (serialised) device time taken by the LU panel leaf, from
 # the committed launch list (profiles/launches_penny2013_fp64_and_mixed_step.md)
-DOMINANT_SHARE = {"penny": 0.571}
+DOMINANT_SHARE = {"penny": 0.532}
 SPACING = 0.06          # lattice spacing of the penny crack (~2013 triangles)
 NU, G = 0.25, 1.0
 TRACTION = -1e-3
