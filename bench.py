@@ -878,13 +878,26 @@ def run_c3(args, rank, world, local_rank):
     # network, blocks on the device) + FP64 GMRES to relative residual 1e-10
     xl = torch.empty(n3, dtype=torch.float64, device=dev)
 
+    # the preconditioner depends on the geometry only: it is built on a second
+    # stream (the context pointed at it for that call) while the matrix is
+    # assembled; the solve waits for both
+    side = torch.cuda.Stream(device=dev)
+    fork, join = torch.cuda.Event(), torch.cuda.Event()
+
     def learned_step(ev):
         if ev:
             ev[0].record(stream)
+        fork.record(stream)
+        side.wait_event(fork)
+        _lib.check(L.cad_set_stream(ctx, ctypes.c_void_p(side.cuda_stream)), ctx)
+        rc = L.cad_lpc_install_dev(ctx, dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(), n, G)
+        _lib.check(L.cad_set_stream(ctx, ctypes.c_void_p(stream.cuda_stream)), ctx)
+        _lib.check(rc, ctx)
+        join.record(side)
         assemble()
         if ev:
             ev[1].record(stream)
-        _lib.check(L.cad_lpc_install_dev(ctx, dP1.data_ptr(), dP2.data_ptr(), dP3.data_ptr(), n, G), ctx)
+        stream.wait_event(join)
         if ev:
             ev[2].record(stream)
         xl.copy_(b0)
@@ -957,7 +970,9 @@ def run_c3(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network bf16)", "data": "synthetic",
         "config": {"workload": WORKLOADS["dipping"][1] % (n, n3), "pairs_per_step": pairs,
-                   "step": "FP64 assembly + learned-preconditioner FP64 GMRES to relative residual 1e-10",
+                   "step": "FP64 assembly + learned-preconditioner FP64 GMRES to relative residual 1e-10 (the "
+                           "preconditioner built on a second stream during the assembly; preconditioner_setup is "
+                           "the part of it left after the assembly)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (A is %.0f MB per step)" % (n3 * n3 * 8 / 1e6)},
         "breakdown_ms": {"assembly": asm_ms, "td_pair_kernel_last": pair_kernel_ms,

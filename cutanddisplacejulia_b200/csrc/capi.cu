@@ -105,6 +105,7 @@ struct cad_ctx {
     int lu_block = 0;                      // cad_set_lu_block: outer block width of single-system LUs (0: default)
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     cudaStream_t leaf_aux[kLeafAux] = {};  // grouped leaves of different cluster sizes, side by side
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;   // work forked onto the side stream
     Tuner tuner;                           // cad_set_autotune
     double tol = 1e-10;
     int max_iter = 200;
@@ -1057,6 +1058,11 @@ int cad_init(int device, cad_ctx** out)
             cad_destroy(ctx);
             return CAD_ERR_CUDA;
         }
+    if (cudaEventCreateWithFlags(&ctx->side_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->side_join, cudaEventDisableTiming) != cudaSuccess) {
+        cad_destroy(ctx);
+        return CAD_ERR_CUDA;
+    }
     ctx->graphs = lu_graph_cache_create();
     *out = ctx;
     return CAD_OK;
@@ -1088,6 +1094,8 @@ int cad_destroy(cad_ctx* ctx)
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     for (auto a : ctx->leaf_aux)
         if (a) cudaStreamDestroy(a);
+    if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
+    if (ctx->side_join) cudaEventDestroy(ctx->side_join);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return CAD_OK;
@@ -1443,13 +1451,26 @@ int cad_slip_calculator(cad_ctx* ctx, const double* P1, const double* P2, const 
     if (int r = upload(ctx, bd, Tn, N)) return r;
     if (int r = upload(ctx, bd + N, Tss, N)) return r;
     if (int r = upload(ctx, bd + 2 * N, Tds, N)) return r;
-    int r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
-                            nullptr, (double*)A, n3);
+    // the learned preconditioner depends on the geometry only: it is built
+    // on the side stream while the system matrix is assembled
+    const bool learned = ctx->solver == CAD_SOLVER_GMRES_LEARNED && N > 0;
+    int r = CAD_OK;
+    if (learned) {
+        CK(cudaEventRecord(ctx->side_fork, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->side_stream, ctx->side_fork, 0));
+        cudaStream_t home = ctx->stream;
+        ctx->stream = ctx->side_stream;
+        r = cad_lpc_install_dev(ctx, g, g + 3 * N, g + 6 * N, N, G);
+        ctx->stream = home;
+        if (r) return r;
+        CK(cudaEventRecord(ctx->side_join, ctx->side_stream));
+    }
+    r = assemble_device(ctx, g + 9 * N, g + 12 * N, g, g + 3 * N, g + 6 * N, N, nu, G, lambda, hs_flag, OUT_AMAT,
+                        nullptr, (double*)A, n3);
+    if (learned) CK(cudaStreamWaitEvent(ctx->stream, ctx->side_join, 0));
     if (r) return r;
     if (A_out) CK(cudaMemcpyAsync(A_out, A, (size_t)n3 * n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (b_out) CK(cudaMemcpyAsync(b_out, bd, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (ctx->solver == CAD_SOLVER_GMRES_LEARNED && N > 0)
-        if ((r = cad_lpc_install_dev(ctx, g, g + 3 * N, g + 6 * N, N, G))) return r;
     if ((r = solve_device(ctx, n3, (double*)A, n3, bd, n3, 1))) return r;
     int info = 0;
     if (n3 > 0)
