@@ -972,7 +972,13 @@ int lu_factor_solve(const LuStreams& s, T* A, int64_t n, int64_t lda, const T* B
     if (nb < 1 || nb > kMaxBlock || n > (int64_t)lu.cluster * kLeafThreads * 8 || n > INT32_MAX)
         return LU_TOO_LARGE;
     LuGraphEntry* entry = nullptr;
-    if (s.graphs && n > 0) {
+    // graphs are captured from the caller's stream: not from CUDA's legacy
+    // default stream (it cannot be captured) nor from a stream the caller is
+    // capturing already (the work then lands in the caller's graph)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const bool cacheable = s.graphs && n > 0 && s.main != nullptr &&
+                           cudaStreamIsCapturing(s.main, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+    if (cacheable) {
         const LuGraphKey key{(int)sizeof(T), A, B, X, n, lda, ldb, ldx, nrhs, nb, ipiv, perm, info, factor, solve,
                              lu.main_st, lu.side_st, lu.wait_limit, lu.min_rpt};
         entry = s.graphs->find(key);

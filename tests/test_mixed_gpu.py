@@ -235,3 +235,25 @@ def test_mixed_many_rhs_general_matrix(cad):
         assert np.linalg.norm(A @ X[:, c] - B[:, c]) <= 2 * RESID_TOL * np.linalg.norm(B[:, c])
     it, rr = _lib.last_solve_stats(_lib.context(0))
     assert rr <= RESID_TOL and it >= 1
+
+
+@pytest.mark.parametrize("solver", ["lu64", "mixed"])
+def test_repeated_solves_on_cuda_default_stream(cad, solver):
+    # the same call signature three times on CUDA's legacy default stream,
+    # which cannot be captured: the solves run eagerly every time
+    from cutanddisplacejulia_b200 import _lib
+    L = _lib.load()
+    ctx = _lib.context(0)
+    own = L.cad_get_stream(ctx)
+    rng = np.random.default_rng(77)
+    n = 600
+    A = rng.standard_normal((n, n)) + 2.0 * np.sqrt(n) * np.eye(n)
+    B = rng.standard_normal((n, 1))
+    Xo = np.linalg.solve(A, B)
+    _lib.check(L.cad_set_stream(ctx, None), ctx)
+    try:
+        for _ in range(3):
+            X = cad.solve(A, B, solver=solver, tol=RESID_TOL)
+            assert _rel(X, Xo) <= SLIP_TOL
+    finally:
+        _lib.check(L.cad_set_stream(ctx, own), ctx)
