@@ -263,9 +263,11 @@ __device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtenso
     extern __shared__ uint8_t tsm_raw[];
     uint8_t* tsm = (uint8_t*)(((uintptr_t)tsm_raw + 1023) & ~(uintptr_t)1023);   // swizzle atoms: 1024-byte aligned
     uint64_t* bars = (uint64_t*)(tsm + TSTAGES * TSTAGE);
-    // bars[0..S): stage full (TMA -> MMA); bars[S..2S): stage empty (MMA ->
-    // TMA); bars[2S]: accumulator ready (MMA -> epilogue)
-    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * TSTAGES + 1);
+    // bars[0..S): stage full (TMA -> rounding warps); bars[S..2S): stage empty
+    // (MMA -> TMA); bars[2S]: accumulator ready (MMA -> epilogue);
+    // bars[2S+1..3S+1): stage rounded to TF32 (the four epilogue warps -> MMA)
+    uint64_t* rounded = bars + 2 * TSTAGES + 1;
+    uint32_t* tmem_slot = (uint32_t*)(bars + 3 * TSTAGES + 1);
     __shared__ int s_fail;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nk = (k + TBK - 1) / TBK;
@@ -273,6 +275,7 @@ __device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtenso
     if (threadIdx.x == 0) {
         s_fail = 0;
         for (int s = 0; s < 2 * TSTAGES + 1; ++s) sm100::mbar_init(sm100::smem_addr(&bars[s]), 1);
+        for (int s = 0; s < TSTAGES; ++s) sm100::mbar_init(sm100::smem_addr(&rounded[s]), 4);
         sm100::fence_barrier_init();
         sm100::prefetch_tensormap(mapA);
         sm100::prefetch_tensormap(mapB);
@@ -311,12 +314,13 @@ __device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtenso
             if (!sm100::mbar_wait(sm100::smem_addr(&bars[kt % TSTAGES]), (uint32_t)((kt / TSTAGES) & 1), kTcWaitLimit))
                 s_fail = 1;
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer: 4 MMAs (K = 8 each) per stage, accumulator in tensor memory
+        // MMA issuer: 4 MMAs (K = 8 each) per stage once the stage is rounded,
+        // accumulator in tensor memory
         bool ok = true;
         for (int kt = 0; kt < nk && ok; ++kt) {
             const int s = kt % TSTAGES;
             const uint32_t ph = (uint32_t)((kt / TSTAGES) & 1);
-            if (!sm100::mbar_wait(sm100::smem_addr(&bars[s]), ph, kTcWaitLimit)) {
+            if (!sm100::mbar_wait(sm100::smem_addr(&rounded[s]), ph, kTcWaitLimit)) {
                 s_fail = 1;
                 ok = false;
                 break;
@@ -341,6 +345,33 @@ __device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtenso
         // every MMA done before tensor memory is released at the end
         if (!sm100::mbar_wait(sm100::smem_addr(&bars[2 * TSTAGES]), 0, kTcWaitLimit)) s_fail = 1;
     } else if (warp >= 2) {
+        // main loop: round every landed stage to TF32 in place (the tensor
+        // cores would truncate the FP32 operands' low mantissa bits, a biased
+        // error that builds up over the factorisation's many updates)
+        const int te = threadIdx.x - 64;   // 0..127
+        bool fine = true;
+        for (int kt = 0; kt < nk && fine; ++kt) {
+            const int s = kt % TSTAGES;
+            const uint32_t ph = (uint32_t)((kt / TSTAGES) & 1);
+            if (!sm100::mbar_wait(sm100::smem_addr(&bars[s]), ph, kTcWaitLimit)) {
+                s_fail = 1;
+                fine = false;
+                break;
+            }
+            uint4* st4 = reinterpret_cast<uint4*>(tsm + s * TSTAGE);
+#pragma unroll 4
+            for (int j = 0; j < (int)(TSTAGE / 16) / 128; ++j) {
+                uint4 v = st4[te + 128 * j];
+                v.x = sm100::tf32_rna(__uint_as_float(v.x));
+                v.y = sm100::tf32_rna(__uint_as_float(v.y));
+                v.z = sm100::tf32_rna(__uint_as_float(v.z));
+                v.w = sm100::tf32_rna(__uint_as_float(v.w));
+                st4[te + 128 * j] = v;
+            }
+            sm100::fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) sm100::mbar_arrive(sm100::smem_addr(&rounded[s]));
+        }
         // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 = tile rows
         const int q = warp & 3;
         const int row = m0 + 32 * q + lane;
