@@ -240,6 +240,7 @@ constexpr uint32_t TSTAGE = TSTAGE_A + TSTAGE_B;
 constexpr size_t TSMEM = (size_t)TSTAGES * TSTAGE + 1024 /* alignment slack */ + 256 /* barriers */;
 constexpr uint32_t TIDESC = sm100::instr_desc(TBM, TBN, 2, 2, 1 /* A MN-major */, 0 /* B K-major */);
 constexpr long kTcWaitLimit = 1L << 24;
+constexpr uint32_t kRoundBytes = TSTAGE;   // bytes of each stage rounded to TF32 (A and B tiles)
 
 struct GemmGroup {
     int count, pad;
@@ -360,7 +361,7 @@ __device__ __forceinline__ void tf32_tile(const CUtensorMap* mapA, const CUtenso
             }
             uint4* st4 = reinterpret_cast<uint4*>(tsm + s * TSTAGE);
 #pragma unroll 4
-            for (int j = 0; j < (int)(TSTAGE / 16) / 128; ++j) {
+            for (int j = 0; j < (int)(kRoundBytes / 16) / 128; ++j) {
                 uint4 v = st4[te + 128 * j];
                 v.x = sm100::tf32_rna(__uint_as_float(v.x));
                 v.y = sm100::tf32_rna(__uint_as_float(v.y));
