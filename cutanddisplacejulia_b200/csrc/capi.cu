@@ -43,6 +43,7 @@ enum Slot {
     S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS, S_COUNT
 };
 
+constexpr int kGmresRestart = 30; // default Krylov dimension of a GMRES cycle
 constexpr int kLuBlock = 256;     // outer block width of the FP64 LU
 constexpr int kLuBlock32 = 512;   // of the FP32 factorisation (its TF32 products gain more from a long k)
 
@@ -103,6 +104,7 @@ struct cad_ctx {
     int gmres_matvec32 = 1;                // cad_set_gmres_matvec: FP32 copy of A for the Arnoldi products
     int batch_mode = CAD_BATCH_GROUPED;    // cad_set_batch_solve
     int lu_block = 0;                      // cad_set_lu_block: outer block width of single-system LUs (0: default)
+    int gmres_restart = kGmresRestart;          // cad_set_gmres_restart: Krylov dimension of a cycle
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     cudaStream_t leaf_aux[kLeafAux] = {};  // grouped leaves of different cluster sizes, side by side
     cudaEvent_t side_fork = nullptr, side_join = nullptr;   // work forked onto the side stream
@@ -315,7 +317,6 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
     return CAD_OK;
 }
 
-constexpr int kRestart = 30;   // Krylov dimension of a GMRES cycle
 constexpr int kIrMaxIter = 20; // refinement sweeps of a multi-column mixed solve before GMRES takes over
 
 int read_info(cad_ctx* ctx, int* info);
@@ -331,7 +332,8 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     if (int r = ensure(ctx, S_PIV, (size_t)n * sizeof(int), &piv)) return r;
     if (int r = ensure(ctx, S_PERM, (size_t)n * sizeof(int), &perm)) return r;
     if (int r = ensure(ctx, S_INFO, sizeof(int), &info)) return r;
-    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (kRestart + 1) + 3 * (size_t)n + 2 * (kRestart + 1)) * sizeof(double),
+    const int rs = ctx->gmres_restart;
+    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (rs + 1) + 3 * (size_t)n + 2 * (rs + 1)) * sizeof(double),
                        &kry))
         return r;
     if (int r = ensure(ctx, S_VEC32, 2 * (size_t)n * sizeof(float), &v32)) return r;
@@ -350,7 +352,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     if (int r = read_info(ctx, info_out)) return r;
     if (*info_out > 0) return CAD_OK;
     double* V = (double*)kry;
-    double* w = V + (size_t)n * (kRestart + 1);
+    double* w = V + (size_t)n * (rs + 1);
     GmresArgs g{};
     g.stream = ctx->stream;
     g.n = n;
@@ -361,7 +363,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     g.perm = (const int*)perm;
     g.tol = ctx->tol;
     g.max_iter = ctx->max_iter;
-    g.restart = kRestart;
+    g.restart = rs;
     g.V = V;
     g.w = w;
     g.z = w + n;
@@ -433,7 +435,8 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     if (!ctx->spai_nbr || 3 * ctx->spai_N != n)
         return fail(ctx, CAD_ERR_ARG, "no preconditioner for this system size (cad_set_preconditioner)");
     void *kry, *sync, *work;
-    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (kRestart + 1) + 3 * (size_t)n + 2 * (kRestart + 1)) * sizeof(double),
+    const int rs = ctx->gmres_restart;
+    if (int r = ensure(ctx, S_KRYLOV, ((size_t)n * (rs + 1) + 3 * (size_t)n + 2 * (rs + 1)) * sizeof(double),
                        &kry))
         return r;
     if (int r = ensure(ctx, S_SYNC, mixed_sync_ints(n) * sizeof(int), &sync)) return r;
@@ -441,7 +444,7 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     ctx->timed[1] = ctx->timed[2] = false;
     double* V = (double*)kry;
-    double* w = V + (size_t)n * (kRestart + 1);
+    double* w = V + (size_t)n * (rs + 1);
     GmresArgs g{};
     g.stream = ctx->stream;
     g.n = n;
@@ -449,7 +452,7 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
     g.lda = lda;
     g.tol = ctx->tol;
     g.max_iter = ctx->max_iter;
-    g.restart = kRestart;
+    g.restart = rs;
     g.V = V;
     g.w = w;
     g.z = w + n;
@@ -1147,6 +1150,14 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32)
     if (!ctx) return CAD_ERR_ARG;
     if (fp32 != 0 && fp32 != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->gmres_matvec32 = fp32;
+    return CAD_OK;
+}
+
+int cad_set_gmres_restart(cad_ctx* ctx, int m)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (m != 0 && (m < 1 || m + 1 > kMaxBasis)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->gmres_restart = m == 0 ? kGmresRestart : m;
     return CAD_OK;
 }
 

@@ -42,7 +42,6 @@ constexpr int DBK = 16, DSTAGES = 3, DTHREADS = 128;
 constexpr int DLDB = DBK;       // shared row (one n) of the B tile, doubles
 template <int BM, int BN>
 struct DTile {
-    static constexpr int LDA = BM;             // shared row (one k) of the A tile, doubles
     static constexpr int STAGE_A = DBK * BM;
     static constexpr int STAGE_B = BN * DLDB;
     static constexpr int MT = BM / 16;         // 8-row DMMA tiles per warp

@@ -150,6 +150,10 @@ int cad_set_gmres_matvec(cad_ctx* ctx, int fp32);
  * update products a longer inner dimension and the panels more work.  Same factors and pivots up to
  * the order of the products' sums.  No counterpart in the reference. */
 int cad_set_lu_block(cad_ctx* ctx, int nb);
+/* Krylov dimension of one restarted-GMRES cycle (the mixed and the
+ * preconditioned GMRES solvers): 1..63, 0 = the default 30.  Every cycle
+ * starts from the FP64 residual b - A x.  No counterpart in the reference. */
+int cad_set_gmres_restart(cad_ctx* ctx, int m);
 #define CAD_BATCH_GROUPED 0
 #define CAD_BATCH_LANES 1
 #define CAD_BATCH_LANES_CHAIN 2
