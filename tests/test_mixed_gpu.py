@@ -257,3 +257,24 @@ def test_repeated_solves_on_cuda_default_stream(cad, solver):
             assert _rel(X, Xo) <= SLIP_TOL
     finally:
         _lib.check(L.cad_set_stream(ctx, own), ctx)
+
+
+def test_gmres_restart_setting(cad):
+    from cutanddisplacejulia_b200 import _lib
+    L = _lib.load()
+    ctx = _lib.context(0)
+    assert L.cad_set_gmres_restart(ctx, 64) == _lib.CAD_ERR_ARG
+    assert L.cad_set_gmres_restart(ctx, -1) == _lib.CAD_ERR_ARG
+    rng = np.random.default_rng(91)
+    n = 450
+    A = rng.standard_normal((n, n)) + 3.0 * np.sqrt(n) * np.eye(n)
+    B = rng.standard_normal((n, 1))
+    Xo = np.linalg.solve(A, B)
+    try:
+        for m in (5, 30, 63):
+            _lib.check(L.cad_set_gmres_restart(ctx, m), ctx)
+            X = cad.solve(A, B, solver="gmres_block_jacobi", tol=RESID_TOL, max_iter=2000)
+            assert np.linalg.norm(A @ X[:, 0] - B[:, 0]) <= 2 * RESID_TOL * np.linalg.norm(B[:, 0])
+            assert _rel(X, Xo) <= SLIP_TOL
+    finally:
+        _lib.check(L.cad_set_gmres_restart(ctx, 0), ctx)
