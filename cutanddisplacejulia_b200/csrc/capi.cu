@@ -1,8 +1,9 @@
 // C ABI of libcad_td.so (declared in include/cad_td.h).
 //
-// Each context owns a CUDA stream, a cuBLAS handle (GEMMs of the dense LU in
-// csrc/lu.cu), and a set of device workspaces that grow on demand and are reused across calls
-// (no allocation in steady state).  Host-pointer entry points copy inputs in,
+// Each context owns its CUDA streams (the caller-visible one, a low-priority
+// side stream for the LU's look-ahead updates, four leaf streams for grouped
+// factorisations) and a set of device workspaces that grow on demand and are
+// reused across calls (no allocation in steady state).  Host-pointer entry points copy inputs in,
 // run the device path and copy results out; *_dev entry points run the device
 // path directly on caller-provided device memory.
 #include <cuda_runtime.h>
@@ -52,8 +53,8 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
-// One lane of the batched solve: its own streams, cuBLAS handles and
-// workspaces, so cracks on different lanes run concurrently.
+// One lane of the batched solve: its own streams and workspaces, so cracks
+// on different lanes run concurrently.
 enum LaneSlot { L_OBS, L_DIRS, L_TRI, L_TRI32, L_NEAR, L_A32, L_PIV, L_PERM, L_INFO, L_IR, L_IR32, L_NORMS,
                 L_KWORK, L_DINV, L_SYNC, L_Z, L_COUNT };
 struct Lane {
@@ -346,7 +347,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
     int rc = mixed_prepare(ls, A, lda, n, (float*)a32, (float*)dinv, (int*)piv, (int*)perm, (int*)info,
                            lu_nb(ctx, true));
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
-    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA or cuBLAS error)");
+    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "FP32 LU failed (CUDA error)");
     CK(cudaEventRecord(ctx->ev[4], ctx->stream));
     ctx->timed[2] = true;
     if (int r = read_info(ctx, info_out)) return r;
@@ -398,7 +399,7 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
                   (double*)norms};
         IrResult res{};
         const int st = ir_solve_batched(ia, &res, done);
-        if (st != GMRES_OK) return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA or cuBLAS error in the refinement");
+        if (st != GMRES_OK) return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA error in the refinement");
         ctx->last_iters += res.iterations;
         for (int64_t c = 0; c < nrhs; ++c)
             if (done[c]) ctx->last_relres = res.max_rel_residual > ctx->last_relres ? res.max_rel_residual
@@ -411,8 +412,8 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
         GmresResult res{};
         const int st = gmres_ir_solve(g, &res);
         if (st == GMRES_TIMEOUT) return fail(ctx, CAD_ERR_TIMEOUT, "mixed solve: a triangular-solve wait ran out");
-        if (st == GMRES_CUDA_ERROR || st == GMRES_BLAS_ERROR)
-            return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA or cuBLAS error in GMRES");
+        if (st == GMRES_CUDA_ERROR)
+            return fail(ctx, CAD_ERR_CUDA, "mixed solve: CUDA error in GMRES");
         converged = converged && st == GMRES_OK;
         ctx->last_iters += res.iterations;
         ctx->last_relres = res.rel_residual > ctx->last_relres ? res.rel_residual : ctx->last_relres;
@@ -499,8 +500,8 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
         g.x = (double*)work;
         GmresResult res{};
         const int st = gmres_ir_solve(g, &res);
-        if (st == GMRES_CUDA_ERROR || st == GMRES_BLAS_ERROR || st == GMRES_TIMEOUT)
-            return fail(ctx, CAD_ERR_CUDA, "preconditioned GMRES: CUDA or cuBLAS error");
+        if (st == GMRES_CUDA_ERROR || st == GMRES_TIMEOUT)
+            return fail(ctx, CAD_ERR_CUDA, "preconditioned GMRES: CUDA error");
         converged = converged && st == GMRES_OK;
         ctx->last_iters += res.iterations;
         ctx->last_relres = res.rel_residual > ctx->last_relres ? res.rel_residual : ctx->last_relres;
@@ -597,7 +598,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
                                          lu_nb(ctx, false), true, false);
         if (rc == LU_OK) rc = lu_pivots_to_perm(ls, (const int*)piv, n, (int*)perm);
         if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
-        if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
+        if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA error)");
         double* y = (double*)chain;
         CK(lu_solve_chain_f64(ctx->stream, A, lda, n, (const int*)perm, B, y, (double*)work, (int*)(y + n),
                               (int*)info, &ctx->launches, ctx->wait_limit));
@@ -609,7 +610,7 @@ int solve_device(cad_ctx* ctx, int64_t n, double* A, int64_t lda, double* B, int
     const int rc = lu_factor_solve<double>(ls, A, n, lda, B, ldb, (int)nrhs, (double*)work, n, (int*)piv, (int*)perm,
                                            (int*)info, lu_nb(ctx, false), true, true);
     if (rc == LU_TOO_LARGE) return fail(ctx, CAD_ERR_ARG, "matrix too large for the dense LU");
-    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA or cuBLAS error)");
+    if (rc != LU_OK) return fail(ctx, CAD_ERR_CUDA, "dense LU failed (CUDA error)");
     CK(cudaMemcpy2DAsync(B, ldb * sizeof(double), work, n * sizeof(double), n * sizeof(double), nrhs,
                          cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));

@@ -8,7 +8,7 @@
 
 namespace cad {
 
-enum { LU_OK = 0, LU_CUDA_ERROR = 1, LU_BLAS_ERROR = 2, LU_TOO_LARGE = 3 };
+enum { LU_OK = 0, LU_CUDA_ERROR = 1, LU_TOO_LARGE = 3 };
 
 // Executable CUDA graphs of lu_factor_solve calls, one per call signature
 // (precision, sizes, every pointer and the streams).  The factorisation

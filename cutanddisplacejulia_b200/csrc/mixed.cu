@@ -504,7 +504,7 @@ int ir_solve_batched(const IrArgs& a, IrResult* res, std::vector<char>& converge
         if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
         const int rc = lu_factor_solve<float>(a.ls, a.A32, n, mixed_ld(n), a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
                                               a.nb, false, true);
-        if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
+        if (rc != LU_OK) return GMRES_CUDA_ERROR;
         add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
         if (launches) ++*launches;
         if (ir_residual(a, st) != cudaSuccess) return GMRES_CUDA_ERROR;
@@ -573,7 +573,7 @@ int ir_solve_fixed(const IrArgs& a, int iters, double* rel_out)
             if (cudaGetLastError() != cudaSuccess) return GMRES_CUDA_ERROR;
             const int rc = lu_factor_solve<float>(a.ls, a.A32, n, mixed_ld(n), a.R32, n, nrhs, a.X32, n, a.ipiv, a.perm, a.info,
                                                   a.nb, false, true);
-            if (rc != LU_OK) return rc == LU_BLAS_ERROR ? GMRES_BLAS_ERROR : GMRES_CUDA_ERROR;
+            if (rc != LU_OK) return GMRES_CUDA_ERROR;
             add_f2d_kernel<<<g, 256, 0, st>>>(a.X32, n, n, a.X, n);
             if (launches) ++*launches;
         }

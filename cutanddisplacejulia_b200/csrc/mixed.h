@@ -23,7 +23,7 @@ size_t mixed_dinv_floats(int64_t n);
 int64_t mixed_ld(int64_t n);
 size_t mixed_sync_ints(int64_t n);   // flags, tickets and the failure word of one preconditioner apply
 
-enum { GMRES_OK = 0, GMRES_NOT_CONVERGED = 1, GMRES_CUDA_ERROR = 2, GMRES_BLAS_ERROR = 3, GMRES_TIMEOUT = 4 };
+enum { GMRES_OK = 0, GMRES_NOT_CONVERGED = 1, GMRES_CUDA_ERROR = 2, GMRES_TIMEOUT = 4 };
 
 struct GmresArgs {
     cudaStream_t stream;
@@ -106,7 +106,7 @@ struct IrArgs {
 };
 
 struct IrResult {
-    int status;         // GMRES_OK / GMRES_CUDA_ERROR / GMRES_BLAS_ERROR
+    int status;         // GMRES_OK / GMRES_CUDA_ERROR / GMRES_TIMEOUT
     int iterations;
     double max_rel_residual;
 };

@@ -81,7 +81,7 @@ double cad_last_time_ms(const cad_ctx* ctx, int which);
 /* Library version string. */
 const char* cad_version(void);
 /* Number of the library's own CUDA kernels launched through this context so
- * far (cuBLAS calls not included).  No counterpart in the reference (an
+ * far.  No counterpart in the reference (an
  * accounting utility). */
 int64_t cad_kernel_launches(const cad_ctx* ctx);
 /* Solver of the dense 3N x 3N system used by cad_slip_calculator, cad_solve and
