@@ -44,7 +44,7 @@ EXPORTS = [
     "cad_lpc_get_network", "cad_lpc_dataset_add", "cad_lpc_dataset_rows", "cad_lpc_dataset_clear",
     "cad_lpc_dataset_get", "cad_lpc_dataset_set", "cad_lpc_forward_backward", "cad_lpc_train", "cad_lpc_install_dev",
     "cad_lpc_install", "cad_set_wait_limit", "cad_wait_timeout_probe", "cad_set_gmres_matvec", "cad_set_batch_solve",
-    "cad_set_lu_block", "cad_set_gmres_restart",
+    "cad_set_lu_block", "cad_set_gmres_restart", "cad_set_shared_edges",
     "cad_set_autotune", "cad_autotune_entries",
 ]
 
@@ -134,6 +134,7 @@ def load():
     L.cad_set_batch_solve.argtypes = [P, INT]
     L.cad_set_lu_block.argtypes = [P, INT]
     L.cad_set_gmres_restart.argtypes = [P, INT]
+    L.cad_set_shared_edges.argtypes = [P, INT]
     L.cad_set_autotune.argtypes = [P, INT, ctypes.c_char_p]
     L.cad_autotune_entries.argtypes = [P, ctypes.POINTER(I64)]
     L.cad_autotune_entries.restype = I64

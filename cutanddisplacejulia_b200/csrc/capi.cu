@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/cad_td.h"
@@ -41,12 +42,14 @@ enum Slot {
     S_OBS, S_GEOM, S_SLIP, S_TRI, S_OUT, S_PART, S_DIRS, S_FLAG, S_A, S_B, S_WORK, S_PIV, S_INFO, S_PERM,
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
-    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS, S_COUNT
+    S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS,
+    S_EDGE_PTS, S_EDGE_CODE, S_EDGE_REC, S_EDGE_G, S_COUNT
 };
 
 constexpr int kGmresRestart = 30; // default Krylov dimension of a GMRES cycle
 constexpr int kLuBlock = 256;     // outer block width of the FP64 LU
 constexpr int kLuBlock32 = 512;   // of the FP32 factorisation (its TF32 products gain more from a long k)
+constexpr size_t kEdgeMapBytes = size_t(8) << 30;   // cap on the shared-edge free-surface maps of one chunk
 
 struct DevBuf {
     void* p = nullptr;
@@ -110,6 +113,13 @@ struct cad_ctx {
     cudaStream_t leaf_aux[kLeafAux] = {};  // grouped leaves of different cluster sizes, side by side
     cudaEvent_t side_fork = nullptr, side_join = nullptr;   // work forked onto the side stream
     Tuner tuner;                           // cad_set_autotune
+    int shared_edges = 1;                  // cad_set_shared_edges
+    // mesh-edge table of the last half-space assembly: the vertices it was
+    // built from (P1, P2, P3, 3 N each), its edges' endpoints (6 per edge)
+    // and each triangle side's signed edge number (0 for none)
+    std::vector<double> edge_geom, edge_pts;
+    std::vector<int> edge_code;
+    int64_t edge_n = -1;
     double tol = 1e-10;
     int max_iter = 200;
     bool fric_ready = false;      // cad_friction_prepare: C = inv(A Scl) of fric_N elements in S_LCPC
@@ -254,6 +264,86 @@ int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, i
     return CAD_OK;
 }
 
+// Number the mesh's distinct triangle sides (edges).  Side s of triangle j
+// runs P1->P2, P2->P3, P3->P1; its code is e + 1 when it runs the way edge e
+// was first seen, -(e + 1) when it runs the other way.  Endpoints match when
+// their coordinates are equal (-0.0 taken as 0.0).  The table is rebuilt only
+// when the vertices differ from the last call's; the device copies of the
+// edge endpoints and codes are uploaded with it.
+struct EdgeKey {
+    double v[6];
+    bool operator==(const EdgeKey& o) const { return std::memcmp(v, o.v, sizeof v) == 0; }
+};
+struct EdgeKeyHash {
+    size_t operator()(const EdgeKey& k) const
+    {
+        uint64_t h = 1469598103934665603ull;
+        for (double d : k.v) {
+            uint64_t u;
+            std::memcpy(&u, &d, sizeof u);
+            h = (h ^ u) * 1099511628211ull;
+            h ^= h >> 29;
+        }
+        return (size_t)h;
+    }
+};
+
+int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, int64_t* E,
+               double** pts_dev, int** code_dev)
+{
+    std::vector<double> geom((size_t)9 * N);
+    CK(cudaMemcpyAsync(geom.data(), P1, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(geom.data() + 3 * N, P2, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(geom.data() + 6 * N, P3, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    void *pts, *code;
+    const bool same = ctx->edge_n == N && ctx->edge_geom == geom;
+    if (!same) {
+        std::unordered_map<EdgeKey, int, EdgeKeyHash> seen;
+        seen.reserve((size_t)3 * N);
+        ctx->edge_pts.clear();
+        ctx->edge_code.assign((size_t)3 * N, 0);
+        for (int64_t j = 0; j < N; ++j)
+            for (int sd = 0; sd < 3; ++sd) {
+                const double* va = geom.data() + 3 * N * sd + j;
+                const double* vb = geom.data() + 3 * N * ((sd + 1) % 3) + j;
+                // + 0.0 turns -0.0 into 0.0
+                const EdgeKey fwd{{va[0] + 0.0, va[N] + 0.0, va[2 * N] + 0.0, vb[0] + 0.0, vb[N] + 0.0, vb[2 * N] + 0.0}};
+                const EdgeKey rev{{fwd.v[3], fwd.v[4], fwd.v[5], fwd.v[0], fwd.v[1], fwd.v[2]}};
+                int c;
+                auto it = seen.find(fwd);
+                if (it != seen.end()) {
+                    c = it->second + 1;
+                } else if ((it = seen.find(rev)) != seen.end()) {
+                    c = -(it->second + 1);
+                } else {
+                    const int e = (int)seen.size();
+                    seen.emplace(fwd, e);
+                    ctx->edge_pts.insert(ctx->edge_pts.end(), fwd.v, fwd.v + 6);
+                    c = e + 1;
+                }
+                ctx->edge_code[(size_t)3 * j + sd] = c;
+            }
+        ctx->edge_n = -1;
+        if (int r = ensure(ctx, S_EDGE_PTS, ctx->edge_pts.size() * sizeof(double), &pts)) return r;
+        if (int r = ensure(ctx, S_EDGE_CODE, ctx->edge_code.size() * sizeof(int), &code)) return r;
+        CK(cudaMemcpyAsync(pts, ctx->edge_pts.data(), ctx->edge_pts.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(code, ctx->edge_code.data(), ctx->edge_code.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->edge_geom.swap(geom);
+        ctx->edge_n = N;
+    } else {
+        pts = ctx->buf[S_EDGE_PTS].p;
+        code = ctx->buf[S_EDGE_CODE].p;
+    }
+    *E = (int64_t)(ctx->edge_pts.size() / 6);
+    *pts_dev = (double*)pts;
+    *code_dev = (int*)code;
+    return CAD_OK;
+}
+
 int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, const double* P1, const double* P2,
                     const double* P3, int64_t N, double nu, double G, double lambda, int hs, int out_kind,
                     double* trac_out, double* A, int64_t lda)
@@ -284,6 +374,26 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         CK(cudaEventRecord(ctx->ev[0], ctx->stream));
         CK(launch_assemble_mixed(a, hs == 1, P1, P2, P3, ctx->near_factor, tri32, (double*)near, ctx->stream,
                                  &ctx->launches));
+        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        ctx->timed[0] = true;
+        return CAD_OK;
+    }
+    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges) {
+        // each mesh edge's free-surface map evaluated once, then read by the
+        // (one or two) triangles that share the edge
+        int64_t E;
+        double* pts;
+        int* codes;
+        if (int r = edge_table(ctx, P1, P2, P3, N, &E, &pts, &codes)) return r;
+        void *rec, *gmap;
+        if (int r = ensure(ctx, S_EDGE_REC, (size_t)(E > 0 ? E : 1) * edge_record_bytes(), &rec)) return r;
+        const int64_t per_point = 18 * (E > 0 ? E : 1) * (int64_t)sizeof(double);
+        int64_t Mc = (int64_t)(kEdgeMapBytes / per_point) / kPairThreads * kPairThreads;
+        if (Mc < kPairThreads) Mc = kPairThreads;
+        if (Mc > N) Mc = N;
+        if (int r = ensure(ctx, S_EDGE_G, (size_t)Mc * per_point, &gmap)) return r;
+        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        CK(launch_assemble_edges(a, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
         CK(cudaEventRecord(ctx->ev[1], ctx->stream));
         ctx->timed[0] = true;
         return CAD_OK;
@@ -1159,6 +1269,14 @@ int cad_set_gmres_restart(cad_ctx* ctx, int m)
     if (!ctx) return CAD_ERR_ARG;
     if (m != 0 && (m < 1 || m + 1 > kMaxBasis)) return fail(ctx, CAD_ERR_ARG, "invalid argument");
     ctx->gmres_restart = m == 0 ? kGmresRestart : m;
+    return CAD_OK;
+}
+
+int cad_set_shared_edges(cad_ctx* ctx, int enable)
+{
+    if (!ctx) return CAD_ERR_ARG;
+    if (enable != 0 && enable != 1) return fail(ctx, CAD_ERR_ARG, "invalid argument");
+    ctx->shared_edges = enable;
     return CAD_OK;
 }
 

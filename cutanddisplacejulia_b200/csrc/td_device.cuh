@@ -82,6 +82,8 @@ static_assert(sizeof(TriDevT<float>) * 2 == sizeof(TriDevT<double>), "records ar
 // Number of values of a record needed by a full-space-only kernel / in all.
 constexpr int kTriWordsFS = (int)(offsetof(TriDev, image) / sizeof(double));
 constexpr int kTriWordsHS = (int)(sizeof(TriDev) / sizeof(double));
+constexpr int kTriWordsImg = (int)(offsetof(TriDev, side) / sizeof(double));   // real + image frames
+constexpr int kSideWords = (int)(sizeof(FscSide) / sizeof(double));
 
 // ------------------------------------------------------------------ helpers
 template <typename R>
@@ -539,6 +541,61 @@ CAD_HD void fsc_strain(const FscSideT<R>& s, double X, double Y, double Z, R Dss
     }
 }
 
+// The same correction as a linear map of the side's Burgers vector: G[j] is
+// the EFCS strain of a unit Burgers vector along EFCS axis j.  A side shared
+// by two triangles is traversed in opposite directions, and the reversed
+// side's map is the negative of this one (the two dislocation segments
+// cancel), so one evaluation per mesh edge serves both triangles.
+template <typename R>
+CAD_HD void fsc_strain_map(const FscSideT<R>& s, double X, double Y, double Z, R G[3][6])
+{
+    R x, y, z;
+    to_adcs(s, X, Y, Z, x, y, z);
+    const bool flip = mul_rn(s.beta, x) >= 0.0;
+    const int c = flip ? 1 : 0;
+    const R f = flip ? R(-1.0) : R(1.0);
+    R d[18];
+    fsc_strain_eval(s.ks[c][0], f * x, f * y, z, d);
+#pragma unroll
+    for (int q = 0; q < 18; ++q) d[q] = -d[q];
+    {
+        R v[18];
+        fsc_strain_eval(s.ks[c][1], f * (x - s.y1B), f * (y - s.y2B), z - s.y3B, v);
+#pragma unroll
+        for (int q = 0; q < 18; ++q) d[q] += v[q];
+    }
+    const R AFlip[9] = {s.ey1[0], s.ey1[1], s.ey1[2], s.ey2[0], s.ey2[1], s.ey2[2], s.ey3[0], s.ey3[1], s.ey3[2]};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        // ADCS slip components of a unit Burgers vector along EFCS axis j (as
+        // build_side forms them: the j-th frame vector ey(j+1))
+        const R c0 = f * AFlip[3 * j], c1 = f * AFlip[3 * j + 1], c2 = AFlip[3 * j + 2];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const R fk = (k >= 4) ? f : R(1.0);
+            const R h = (k >= 3) ? R(0.5) : R(1.0);
+            G[j][k] = h * fk * (c0 * d[k] + c1 * d[6 + k] + c2 * d[12 + k]);
+        }
+        tensor_rot(G[j], AFlip);
+    }
+}
+
+// E[m] += sign * (the map G applied to the EFCS Burgers vector of unit mode m
+// of the triangle with frame `real`), for the modes with non-zero slip.
+template <typename R>
+CAD_HD void fsc_apply_map(const R G[3][6], R sign, const FrameT<R>& real, R Dss, R Dds, R Dn, R E[3][6])
+{
+    const R slip[3] = {Dn, Dss, Dds};
+    const R* axes[3] = {real.Vn, real.Vs, real.Vd};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!(slip[m] != 0.0)) continue;
+        const R w0 = sign * axes[m][0] * slip[m], w1 = sign * axes[m][1] * slip[m], w2 = sign * axes[m][2] * slip[m];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[m][k] += w0 * G[0][k] + w1 * G[1][k] + w2 * G[2][k];
+    }
+}
+
 // One side's harmonic correction to the displacement, added into U (EFCS).
 template <typename R>
 CAD_HD void fsc_disp(const FscSideT<R>& s, double X, double Y, double Z, R Dss, R Dds, R Dn, R U[3][3])
@@ -650,9 +707,12 @@ CAD_HD void build_frame(const double P1[3], const double P2[3], const double P3[
     for (int i = 0; i < 3; ++i) f.P2lo[i] = 0.0;
 }
 
-CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real, double Dss, double Dds,
-                       double Dn, double nu, FscSide& s)
+// The geometry of side PA -> PB (frame, beta test, closed-form constants);
+// its slip coefficients cs, cd are left zero.
+CAD_HD void build_side_geom(const double PA[3], const double PB[3], double nu, FscSide& s)
 {
+    for (int m = 0; m < 3; ++m)
+        for (int g = 0; g < 3; ++g) s.cs[m][g] = s.cd[m][g] = 0.0;
     const double S[3] = {sub_rn(PB[0], PA[0]), sub_rn(PB[1], PA[1]), sub_rn(PB[2], PA[2])};
     const double Sv = norm3_rn(S[0], S[1], S[2]);
     const double beta = acos(-S[2] / Sv);
@@ -669,17 +729,6 @@ CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real
     s.y1B = add_rn(add_rn(mul_rn(e1[0], S[0]), mul_rn(e2[0], S[1])), mul_rn(e3[0], S[2]));
     s.y2B = add_rn(add_rn(mul_rn(e1[1], S[0]), mul_rn(e2[1], S[1])), mul_rn(e3[1], S[2]));
     s.y3B = add_rn(add_rn(mul_rn(e1[2], S[0]), mul_rn(e2[2], S[1])), mul_rn(e3[2], S[2]));
-    // unit-mode slip vectors: TDCS (n, s, d) -> EFCS -> ADCS
-    const double slip[3] = {Dn, Dss, Dds};
-    const double* axes[3] = {real.Vn, real.Vs, real.Vd};
-    for (int m = 0; m < 3; ++m) {
-        double w[3];
-        for (int i = 0; i < 3; ++i) w[i] = mul_rn(axes[m][i], slip[m]);
-        for (int g = 0; g < 3; ++g) {
-            s.cs[m][g] = add_rn(add_rn(mul_rn(e1[g], w[0]), mul_rn(e2[g], w[1])), mul_rn(e3[g], w[2]));
-            s.cd[m][g] = s.cs[m][g] / 4.0 / M_PI / sub_rn(1.0, nu);
-        }
-    }
     const double a_end[2] = {-PA[2], -PB[2]};
     const double pibs = M_PI - beta, pibd = -M_PI + beta;
     for (int e = 0; e < 2; ++e) {
@@ -689,6 +738,24 @@ CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real
                                s.kd[0][e]);
         ang_dis_disp_fsc_setup(cos(pibd), sin(pibd), 1.0 / tan(pibd), 1.0 / tan(pibd / 2.0), nu, a_end[e],
                                s.kd[1][e]);
+    }
+}
+
+CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real, double Dss, double Dds,
+                       double Dn, double nu, FscSide& s)
+{
+    build_side_geom(PA, PB, nu, s);
+    if (s.skip != 0.0) return;
+    // unit-mode slip vectors: TDCS (n, s, d) -> EFCS -> ADCS
+    const double slip[3] = {Dn, Dss, Dds};
+    const double* axes[3] = {real.Vn, real.Vs, real.Vd};
+    for (int m = 0; m < 3; ++m) {
+        double w[3];
+        for (int i = 0; i < 3; ++i) w[i] = mul_rn(axes[m][i], slip[m]);
+        for (int g = 0; g < 3; ++g) {
+            s.cs[m][g] = add_rn(add_rn(mul_rn(s.ey1[g], w[0]), mul_rn(s.ey2[g], w[1])), mul_rn(s.ey3[g], w[2]));
+            s.cd[m][g] = s.cs[m][g] / 4.0 / M_PI / sub_rn(1.0, nu);
+        }
     }
 }
 
@@ -707,6 +774,31 @@ CAD_HD void pair_strain(const TriDevT<R>& t, double X, double Y, double Z, R E[3
             if (t.side[sd].skip == R(0)) fsc_strain(t.side[sd], X, Y, Z, t.Dss, t.Dds, t.Dn, E);
         strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
     }
+}
+
+// Half-space strain with the free-surface corrections of the triangle's sides
+// read from per-edge maps (fsc_strain_map): entry (edge e, value q) of this
+// observation point at G[e * ge + q * gq]; code[sd] = +-(e + 1) for side sd
+// traversed along / against edge e's direction, 0 for no correction.
+CAD_HD void pair_strain_edges(const TriDev& t, double X, double Y, double Z, const double* G, int64_t gq, int64_t ge,
+                              const int* code, double E[3][6])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[m][k] = 0.0;
+    strain_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+#pragma unroll 1
+    for (int sd = 0; sd < 3; ++sd) {
+        const int c = code[sd];
+        if (c == 0) continue;
+        const int64_t e = (int64_t)(c > 0 ? c : -c) - 1;
+        double Gm[3][6];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) Gm[q / 6][q % 6] = G[e * ge + q * gq];
+        fsc_apply_map(Gm, c > 0 ? 1.0 : -1.0, t.real, t.Dss, t.Dds, t.Dn, E);
+    }
+    strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
 }
 
 template <bool HS, typename R>

@@ -122,18 +122,22 @@ __device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, co
 // MINB > 1: compiled for MINB resident blocks per SM (fewer registers per
 // thread, more warps to hide the FP64 latency, some spilling) -- a launch
 // shape the autotuner may pick for the half-space system matrix.
-template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false, int MINB = 1>
+// EDGE (half space, strain, OUT_AMAT): the free-surface corrections come from
+// the per-edge maps a.fscG; the staged record is the two frames only
+template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false, int MINB = 1,
+          bool EDGE = false>
 __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 {
+    static_assert(!EDGE || (HS && STRAIN && !DISP && OUT == OUT_AMAT && !LIST), "edge maps: HS system matrix only");
     extern __shared__ double smem[];
-    constexpr int words = HS ? kTriWordsHS : kTriWordsFS;
+    constexpr int words = HS ? (EDGE ? kTriWordsImg : kTriWordsHS) : kTriWordsFS;
     const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
     const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
     const bool active = i < a.M;
     // LIST: this thread's point (system row) and the full system's size
     const int64_t io = (LIST && a.obs_list && active) ? (int64_t)a.obs_list[i] : i;
-    const int64_t NS = LIST ? a.Ntot : a.N;
-    const int64_t MD = LIST ? a.Ntot : a.M;
+    const int64_t NS = (LIST || EDGE) ? a.Ntot : a.N;
+    const int64_t MD = (LIST || EDGE) ? a.Ntot : a.M;
     double X = 0.0, Y = 0.0, Z = 0.0;
     if (active) { X = a.X[io]; Y = a.Y[io]; Z = a.Z[io]; }
     const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
@@ -167,7 +171,10 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
         if (!active) continue;
         if (STRAIN) {
             double E[3][6];
-            pair_strain<HS>(t, X, Y, Z, E);
+            if constexpr (EDGE)
+                pair_strain_edges(t, X, Y, Z, a.fscG + i, a.M, 18 * a.M, a.side_edge + 3 * jt, E);
+            else
+                pair_strain<HS>(t, X, Y, Z, E);
             if (OUT == OUT_INF) {
 #pragma unroll
                 for (int m = 0; m < 3; ++m)
@@ -444,6 +451,98 @@ cudaError_t launch_td_pairs(const PairArgs& a, int out, bool hs, bool strain, bo
             return launch_pair<false, true, false, OUT_AMAT>(a, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------ shared-edge half space
+// One mesh edge's free-surface record (geometry only) per thread; edge e's
+// endpoints PA, PB at pts[6 e ..].
+__global__ void edge_setup_kernel(const double* __restrict__ pts, int64_t E, double nu, FscSide* __restrict__ out)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const double PA[3] = {pts[6 * e], pts[6 * e + 1], pts[6 * e + 2]};
+    const double PB[3] = {pts[6 * e + 3], pts[6 * e + 4], pts[6 * e + 5]};
+    build_side_geom(PA, PB, nu, out[e]);
+}
+
+// G[(e * 18 + q) M + i] = value q of edge e's free-surface map at point i
+// (fsc_strain_map; zero for an edge the beta test drops).  Block = 128 points
+// x a chunk of edges, each edge record staged in shared memory.
+__global__ void __launch_bounds__(kPairThreads, 1) fsc_edge_kernel(const FscSide* __restrict__ edges, int64_t E,
+                                                                 int64_t echunk, const double* __restrict__ X,
+                                                                 const double* __restrict__ Y,
+                                                                 const double* __restrict__ Z, int64_t M,
+                                                                 double* __restrict__ G)
+{
+    extern __shared__ double smem[];
+    const FscSide& s = *reinterpret_cast<const FscSide*>(smem);
+    const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
+    const bool active = i < M;
+    double x = 0.0, y = 0.0, z = 0.0;
+    if (active) { x = X[i]; y = Y[i]; z = Z[i]; }
+    const int64_t e0 = (int64_t)blockIdx.y * echunk;
+    const int64_t e1 = min(E, e0 + echunk);
+    for (int64_t e = e0; e < e1; ++e) {
+        __syncthreads();
+        const double* src = reinterpret_cast<const double*>(edges + e);
+        for (int w = threadIdx.x; w < kSideWords; w += kPairThreads) smem[w] = src[w];
+        __syncthreads();
+        if (!active) continue;
+        double Gm[3][6];
+        if (s.skip != 0.0) {
+#pragma unroll
+            for (int q = 0; q < 18; ++q) Gm[q / 6][q % 6] = 0.0;
+        } else {
+            fsc_strain_map(s, x, y, z, Gm);
+        }
+#pragma unroll
+        for (int q = 0; q < 18; ++q) G[(e * 18 + q) * M + i] = Gm[q / 6][q % 6];
+    }
+}
+
+size_t edge_record_bytes() { return sizeof(FscSide); }
+
+cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E, const int* side_edge, void* edge_rec,
+                                  double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches)
+{
+    if (a.M == 0 || a.N == 0) return cudaSuccess;
+    if (E > 0) {
+        edge_setup_kernel<<<(unsigned)((E + 127) / 128), 128, 0, st>>>(edge_pts, E, nu, (FscSide*)edge_rec);
+        if (launches) ++*launches;
+        if (cudaError_t e = cudaGetLastError()) return e;
+    }
+    auto pk = td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>;
+    const size_t psmem = (size_t)kTriWordsImg * sizeof(double);
+    const size_t esmem = (size_t)kSideWords * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fsc_edge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
+    if (e != cudaSuccess) return e;
+    const int64_t echunk = 32;
+    for (int64_t c0 = 0; c0 < a.M; c0 += Mc) {
+        const int64_t mc = a.M - c0 < Mc ? a.M - c0 : Mc;
+        const unsigned tiles = (unsigned)((mc + kPairThreads - 1) / kPairThreads);
+        if (E > 0) {
+            fsc_edge_kernel<<<dim3(tiles, (unsigned)((E + echunk - 1) / echunk)), kPairThreads, esmem, st>>>(
+                (const FscSide*)edge_rec, E, echunk, a.X + c0, a.Y + c0, a.Z + c0, mc, G);
+            if (launches) ++*launches;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        PairArgs b = a;
+        b.X = a.X + c0;
+        b.Y = a.Y + c0;
+        b.Z = a.Z + c0;
+        b.dirs = a.dirs + c0;
+        b.A = a.A + c0;
+        b.M = mc;
+        b.Ntot = a.N;
+        b.fscG = G;
+        b.side_edge = side_edge;
+        pk<<<dim3(tiles, (unsigned)((a.N + a.tri_chunk - 1) / a.tri_chunk)), kPairThreads, psmem, st>>>(b);
+        if (launches) ++*launches;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_splice_fixed(const double* trac, const double* disp, int64_t N, int64_t nfix, const int* fixrow,

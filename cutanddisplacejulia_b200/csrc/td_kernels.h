@@ -44,7 +44,22 @@ struct PairArgs {
     // half-space system matrix: the kernel variant compiled for this many
     // resident blocks per SM (1: the full register file; 3 or 4)
     int min_blocks = 1;
+    // half-space system matrix with shared-edge free-surface maps: the maps
+    // of this launch's points (18 x M per edge, fsc_edge_kernel) and each
+    // triangle's three side codes (+-(edge + 1), 0: none); rows are then a
+    // block of an Ntot-point system (X, Y, Z, dirs and A start at the block)
+    const double* fscG = nullptr;
+    const int* side_edge = nullptr;
 };
+
+// Half-space system matrix (OUT_AMAT, FP64) with the free-surface correction
+// evaluated once per mesh edge: edge_pts holds E edges (PA, PB: 6 doubles
+// each), side_edge each triangle's three side codes; edge_rec
+// (edge_record_bytes() x E) and G (18 x Mc x E doubles) are workspaces; the
+// points are processed in blocks of Mc.  a.M == a.N (a square system).
+cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E, const int* side_edge, void* edge_rec,
+                                  double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches);
+size_t edge_record_bytes();
 
 // Mixed-precision system matrix: every pair in FP32 (far field), then the
 // pairs of every 128-point tile that has a point within the near radius of

@@ -2,7 +2,9 @@
 system matrix sharded by element columns as dist.column_block splits it for
 3 ranks (run one after another on this GPU; the blocks need no exchange)
 must reproduce the columns of the full assembly (cad_assemble_dev) exactly,
-in full space and half space, and seeded columns of each block must match the
+in full space and half space (the full assembly with per-side free-surface
+corrections, as the block computes them; within the parity tolerance of the
+default shared-edge one), and seeded columns of each block must match the
 oracle's restatement of the assembly."""
 import numpy as np
 import pytest
@@ -32,7 +34,15 @@ def test_column_blocks_equal_full_assembly(cad, oracle, hs):
     A = torch.empty(n3 * n3, dtype=torch.float64, device=dev)
     _lib.check(L.cad_assemble_dev(ctx, *[x.data_ptr() for x in g], n, nu, G, lam, hs, A.data_ptr(), n3), ctx)
     torch.cuda.synchronize()
-    full = A.view(n3, n3).cpu().numpy().T   # column-major 3N x 3N
+    shared = A.view(n3, n3).cpu().numpy().T   # column-major 3N x 3N
+    _lib.check(L.cad_set_shared_edges(ctx, 0), ctx)
+    try:
+        _lib.check(L.cad_assemble_dev(ctx, *[x.data_ptr() for x in g], n, nu, G, lam, hs, A.data_ptr(), n3), ctx)
+        torch.cuda.synchronize()
+    finally:
+        _lib.check(L.cad_set_shared_edges(ctx, 1), ctx)
+    full = A.view(n3, n3).cpu().numpy().T
+    assert_parity(shared[None], full[None])
     for rank in range(3):
         j0, j1 = dist.column_block(n, rank, 3)
         nb = j1 - j0
