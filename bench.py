@@ -43,9 +43,16 @@ FALG_ASSEMBLY_FS = 2960.0 + 288.0
 # Half-space strain of all three unit modes (43867 on the dipping-crack
 # collocation pairs) plus the same traction epilogue.
 FALG_ASSEMBLY_HS = 43867.0 + 288.0
-# DRAM bytes (read + write) of one assembly launch from the committed ncu captures
-# (profiles/td_pair_kernel_*.md): (triangles captured, bytes).  Output scales as N^2.
-PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (3968, 75.39e6 + 3.003e9)}
+# DRAM bytes (read + write) of one assembly from the committed ncu captures
+# (profiles/td_pair_kernel_*.md, profiles/fsc_edge_kernel_*.md): (triangles
+# captured, bytes).  Both scale as N^2.  Half space: the shared-edge path's two
+# kernels, fsc_edge_kernel (17.75 MB + 1.0328 GB) and the edge pair kernel
+# (966.74 MB + 267.54 MB), at 1980 triangles and 3037 edges.
+PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 17.75e6 + 1.0328e9 + 966.74e6 + 267.54e6)}
+# FP64-pipe activity (fraction of peak, ncu sm__pipe_fp64_cycles_active) of the
+# shared-edge half-space assembly's kernels, from the committed capture at 1980
+# triangles (profiles/fsc_edge_kernel_*.md)
+FP64_PIPE_ACTIVE_HS = {"fsc_edge_kernel": 0.538, "td_pair_kernel_edge": 0.518}
 # share of the step's (serialised) device time taken by the LU panel leaf, from
 # the committed launch list (profiles/launches_penny2013_fp64_and_mixed_step.md)
 DOMINANT_SHARE = {"penny": 0.532}
@@ -975,7 +982,7 @@ def run_c3(args, rank, world, local_rank):
                            "the part of it left after the assembly)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (A is %.0f MB per step)" % (n3 * n3 * 8 / 1e6)},
-        "breakdown_ms": {"assembly": asm_ms, "td_pair_kernel_last": pair_kernel_ms,
+        "breakdown_ms": {"assembly": asm_ms, "assembly_kernels_last": pair_kernel_ms,
                          "preconditioner_setup": setup_ms, "gmres": gmres_ms},
         "gmres_iterations": its, "rel_residual": resid, "slip_rel_err_vs_fp64_lu": slip_err,
         "solve_ms_to_rel_residual_1e-10": {"learned_gmres": setup_ms + gmres_ms, "fp64_lu": sol64,
@@ -990,15 +997,23 @@ def run_c3(args, rank, world, local_rank):
                 "ms_per_step": e2e_ms, "slip_rel_err_vs_fp64_lu": e2e_err,
                 "api": "cad_slip_calculator, solver CAD_SOLVER_GMRES_LEARNED (host C ABI, pinned host buffers)"},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "td_pair_kernel<HS, strain, A-matrix> (the step's dominant phase: FP64 assembly)",
+        "roofline": {"kernel": "fsc_edge_kernel + td_pair_kernel<HS, strain, A-matrix, EDGE> (the step's dominant "
+                               "phase: the FP64 shared-edge half-space assembly)",
                      "bound": "fp64", "achieved": asm_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": asm_tflops / fp64_peak,
                      "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run); "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "falg_per_pair": falg,
                      "traffic": PAIR_TRAFFIC["dipping"][1] * (n / PAIR_TRAFFIC["dipping"][0]) ** 2,
-                     "traffic_source": "ncu DRAM bytes (read + write) of one launch at N=%d, scaled by (N/%d)^2"
-                                       % (PAIR_TRAFFIC["dipping"][0], PAIR_TRAFFIC["dipping"][0]),
+                     "traffic_source": "ncu DRAM bytes (read + write) of the assembly's two kernels at N=%d, "
+                                       "scaled by (N/%d)^2; the edge maps (18 doubles per edge and point) are "
+                                       "written once and read by the triangles sharing each edge, the rest is "
+                                       "the matrix" % (PAIR_TRAFFIC["dipping"][0], PAIR_TRAFFIC["dipping"][0]),
+                     "falg_note": "F_alg is the reference's literal count per pair, which evaluates each "
+                                  "side's free-surface correction per triangle and slip mode; the shared-edge "
+                                  "path evaluates it once per edge, so the algorithmic rate exceeds the FP64 "
+                                  "pipe's peak while the pipe itself is about half busy (fp64_pipe_active_ncu)",
+                     "fp64_pipe_active_ncu": FP64_PIPE_ACTIVE_HS,
                      "step_share": asm_ms / ms},
         "roofline_gmres": {"kernel": "GMRES(30): FP32 copy of A, one FP32 pass over A per Arnoldi product, "
                                      "one FP64 pass per restart residual",
