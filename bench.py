@@ -47,12 +47,13 @@ FALG_ASSEMBLY_HS = 43867.0 + 288.0
 # (profiles/td_pair_kernel_*.md, profiles/fsc_edge_kernel_*.md): (triangles
 # captured, bytes).  Both scale as N^2.  Half space: the shared-edge path's two
 # kernels, fsc_edge_kernel (17.75 MB + 1.0328 GB) and the edge pair kernel
-# (966.74 MB + 267.54 MB), at 1980 triangles and 3037 edges.
-PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 17.75e6 + 1.0328e9 + 966.74e6 + 267.54e6)}
+# built for three blocks per SM (1.0982 GB + 307.38 MB), at 1980 triangles and
+# 3037 edges.
+PAIR_TRAFFIC = {"penny": (2013, 2.49e6 + 233.84e6), "dipping": (1980, 17.75e6 + 1.0328e9 + 1.0982e9 + 307.38e6)}
 # FP64-pipe activity (fraction of peak, ncu sm__pipe_fp64_cycles_active) of the
 # shared-edge half-space assembly's kernels, from the committed capture at 1980
 # triangles (profiles/fsc_edge_kernel_*.md)
-FP64_PIPE_ACTIVE_HS = {"fsc_edge_kernel": 0.538, "td_pair_kernel_edge": 0.518}
+FP64_PIPE_ACTIVE_HS = {"fsc_edge_kernel": 0.538, "td_pair_kernel_edge": 0.591}
 # share of the step's (serialised) device time taken by the LU panel leaf, from
 # the committed launch list (profiles/launches_penny2013_fp64_and_mixed_step.md)
 DOMINANT_SHARE = {"penny": 0.532}

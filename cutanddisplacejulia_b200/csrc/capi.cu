@@ -392,6 +392,28 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         if (Mc < kPairThreads) Mc = kPairThreads;
         if (Mc > N) Mc = N;
         if (int r = ensure(ctx, S_EDGE_G, (size_t)Mc * per_point, &gmap)) return r;
+        a.min_blocks = kEdgeMinBlocks;
+        if (ctx->tuner.mode != TUNE_OFF) {
+            // triangles per block of the edge pair kernel, then its build
+            // (resident blocks per SM); each candidate runs the whole path
+            char key[96];
+            auto run = [&](const PairArgs& t) {
+                return launch_assemble_edges(t, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream,
+                                             &ctx->launches);
+            };
+            std::snprintf(key, sizeof key, "pair_amat_f64_hs1_edge_N%lld", (long long)tune_class(N));
+            PairArgs t = a;
+            a.tri_chunk = tune_choice(ctx->tuner, key, ctx->stream, {2, 4, 8, 16, 32}, (int)a.tri_chunk, [&](int c) {
+                t.tri_chunk = c;
+                return run(t);
+            });
+            std::snprintf(key, sizeof key, "pair_amat_f64_hs1_edge_minblocks_N%lld", (long long)tune_class(N));
+            t = a;
+            a.min_blocks = tune_choice(ctx->tuner, key, ctx->stream, {kEdgeMinBlocks, 1}, kEdgeMinBlocks, [&](int c) {
+                t.min_blocks = c;
+                return run(t);
+            });
+        }
         CK(cudaEventRecord(ctx->ev[0], ctx->stream));
         CK(launch_assemble_edges(a, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
         CK(cudaEventRecord(ctx->ev[1], ctx->stream));

@@ -511,9 +511,11 @@ cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E,
         if (launches) ++*launches;
         if (cudaError_t e = cudaGetLastError()) return e;
     }
-    // three resident blocks per SM (168 registers, 308 B of spills): 69.8 ms
-    // against 73.9 ms with the full register file at 10 000 triangles
-    auto pk = td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>;
+    // a.min_blocks 3: three resident blocks per SM (168 registers, 308 B of
+    // spills), 69.8 ms against 73.9 ms with the full register file (1) at
+    // 10 000 triangles
+    auto pk = a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>
+                                : td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>;
     const size_t psmem = (size_t)kTriWordsImg * sizeof(double);
     const size_t esmem = (size_t)kSideWords * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);

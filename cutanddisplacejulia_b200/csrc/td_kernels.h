@@ -11,6 +11,7 @@ struct TriDevT;
 using TriDev = TriDevT<double>;
 
 constexpr int kPairThreads = 128;
+constexpr int kEdgeMinBlocks = 3;   // default build of the shared-edge pair kernel
 
 enum OutKind { OUT_INF = 0, OUT_SUM = 1, OUT_TRAC = 2, OUT_AMAT = 3 };
 
@@ -57,6 +58,8 @@ struct PairArgs {
 // each), side_edge each triangle's three side codes; edge_rec
 // (edge_record_bytes() x E) and G (18 x Mc x E doubles) are workspaces; the
 // points are processed in blocks of Mc.  a.M == a.N (a square system).
+// a.min_blocks selects the pair kernel's build: 1 (the full register file)
+// or anything else for three resident blocks per SM (kEdgeMinBlocks).
 cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E, const int* side_edge, void* edge_rec,
                                   double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches);
 size_t edge_record_bytes();

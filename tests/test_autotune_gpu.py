@@ -35,7 +35,7 @@ def test_autotune_cache_round_trip(cad, tmp_path):
     L = _lib.load()
     ctx = _lib.context(0)
     cache = str(tmp_path / "tune.txt")
-    A0, n = _system(L, ctx, torch, dev, 600, 1)            # untuned
+    A0, n = _system(L, ctx, torch, dev, 600, 1)            # untuned (shared-edge half-space path)
     b = torch.linspace(-1e-3, 1e-3, 3 * n, dtype=torch.float64, device=dev)
     F = A0.clone()
     x0 = b.clone()
@@ -53,7 +53,8 @@ def test_autotune_cache_round_trip(cad, tmp_path):
         entries = L.cad_autotune_entries(ctx, ctypes.byref(tuned))
         assert entries >= 2 and tuned.value >= 2
         text = open(cache).read()
-        assert "pair_amat_f64_hs1_N1024" in text and "lu_leaf_f64_n2048" in text
+        assert "pair_amat_f64_hs1_edge_N1024" in text and "pair_amat_f64_hs1_edge_minblocks_N1024" in text
+        assert "lu_leaf_f64_n2048" in text
         # a fresh load of the file in cached-only mode: nothing is timed again
         _lib.check(L.cad_set_autotune(ctx, 2, cache.encode()), ctx)
         before = ctypes.c_int64(0)
