@@ -80,6 +80,9 @@ WORKLOADS = {
               "%d full-space penny/elliptical cracks, semi-axis U[0.5,2], aspect U[0.3,1], random orientation, "
               "200-2000 triangles each (log-uniform), %d triangles in all"),
 }
+WORKLOADS["tdsum"] = ("TD pair-evals/s (HS summed strain + displacement of a slipping crack at observation points)",
+                      "2x1 crack dipping 60 deg, top at depth 2, half space, %d triangles with smooth seeded slip; "
+                      "%d observation points (a %d x %d grid on the free surface z = 0, x, y in [-4, 4])")
 WORKLOADS["gemm"] = ("LU trailing-update GEMM TFLOP/s (C -= A B, column-major)",
                      "%d x %d x %d, FP64 DMMA (each instruction shape) and TF32 tcgen05")
 METRIC = WORKLOADS["penny"][0]
@@ -1303,6 +1306,142 @@ def run_gemm(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# Half-space strain + displacement per pair, both frozen oracle counts (the
+# summing TD overload evaluates all three slip modes of each).
+FALG_SUM_HS = 43867.0 + 6780.0
+TDSUM_GRID = 100
+
+
+def tdsum_case(ntri, grid=TDSUM_GRID):
+    """The dipping crack with smooth seeded slip, and a grid of surface points."""
+    import numpy as np
+
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=0, ntri=ntri)
+    mid = (P1 + P2 + P3) / 3.0
+    rng = np.random.default_rng(1)
+    sl = np.stack([1e-3 * np.cos(0.7 * mid[:, 0] + k) * np.cos(0.9 * mid[:, 2] - k) for k in range(3)])
+    sl += rng.uniform(-1e-4, 1e-4, sl.shape)
+    g = np.linspace(-4.0, 4.0, grid)
+    X, Y = np.meshgrid(g, g)
+    return P1, P2, P3, sl, X.ravel(), Y.ravel(), np.zeros(X.size)
+
+
+def run_tdsum(args, rank, world, local_rank):
+    """The summing TD overload (src/TD.jl:219-410) in half space: strain and
+    displacement at the free surface of a slipping dipping crack.  One step =
+    one cad_td_sum_eval_dev call on device-resident inputs (the shared-edge
+    path: each mesh edge's free-surface correction once, for the net Burgers
+    vector of its sides); the per-side path and the host API (cad.TD with
+    Strains/Disps, host arrays) are timed beside it."""
+    import numpy as np
+    import torch
+
+    import cutanddisplacejulia_b200 as cad
+    from cutanddisplacejulia_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    L = _lib.load()
+    ctx = _lib.context(local_rank)
+    stream = torch.cuda.ExternalStream(L.cad_get_stream(ctx), device=dev)
+    P1, P2, P3, sl, X, Y, Z = tdsum_case(args.ntri)
+    n, m = len(P1), X.size
+    pairs = float(n) * m
+    col = (lambda a: torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device=dev))
+    Xd, Yd, Zd = col(X), col(Y), col(Z)
+    Pd = [col(P) for P in (P1, P2, P3)]
+    Sd = [col(v) for v in sl]   # Dss, Dds, Dn
+    S = torch.empty(6 * m, dtype=torch.float64, device=dev)
+    U = torch.empty(3 * m, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.cad_fp64_fma_probe(ctx, 20000, ctypes.byref(peak)), ctx)
+
+    def call():
+        _lib.check(L.cad_td_sum_eval_dev(ctx, Xd.data_ptr(), Yd.data_ptr(), Zd.data_ptr(), m,
+                                         *[p.data_ptr() for p in Pd], n, *[v.data_ptr() for v in Sd], NU, 1, 1, 1,
+                                         S.data_ptr(), U.data_ptr()), ctx)
+
+    def timed(shared, steps, clocks=None):
+        _lib.check(L.cad_set_shared_edges(ctx, shared), ctx)
+        for _ in range(args.warmup):
+            call()
+        if clocks:
+            clocks.start()
+            time.sleep(0.3)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = L.cad_kernel_launches(ctx)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop() if clocks else None
+        ms = cdist.max_over_ranks(e0.elapsed_time(e1) / steps, dev)
+        return ms, (L.cad_kernel_launches(ctx) - l0), torch.cat([S, U]).cpu().numpy(), clk
+
+    ms_side, _, out_side, _ = timed(0, max(1, args.steps // 2))
+    ms, launches, out, clk = timed(1, args.steps, ClockSampler(local_rank))
+    kern_ms = L.cad_last_time_ms(ctx, 0)
+    rel = float(np.abs(out - out_side).max() / np.abs(out_side).max())
+    # end to end through the public API with host arrays
+    Xh, Yh, Zh = X.copy(), Y.copy(), Z.copy()
+    cad.TD(Xh, Yh, Zh, P1, P2, P3, *sl, NU, G, 1, 1, 1, cad.Strains(), cad.Disps())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        Sh, Uh = cad.TD(Xh, Yh, Zh, P1, P2, P3, *sl, NU, G, 1, 1, 1, cad.Strains(), cad.Disps())
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        nthreads = os.cpu_count() or 1
+        pick = np.random.default_rng(7).choice(m, 300, replace=False)
+        t0 = time.perf_counter()
+        So, Uo = O.td_sum_eval(X[pick], Y[pick], Z[pick], P1, P2, P3, *sl, NU, G, 1, 1, 1)
+        cpu_s = time.perf_counter() - t0
+        got_s = out[:6 * m].reshape(6, m)[:, pick]
+        got_u = out[6 * m:].reshape(3, m)[:, pick]
+        err = max(float(np.abs(got_s - So).max() / np.abs(So).max()), float(np.abs(got_u - Uo).max() / np.abs(Uo).max()))
+        cpu = {"value": 300.0 * n / cpu_s, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": "oracle HS sums of all %d triangles at 300 seeded grid points (%d threads): %.1f s; "
+                         "max rel err of the GPU result there %.2e" % (n, nthreads, cpu_s, err)}
+    achieved = pairs * FALG_SUM_HS / (ms * 1e-3) / 1e12
+    line = {
+        "metric": WORKLOADS["tdsum"][0], "value": cdist.replica_throughput(pairs, ms, world), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS["tdsum"][1] % (n, m, TDSUM_GRID, TDSUM_GRID), "pairs_per_step": pairs,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs and partial sums fit in L2; the step is FP64-bound, not memory-bound"},
+        "breakdown_ms": {"kernels_last": kern_ms},
+        "per_side": {"ms_per_step": ms_side, "value": pairs / (ms_side * 1e-3), "max_rel_diff": rel},
+        "speedup_vs_per_side": ms_side / ms,
+        "clocks": clk,
+        "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": (3 * m + 9 * n + 3 * n) * 8, "d2h_bytes_per_step": 9 * m * 8,
+                "api": "cad.TD(..., Strains(), Disps()) with host arrays (cad_td_sum_eval, host C ABI)"},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "td_pair_kernel<HS, sum, EDGE> + fsc_sum_kernel (shared-edge half-space sums)",
+                     "bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                     "frac": achieved / peak.value, "falg_per_pair": FALG_SUM_HS,
+                     "peak_source": "measured FP64 FMA throughput (cad_fp64_fma_probe, this run)",
+                     "falg_note": "the reference's literal count per pair; the shared-edge path evaluates each "
+                                  "edge's free-surface correction once instead of per side and mode",
+                     "traffic": None},
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_friction(args, rank, world, local_rank):
     """Frictional slip (src/SlipCalculator3D.jl:36-238) through the C ABI with
     host buffers: one step = assembly of A, C = inv(A Scl) by the FP64 LU,
@@ -1430,6 +1569,8 @@ def main():
             run_friction(args, rank, world, local_rank)
         elif args.workload == "gemm":
             run_gemm(args, rank, world, local_rank)
+        elif args.workload == "tdsum":
+            run_tdsum(args, rank, world, local_rank)
         elif args.workload == "dipping":
             run_c3(args, rank, world, local_rank)
         else:

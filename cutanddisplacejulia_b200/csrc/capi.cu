@@ -43,7 +43,7 @@ enum Slot {
     S_A32, S_DINV, S_KRYLOV, S_VEC32, S_SYNC, S_TRI32, S_NEAR, S_IR, S_IR32, S_NORMS, S_REL, S_BGEOM, S_BTD, S_MLP,
     S_FIX, S_FOBS, S_FDISP, S_ATA, S_LIST, S_CHAIN, S_LCPJ, S_LCPC, S_LCPV, S_LCPP, S_GEMM, S_LPC_NET, S_LPC_WS, S_LPC_GEOM, S_LPC_TNBR, S_LPC_FEAT, S_LPC_OUT,
     S_LPC_NBR, S_LPC_BLK, S_LPC_MAT, S_LPC_PGEOM, S_BJ_NBR, S_BJ_BLK, S_KWORK, S_A32MV, S_TUNE, S_AT, S_G_A32, S_G_INT, S_G_F32, S_G_F64, S_G_MAPS,
-    S_EDGE_PTS, S_EDGE_CODE, S_EDGE_REC, S_EDGE_G, S_COUNT
+    S_EDGE_PTS, S_EDGE_CODE, S_EDGE_REC, S_EDGE_G, S_EDGE_PTR, S_EDGE_TRIS, S_COUNT
 };
 
 constexpr int kGmresRestart = 30; // default Krylov dimension of a GMRES cycle
@@ -116,9 +116,10 @@ struct cad_ctx {
     int shared_edges = 1;                  // cad_set_shared_edges
     // mesh-edge table of the last half-space assembly: the vertices it was
     // built from (P1, P2, P3, 3 N each), its edges' endpoints (6 per edge)
-    // and each triangle side's signed edge number (0 for none)
+    // and each triangle side's signed edge number (0 for none); per edge, the
+    // signed triangles on it (edge_ptr offsets into edge_tris)
     std::vector<double> edge_geom, edge_pts;
-    std::vector<int> edge_code;
+    std::vector<int> edge_code, edge_ptr, edge_tris;
     int64_t edge_n = -1;
     double tol = 1e-10;
     int max_iter = 200;
@@ -225,45 +226,6 @@ int hs_check(cad_ctx* ctx, const double* Z, int64_t M, const double* P1, const d
     return CAD_OK;
 }
 
-// Device path shared by the TD entry points (inputs already on the device).
-int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
-              const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds, const double* Dn,
-              double nu, int disp, int strain, int hs, int out_kind, double* strain_out, double* disp_out,
-              double* sum_out /* 9 x M for OUT_SUM */)
-{
-    if (hs == 1 && N > 0)
-        if (int r = hs_check(ctx, Z, M, P1, P2, P3, N)) return r;
-    if (M == 0 || N == 0) {
-        if (out_kind == OUT_SUM && sum_out) CK(cudaMemsetAsync(sum_out, 0, 9 * M * sizeof(double), ctx->stream));
-        return CAD_OK;
-    }
-    void* tri;
-    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
-    ++ctx->launches;
-    CK(launch_td_setup(P1, P2, P3, N, Dss, Dds, Dn, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
-    PairArgs a{};
-    a.X = X; a.Y = Y; a.Z = Z; a.M = M; a.tri = (const TriDev*)tri; a.N = N;
-    a.tri_chunk = pick_chunk(M, N, out_kind == OUT_SUM);
-    a.strain = strain_out; a.disp = disp_out;
-    const int64_t nchunk = (N + a.tri_chunk - 1) / a.tri_chunk;
-    if (out_kind == OUT_SUM) {
-        void* part;
-        if (int r = ensure(ctx, S_PART, (size_t)nchunk * 9 * M * sizeof(double), &part)) return r;
-        a.partial = (double*)part;
-    }
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    ++ctx->launches;
-    CK(launch_td_pairs(a, out_kind, hs == 1, strain == 1, disp == 1, ctx->stream));
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    ctx->timed[0] = true;
-    if (out_kind == OUT_SUM) {
-        const int mask = (strain == 1 ? 0x3f : 0) | (disp == 1 ? 0x1c0 : 0);
-        ++ctx->launches;
-    CK(launch_sum_chunks(a.partial, nchunk, M, mask, sum_out, ctx->stream));
-    }
-    return CAD_OK;
-}
-
 // Number the mesh's distinct triangle sides (edges).  Side s of triangle j
 // runs P1->P2, P2->P3, P3->P1; its code is e + 1 when it runs the way edge e
 // was first seen, -(e + 1) when it runs the other way.  Endpoints match when
@@ -288,15 +250,27 @@ struct EdgeKeyHash {
     }
 };
 
-int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, int64_t* E,
-               double** pts_dev, int** code_dev)
+struct EdgeTable {
+    int64_t E = 0;
+    double* pts = nullptr;   // device: 6 doubles per edge
+    int* code = nullptr;     // device: 3 per triangle
+    int* ptr = nullptr;      // device: E + 1 offsets into tris
+    int* tris = nullptr;     // device: +-(triangle + 1) per side, by edge
+};
+
+// Shared-edge work pays when the mesh's edges are clearly fewer than its
+// triangle sides (a manifold mesh has about half); a soup of unconnected
+// triangles stays on the per-side kernels.
+bool edges_pay(int64_t E, int64_t N) { return 10 * E < 9 * 3 * N; }
+
+int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, EdgeTable* out)
 {
     std::vector<double> geom((size_t)9 * N);
     CK(cudaMemcpyAsync(geom.data(), P1, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(geom.data() + 3 * N, P2, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(geom.data() + 6 * N, P3, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    void *pts, *code;
+    void *pts, *code, *eptr, *etris;
     const bool same = ctx->edge_n == N && ctx->edge_geom == geom;
     if (!same) {
         std::unordered_map<EdgeKey, int, EdgeKeyHash> seen;
@@ -324,9 +298,27 @@ int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P
                 }
                 ctx->edge_code[(size_t)3 * j + sd] = c;
             }
+        // edge -> sides, in triangle order (counting sort on the edge number)
+        const size_t E = ctx->edge_pts.size() / 6;
+        ctx->edge_ptr.assign(E + 1, 0);
+        for (int c : ctx->edge_code) ++ctx->edge_ptr[(size_t)(c > 0 ? c : -c)];
+        for (size_t e = 0; e < E; ++e) ctx->edge_ptr[e + 1] += ctx->edge_ptr[e];
+        ctx->edge_tris.assign((size_t)3 * N, 0);
+        std::vector<int> fill(ctx->edge_ptr.begin(), ctx->edge_ptr.end() - 1);
+        for (int64_t k = 0; k < 3 * N; ++k) {
+            const int c = ctx->edge_code[(size_t)k];
+            const int t = (int)(k / 3) + 1;
+            ctx->edge_tris[(size_t)fill[(size_t)((c > 0 ? c : -c) - 1)]++] = c > 0 ? t : -t;
+        }
         ctx->edge_n = -1;
         if (int r = ensure(ctx, S_EDGE_PTS, ctx->edge_pts.size() * sizeof(double), &pts)) return r;
         if (int r = ensure(ctx, S_EDGE_CODE, ctx->edge_code.size() * sizeof(int), &code)) return r;
+        if (int r = ensure(ctx, S_EDGE_PTR, ctx->edge_ptr.size() * sizeof(int), &eptr)) return r;
+        if (int r = ensure(ctx, S_EDGE_TRIS, ctx->edge_tris.size() * sizeof(int), &etris)) return r;
+        CK(cudaMemcpyAsync(eptr, ctx->edge_ptr.data(), ctx->edge_ptr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemcpyAsync(etris, ctx->edge_tris.data(), ctx->edge_tris.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemcpyAsync(pts, ctx->edge_pts.data(), ctx->edge_pts.size() * sizeof(double),
                            cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemcpyAsync(code, ctx->edge_code.data(), ctx->edge_code.size() * sizeof(int),
@@ -337,10 +329,76 @@ int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P
     } else {
         pts = ctx->buf[S_EDGE_PTS].p;
         code = ctx->buf[S_EDGE_CODE].p;
+        eptr = ctx->buf[S_EDGE_PTR].p;
+        etris = ctx->buf[S_EDGE_TRIS].p;
     }
-    *E = (int64_t)(ctx->edge_pts.size() / 6);
-    *pts_dev = (double*)pts;
-    *code_dev = (int*)code;
+    out->E = (int64_t)(ctx->edge_pts.size() / 6);
+    out->pts = (double*)pts;
+    out->code = (int*)code;
+    out->ptr = (int*)eptr;
+    out->tris = (int*)etris;
+    return CAD_OK;
+}
+
+// Device path shared by the TD entry points (inputs already on the device).
+int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, int64_t M, const double* P1,
+              const double* P2, const double* P3, int64_t N, const double* Dss, const double* Dds, const double* Dn,
+              double nu, int disp, int strain, int hs, int out_kind, double* strain_out, double* disp_out,
+              double* sum_out /* 9 x M for OUT_SUM */)
+{
+    if (hs == 1 && N > 0)
+        if (int r = hs_check(ctx, Z, M, P1, P2, P3, N)) return r;
+    if (M == 0 || N == 0) {
+        if (out_kind == OUT_SUM && sum_out) CK(cudaMemsetAsync(sum_out, 0, 9 * M * sizeof(double), ctx->stream));
+        return CAD_OK;
+    }
+    void* tri;
+    if (int r = ensure(ctx, S_TRI, (size_t)N * tri_record_bytes(), &tri)) return r;
+    ++ctx->launches;
+    CK(launch_td_setup(P1, P2, P3, N, Dss, Dds, Dn, 1, nu, hs == 1, (TriDev*)tri, ctx->stream));
+    PairArgs a{};
+    a.X = X; a.Y = Y; a.Z = Z; a.M = M; a.tri = (const TriDev*)tri; a.N = N;
+    a.tri_chunk = pick_chunk(M, N, out_kind == OUT_SUM);
+    a.strain = strain_out; a.disp = disp_out;
+    const int64_t nchunk = (N + a.tri_chunk - 1) / a.tri_chunk;
+    EdgeTable et;
+    if (out_kind == OUT_SUM && hs == 1 && ctx->shared_edges)
+        if (int r = edge_table(ctx, P1, P2, P3, N, &et)) return r;
+    if (out_kind == OUT_SUM && hs == 1 && ctx->shared_edges && edges_pay(et.E, N)) {
+        // real + image terms per triangle chunk, then each mesh edge's
+        // free-surface correction once, for the net Burgers vector of the
+        // sides on it; all partials summed in one fixed order
+        const int64_t echunk = pick_chunk(M, et.E, true);
+        const int64_t nechunk = (et.E + echunk - 1) / echunk;
+        void *part, *rec;
+        if (int r = ensure(ctx, S_PART, (size_t)(nchunk + nechunk) * 9 * M * sizeof(double), &part)) return r;
+        if (int r = ensure(ctx, S_EDGE_REC, (size_t)et.E * edge_record_bytes(), &rec)) return r;
+        a.partial = (double*)part;
+        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        CK(launch_td_sum_edges(a, strain == 1, disp == 1, et.pts, et.E, et.ptr, et.tris, rec, nu, echunk,
+                               a.partial + (size_t)nchunk * 9 * M, ctx->stream, &ctx->launches));
+        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        ctx->timed[0] = true;
+        const int mask = (strain == 1 ? 0x3f : 0) | (disp == 1 ? 0x1c0 : 0);
+        ++ctx->launches;
+        CK(launch_sum_chunks(a.partial, nchunk + nechunk, M, mask, sum_out, ctx->stream));
+        return CAD_OK;
+    }
+    if (out_kind == OUT_SUM) {
+        void* part;
+        if (int r = ensure(ctx, S_PART, (size_t)nchunk * 9 * M * sizeof(double), &part)) return r;
+        a.partial = (double*)part;
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    ++ctx->launches;
+    CK(launch_td_pairs(a, out_kind, hs == 1, strain == 1, disp == 1, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->timed[0] = true;
+    if (out_kind == OUT_SUM) {
+        const int mask = (strain == 1 ? 0x3f : 0) | (disp == 1 ? 0x1c0 : 0);
+        ++ctx->launches;
+    CK(launch_sum_chunks(a.partial, nchunk, M, mask, sum_out, ctx->stream));
+    }
     return CAD_OK;
 }
 
@@ -378,13 +436,15 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         ctx->timed[0] = true;
         return CAD_OK;
     }
-    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges) {
+    EdgeTable et;
+    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges)
+        if (int r = edge_table(ctx, P1, P2, P3, N, &et)) return r;
+    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges && edges_pay(et.E, N)) {
         // each mesh edge's free-surface map evaluated once, then read by the
         // (one or two) triangles that share the edge
-        int64_t E;
-        double* pts;
-        int* codes;
-        if (int r = edge_table(ctx, P1, P2, P3, N, &E, &pts, &codes)) return r;
+        const int64_t E = et.E;
+        double* pts = et.pts;
+        int* codes = et.code;
         void *rec, *gmap;
         if (int r = ensure(ctx, S_EDGE_REC, (size_t)(E > 0 ? E : 1) * edge_record_bytes(), &rec)) return r;
         const int64_t per_point = 18 * (E > 0 ? E : 1) * (int64_t)sizeof(double);

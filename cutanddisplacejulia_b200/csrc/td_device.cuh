@@ -759,6 +759,19 @@ CAD_HD void build_side(const double PA[3], const double PB[3], const Frame& real
     }
 }
 
+// Side PA -> PB carrying the net Burgers vector B (EFCS) of every triangle side
+// on that mesh edge, as unit mode 0 (evaluate with Dn = 1, Dss = Dds = 0).  The
+// slip coefficients follow build_side's for w = B.
+CAD_HD void build_side_burgers(const double PA[3], const double PB[3], const double B[3], double nu, FscSide& s)
+{
+    build_side_geom(PA, PB, nu, s);
+    if (s.skip != 0.0) return;
+    for (int g = 0; g < 3; ++g) {
+        s.cs[0][g] = add_rn(add_rn(mul_rn(s.ey1[g], B[0]), mul_rn(s.ey2[g], B[1])), mul_rn(s.ey3[g], B[2]));
+        s.cd[0][g] = s.cs[0][g] / 4.0 / M_PI / sub_rn(1.0, nu);
+    }
+}
+
 // ------------------------------------------------------------ pair drivers
 template <bool HS, typename R>
 CAD_HD void pair_strain(const TriDevT<R>& t, double X, double Y, double Z, R E[3][6])
@@ -799,6 +812,29 @@ CAD_HD void pair_strain_edges(const TriDev& t, double X, double Y, double Z, con
         fsc_apply_map(Gm, c > 0 ? 1.0 : -1.0, t.real, t.Dss, t.Dds, t.Dn, E);
     }
     strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+}
+
+// Half-space strain and displacement without the free-surface corrections
+// (real and image full-space terms only): the shared-edge sums add the
+// corrections once per mesh edge.
+CAD_HD void pair_strain_fs_image(const TriDev& t, double X, double Y, double Z, double E[3][6])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) E[m][k] = 0.0;
+    strain_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+    strain_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, E);
+}
+
+CAD_HD void pair_disp_fs_image(const TriDev& t, double X, double Y, double Z, double U[3][3])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) U[m][c] = 0.0;
+    disp_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+    disp_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
 }
 
 template <bool HS, typename R>

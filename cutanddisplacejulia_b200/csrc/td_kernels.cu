@@ -122,13 +122,17 @@ __device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, co
 // MINB > 1: compiled for MINB resident blocks per SM (fewer registers per
 // thread, more warps to hide the FP64 latency, some spilling) -- a launch
 // shape the autotuner may pick for the half-space system matrix.
-// EDGE (half space, strain, OUT_AMAT): the free-surface corrections come from
-// the per-edge maps a.fscG; the staged record is the two frames only
+// EDGE (half space): the free-surface corrections are left to per-edge work;
+// the staged record is the two frames only.  OUT_AMAT (strain): they come
+// from the per-edge maps a.fscG.  OUT_SUM: they are left out here, and
+// fsc_sum_kernel adds each edge's once.
 template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false, int MINB = 1,
           bool EDGE = false>
 __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 {
-    static_assert(!EDGE || (HS && STRAIN && !DISP && OUT == OUT_AMAT && !LIST), "edge maps: HS system matrix only");
+    static_assert(!EDGE || (HS && !LIST && !NEAR && ((OUT == OUT_AMAT && STRAIN && !DISP) || OUT == OUT_SUM)),
+                  "shared edges: HS system matrix or HS sums only");
+    constexpr bool EDGE_MAPS = EDGE && OUT == OUT_AMAT;
     extern __shared__ double smem[];
     constexpr int words = HS ? (EDGE ? kTriWordsImg : kTriWordsHS) : kTriWordsFS;
     const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
@@ -136,8 +140,8 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
     const bool active = i < a.M;
     // LIST: this thread's point (system row) and the full system's size
     const int64_t io = (LIST && a.obs_list && active) ? (int64_t)a.obs_list[i] : i;
-    const int64_t NS = (LIST || EDGE) ? a.Ntot : a.N;
-    const int64_t MD = (LIST || EDGE) ? a.Ntot : a.M;
+    const int64_t NS = (LIST || EDGE_MAPS) ? a.Ntot : a.N;
+    const int64_t MD = (LIST || EDGE_MAPS) ? a.Ntot : a.M;
     double X = 0.0, Y = 0.0, Z = 0.0;
     if (active) { X = a.X[io]; Y = a.Y[io]; Z = a.Z[io]; }
     const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
@@ -171,8 +175,10 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
         if (!active) continue;
         if (STRAIN) {
             double E[3][6];
-            if constexpr (EDGE)
+            if constexpr (EDGE_MAPS)
                 pair_strain_edges(t, X, Y, Z, a.fscG + i, a.M, 18 * a.M, a.side_edge + 3 * jt, E);
+            else if constexpr (EDGE)
+                pair_strain_fs_image(t, X, Y, Z, E);
             else
                 pair_strain<HS>(t, X, Y, Z, E);
             if (OUT == OUT_INF) {
@@ -201,7 +207,10 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
         }
         if (DISP) {
             double U[3][3];
-            pair_disp<HS>(t, X, Y, Z, U);
+            if constexpr (EDGE)
+                pair_disp_fs_image(t, X, Y, Z, U);
+            else
+                pair_disp<HS>(t, X, Y, Z, U);
             if (OUT == OUT_INF) {
 #pragma unroll
                 for (int m = 0; m < 3; ++m)
@@ -547,6 +556,102 @@ cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E,
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// Net Burgers vector of each mesh edge: the signed sum over the triangle sides
+// on it (edge_tris[edge_ptr[e] .. edge_ptr[e + 1]) = +-(triangle + 1), in
+// triangle order) of Dn Vn + Dss Vs + Dds Vd, then the edge's record for it.
+__global__ void edge_burgers_kernel(const double* __restrict__ pts, int64_t E, const int* __restrict__ edge_ptr,
+                                    const int* __restrict__ edge_tris, const TriDev* __restrict__ tri, double nu,
+                                    FscSide* __restrict__ out)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    double B[3] = {0.0, 0.0, 0.0};
+    for (int k = edge_ptr[e]; k < edge_ptr[e + 1]; ++k) {
+        const int c = edge_tris[k];
+        const TriDev& t = tri[(c > 0 ? c : -c) - 1];
+        const double sg = c > 0 ? 1.0 : -1.0;
+        const double slip[3] = {t.Dn, t.Dss, t.Dds};
+        const double* axes[3] = {t.real.Vn, t.real.Vs, t.real.Vd};
+        for (int m = 0; m < 3; ++m)
+            for (int i = 0; i < 3; ++i) B[i] = add_rn(B[i], sg * mul_rn(axes[m][i], slip[m]));
+    }
+    const double PA[3] = {pts[6 * e], pts[6 * e + 1], pts[6 * e + 2]};
+    const double PB[3] = {pts[6 * e + 3], pts[6 * e + 4], pts[6 * e + 5]};
+    build_side_burgers(PA, PB, B, nu, out[e]);
+}
+
+// partial[(blockIdx.y * 9 + f) M + i] = the free-surface strain (f 0-5) and
+// displacement (f 6-8) at point i of the edges of chunk blockIdx.y, summed in
+// edge order (each edge record staged in shared memory).
+template <bool STRAIN, bool DISP>
+__global__ void __launch_bounds__(kPairThreads, 1) fsc_sum_kernel(const FscSide* __restrict__ edges, int64_t E,
+                                                                int64_t echunk, const double* __restrict__ X,
+                                                                const double* __restrict__ Y,
+                                                                const double* __restrict__ Z, int64_t M,
+                                                                double* __restrict__ partial)
+{
+    extern __shared__ double smem[];
+    const FscSide& s = *reinterpret_cast<const FscSide*>(smem);
+    const int64_t i = (int64_t)blockIdx.x * kPairThreads + threadIdx.x;
+    const bool active = i < M;
+    double x = 0.0, y = 0.0, z = 0.0;
+    if (active) { x = X[i]; y = Y[i]; z = Z[i]; }
+    double Es[3][6] = {}, Us[3][3] = {};
+    const int64_t e0 = (int64_t)blockIdx.y * echunk;
+    const int64_t e1 = min(E, e0 + echunk);
+    for (int64_t e = e0; e < e1; ++e) {
+        __syncthreads();
+        const double* src = reinterpret_cast<const double*>(edges + e);
+        for (int w = threadIdx.x; w < kSideWords; w += kPairThreads) smem[w] = src[w];
+        __syncthreads();
+        if (!active || s.skip != 0.0) continue;
+        if (STRAIN) fsc_strain(s, x, y, z, 0.0, 0.0, 1.0, Es);
+        if (DISP) fsc_disp(s, x, y, z, 0.0, 0.0, 1.0, Us);
+    }
+    if (!active) return;
+    double* p = partial + (int64_t)blockIdx.y * 9 * M;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) p[k * M + i] = STRAIN ? Es[0][k] : 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p[(6 + c) * M + i] = DISP ? Us[0][c] : 0.0;
+}
+
+cudaError_t launch_td_sum_edges(PairArgs a, bool strain, bool disp, const double* edge_pts, int64_t E,
+                                const int* edge_ptr, const int* edge_tris, void* edge_rec, double nu, int64_t echunk,
+                                double* edge_partial, cudaStream_t st, int64_t* launches)
+{
+    if (a.M == 0 || a.N == 0 || !(strain || disp)) return cudaSuccess;
+    const size_t psmem = (size_t)kTriWordsImg * sizeof(double);
+    const size_t esmem = (size_t)kSideWords * sizeof(double);
+    const unsigned tiles = (unsigned)((a.M + kPairThreads - 1) / kPairThreads);
+    auto pairs = [&](auto kern) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3(tiles, (unsigned)((a.N + a.tri_chunk - 1) / a.tri_chunk)), kPairThreads, psmem, st>>>(a);
+        if (launches) ++*launches;
+        return cudaGetLastError();
+    };
+    auto sums = [&](auto kern) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3(tiles, (unsigned)((E + echunk - 1) / echunk)), kPairThreads, esmem, st>>>(
+            (const FscSide*)edge_rec, E, echunk, a.X, a.Y, a.Z, a.M, edge_partial);
+        if (launches) ++*launches;
+        return cudaGetLastError();
+    };
+    cudaError_t e = strain && disp ? pairs(td_pair_kernel<true, true, true, OUT_SUM, false, false, 1, true>)
+                    : strain       ? pairs(td_pair_kernel<true, true, false, OUT_SUM, false, false, 1, true>)
+                                   : pairs(td_pair_kernel<true, false, true, OUT_SUM, false, false, 1, true>);
+    if (e != cudaSuccess || E == 0) return e;
+    edge_burgers_kernel<<<(unsigned)((E + 127) / 128), 128, 0, st>>>(edge_pts, E, edge_ptr, edge_tris, a.tri, nu,
+                                                                      (FscSide*)edge_rec);
+    if (launches) ++*launches;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return strain && disp ? sums(fsc_sum_kernel<true, true>)
+           : strain       ? sums(fsc_sum_kernel<true, false>)
+                          : sums(fsc_sum_kernel<false, true>);
 }
 
 cudaError_t launch_splice_fixed(const double* trac, const double* disp, int64_t N, int64_t nfix, const int* fixrow,

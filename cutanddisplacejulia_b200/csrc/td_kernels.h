@@ -64,6 +64,17 @@ cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E,
                                   double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches);
 size_t edge_record_bytes();
 
+// Half-space sums (OUT_SUM) with the free-surface correction evaluated once
+// per mesh edge for the net Burgers vector of the triangle sides on it:
+// a.partial receives the real + image terms of each triangle chunk (as
+// launch_td_pairs), edge_partial the corrections of each chunk of echunk
+// edges (9 x a.M each).  edge_ptr / edge_tris list each edge's sides as
+// +-(triangle + 1), + for a side running the edge's way.  a.tri must hold the
+// records of launch_td_setup (with the triangles' slip).
+cudaError_t launch_td_sum_edges(PairArgs a, bool strain, bool disp, const double* edge_pts, int64_t E,
+                                const int* edge_ptr, const int* edge_tris, void* edge_rec, double nu, int64_t echunk,
+                                double* edge_partial, cudaStream_t st, int64_t* launches);
+
 // Mixed-precision system matrix: every pair in FP32 (far field), then the
 // pairs of every 128-point tile that has a point within the near radius of
 // the source centroid again in FP64.  near_factor: radius in mean edge lengths.

@@ -154,12 +154,15 @@ int cad_set_lu_block(cad_ctx* ctx, int nb);
  * preconditioned GMRES solvers): 1..63, 0 = the default 30.  Every cycle
  * starts from the FP64 residual b - A x.  No counterpart in the reference. */
 int cad_set_gmres_restart(cad_ctx* ctx, int m);
-/* Half-space system-matrix assembly (cad_assemble*, cad_slip_calculator*
- * with hs_flag 1, FP64 assembly): 1 (default) evaluates the free-surface
- * correction of each mesh edge once per collocation point and lets the
- * triangles that share the edge reuse it (with the sign of their side's
- * direction); 0 evaluates it per triangle side, as the reference does.
- * Same matrix to rounding.  No counterpart in the reference. */
+/* Half-space work on meshes whose triangles share edges (fewer edges than
+ * 0.9 x the triangle sides; other meshes always take the per-side path).
+ * 1 (default): the FP64 system matrix (cad_assemble*, cad_slip_calculator*
+ * with hs_flag 1) evaluates the free-surface correction of each mesh edge
+ * once per collocation point, and the triangles that share the edge reuse it
+ * with the sign of their side's direction; the summed evaluations
+ * (cad_td_sum_eval*) evaluate it once per edge for the net Burgers vector of
+ * the sides on it.  0: per triangle side, as the reference does.  Same
+ * results to rounding.  No counterpart in the reference. */
 int cad_set_shared_edges(cad_ctx* ctx, int enable);
 #define CAD_BATCH_GROUPED 0
 #define CAD_BATCH_LANES 1

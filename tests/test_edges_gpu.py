@@ -1,11 +1,15 @@
-"""GPU tests of the shared-edge half-space assembly (cad_set_shared_edges):
-the free-surface correction of each mesh edge is evaluated once per point and
-reused, with the sign of the side's direction, by the triangles that share
-the edge.  The matrix must agree with the per-side assembly (the reference's
-order of work, src/TDstressHS.jl) and with the oracle's sampled columns to the
-parity tolerance, on meshes that reach the free surface, with triangles whose
+"""GPU tests of the shared-edge half-space paths (cad_set_shared_edges).
+
+System matrix: the free-surface correction of each mesh edge is evaluated
+once per point and reused, with the sign of the side's direction, by the
+triangles that share the edge.  Sums (TD with Strains/Disps): each edge's
+correction is evaluated once for the net Burgers vector of the sides on it.
+Both must agree with the per-side evaluation (the reference's order of work,
+src/TD.jl:1831-1866 and 1222-1262) and with the oracle to the parity
+tolerance, on meshes that reach the free surface, with triangles whose
 orientation disagrees with their neighbours' (shared sides running the same
-way) and after the geometry changes (the cached edge table is rebuilt)."""
+way) and after the geometry changes (the cached edge table is rebuilt).
+Unconnected triangles (no shared edges) stay on the per-side kernels."""
 import numpy as np
 import pytest
 
@@ -78,3 +82,66 @@ def test_shared_edges_argument_check(cad):
     assert L.cad_set_shared_edges(ctx, 2) == _lib.CAD_ERR_ARG
     assert L.cad_set_shared_edges(ctx, -1) == _lib.CAD_ERR_ARG
     _lib.check(L.cad_set_shared_edges(ctx, 1), ctx)
+
+
+def _td_sum(cad, pts, P1, P2, P3, sl, shared, disp=1, strain=1):
+    from cutanddisplacejulia_b200 import _lib
+    L, ctx = _lib.load(), _lib.context(0)
+    _lib.check(L.cad_set_shared_edges(ctx, int(shared)), ctx)
+    try:
+        S, U = cad.TD(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, disp, strain, 1, cad.Strains(), cad.Disps())
+    finally:
+        _lib.check(L.cad_set_shared_edges(ctx, 1), ctx)
+    return np.stack(list(S)), np.stack(list(U))
+
+
+def _sum_case(seed, top_depth, ntri=300, m=500, flip_frac=0.0):
+    from cutanddisplacejulia_b200 import workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=seed, ntri=ntri, top_depth=top_depth)
+    zmax = max(P[:, 2].max() for P in (P1, P2, P3))
+    P1, P2, P3 = (P - [0.0, 0.0, zmax + top_depth] for P in (P1, P2, P3))
+    rng = np.random.default_rng(seed)
+    if flip_frac:
+        flip = rng.random(len(P1)) < flip_frac
+        P2, P3 = np.where(flip[:, None], P3, P2), np.where(flip[:, None], P2, P3)
+    n = len(P1)
+    mid = (P1 + P2 + P3) / 3.0
+    # smooth slip plus noise: interior edges carry small net Burgers vectors
+    sl = np.stack([1e-3 * np.cos(mid[:, 0] + k) * np.sin(2 * mid[:, 2] - k) for k in range(3)])
+    sl += rng.uniform(-1e-4, 1e-4, (3, n))
+    pts = np.column_stack([rng.uniform(-2.0, 2.0, m), rng.uniform(-1.5, 1.5, m), rng.uniform(-3.0, -0.02, m)])
+    return pts, (P1, P2, P3), sl
+
+
+@pytest.mark.parametrize("top_depth", [0.0, 0.3])
+def test_shared_edges_td_sum_matches_per_side_and_oracle(cad, oracle, top_depth):
+    pts, P, sl = _sum_case(21, top_depth)
+    S_e, U_e = _td_sum(cad, pts, *P, sl, True)
+    S_s, U_s = _td_sum(cad, pts, *P, sl, False)
+    assert_parity(S_e, S_s)
+    assert_parity(U_e, U_s)
+    So, Uo = oracle.td_sum_eval(*pts.T, *P, *sl, 0.25, 1.0, 1, 1, 1)
+    assert_parity(S_e, So)
+    assert_parity(U_e, Uo)
+
+
+def test_shared_edges_td_sum_flags_and_mixed_orientation(cad, oracle):
+    pts, P, sl = _sum_case(22, 0.1, ntri=240, m=300, flip_frac=0.3)
+    So, Uo = oracle.td_sum_eval(*pts.T, *P, *sl, 0.25, 1.0, 1, 1, 1)
+    S, U = _td_sum(cad, pts, *P, sl, True, disp=0, strain=1)
+    assert_parity(S, So)
+    assert not U.any()
+    S, U = _td_sum(cad, pts, *P, sl, True, disp=1, strain=0)
+    assert_parity(U, Uo)
+    assert not S.any()
+
+
+def test_unconnected_triangles_stay_per_side(cad):
+    from helpers import random_points, random_triangles
+    rng = np.random.default_rng(23)
+    P1, P2, P3 = random_triangles(rng, 30)
+    pts = random_points(rng, 200)
+    sl = rng.uniform(-1e-3, 1e-3, (3, 30))
+    S_e, U_e = _td_sum(cad, pts, P1, P2, P3, sl, True)
+    S_s, U_s = _td_sum(cad, pts, P1, P2, P3, sl, False)
+    assert np.array_equal(S_e, S_s) and np.array_equal(U_e, U_s)
