@@ -235,6 +235,32 @@ def reference_line(args, metric, value, unit, higher, ms, workload_desc, sample,
     return line
 
 
+def run_reference_tdsum(args, nthreads):
+    """Reference arm of the tdsum workload: the oracle's half-space sums of all
+    triangles at a seeded sample of 300 grid points per step (all host
+    threads), scaled to pair-evals/s."""
+    import numpy as np
+    from oracle import oracle as O
+    P1, P2, P3, sl, X, Y, Z = tdsum_case(args.ntri)
+    n, m = len(P1), X.size
+
+    def step(seed):
+        pick = np.random.default_rng(seed).choice(m, 300, replace=False)
+        t0 = time.perf_counter()
+        O.td_sum_eval(X[pick], Y[pick], Z[pick], P1, P2, P3, *sl, NU, G, 1, 1, 1)
+        return time.perf_counter() - t0
+    for w in range(args.warmup):
+        step(100 + w)
+    ts = [step(k) for k in range(args.steps)]
+    sec = sum(ts) / len(ts)
+    value = 300.0 * n / sec
+    return reference_line(args, WORKLOADS["tdsum"][0], value, UNIT, True, sec * 1e3 * m / 300.0,
+                          WORKLOADS["tdsum"][1] % (n, m, TDSUM_GRID, TDSUM_GRID),
+                          "oracle HS sums of all %d triangles at 300 seeded grid points per step (%d threads), "
+                          "%.2f s per sample; ms_per_step scaled to all %d points" % (n, nthreads, sec, m),
+                          nthreads)
+
+
 def run_reference_friction(args, nthreads):
     """Reference arm of the friction workload: the oracle's frictional solve
     (assembly, numpy inverse, numpy Fischer-Newton on the full 5N system) of
@@ -306,6 +332,9 @@ def run_reference(args, rank):
     if args.workload in ("friction", "batch"):
         fn = run_reference_friction if args.workload == "friction" else run_reference_batch
         print(json.dumps(fn(args, nthreads)), flush=True)
+        return
+    if args.workload == "tdsum":
+        print(json.dumps(run_reference_tdsum(args, nthreads)), flush=True)
         return
     if args.workload == "learned":
         print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement needs well over an hour per "
@@ -1399,7 +1428,7 @@ def run_tdsum(args, rank, world, local_rank):
         Sh, Uh = cad.TD(Xh, Yh, Zh, P1, P2, P3, *sl, NU, G, 1, 1, 1, cad.Strains(), cad.Disps())
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         O.build()
         nthreads = os.cpu_count() or 1
