@@ -437,9 +437,10 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         return CAD_OK;
     }
     EdgeTable et;
-    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges)
+    const bool edge_kind = (out_kind == OUT_AMAT && ctx->assembly != CAD_ASSEMBLY_MIXED) || out_kind == OUT_TRAC;
+    if (edge_kind && hs == 1 && ctx->shared_edges)
         if (int r = edge_table(ctx, P1, P2, P3, N, &et)) return r;
-    if (out_kind == OUT_AMAT && hs == 1 && ctx->shared_edges && edges_pay(et.E, N)) {
+    if (edge_kind && hs == 1 && ctx->shared_edges && edges_pay(et.E, N)) {
         // each mesh edge's free-surface map evaluated once, then read by the
         // (one or two) triangles that share the edge
         const int64_t E = et.E;
@@ -453,12 +454,12 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
         if (Mc > N) Mc = N;
         if (int r = ensure(ctx, S_EDGE_G, (size_t)Mc * per_point, &gmap)) return r;
         a.min_blocks = kEdgeMinBlocks;
-        if (ctx->tuner.mode != TUNE_OFF) {
+        if (ctx->tuner.mode != TUNE_OFF && out_kind == OUT_AMAT) {
             // triangles per block of the edge pair kernel, then its build
             // (resident blocks per SM); each candidate runs the whole path
             char key[96];
             auto run = [&](const PairArgs& t) {
-                return launch_assemble_edges(t, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream,
+                return launch_assemble_edges(t, out_kind, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream,
                                              &ctx->launches);
             };
             std::snprintf(key, sizeof key, "pair_amat_f64_hs1_edge_N%lld", (long long)tune_class(N));
@@ -475,7 +476,7 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
             });
         }
         CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-        CK(launch_assemble_edges(a, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
+        CK(launch_assemble_edges(a, out_kind, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
         CK(cudaEventRecord(ctx->ev[1], ctx->stream));
         ctx->timed[0] = true;
         return CAD_OK;

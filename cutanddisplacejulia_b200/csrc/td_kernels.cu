@@ -130,9 +130,10 @@ template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST
           bool EDGE = false>
 __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 {
-    static_assert(!EDGE || (HS && !LIST && !NEAR && ((OUT == OUT_AMAT && STRAIN && !DISP) || OUT == OUT_SUM)),
-                  "shared edges: HS system matrix or HS sums only");
-    constexpr bool EDGE_MAPS = EDGE && OUT == OUT_AMAT;
+    static_assert(!EDGE || (HS && !LIST && !NEAR &&
+                            (((OUT == OUT_AMAT || OUT == OUT_TRAC) && STRAIN && !DISP) || OUT == OUT_SUM)),
+                  "shared edges: HS system matrix, traction fields or sums only");
+    constexpr bool EDGE_MAPS = EDGE && (OUT == OUT_AMAT || OUT == OUT_TRAC);
     extern __shared__ double smem[];
     constexpr int words = HS ? (EDGE ? kTriWordsImg : kTriWordsHS) : kTriWordsFS;
     const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
@@ -146,7 +147,10 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
     if (active) { X = a.X[io]; Y = a.Y[io]; Z = a.Z[io]; }
     const int64_t j0 = (int64_t)blockIdx.y * a.tri_chunk;
     const int64_t j1 = min(a.N, j0 + a.tri_chunk);
-    const int64_t MN = a.M * a.N;
+    // row stride of the M x N output fields: a block of an Ntot-point system
+    // with the edge maps
+    const int64_t MR = EDGE_MAPS ? MD : a.M;
+    const int64_t MN = MR * a.N;
     double sumE[6] = {0, 0, 0, 0, 0, 0}, sumU[3] = {0, 0, 0};
     double n[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, ds[3] = {0, 0, 0};
     if ((OUT == OUT_TRAC || OUT == OUT_AMAT) && active) {
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
                     strain_to_traction(E[m], a.lambda, 2.0 * a.G, n, ss, ds, tr);
                     if (OUT == OUT_TRAC) {
 #pragma unroll
-                        for (int r = 0; r < 3; ++r) a.trac[(3 * m + r) * MN + i + a.M * j] = tr[r];
+                        for (int r = 0; r < 3; ++r) a.trac[(3 * m + r) * MN + i + MR * j] = tr[r];
                     } else {
 #pragma unroll
                         for (int r = 0; r < 3; ++r)
@@ -511,9 +515,10 @@ __global__ void __launch_bounds__(kPairThreads, 1) fsc_edge_kernel(const FscSide
 
 size_t edge_record_bytes() { return sizeof(FscSide); }
 
-cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E, const int* side_edge, void* edge_rec,
-                                  double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches)
+cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_pts, int64_t E, const int* side_edge,
+                                  void* edge_rec, double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches)
 {
+    if (out_kind != OUT_AMAT && out_kind != OUT_TRAC) return cudaErrorInvalidValue;
     if (a.M == 0 || a.N == 0) return cudaSuccess;
     if (E > 0) {
         edge_setup_kernel<<<(unsigned)((E + 127) / 128), 128, 0, st>>>(edge_pts, E, nu, (FscSide*)edge_rec);
@@ -523,8 +528,11 @@ cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E,
     // a.min_blocks 3: three resident blocks per SM (168 registers, 308 B of
     // spills), 69.8 ms against 73.9 ms with the full register file (1) at
     // 10 000 triangles
-    auto pk = a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>
-                                : td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>;
+    auto pk = out_kind == OUT_TRAC
+                  ? (a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_TRAC, false, false, 1, true>
+                                       : td_pair_kernel<true, true, false, OUT_TRAC, false, false, 3, true>)
+                  : (a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>
+                                       : td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>);
     const size_t psmem = (size_t)kTriWordsImg * sizeof(double);
     const size_t esmem = (size_t)kSideWords * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
@@ -546,7 +554,8 @@ cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E,
         b.Y = a.Y + c0;
         b.Z = a.Z + c0;
         b.dirs = a.dirs + c0;
-        b.A = a.A + c0;
+        b.A = a.A ? a.A + c0 : nullptr;
+        b.trac = a.trac ? a.trac + c0 : nullptr;
         b.M = mc;
         b.Ntot = a.N;
         b.fscG = G;

@@ -48,20 +48,23 @@ struct PairArgs {
     // half-space system matrix with shared-edge free-surface maps: the maps
     // of this launch's points (18 x M per edge, fsc_edge_kernel) and each
     // triangle's three side codes (+-(edge + 1), 0: none); rows are then a
-    // block of an Ntot-point system (X, Y, Z, dirs and A start at the block)
+    // block of an Ntot-point system (X, Y, Z, dirs and A or trac start at the
+    // block; the output fields keep the system's row stride)
     const double* fscG = nullptr;
     const int* side_edge = nullptr;
 };
 
-// Half-space system matrix (OUT_AMAT, FP64) with the free-surface correction
-// evaluated once per mesh edge: edge_pts holds E edges (PA, PB: 6 doubles
+// Half-space system matrix (out_kind OUT_AMAT) or traction fields (OUT_TRAC),
+// FP64, with the free-surface correction evaluated once per mesh edge at the
+// collocation points: edge_pts holds E edges (PA, PB: 6 doubles
 // each), side_edge each triangle's three side codes; edge_rec
 // (edge_record_bytes() x E) and G (18 x Mc x E doubles) are workspaces; the
 // points are processed in blocks of Mc.  a.M == a.N (a square system).
 // a.min_blocks selects the pair kernel's build: 1 (the full register file)
 // or anything else for three resident blocks per SM (kEdgeMinBlocks).
-cudaError_t launch_assemble_edges(PairArgs a, const double* edge_pts, int64_t E, const int* side_edge, void* edge_rec,
-                                  double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches);
+cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_pts, int64_t E, const int* side_edge,
+                                  void* edge_rec, double* G, int64_t Mc, double nu, cudaStream_t st,
+                                  int64_t* launches);
 size_t edge_record_bytes();
 
 // Half-space sums (OUT_SUM) with the free-surface correction evaluated once

@@ -145,3 +145,22 @@ def test_unconnected_triangles_stay_per_side(cad):
     S_e, U_e = _td_sum(cad, pts, P1, P2, P3, sl, True)
     S_s, U_s = _td_sum(cad, pts, P1, P2, P3, sl, False)
     assert np.array_equal(S_e, S_s) and np.array_equal(U_e, U_s)
+
+
+def test_shared_edges_traction_fields_match_per_side(cad):
+    from cutanddisplacejulia_b200 import _lib, workloads
+    P1, P2, P3 = workloads.dipping_rect(seed=13, ntri=500, top_depth=0.1)
+    nrm, mid = cad.CreateFaceNormalAndMidPoint(P1, P2, P3)
+    _, _, lam, nu, G = cad.ElasticConstantsCheck(1.0, 0.25)
+    n = len(P1)
+    L, ctx = _lib.load(), _lib.context(0)
+    out = []
+    for shared in (1, 0):
+        _lib.check(L.cad_set_shared_edges(ctx, shared), ctx)
+        try:
+            T = cad.CalculateInfluenceMatrices3D(nrm, mid, P1, P2, P3, nu, G, lam, np.zeros(n), 1, n)
+        finally:
+            _lib.check(L.cad_set_shared_edges(ctx, 1), ctx)
+        out.append(np.stack(list(T)))
+    assert_parity(out[0], out[1])
+    assert rel_inf_err(out[0], out[1]) < 1e-13
