@@ -156,9 +156,10 @@ int cad_set_lu_block(cad_ctx* ctx, int nb);
 int cad_set_gmres_restart(cad_ctx* ctx, int m);
 /* Half-space work on meshes whose triangles share edges (fewer edges than
  * 0.9 x the triangle sides; other meshes always take the per-side path).
- * 1 (default): the FP64 system matrix (cad_assemble*, cad_slip_calculator*
- * with hs_flag 1) evaluates the free-surface correction of each mesh edge
- * once per collocation point, and the triangles that share the edge reuse it
+ * 1 (default): the FP64 system matrix and traction influence fields
+ * (cad_assemble*, cad_slip_calculator*, cad_influence_traction with hs_flag
+ * 1) evaluate the free-surface correction of each mesh edge once per
+ * collocation point, and the triangles that share the edge reuse it
  * with the sign of their side's direction; the summed evaluations
  * (cad_td_sum_eval*) evaluate it once per edge for the net Burgers vector of
  * the sides on it.  0: per triangle side, as the reference does.  Same
