@@ -362,9 +362,28 @@ int td_device(cad_ctx* ctx, const double* X, const double* Y, const double* Z, i
     a.strain = strain_out; a.disp = disp_out;
     const int64_t nchunk = (N + a.tri_chunk - 1) / a.tri_chunk;
     EdgeTable et;
-    if (out_kind == OUT_SUM && hs == 1 && ctx->shared_edges)
+    const bool edge_kind = (out_kind == OUT_SUM || out_kind == OUT_INF) && hs == 1 && ctx->shared_edges &&
+                           (strain == 1 || disp == 1);
+    if (edge_kind)
         if (int r = edge_table(ctx, P1, P2, P3, N, &et)) return r;
-    if (out_kind == OUT_SUM && hs == 1 && ctx->shared_edges && edges_pay(et.E, N)) {
+    if (edge_kind && out_kind == OUT_INF && edges_pay(et.E, N)) {
+        // per-edge free-surface maps at the points (strain 18, displacement
+        // 9 values), read by the triangles that share each edge
+        void *rec, *gmap;
+        if (int r = ensure(ctx, S_EDGE_REC, (size_t)et.E * edge_record_bytes(), &rec)) return r;
+        const int64_t per_point = (18 * (strain == 1) + 9 * (disp == 1)) * et.E * (int64_t)sizeof(double);
+        int64_t Mc = (int64_t)(kEdgeMapBytes / per_point) / kPairThreads * kPairThreads;
+        if (Mc < kPairThreads) Mc = kPairThreads;
+        if (Mc > M) Mc = M;
+        if (int r = ensure(ctx, S_EDGE_G, (size_t)Mc * per_point, &gmap)) return r;
+        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        CK(launch_assemble_edges(a, OUT_INF, strain == 1, disp == 1, et.pts, et.E, et.code, rec, (double*)gmap, Mc,
+                                 nu, ctx->stream, &ctx->launches));
+        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        ctx->timed[0] = true;
+        return CAD_OK;
+    }
+    if (edge_kind && out_kind == OUT_SUM && edges_pay(et.E, N)) {
         // real + image terms per triangle chunk, then each mesh edge's
         // free-surface correction once, for the net Burgers vector of the
         // sides on it; all partials summed in one fixed order
@@ -459,7 +478,7 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
             // (resident blocks per SM); each candidate runs the whole path
             char key[96];
             auto run = [&](const PairArgs& t) {
-                return launch_assemble_edges(t, out_kind, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream,
+                return launch_assemble_edges(t, out_kind, true, false, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream,
                                              &ctx->launches);
             };
             std::snprintf(key, sizeof key, "pair_amat_f64_hs1_edge_N%lld", (long long)tune_class(N));
@@ -476,7 +495,7 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
             });
         }
         CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-        CK(launch_assemble_edges(a, out_kind, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
+        CK(launch_assemble_edges(a, out_kind, true, false, pts, E, codes, rec, (double*)gmap, Mc, nu, ctx->stream, &ctx->launches));
         CK(cudaEventRecord(ctx->ev[1], ctx->stream));
         ctx->timed[0] = true;
         return CAD_OK;

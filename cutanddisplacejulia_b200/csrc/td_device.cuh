@@ -622,6 +622,51 @@ CAD_HD void fsc_disp(const FscSideT<R>& s, double X, double Y, double Z, R Dss, 
     }
 }
 
+// The free-surface displacement of side s at (X, Y, Z) for a unit Burgers
+// vector along EFCS axis j, without the factor 1 / (4 pi (1 - nu)):
+// Gu[j][c] = sum_d ey_c[d] sum_g ey_j[g] (uB - uA)[3 d + g] (fsc_disp with
+// cs = ey_j).  As for the strain map, the reversed side's map is the
+// negative of this one.
+template <typename R>
+CAD_HD void fsc_disp_map(const FscSideT<R>& s, double X, double Y, double Z, R Gu[3][3])
+{
+    R x, y, z;
+    to_adcs(s, X, Y, Z, x, y, z);
+    const int c = mul_rn(s.beta, x) >= 0.0 ? 1 : 0;
+    R uA[9], uB[9];
+    ang_dis_disp_fsc(s.kd[c][0], x, y, z, uA);
+    ang_dis_disp_fsc(s.kd[c][1], x - s.y1B, y - s.y2B, z - s.y3B, uB);
+    const R* ey[3] = {s.ey1, s.ey2, s.ey3};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        R u[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            u[d] = ey[j][0] * (uB[3 * d] - uA[3 * d]) + ey[j][1] * (uB[3 * d + 1] - uA[3 * d + 1]) +
+                   ey[j][2] * (uB[3 * d + 2] - uA[3 * d + 2]);
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) Gu[j][cc] = ey[cc][0] * u[0] + ey[cc][1] * u[1] + ey[cc][2] * u[2];
+    }
+}
+
+// U[m] += sign * 2 K8 * (the map Gu applied to the EFCS Burgers vector of
+// unit mode m of the triangle with frame `real`), for the modes with
+// non-zero slip (2 K8 = 1 / (4 pi (1 - nu))).
+template <typename R>
+CAD_HD void fsc_apply_disp_map(const R Gu[3][3], R sign, const FrameT<R>& real, R Dss, R Dds, R Dn, R K8, R U[3][3])
+{
+    const R slip[3] = {Dn, Dss, Dds};
+    const R* axes[3] = {real.Vn, real.Vs, real.Vd};
+    const R f = sign * (K8 + K8);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!(slip[m] != 0.0)) continue;
+        const R w0 = axes[m][0] * slip[m], w1 = axes[m][1] * slip[m], w2 = axes[m][2] * slip[m];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) U[m][c] += f * (w0 * Gu[0][c] + w1 * Gu[1][c] + w2 * Gu[2][c]);
+    }
+}
+
 // -------------------------------------------------------- triangle setup
 // The per-triangle setup uses unfused arithmetic throughout: it is negligible
 // work, and the half-space terms of the two ends of a side cancel far from the
@@ -834,6 +879,30 @@ CAD_HD void pair_disp_fs_image(const TriDev& t, double X, double Y, double Z, do
 #pragma unroll
         for (int c = 0; c < 3; ++c) U[m][c] = 0.0;
     disp_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+    disp_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+}
+
+// Half-space displacement with the free-surface corrections of the triangle's
+// sides read from per-edge maps (fsc_disp_map), addressed as in
+// pair_strain_edges.
+CAD_HD void pair_disp_edges(const TriDev& t, double X, double Y, double Z, const double* G, int64_t gq, int64_t ge,
+                            const int* code, double U[3][3])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) U[m][c] = 0.0;
+    disp_fs<false>(t.real, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
+#pragma unroll 1
+    for (int sd = 0; sd < 3; ++sd) {
+        const int c = code[sd];
+        if (c == 0) continue;
+        const int64_t e = (int64_t)(c > 0 ? c : -c) - 1;
+        double Gu[3][3];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Gu[q / 3][q % 3] = G[e * ge + q * gq];
+        fsc_apply_disp_map(Gu, c > 0 ? 1.0 : -1.0, t.real, t.Dss, t.Dds, t.Dn, t.K8, U);
+    }
     disp_fs<true>(t.image, X, Y, Z, t.Dss, t.Dds, t.Dn, t.K8, U);
 }
 

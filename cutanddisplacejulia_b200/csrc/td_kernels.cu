@@ -131,9 +131,12 @@ template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST
 __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 {
     static_assert(!EDGE || (HS && !LIST && !NEAR &&
-                            (((OUT == OUT_AMAT || OUT == OUT_TRAC) && STRAIN && !DISP) || OUT == OUT_SUM)),
-                  "shared edges: HS system matrix, traction fields or sums only");
-    constexpr bool EDGE_MAPS = EDGE && (OUT == OUT_AMAT || OUT == OUT_TRAC);
+                            (((OUT == OUT_AMAT || OUT == OUT_TRAC) && STRAIN && !DISP) || OUT == OUT_SUM ||
+                             OUT == OUT_INF)),
+                  "shared edges: HS system matrix, traction or influence fields, or sums only");
+    constexpr bool EDGE_MAPS = EDGE && OUT != OUT_SUM;
+    // values per (edge, point) in the maps: strain 18, then displacement 9
+    constexpr int64_t kQ = (STRAIN ? 18 : 0) + (DISP ? 9 : 0);
     extern __shared__ double smem[];
     constexpr int words = HS ? (EDGE ? kTriWordsImg : kTriWordsHS) : kTriWordsFS;
     const TriDev& t = *reinterpret_cast<const TriDev*>(smem);
@@ -141,7 +144,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
     const bool active = i < a.M;
     // LIST: this thread's point (system row) and the full system's size
     const int64_t io = (LIST && a.obs_list && active) ? (int64_t)a.obs_list[i] : i;
-    const int64_t NS = (LIST || EDGE_MAPS) ? a.Ntot : a.N;
+    const int64_t NS = LIST ? a.Ntot : a.N;
     const int64_t MD = (LIST || EDGE_MAPS) ? a.Ntot : a.M;
     double X = 0.0, Y = 0.0, Z = 0.0;
     if (active) { X = a.X[io]; Y = a.Y[io]; Z = a.Z[io]; }
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
         if (STRAIN) {
             double E[3][6];
             if constexpr (EDGE_MAPS)
-                pair_strain_edges(t, X, Y, Z, a.fscG + i, a.M, 18 * a.M, a.side_edge + 3 * jt, E);
+                pair_strain_edges(t, X, Y, Z, a.fscG + i, a.M, kQ * a.M, a.side_edge + 3 * jt, E);
             else if constexpr (EDGE)
                 pair_strain_fs_image(t, X, Y, Z, E);
             else
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 #pragma unroll
                 for (int m = 0; m < 3; ++m)
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) a.strain[(6 * m + k) * MN + i + a.M * j] = E[m][k];
+                    for (int k = 0; k < 6; ++k) a.strain[(6 * m + k) * MN + i + MR * j] = E[m][k];
             } else if (OUT == OUT_SUM) {
 #pragma unroll
                 for (int k = 0; k < 6; ++k) sumE[k] += (E[0][k] + E[1][k]) + E[2][k];
@@ -211,7 +214,10 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
         }
         if (DISP) {
             double U[3][3];
-            if constexpr (EDGE)
+            if constexpr (EDGE_MAPS)
+                pair_disp_edges(t, X, Y, Z, a.fscG + i + (STRAIN ? 18 : 0) * a.M, a.M, kQ * a.M, a.side_edge + 3 * jt,
+                                U);
+            else if constexpr (EDGE)
                 pair_disp_fs_image(t, X, Y, Z, U);
             else
                 pair_disp<HS>(t, X, Y, Z, U);
@@ -219,7 +225,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
 #pragma unroll
                 for (int m = 0; m < 3; ++m)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) a.disp[(3 * m + c) * MN + i + a.M * j] = U[m][c];
+                    for (int c = 0; c < 3; ++c) a.disp[(3 * m + c) * MN + i + MR * j] = U[m][c];
             } else if (OUT == OUT_SUM) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) sumU[c] += (U[0][c] + U[1][c]) + U[2][c];
@@ -478,9 +484,12 @@ __global__ void edge_setup_kernel(const double* __restrict__ pts, int64_t E, dou
     build_side_geom(PA, PB, nu, out[e]);
 }
 
-// G[(e * 18 + q) M + i] = value q of edge e's free-surface map at point i
-// (fsc_strain_map; zero for an edge the beta test drops).  Block = 128 points
-// x a chunk of edges, each edge record staged in shared memory.
+// G[(e * Q + q) M + i] = value q of edge e's free-surface maps at point i:
+// the strain map (fsc_strain_map, 18 values) when STRAIN, then the
+// displacement map (fsc_disp_map, 9) when DISP; zero for an edge the beta test
+// drops.  Block = 128 points x a chunk of edges, each edge record staged in
+// shared memory.
+template <bool STRAIN, bool DISP>
 __global__ void __launch_bounds__(kPairThreads, 1) fsc_edge_kernel(const FscSide* __restrict__ edges, int64_t E,
                                                                  int64_t echunk, const double* __restrict__ X,
                                                                  const double* __restrict__ Y,
@@ -501,24 +510,45 @@ __global__ void __launch_bounds__(kPairThreads, 1) fsc_edge_kernel(const FscSide
         for (int w = threadIdx.x; w < kSideWords; w += kPairThreads) smem[w] = src[w];
         __syncthreads();
         if (!active) continue;
-        double Gm[3][6];
-        if (s.skip != 0.0) {
+        constexpr int64_t Q = (STRAIN ? 18 : 0) + (DISP ? 9 : 0);
+        if (STRAIN) {
+            double Gm[3][6];
+            if (s.skip != 0.0) {
 #pragma unroll
-            for (int q = 0; q < 18; ++q) Gm[q / 6][q % 6] = 0.0;
-        } else {
-            fsc_strain_map(s, x, y, z, Gm);
+                for (int q = 0; q < 18; ++q) Gm[q / 6][q % 6] = 0.0;
+            } else {
+                fsc_strain_map(s, x, y, z, Gm);
+            }
+#pragma unroll
+            for (int q = 0; q < 18; ++q) G[(e * Q + q) * M + i] = Gm[q / 6][q % 6];
         }
+        if (DISP) {
+            double Gu[3][3];
+            if (s.skip != 0.0) {
 #pragma unroll
-        for (int q = 0; q < 18; ++q) G[(e * 18 + q) * M + i] = Gm[q / 6][q % 6];
+                for (int q = 0; q < 9; ++q) Gu[q / 3][q % 3] = 0.0;
+            } else {
+                fsc_disp_map(s, x, y, z, Gu);
+            }
+            constexpr int64_t q0 = STRAIN ? 18 : 0;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) G[(e * Q + q0 + q) * M + i] = Gu[q / 3][q % 3];
+        }
     }
 }
 
 size_t edge_record_bytes() { return sizeof(FscSide); }
 
-cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_pts, int64_t E, const int* side_edge,
-                                  void* edge_rec, double* G, int64_t Mc, double nu, cudaStream_t st, int64_t* launches)
+cudaError_t launch_assemble_edges(PairArgs a, int out_kind, bool strain, bool disp, const double* edge_pts,
+                                  int64_t E, const int* side_edge, void* edge_rec, double* G, int64_t Mc, double nu,
+                                  cudaStream_t st, int64_t* launches)
 {
-    if (out_kind != OUT_AMAT && out_kind != OUT_TRAC) return cudaErrorInvalidValue;
+    if (out_kind == OUT_AMAT || out_kind == OUT_TRAC) {
+        strain = true;
+        disp = false;
+    } else if (out_kind != OUT_INF || !(strain || disp)) {
+        return cudaErrorInvalidValue;
+    }
     if (a.M == 0 || a.N == 0) return cudaSuccess;
     if (E > 0) {
         edge_setup_kernel<<<(unsigned)((E + 127) / 128), 128, 0, st>>>(edge_pts, E, nu, (FscSide*)edge_rec);
@@ -527,24 +557,38 @@ cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_p
     }
     // a.min_blocks 3: three resident blocks per SM (168 registers, 308 B of
     // spills), 69.8 ms against 73.9 ms with the full register file (1) at
-    // 10 000 triangles
-    auto pk = out_kind == OUT_TRAC
-                  ? (a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_TRAC, false, false, 1, true>
-                                       : td_pair_kernel<true, true, false, OUT_TRAC, false, false, 3, true>)
-                  : (a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>
-                                       : td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>);
+    // 10 000 triangles (system matrix; the influence fields keep 1)
+    using PairKernel = void (*)(PairArgs);
+    using EdgeKernel = void (*)(const FscSide*, int64_t, int64_t, const double*, const double*, const double*,
+                                int64_t, double*);
+    PairKernel pk;
+    EdgeKernel ek = fsc_edge_kernel<true, false>;
+    if (out_kind == OUT_TRAC) {
+        pk = a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_TRAC, false, false, 1, true>
+                               : td_pair_kernel<true, true, false, OUT_TRAC, false, false, 3, true>;
+    } else if (out_kind == OUT_AMAT) {
+        pk = a.min_blocks == 1 ? td_pair_kernel<true, true, false, OUT_AMAT, false, false, 1, true>
+                               : td_pair_kernel<true, true, false, OUT_AMAT, false, false, 3, true>;
+    } else if (strain && disp) {
+        pk = td_pair_kernel<true, true, true, OUT_INF, false, false, 1, true>;
+        ek = fsc_edge_kernel<true, true>;
+    } else if (strain) {
+        pk = td_pair_kernel<true, true, false, OUT_INF, false, false, 1, true>;
+    } else {
+        pk = td_pair_kernel<true, false, true, OUT_INF, false, false, 1, true>;
+        ek = fsc_edge_kernel<false, true>;
+    }
     const size_t psmem = (size_t)kTriWordsImg * sizeof(double);
     const size_t esmem = (size_t)kSideWords * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fsc_edge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(ek, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
     if (e != cudaSuccess) return e;
     const int64_t echunk = 32;
     for (int64_t c0 = 0; c0 < a.M; c0 += Mc) {
         const int64_t mc = a.M - c0 < Mc ? a.M - c0 : Mc;
         const unsigned tiles = (unsigned)((mc + kPairThreads - 1) / kPairThreads);
         if (E > 0) {
-            fsc_edge_kernel<<<dim3(tiles, (unsigned)((E + echunk - 1) / echunk)), kPairThreads, esmem, st>>>(
+            ek<<<dim3(tiles, (unsigned)((E + echunk - 1) / echunk)), kPairThreads, esmem, st>>>(
                 (const FscSide*)edge_rec, E, echunk, a.X + c0, a.Y + c0, a.Z + c0, mc, G);
             if (launches) ++*launches;
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -553,11 +597,13 @@ cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_p
         b.X = a.X + c0;
         b.Y = a.Y + c0;
         b.Z = a.Z + c0;
-        b.dirs = a.dirs + c0;
+        b.dirs = a.dirs ? a.dirs + c0 : nullptr;
         b.A = a.A ? a.A + c0 : nullptr;
         b.trac = a.trac ? a.trac + c0 : nullptr;
+        b.strain = a.strain ? a.strain + c0 : nullptr;
+        b.disp = a.disp ? a.disp + c0 : nullptr;
         b.M = mc;
-        b.Ntot = a.N;
+        b.Ntot = a.M;   // the output fields' row stride
         b.fscG = G;
         b.side_edge = side_edge;
         pk<<<dim3(tiles, (unsigned)((a.N + a.tri_chunk - 1) / a.tri_chunk)), kPairThreads, psmem, st>>>(b);

@@ -54,17 +54,19 @@ struct PairArgs {
     const int* side_edge = nullptr;
 };
 
-// Half-space system matrix (out_kind OUT_AMAT) or traction fields (OUT_TRAC),
-// FP64, with the free-surface correction evaluated once per mesh edge at the
-// collocation points: edge_pts holds E edges (PA, PB: 6 doubles
-// each), side_edge each triangle's three side codes; edge_rec
-// (edge_record_bytes() x E) and G (18 x Mc x E doubles) are workspaces; the
-// points are processed in blocks of Mc.  a.M == a.N (a square system).
-// a.min_blocks selects the pair kernel's build: 1 (the full register file)
-// or anything else for three resident blocks per SM (kEdgeMinBlocks).
-cudaError_t launch_assemble_edges(PairArgs a, int out_kind, const double* edge_pts, int64_t E, const int* side_edge,
-                                  void* edge_rec, double* G, int64_t Mc, double nu, cudaStream_t st,
-                                  int64_t* launches);
+// Half-space system matrix (out_kind OUT_AMAT), traction fields (OUT_TRAC) or
+// influence fields (OUT_INF, strain and / or displacement), FP64, with the
+// free-surface correction evaluated once per mesh edge at each point:
+// edge_pts holds E edges (PA, PB: 6 doubles each), side_edge each triangle's
+// three side codes; edge_rec (edge_record_bytes() x E) and G (Q x Mc x E
+// doubles, Q = 18 for strain + 9 for displacement) are workspaces; the points
+// are processed in blocks of Mc.  OUT_AMAT / OUT_TRAC: a.M == a.N (the
+// collocation points).  a.min_blocks selects the system-matrix and traction
+// kernels' build: 1 (the full register file) or anything else for three
+// resident blocks per SM (kEdgeMinBlocks).
+cudaError_t launch_assemble_edges(PairArgs a, int out_kind, bool strain, bool disp, const double* edge_pts,
+                                  int64_t E, const int* side_edge, void* edge_rec, double* G, int64_t Mc, double nu,
+                                  cudaStream_t st, int64_t* launches);
 size_t edge_record_bytes();
 
 // Half-space sums (OUT_SUM) with the free-surface correction evaluated once

@@ -164,3 +164,31 @@ def test_shared_edges_traction_fields_match_per_side(cad):
         out.append(np.stack(list(T)))
     assert_parity(out[0], out[1])
     assert rel_inf_err(out[0], out[1]) < 1e-13
+
+
+def _td_inf(cad, pts, P1, P2, P3, sl, shared, disp=1, strain=1):
+    from cutanddisplacejulia_b200 import _lib
+    L, ctx = _lib.load(), _lib.context(0)
+    _lib.check(L.cad_set_shared_edges(ctx, int(shared)), ctx)
+    try:
+        S, U = cad.TD(*pts.T, P1, P2, P3, *sl, 0.25, 1.0, disp, strain, 1)
+    finally:
+        _lib.check(L.cad_set_shared_edges(ctx, 1), ctx)
+    return (np.stack(list(S)) if strain else None), (np.stack(list(U)) if disp else None)
+
+
+@pytest.mark.parametrize("top_depth", [0.0, 0.2])
+def test_shared_edges_influence_fields_match_per_side_and_oracle(cad, oracle, top_depth):
+    pts, P, sl = _sum_case(24, top_depth, ntri=260, m=240, flip_frac=0.2)
+    S_e, U_e = _td_inf(cad, pts, *P, sl, True)
+    S_s, U_s = _td_inf(cad, pts, *P, sl, False)
+    assert_parity(S_e, S_s)
+    assert_parity(U_e, U_s)
+    So, Uo = oracle.td_inf(*pts.T, *P, *sl, 0.25, 1.0, 1, 1, 1)
+    assert_parity(S_e, So)
+    assert_parity(U_e, Uo)
+    # one output at a time
+    S1, _ = _td_inf(cad, pts, *P, sl, True, disp=0, strain=1)
+    _, U1 = _td_inf(cad, pts, *P, sl, True, disp=1, strain=0)
+    assert_parity(S1, So)
+    assert_parity(U1, Uo)
