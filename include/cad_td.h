@@ -160,7 +160,8 @@ int cad_set_gmres_restart(cad_ctx* ctx, int m);
  * (cad_assemble*, cad_slip_calculator*, cad_influence_traction with hs_flag
  * 1) evaluate the free-surface correction of each mesh edge once per
  * collocation point, and the triangles that share the edge reuse it
- * with the sign of their side's direction; the summed evaluations
+ * with the sign of their side's direction, and so do the influence fields
+ * (cad_td_inf*, strain and displacement maps per edge); the summed evaluations
  * (cad_td_sum_eval*) evaluate it once per edge for the net Burgers vector of
  * the sides on it.  0: per triangle side, as the reference does.  Same
  * results to rounding.  No counterpart in the reference. */
