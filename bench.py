@@ -1574,6 +1574,9 @@ def main():
     ap.add_argument("--train-max", type=int, default=2000, help="largest training mesh (triangles)")
     ap.add_argument("--train-steps", type=int, default=3000, help="training steps of the learned workload")
     ap.add_argument("--max-iter", type=int, default=3000, help="GMRES iteration cap of the learned workload")
+    ap.add_argument("--shared-edges", type=int, choices=[0, 1], default=1,
+                    help="half-space free-surface corrections once per mesh edge (1, the library default) or per "
+                         "triangle side (0, the reference's order of work); cad_set_shared_edges")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1589,6 +1592,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    if args.shared_edges != 1:
+        from cutanddisplacejulia_b200 import _lib
+        ctx = _lib.context(local_rank)
+        _lib.check(_lib.load().cad_set_shared_edges(ctx, args.shared_edges), ctx)
     try:
         if args.workload == "batch":
             run_batch(args, rank, world, local_rank)
