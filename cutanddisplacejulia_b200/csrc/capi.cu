@@ -112,8 +112,6 @@ struct cad_ctx {
     std::vector<CUtensorMap> gmaps_host;   // tensor maps of the grouped batch's FP32 systems
     cudaStream_t leaf_aux[kLeafAux] = {};  // grouped leaves of different cluster sizes, side by side
     cudaEvent_t side_fork = nullptr, side_join = nullptr;   // work forked onto the side stream
-    double* gm_pin = nullptr;                 // pinned Hessenberg columns of the pipelined GMRES loop
-    cudaEvent_t gm_ev[2] = {nullptr, nullptr};
     Tuner tuner;                           // cad_set_autotune
     int shared_edges = 1;                  // cad_set_shared_edges
     // mesh-edge table of the last half-space assembly: the vertices it was
@@ -534,18 +532,6 @@ int assemble_device(cad_ctx* ctx, const double* normals, const double* mid, cons
 
 constexpr int kIrMaxIter = 20; // refinement sweeps of a multi-column mixed solve before GMRES takes over
 
-// The pipelined GMRES loop's pinned columns and events (created on first use).
-int gmres_pipe(cad_ctx* ctx, GmresArgs& g)
-{
-    if (!ctx->gm_pin) CK(cudaMallocHost(&ctx->gm_pin, 2 * (kMaxBasis + 1) * sizeof(double)));
-    for (auto& e : ctx->gm_ev)
-        if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    g.hpin = ctx->gm_pin;
-    g.hev[0] = ctx->gm_ev[0];
-    g.hev[1] = ctx->gm_ev[1];
-    return CAD_OK;
-}
-
 int read_info(cad_ctx* ctx, int* info);
 
 // FP32/TF32 LU + FP64 GMRES: B := A^-1 B, A left unchanged.  Sets *info from
@@ -636,7 +622,6 @@ int solve_mixed_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, do
         g.b = B + c * ldb;
         g.x = X ? X + c * n : (double*)work;
         GmresResult res{};
-        if (int r = gmres_pipe(ctx, g)) return r;
         const int st = gmres_ir_solve(g, &res);
         if (st == GMRES_TIMEOUT) return fail(ctx, CAD_ERR_TIMEOUT, "mixed solve: a triangular-solve wait ran out");
         if (st == GMRES_CUDA_ERROR)
@@ -726,7 +711,6 @@ int solve_spai_device(cad_ctx* ctx, int64_t n, const double* A, int64_t lda, dou
         g.b = B + c * ldb;
         g.x = (double*)work;
         GmresResult res{};
-        if (int r = gmres_pipe(ctx, g)) return r;
         const int st = gmres_ir_solve(g, &res);
         if (st == GMRES_CUDA_ERROR || st == GMRES_TIMEOUT)
             return fail(ctx, CAD_ERR_CUDA, "preconditioned GMRES: CUDA error");
@@ -1328,9 +1312,6 @@ int cad_destroy(cad_ctx* ctx)
         if (a) cudaStreamDestroy(a);
     if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
     if (ctx->side_join) cudaEventDestroy(ctx->side_join);
-    for (auto e : ctx->gm_ev)
-        if (e) cudaEventDestroy(e);
-    if (ctx->gm_pin) cudaFreeHost(ctx->gm_pin);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return CAD_OK;

@@ -14,7 +14,6 @@
 // explicitly inverted diagonal block.
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <math.h>
@@ -345,7 +344,6 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
 
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hcol(m + 2), y(m);
     int total = 0;
-    const bool pipe = a.hpin && a.hev[0] && a.hev[1];
     while (true) {
         // true residual r = b - A x, in FP64
         GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, x, -1.0, a.b, r, kw, nullptr, 0, 0, L));
@@ -364,41 +362,20 @@ int gmres_ir_solve(const GmresArgs& a, GmresResult* res)
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int kend = 0;
-        // Arnoldi step k on the device: V[k+1] and the Hessenberg column in hd
-        // (and, pipelined, its copy into pinned slot k & 1 with an event)
-        auto arnoldi = [&](int k) -> cudaError_t {
+        for (int k = 0; k < m; ++k) {
             double* vk = V + (int64_t)k * n;
-            if (!M.apply(vk, z)) return cudaErrorUnknown;
+            if (!M.apply(vk, z)) return GMRES_CUDA_ERROR;
             // w = A z (the FP32 copy of A when one is given: the Arnoldi
             // matrix only needs to be accurate to the restart's reduction),
             // with the first Gram-Schmidt pass's dot products
             const int gc = a.gemv_chunks > 0 ? a.gemv_chunks : kGemvChunks;
-            cudaError_t e = a.A32mv
-                                ? krylov_gemv<float>(st, a.A32mv, a.ld32, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc)
-                                : krylov_gemv<double>(st, a.A, a.lda, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc);
-            if (e == cudaSuccess) e = krylov_orthogonalise(st, V, n, nn, k + 1, w, hd, V + (int64_t)(k + 1) * n, kw, L);
-            if (e == cudaSuccess && pipe) {
-                e = cudaMemcpyAsync(a.hpin + (k & 1) * (kMaxBasis + 1), hd, (k + 2) * sizeof(double),
-                                    cudaMemcpyDeviceToHost, st);
-                if (e == cudaSuccess) e = cudaEventRecord(a.hev[k & 1], st);
-            }
-            return e;
-        };
-        if (pipe) GM_CK(arnoldi(0));
-        for (int k = 0; k < m; ++k) {
-            if (pipe) {
-                // step k + 1 is queued before column k is read, so the GPU
-                // does not wait for the host; if the cycle stops at k, its
-                // results are left unused
-                if (k + 1 < m && total + 2 <= a.max_iter) GM_CK(arnoldi(k + 1));
-                GM_CK(cudaEventSynchronize(a.hev[k & 1]));
-                const double* src = a.hpin + (k & 1) * (kMaxBasis + 1);
-                std::copy(src, src + k + 2, hcol.begin());
-            } else {
-                GM_CK(arnoldi(k));
-                GM_CK(cudaMemcpyAsync(hcol.data(), hd, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
-                GM_CK(cudaStreamSynchronize(st));
-            }
+            if (a.A32mv)
+                GM_CK(krylov_gemv<float>(st, a.A32mv, a.ld32, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc));
+            else
+                GM_CK(krylov_gemv<double>(st, a.A, a.lda, nn, z, 1.0, nullptr, w, kw, V, n, k + 1, L, gc));
+            GM_CK(krylov_orthogonalise(st, V, n, nn, k + 1, w, hd, V + (int64_t)(k + 1) * n, kw, L));
+            GM_CK(cudaMemcpyAsync(hcol.data(), hd, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            GM_CK(cudaStreamSynchronize(st));
             double* Hk = H.data() + (size_t)k * (m + 1);
             for (int q = 0; q <= k + 1; ++q) Hk[q] = hcol[q];
             const double hn = hcol[k + 1];

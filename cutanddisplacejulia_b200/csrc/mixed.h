@@ -58,11 +58,6 @@ struct GmresArgs {
     const float* A32mv = nullptr;  // if set, an FP32 copy of A (ld32) for the Arnoldi products
     int64_t ld32 = 0;
     int gemv_chunks = 0;           // column chunks of the Arnoldi product (0: the default)
-    // pipelined Arnoldi loop (when both are set): pinned host memory for two
-    // Hessenberg columns (2 x (kMaxBasis + 1) doubles) and an event per column;
-    // each iteration's kernels are queued before the previous column is read
-    double* hpin = nullptr;
-    cudaEvent_t hev[2] = {nullptr, nullptr};
 };
 
 struct GmresResult {
