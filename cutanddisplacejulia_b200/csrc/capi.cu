@@ -265,6 +265,10 @@ bool edges_pay(int64_t E, int64_t N) { return 10 * E < 9 * 3 * N; }
 
 int edge_table(cad_ctx* ctx, const double* P1, const double* P2, const double* P3, int64_t N, EdgeTable* out)
 {
+    if (3 * N > INT32_MAX) {   // side codes are ints: such meshes stay on the per-side path
+        out->E = 3 * N;
+        return CAD_OK;
+    }
     std::vector<double> geom((size_t)9 * N);
     CK(cudaMemcpyAsync(geom.data(), P1, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(geom.data() + 3 * N, P2, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
