@@ -123,9 +123,9 @@ __device__ __forceinline__ void strain_to_traction(const R e[6], R lam, R G2, co
 // thread, more warps to hide the FP64 latency, some spilling) -- a launch
 // shape the autotuner may pick for the half-space system matrix.
 // EDGE (half space): the free-surface corrections are left to per-edge work;
-// the staged record is the two frames only.  OUT_AMAT (strain): they come
-// from the per-edge maps a.fscG.  OUT_SUM: they are left out here, and
-// fsc_sum_kernel adds each edge's once.
+// the staged record is the two frames only.  OUT_AMAT, OUT_TRAC (strain) and
+// OUT_INF: they come from the per-edge maps a.fscG (fsc_edge_kernel).
+// OUT_SUM: they are left out here, and fsc_sum_kernel adds each edge's once.
 template <bool HS, bool STRAIN, bool DISP, int OUT, bool NEAR = false, bool LIST = false, int MINB = 1,
           bool EDGE = false>
 __global__ void __launch_bounds__(kPairThreads, MINB) td_pair_kernel(PairArgs a)
