@@ -74,7 +74,9 @@ const char* cad_last_error(const cad_ctx* ctx);
 int cad_set_stream(cad_ctx* ctx, void* stream);
 void* cad_get_stream(const cad_ctx* ctx);
 /* Device time (ms, CUDA events on the context stream) of the most recent
- * launch of: 0 = TD pair kernel, 1 = dense factorisation + solve, 2 = the
+ * launch of: 0 = the TD kernels of the last assembly or evaluation (with
+ * shared edges: the edge kernels and the pair kernel together), 1 = dense
+ * factorisation + solve, 2 = the
  * factorisation part of the last mixed-precision solve (cast to FP32, FP32 LU,
  * diagonal-block inverses; -1 after an FP64 LU solve). */
 double cad_last_time_ms(const cad_ctx* ctx, int which);
